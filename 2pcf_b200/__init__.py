@@ -1,0 +1,364 @@
+"""2pcf_b200 -- B200-native pair sums for shear-scalar and scalar-scalar
+correlation functions (the hot path of tilmantroester/2pcf).
+
+The Python names mirror the reference's Fortran interface:
+
+    create_bins              src/utils.f90:139-230
+    shear_2pcf, kappa_2pcf   src/tpcf.f90:134-188
+    tangential_shear_tpcf    src/tpcf.f90:190-378
+    scalar_kappa_tpcf        src/tpcf.f90:380-545
+
+Every computation runs through libtpcf_b200.so (C ABI: include/tpcf_b200.h)
+on the GPU; there is no CPU fallback.  The package directory name starts with
+a digit, so import it with ``importlib.import_module("2pcf_b200")``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import Bins, LensCat, Opts, Result, ShearCat, Stats, TPCFError, lib
+
+LIN_BINNING, LOG_BINNING, IHS_BINNING, SQRT_BINNING = 0, 1, 2, 3  # src/utils.f90:7
+_SPACING = {"lin": 0, "log": 1, "ihs": 2, "sqrt": 3}
+
+__all__ = [
+    "Binning", "create_bins", "Context", "ShapeCatalog", "LensCatalog", "KappaMap",
+    "LensingSurveyField", "Shear2pcfResults", "shear_2pcf", "kappa_2pcf",
+    "tangential_shear_tpcf", "scalar_kappa_tpcf", "batch_shear_2pcf", "TPCFError",
+]
+
+
+# --------------------------------------------------------------- arrays ------
+def _is_torch(a):
+    return type(a).__module__.startswith("torch")
+
+
+class _Arr:
+    """Holds a contiguous float32/int32 view of an input and its raw pointer."""
+
+    def __init__(self, a, dtype=np.float32):
+        self.keep = None
+        self.n = 0
+        if a is None:
+            self.ptr = None
+            return
+        if _is_torch(a):
+            import torch
+            tdt = torch.float32 if dtype == np.float32 else torch.int32
+            if a.is_cuda:
+                t = a.detach().to(tdt).contiguous()
+                self.keep, self.ptr, self.n = t, t.data_ptr(), t.numel()
+                return
+            a = a.detach().cpu().numpy()
+        arr = np.ascontiguousarray(a, dtype=dtype)
+        self.keep, self.ptr, self.n = arr, arr.ctypes.data, arr.size
+
+
+def _check(status, ctx=None):
+    if status != _lib.TPCF_OK:
+        msg = ""
+        if ctx is not None:
+            msg = (lib().tpcf_last_error(ctx) or b"").decode()
+        raise TPCFError(status, msg)
+
+
+# --------------------------------------------------------------- binning -----
+@dataclass
+class Binning:
+    """type(binning) of src/utils.f90:18-24.  ``bin_edges`` are the canonical
+    FP64 edges the kernels bin against; ``bin_centers`` are computed in FP32
+    exactly as create_bins does."""
+    x_min: float
+    x_max: float
+    n_bin: int
+    spacing: int = LOG_BINNING
+    ihs_theta: float = 1.0
+    bin_edges: np.ndarray = field(default=None, repr=False)
+    bin_edges_sq: np.ndarray = field(default=None, repr=False)
+    bin_centers: np.ndarray = field(default=None, repr=False)
+
+    def c_struct(self) -> Bins:
+        return Bins(int(self.n_bin), int(self.spacing), float(self.x_min), float(self.x_max),
+                    float(self.ihs_theta))
+
+
+def create_bins(x_min, x_max, n_bin, spacing=LOG_BINNING, p=1.0) -> Binning:
+    """create_bins(x_min, x_max, n_bin, p, spacing) of src/utils.f90:139-230."""
+    if isinstance(spacing, str):
+        spacing = _SPACING[spacing]
+    b = Binning(float(x_min), float(x_max), int(n_bin), int(spacing), float(p))
+    cb = b.c_struct()
+    e = np.zeros(n_bin + 1)
+    e2 = np.zeros(n_bin + 1)
+    _check(lib().tpcf_canonical_edges(C.byref(cb), e.ctypes.data, e2.ctypes.data))
+    c = np.zeros(n_bin, np.float32)
+    _check(lib().tpcf_bin_centers(C.byref(cb), c.ctypes.data))
+    b.bin_edges, b.bin_edges_sq, b.bin_centers = e, e2, c
+    return b
+
+
+# --------------------------------------------------------------- context -----
+class Context:
+    """One device, one stream (tpcf_ctx).  ``use_kd_tree`` of the reference maps
+    to ``use_grid`` (the device cell grid that replaces the kd-tree)."""
+
+    def __init__(self, device: int = 0, use_grid: bool = True, cell_size: float = 0.0,
+                 verbose: bool = False):
+        self._h = C.c_void_p()
+        o = Opts(int(use_grid), int(verbose), float(cell_size), 0, 0, 0, (C.c_int32 * 5)())
+        _check(lib().tpcf_create(C.byref(self._h), int(device), C.byref(o)))
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            lib().tpcf_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        _check(lib().tpcf_set_stream(self._h, stream_ptr), self._h)
+
+    def set_timing(self, enable: bool):
+        _check(lib().tpcf_set_timing(self._h, int(enable)), self._h)
+
+    def set_shard(self, index: int, count: int):
+        """Compute only work items i % count == index (sums become partial)."""
+        _check(lib().tpcf_set_shard(self._h, int(index), int(count)), self._h)
+
+    def measure_fp32_peak(self) -> float:
+        """Measured FP32 FMA throughput of this GPU in TFLOP/s."""
+        v = C.c_double()
+        _check(lib().tpcf_measure_fp32_peak(self._h, C.byref(v)), self._h)
+        return v.value
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(lib().tpcf_last_stats(self._h, C.byref(s)), self._h)
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().tpcf_kernel_launches(self._h))
+
+
+_default_ctx: dict = {}
+
+
+def default_context(device: int = 0) -> Context:
+    if device not in _default_ctx:
+        _default_ctx[device] = Context(device)
+    return _default_ctx[device]
+
+
+# ------------------------------------------------------------- catalogues ----
+@dataclass
+class ShapeCatalog:  # shape_catalog, src/tpcf.f90:24-27
+    x: object
+    y: object
+    e1: object
+    e2: object
+    w: object
+    z: object = None
+    m: object = None
+
+    @property
+    def n(self):
+        return len(self.x)
+
+
+@dataclass
+class LensCatalog:  # lens_catalog, src/tpcf.f90:34-37
+    x: object
+    y: object
+    val: object
+    w: object
+    z: object = None
+
+    @property
+    def n(self):
+        return len(self.x)
+
+
+@dataclass
+class KappaMap:  # kappa_map, src/tpcf.f90:29-32
+    x: object
+    y: object
+    kappa_E: object
+    kappa_B: object
+    w: object
+
+    @property
+    def n(self):
+        return len(self.x)
+
+
+@dataclass
+class LensingSurveyField:  # lensing_survey_field, src/tpcf.f90:39-43
+    lenses: LensCatalog
+    shapes: Optional[ShapeCatalog] = None
+    convergence: Optional[KappaMap] = None
+
+
+@dataclass
+class Shear2pcfResults:
+    """shear_2pcf_results (src/tpcf.f90:17-22) plus the FP64 sums behind it."""
+    n_bin: int
+    theta: np.ndarray
+    mean_theta: np.ndarray
+    g_t: np.ndarray
+    g_x: np.ndarray
+    weights: np.ndarray
+    n_pairs: np.ndarray
+    sum_dw: np.ndarray
+    sum_gt: np.ndarray
+    sum_gx: np.ndarray
+    sum_w: np.ndarray
+    sum_K: np.ndarray
+    xi_E_marks: Optional[np.ndarray] = None
+    xi_B_marks: Optional[np.ndarray] = None
+    K_marks: Optional[np.ndarray] = None
+    w_marks: Optional[np.ndarray] = None
+    marks_weight: Optional[np.ndarray] = None
+    lens_sums: Optional[np.ndarray] = None
+    patch_sums: Optional[np.ndarray] = None
+
+
+def _alloc_result(nb, nA, marks, lens_sums, n_patch):
+    r = {k: np.zeros(nb) for k in ("sum_dw", "sum_gt", "sum_gx", "sum_w", "sum_K")}
+    r["n_pairs"] = np.zeros(nb, np.int64)
+    for k in ("theta", "mean_theta", "g_t", "g_x", "weights"):
+        r[k] = np.zeros(nb, np.float32)
+    if marks:
+        for k in ("xi_E_marks", "xi_B_marks", "K_marks", "w_marks"):
+            r[k] = np.zeros((nA, nb), np.float32)
+        r["marks_weight"] = np.zeros(nA, np.float32)
+    if lens_sums:
+        r["lens_sums"] = np.zeros((nA, 6, nb))
+    if n_patch and n_patch > 0:
+        r["patch_sums"] = np.zeros((n_patch, 6, nb))
+    cres = Result(**{k: (v.ctypes.data if v is not None else None) for k, v in r.items()})
+    return r, cres
+
+
+def _finish(r, nb):
+    return Shear2pcfResults(n_bin=nb, **r)
+
+
+def _resolve_ctx(ctx):
+    return ctx if ctx is not None else default_context(0)
+
+
+# -------------------------------------------------------------- pair sums ----
+def tangential_shear_tpcf(x_A, y_A, z_A, val_A, weight_A, x_B, y_B, z_B, e1_B, e2_B, weight_B, m_B,
+                          bins: Binning, spherical_coords=False, num_threads=None,
+                          use_kd_tree=True, verbose=False, calculate_marks=True,
+                          patch_A=None, n_patch=0, lens_sums=False, ctx: Context = None):
+    """tangential_shear_tpcf (src/tpcf.f90:190-378) on the GPU.
+
+    Returns a Shear2pcfResults: avg_theta is ``mean_theta``; the marks arrays
+    are [n_A][n_bin] (the memory layout of the reference's (n_bin, n_A)).
+    ``num_threads`` is accepted and ignored; ``use_kd_tree`` selects the cell
+    grid (True) or the all-pairs scan (False) when ``ctx`` is not given."""
+    if spherical_coords:
+        raise TPCFError(6, "spherical coordinates are not supported")
+    if ctx is None:
+        ctx = default_context(0) if use_kd_tree else Context(0, use_grid=False, verbose=verbose)
+    A = [_Arr(a) for a in (x_A, y_A, z_A, val_A, weight_A)]
+    B = [_Arr(a) for a in (x_B, y_B, z_B, e1_B, e2_B, weight_B, m_B)]
+    P = _Arr(patch_A, np.int32)
+    nA, nB = A[0].n, B[0].n
+    nb = bins.n_bin
+    r, cres = _alloc_result(nb, nA, calculate_marks, lens_sums, n_patch if patch_A is not None else 0)
+    cb = bins.c_struct()
+    st = lib().tpcf_shear_scalar(ctx.handle, *[a.ptr for a in A], nA, *[b.ptr for b in B], nB,
+                                 C.byref(cb), P.ptr, int(n_patch), C.byref(cres))
+    _check(st, ctx.handle)
+    return _finish(r, nb)
+
+
+def scalar_kappa_tpcf(x_A, y_A, val_A, w_A, x_B, y_B, kappa_E, kappa_B, w_B, bins: Binning,
+                      spherical_coords=False, num_threads=None, use_kd_tree=True, verbose=False,
+                      calculate_marks=True, patch_A=None, n_patch=0, lens_sums=False,
+                      ctx: Context = None):
+    """scalar_kappa_tpcf (src/tpcf.f90:380-545) on the GPU."""
+    if spherical_coords:
+        raise TPCFError(6, "spherical coordinates are not supported")
+    if ctx is None:
+        ctx = default_context(0) if use_kd_tree else Context(0, use_grid=False, verbose=verbose)
+    A = [_Arr(a) for a in (x_A, y_A, val_A, w_A)]
+    B = [_Arr(a) for a in (x_B, y_B, kappa_E, kappa_B, w_B)]
+    P = _Arr(patch_A, np.int32)
+    nA, nB = A[0].n, B[0].n
+    nb = bins.n_bin
+    r, cres = _alloc_result(nb, nA, calculate_marks, lens_sums, n_patch if patch_A is not None else 0)
+    cb = bins.c_struct()
+    st = lib().tpcf_scalar_scalar(ctx.handle, *[a.ptr for a in A], nA, *[b.ptr for b in B], nB,
+                                  C.byref(cb), P.ptr, int(n_patch), C.byref(cres))
+    _check(st, ctx.handle)
+    return _finish(r, nb)
+
+
+def shear_2pcf(field: LensingSurveyField, bins: Binning, spherical_coords=False, num_threads=None,
+               use_kd_tree=True, verbose=False, **kw):
+    """shear_2pcf (src/tpcf.f90:134-160)."""
+    L, S = field.lenses, field.shapes
+    return tangential_shear_tpcf(L.x, L.y, L.z, L.val, L.w, S.x, S.y, S.z, S.e1, S.e2, S.w, S.m,
+                                 bins, spherical_coords, num_threads, use_kd_tree, verbose, **kw)
+
+
+def kappa_2pcf(field: LensingSurveyField, bins: Binning, spherical_coords=False, num_threads=None,
+               use_kd_tree=True, verbose=False, **kw):
+    """kappa_2pcf (src/tpcf.f90:162-188)."""
+    L, K = field.lenses, field.convergence
+    return scalar_kappa_tpcf(L.x, L.y, L.val, L.w, K.x, K.y, K.kappa_E, K.kappa_B, K.w, bins,
+                             spherical_coords, num_threads, use_kd_tree, verbose, **kw)
+
+
+def batch_shear_2pcf(lenses: Sequence[LensCatalog], shapes: Sequence[ShapeCatalog],
+                     tasks: Sequence[tuple], bins: Binning, lens_patches=None, n_patch=0,
+                     marks=False, lens_sums=False, ctx: Context = None):
+    """All (lens catalogue, shape catalogue) tasks in one persistent launch
+    (tpcf_batch_shear_scalar).  ``lens_patches[i]`` labels lens catalogue i."""
+    ctx = _resolve_ctx(ctx)
+    keep = []
+    lc = (LensCat * len(lenses))()
+    for i, L in enumerate(lenses):
+        arrs = [_Arr(a) for a in (L.x, L.y, L.z, L.val, L.w)]
+        p = _Arr(None if lens_patches is None else lens_patches[i], np.int32)
+        keep += arrs + [p]
+        lc[i] = LensCat(arrs[0].n, *[a.ptr for a in arrs], p.ptr)
+    sc = (ShearCat * len(shapes))()
+    for i, S in enumerate(shapes):
+        arrs = [_Arr(a) for a in (S.x, S.y, S.z, S.e1, S.e2, S.w, S.m)]
+        keep += arrs
+        sc[i] = ShearCat(arrs[0].n, *[a.ptr for a in arrs])
+    tl = np.ascontiguousarray([t[0] for t in tasks], np.int32)
+    ts = np.ascontiguousarray([t[1] for t in tasks], np.int32)
+    nb = bins.n_bin
+    outs = (Result * len(tasks))()
+    pyouts = []
+    for t in range(len(tasks)):
+        nA = lenses[tasks[t][0]].n
+        r, cres = _alloc_result(nb, nA, marks, lens_sums, n_patch if lens_patches is not None else 0)
+        outs[t] = cres
+        pyouts.append(r)
+    cb = bins.c_struct()
+    st = lib().tpcf_batch_shear_scalar(ctx.handle, len(lenses), lc, len(shapes), sc, len(tasks),
+                                       tl.ctypes.data, ts.ctypes.data, C.byref(cb),
+                                       int(n_patch) if lens_patches is not None else 0, outs)
+    _check(st, ctx.handle)
+    return [_finish(r, nb) for r in pyouts]

@@ -1,0 +1,769 @@
+// capi.cu -- C ABI and host orchestration of libtpcf_b200.
+//
+// One call = stage inputs -> per-catalogue grid / lens-group build on the
+// device -> one persistent pair-kernel launch over every (task, lens group)
+// work item -> deterministic per-patch reduction -> outputs.  The reference
+// counterparts are cited at each entry point in include/tpcf_b200.h.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "tpcf_b200.h"
+#include "tpcf_internal.cuh"
+#include "tpcf_kernels.h"
+#include "tpcf_ctx.h"
+
+using namespace tpcf;
+
+// ------------------------------------------------------------- ctx helpers --
+namespace tpcf {
+
+void* ws_alloc(tpcf_ctx* c, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (c->next_slot == c->slots.size()) c->slots.push_back(Slot{nullptr, 0});
+  Slot& s = c->slots[c->next_slot++];
+  if (s.bytes < bytes) {
+    if (s.ptr) {
+      cudaError_t e = cudaFree(s.ptr);
+      s.ptr = nullptr;
+      s.bytes = 0;
+      if (e != cudaSuccess) throw Failure(TPCF_ERR_CUDA, std::string("cudaFree: ") + cudaGetErrorString(e));
+    }
+    size_t want = bytes + bytes / 4 + 256;
+    cudaError_t e = cudaMalloc(&s.ptr, want);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      s.ptr = nullptr;
+      throw Failure(TPCF_ERR_OOM, "device allocation of " + std::to_string(want) + " bytes failed");
+    }
+    s.bytes = want;
+  }
+  return s.ptr;
+}
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw Failure(TPCF_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void counted(tpcf_ctx* c, cudaError_t e, const char* what) {
+  check(e, what);
+  c->launches += 1;
+}
+
+template <class T>
+const T* stage(tpcf_ctx* c, const T* p, int64_t n) {
+  if (!p || n <= 0) return p;
+  if (is_device_ptr(p)) return p;
+  T* d = static_cast<T*>(ws_alloc(c, sizeof(T) * (size_t)n));
+  check(cudaMemcpyAsync(d, p, sizeof(T) * (size_t)n, cudaMemcpyHostToDevice, c->stream), "H2D input");
+  c->h2d_bytes += sizeof(T) * (size_t)n;
+  return d;
+}
+template const float* stage<float>(tpcf_ctx*, const float*, int64_t);
+template const int* stage<int>(tpcf_ctx*, const int*, int64_t);
+template const double* stage<double>(tpcf_ctx*, const double*, int64_t);
+
+void copy_out(tpcf_ctx* c, void* dst, const void* src, size_t bytes) {
+  if (!dst || bytes == 0) return;
+  check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c->stream), "output copy");
+}
+
+void begin_call(tpcf_ctx* c) {
+  c->next_slot = 0;
+  c->h2d_bytes = 0;
+  check(cudaSetDevice(c->device), "cudaSetDevice");
+}
+
+void vlog(tpcf_ctx* c, const char* fmt, ...) {
+  if (!c->opts.verbose) return;
+  va_list ap;
+  va_start(ap, fmt);
+  std::fprintf(stderr, "[tpcf_b200] ");
+  std::vfprintf(stderr, fmt, ap);
+  std::fprintf(stderr, "\n");
+  va_end(ap);
+}
+
+// Canonical FP64 edges (same formulas as the oracle's canon::edges).
+tpcf_status canonical_edges(const tpcf_bins* b, double* e, double* e2) {
+  if (!b) return TPCF_ERR_INVALID_ARG;
+  const int n = b->n_bin;
+  const double x_min = b->x_min, x_max = b->x_max, p = b->ihs_theta;
+  if (n < 1 || n > kMaxBins || !(x_max > x_min) || !std::isfinite(x_max) || !std::isfinite(x_min))
+    return TPCF_ERR_INVALID_ARG;
+  if (b->spacing == TPCF_LOG && !(x_min > 0)) return TPCF_ERR_INVALID_ARG;
+  if (b->spacing == TPCF_SQRT && !(x_min >= 0)) return TPCF_ERR_INVALID_ARG;
+  if (b->spacing == TPCF_IHS && !(p > 0)) return TPCF_ERR_INVALID_ARG;
+  if (b->spacing < TPCF_LIN || b->spacing > TPCF_SQRT) return TPCF_ERR_INVALID_ARG;
+  e[0] = x_min;
+  e[n] = x_max;
+  if (b->spacing == TPCF_LIN) {
+    const double d = (x_max - x_min) / n;
+    for (int i = 1; i < n; ++i) e[i] = x_min + i * d;
+  } else if (b->spacing == TPCF_LOG) {
+    const double l0 = std::log10(x_min), d = (std::log10(x_max) - l0) / n;
+    for (int i = 1; i < n; ++i) e[i] = std::pow(10.0, l0 + i * d);
+  } else if (b->spacing == TPCF_SQRT) {
+    const double s0 = std::sqrt(x_min), d = (std::sqrt(x_max) - s0) / n;
+    for (int i = 1; i < n; ++i) {
+      const double s = s0 + i * d;
+      e[i] = s * s;
+    }
+  } else {
+    const double t0 = std::log(p * x_min + std::sqrt((p * x_min) * (p * x_min) + 1.0)) / p;
+    const double t1 = std::log(p * x_max + std::sqrt((p * x_max) * (p * x_max) + 1.0)) / p;
+    const double d = (t1 - t0) / n;
+    for (int i = 1; i < n; ++i) e[i] = std::sinh(p * (t0 + i * d)) / p;
+  }
+  for (int i = 0; i <= n; ++i) e2[i] = e[i] * e[i];
+  for (int i = 0; i < n; ++i)
+    if (!(e2[i + 1] > e2[i])) return TPCF_ERR_INVALID_ARG;
+  return TPCF_OK;
+}
+
+// Bin centres in FP32 as create_bins computes them (src/utils.f90:202-229).
+void bin_centers_f32(const tpcf_bins* b, float* centers) {
+  const int n = b->n_bin;
+  const float x_min = (float)b->x_min, x_max = (float)b->x_max, p = (float)b->ihs_theta;
+  std::vector<float> e(n + 1);
+  float bs;
+  auto T = [&](float x) { return logf(p * x + sqrtf((p * x) * (p * x) + 1.0f)) / p; };
+  if (b->spacing == TPCF_LIN) bs = (x_max - x_min) / (float)n;
+  else if (b->spacing == TPCF_LOG) bs = (log10f(x_max) - log10f(x_min)) / (float)n;
+  else if (b->spacing == TPCF_IHS) bs = (T(x_max) - T(x_min)) / (float)n;
+  else bs = (sqrtf(x_max) - sqrtf(x_min)) / (float)n;
+  e[n] = x_max;
+  for (int i = 0; i < n; ++i) {
+    if (b->spacing == TPCF_LIN) e[i] = x_min + bs * (float)i;
+    else if (b->spacing == TPCF_LOG) e[i] = powf(10.0f, log10f(x_min) + bs * (float)i);
+    else if (b->spacing == TPCF_IHS) e[i] = sinhf(p * (T(x_min) + bs * (float)i)) / p;
+    else {
+      const float s = sqrtf(x_min) + bs * (float)i;
+      e[i] = s * s;
+    }
+  }
+  for (int i = 0; i < n; ++i) centers[i] = e[i] + (e[i + 1] - e[i]) / 2.0f;
+}
+
+}  // namespace tpcf
+
+// ---------------------------------------------------------- batch engine --
+namespace {
+
+struct LensIn {
+  int64_t n;
+  const float *x, *y, *z, *val, *w;
+  const int* patch;
+};
+struct SrcIn {
+  int64_t n;
+  const float *x, *y, *z, *f1, *f2, *w, *m;
+};
+
+struct LensBuilt {
+  int n_valid = 0;
+  int n_groups = 0;
+  float4* rec = nullptr;
+  float* zs = nullptr;
+  int* perm = nullptr;
+  int* group_start = nullptr;
+  float4* group_box = nullptr;
+  std::vector<int> patch_groups;  // [n_patch_eff + 1], host
+  int* d_patch_groups = nullptr;
+};
+
+struct SrcBuilt {
+  GridDesc g{};
+};
+
+// Everything one batched call needs; outs[t] receives task t.
+tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vector<SrcIn> srcs,
+                      const std::vector<int>& tl, const std::vector<int>& ts, const tpcf_bins* bins, int n_patch,
+                      tpcf_result* outs) {
+  auto t_start = std::chrono::steady_clock::now();
+  begin_call(c);
+  cudaStream_t st = c->stream;
+  const int nb = bins->n_bin;
+  std::vector<double> e(nb + 1), e2(nb + 1);
+  tpcf_status bs = canonical_edges(bins, e.data(), e2.data());
+  if (bs != TPCF_OK) throw Failure(bs, "invalid binning");
+  if (c->opts.spherical) throw Failure(TPCF_ERR_NOT_SUPPORTED, "spherical coordinates are not supported");
+  if (c->opts.shard_count > 1 && (c->opts.shard_index < 0 || c->opts.shard_index >= c->opts.shard_count))
+    throw Failure(TPCF_ERR_INVALID_ARG, "shard_index outside [0, shard_count)");
+  const bool sharded = c->opts.shard_count > 1;
+  const int nL = (int)lens.size(), nS = (int)srcs.size(), nT = (int)tl.size();
+  for (int t = 0; t < nT; ++t)
+    if (tl[t] < 0 || tl[t] >= nL || ts[t] < 0 || ts[t] >= nS) throw Failure(TPCF_ERR_INVALID_ARG, "task index out of range");
+  const bool use_patch_any = n_patch > 0;
+  const int n_patch_eff = use_patch_any ? n_patch : 1;
+  for (auto& l : lens) {
+    if (l.n < 0 || l.n > (1ll << 31) - 2) throw Failure(TPCF_ERR_INVALID_ARG, "lens catalogue size out of range");
+    if (l.n > 0 && (!l.x || !l.y || !l.val || !l.w)) throw Failure(TPCF_ERR_INVALID_ARG, "missing lens array");
+    if (l.patch && !use_patch_any) throw Failure(TPCF_ERR_INVALID_ARG, "patch labels given with n_patch <= 0");
+  }
+  for (auto& s : srcs) {
+    if (s.n < 0 || s.n > (1ll << 31) - 2) throw Failure(TPCF_ERR_INVALID_ARG, "source catalogue size out of range");
+    if (s.n > 0 && (!s.x || !s.y || !s.f1 || !s.f2 || !s.w)) throw Failure(TPCF_ERR_INVALID_ARG, "missing source array");
+  }
+
+  // ---- stage inputs
+  for (auto& l : lens) {
+    l.x = stage(c, l.x, l.n); l.y = stage(c, l.y, l.n); l.z = stage(c, l.z, l.n);
+    l.val = stage(c, l.val, l.n); l.w = stage(c, l.w, l.n); l.patch = stage(c, l.patch, l.n);
+  }
+  for (auto& s : srcs) {
+    s.x = stage(c, s.x, s.n); s.y = stage(c, s.y, s.n); s.z = stage(c, s.z, s.n);
+    s.f1 = stage(c, s.f1, s.n); s.f2 = stage(c, s.f2, s.n); s.w = stage(c, s.w, s.n); s.m = stage(c, s.m, s.n);
+  }
+
+  // ---- bounding boxes, z ranges, max |m|, counts, patch ranges (one sync)
+  const int ncat = nL + nS;
+  int* box_ord = (int*)ws_alloc(c, sizeof(int) * 8 * ncat);
+  unsigned long long* cnt = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * ncat);
+  int* pr = (int*)ws_alloc(c, sizeof(int) * 2 * ncat);
+  float* boxf = (float*)ws_alloc(c, sizeof(float) * 8 * ncat);
+  counted(c, launch_bbox_init(box_ord, cnt, pr, ncat, st), "bbox init");
+  for (int i = 0; i < nL; ++i)
+    counted(c, launch_bbox(lens[i].x, lens[i].y, lens[i].z, lens[i].w, lens[i].patch, nullptr, lens[i].n, 1,
+                           box_ord + 8 * i, cnt + i, pr + 2 * i, st), "bbox lens");
+  for (int i = 0; i < nS; ++i)
+    counted(c, launch_bbox(srcs[i].x, srcs[i].y, srcs[i].z, nullptr, nullptr, srcs[i].m, srcs[i].n, 0,
+                           box_ord + 8 * (nL + i), cnt + nL + i, pr + 2 * (nL + i), st), "bbox src");
+  counted(c, launch_bbox_finish(box_ord, boxf, 8 * ncat, st), "bbox finish");
+  std::vector<float> hbox(8 * ncat);
+  std::vector<unsigned long long> hcnt(ncat);
+  std::vector<int> hpr(2 * ncat);
+  check(cudaMemcpyAsync(hbox.data(), boxf, sizeof(float) * 8 * ncat, cudaMemcpyDeviceToHost, st), "D2H box");
+  check(cudaMemcpyAsync(hcnt.data(), cnt, sizeof(unsigned long long) * ncat, cudaMemcpyDeviceToHost, st), "D2H count");
+  check(cudaMemcpyAsync(hpr.data(), pr, sizeof(int) * 2 * ncat, cudaMemcpyDeviceToHost, st), "D2H prange");
+  check(cudaStreamSynchronize(st), "sync bbox");
+  for (int i = 0; i < nL; ++i)
+    if (lens[i].patch && hcnt[i] > 0 && (hpr[2 * i] < 0 || hpr[2 * i + 1] >= n_patch))
+      throw Failure(TPCF_ERR_INVALID_ARG, "patch label outside [0, n_patch)");
+
+  // ---- kernel configuration
+  bool has_m = false, has_z = false;
+  for (int i = 0; i < nS; ++i)  // K differs from w only where some m != 0
+    has_m = has_m || (mode == 0 && srcs[i].m != nullptr && hcnt[nL + i] > 0 && hbox[8 * (nL + i) + 6] != 0.f);
+  for (int t = 0; t < nT; ++t) {
+    const int li = tl[t], si = ts[t];
+    if (mode == 0 && hcnt[li] > 0 && hcnt[nL + si] > 0) {
+      const float lz_max = hbox[8 * li + 5], sz_min = hbox[8 * (nL + si) + 4];
+      if (lz_max > sz_min) has_z = true;
+    }
+  }
+  const bool logb = bins->spacing == TPCF_LOG;
+  const int qa = has_m ? 6 : 5;
+  int bt = 128;
+  while (bt > 32 && (size_t)nb * qa * bt * 4 > 100 * 1024) bt /= 2;
+
+  const double Rd = bins->x_max;
+  float R = (float)(Rd * (1.0 + 1e-6));
+
+  // ---- source grids
+  std::vector<GridDesc> grids(nS);
+  for (int i = 0; i < nS; ++i) {
+    const SrcIn& s = srcs[i];
+    GridDesc& g = grids[i];
+    const float* b = &hbox[8 * (nL + i)];
+    const int n_valid = (int)hcnt[nL + i];
+    float x0 = n_valid ? b[0] : 0.f, y0 = n_valid ? b[1] : 0.f;
+    float ex = n_valid ? b[2] - b[0] : 0.f, ey = n_valid ? b[3] - b[1] : 0.f;
+    double cell = c->opts.cell_size > 0 ? c->opts.cell_size : Rd / 16.0;
+    const double span = std::max((double)ex, (double)ey);
+    if (!c->opts.use_grid) cell = span * 2.0 + 1.0;
+    // keep the grid below 2^24 cells
+    while ((span / cell + 2.0) * (span / cell + 2.0) > (double)(1 << 24)) cell *= 1.5;
+    if (!(cell > 0)) cell = 1.0;
+    int ncx = (int)std::floor(ex / cell) + 1, ncy = (int)std::floor(ey / cell) + 1;
+    ncx = std::max(1, ncx); ncy = std::max(1, ncy);
+    const unsigned ncells = (unsigned)ncx * (unsigned)ncy;
+    g.x0 = x0; g.y0 = y0; g.cell = (float)cell; g.inv_cell = (float)(1.0 / cell);
+    g.ncx = ncx; g.ncy = ncy; g.n_valid = n_valid;
+    int* cs = (int*)ws_alloc(c, sizeof(int) * (ncells + 1));
+    SrcRec* rec = (SrcRec*)ws_alloc(c, sizeof(SrcRec) * std::max(n_valid, 1));
+    if (s.n > 0) {
+      unsigned* k0 = (unsigned*)ws_alloc(c, sizeof(unsigned) * s.n);
+      unsigned* k1 = (unsigned*)ws_alloc(c, sizeof(unsigned) * s.n);
+      int* i0 = (int*)ws_alloc(c, sizeof(int) * s.n);
+      int* i1 = (int*)ws_alloc(c, sizeof(int) * s.n);
+      counted(c, launch_src_keys(s.x, s.y, s.z, s.n, x0, y0, g.inv_cell, ncx, ncy, k0, i0, st), "src keys");
+      int end_bit = 1;
+      while (end_bit < 32 && (1ull << end_bit) <= (unsigned long long)ncells) ++end_bit;
+      size_t tb = 0;
+      check(sort_pairs_u32(nullptr, tb, k0, k1, i0, i1, (int)s.n, end_bit, st), "sort size");
+      void* tmp = ws_alloc(c, tb);
+      check(sort_pairs_u32(tmp, tb, k0, k1, i0, i1, (int)s.n, end_bit, st), "sort sources");
+      counted(c, launch_cell_start(k1, s.n, ncells, cs, st), "cell start");
+      counted(c, launch_src_gather(i1, n_valid, mode, s.x, s.y, s.z, s.f1, s.f2, s.w, s.m, rec, st), "src gather");
+    } else {
+      check(cudaMemsetAsync(cs, 0, sizeof(int) * (ncells + 1), st), "memset cells");
+    }
+    g.cell_start = cs;
+    g.rec = rec;
+  }
+  float margin = 0.f;
+  for (int i = 0; i < ncat; ++i) {
+    const float* b = &hbox[8 * i];
+    if (hcnt[i] == 0) continue;
+    margin = std::max(margin, std::fabs(b[0]) + std::fabs(b[1]) + std::fabs(b[2]) + std::fabs(b[3]));
+  }
+  float maxcell = 0.f;
+  for (auto& g : grids) maxcell = std::max(maxcell, g.cell);
+  margin = (float)(1e-5 * (margin + Rd) + 1e-4 * maxcell);
+
+  // ---- lens catalogues: sort by (patch, Morton), groups of <= bt lenses
+  std::vector<LensBuilt> lb(nL);
+  std::vector<LensDesc> ldesc(nL);
+  for (int i = 0; i < nL; ++i) {
+    const LensIn& l = lens[i];
+    LensBuilt& B = lb[i];
+    B.n_valid = (int)hcnt[i];
+    const float* b = &hbox[8 * i];
+    B.rec = (float4*)ws_alloc(c, sizeof(float4) * std::max(B.n_valid, 1));
+    B.zs = mode == 0 ? (float*)ws_alloc(c, sizeof(float) * std::max(B.n_valid, 1)) : nullptr;
+    B.perm = (int*)ws_alloc(c, sizeof(int) * std::max(B.n_valid, 1));
+    std::vector<int> off(n_patch_eff + 1, 0);
+    if (l.n > 0 && B.n_valid > 0) {
+      unsigned long long* k0 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * l.n);
+      unsigned long long* k1 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * l.n);
+      int* i0 = (int*)ws_alloc(c, sizeof(int) * l.n);
+      int* i1 = (int*)ws_alloc(c, sizeof(int) * l.n);
+      float4 box = make_float4(b[0], b[1], b[2], b[3]);
+      counted(c, launch_lens_keys(l.x, l.y, l.z, l.w, l.patch, l.n, box, k0, i0, st), "lens keys");
+      size_t tb = 0;
+      check(sort_pairs_u64(nullptr, tb, k0, k1, i0, i1, (int)l.n, st), "sort size");
+      void* tmp = ws_alloc(c, tb);
+      check(sort_pairs_u64(tmp, tb, k0, k1, i0, i1, (int)l.n, st), "sort lenses");
+      counted(c, launch_lens_gather(i1, B.n_valid, l.x, l.y, l.z, l.val, l.w, B.rec, B.zs, B.perm, st), "lens gather");
+      if (l.patch) {
+        int* doff = (int*)ws_alloc(c, sizeof(int) * (n_patch_eff + 1));
+        counted(c, launch_patch_offsets(k1, B.n_valid, n_patch_eff, doff, st), "patch offsets");
+        check(cudaMemcpyAsync(off.data(), doff, sizeof(int) * (n_patch_eff + 1), cudaMemcpyDeviceToHost, st), "D2H off");
+        check(cudaStreamSynchronize(st), "sync offsets");
+      } else {
+        for (int p = 1; p <= n_patch_eff; ++p) off[p] = B.n_valid;
+      }
+    }
+    std::vector<int> gstart;
+    B.patch_groups.assign(n_patch_eff + 1, 0);
+    for (int p = 0; p < n_patch_eff; ++p) {
+      B.patch_groups[p] = (int)gstart.size();
+      for (int s0 = off[p]; s0 < off[p + 1]; s0 += bt) gstart.push_back(s0);
+    }
+    B.patch_groups[n_patch_eff] = (int)gstart.size();
+    B.n_groups = (int)gstart.size();
+    gstart.push_back(B.n_valid);
+    B.group_start = (int*)ws_alloc(c, sizeof(int) * gstart.size());
+    check(cudaMemcpyAsync(B.group_start, gstart.data(), sizeof(int) * gstart.size(), cudaMemcpyHostToDevice, st), "H2D groups");
+    B.d_patch_groups = (int*)ws_alloc(c, sizeof(int) * (n_patch_eff + 1));
+    check(cudaMemcpyAsync(B.d_patch_groups, B.patch_groups.data(), sizeof(int) * (n_patch_eff + 1),
+                          cudaMemcpyHostToDevice, st), "H2D patch groups");
+    B.group_box = (float4*)ws_alloc(c, sizeof(float4) * std::max(B.n_groups, 1));
+    counted(c, launch_group_box(B.rec, B.group_start, B.n_groups, B.group_box, st), "group box");
+    check(cudaStreamSynchronize(st), "sync groups");  // host vectors above must outlive the async copies
+    LensDesc& d = ldesc[i];
+    d.rec = B.rec; d.z = B.zs; d.group_start = B.group_start; d.group_box = B.group_box;
+    d.n_valid = B.n_valid; d.n_groups = B.n_groups;
+  }
+
+  // ---- tasks and work items
+  std::vector<TaskDesc> tdesc(nT);
+  std::vector<int2> items;
+  std::vector<char> want_lens(nT, 0);
+  long long lens_acc_elems = 0;
+  for (int t = 0; t < nT; ++t) {
+    TaskDesc& d = tdesc[t];
+    d.lens_cat = tl[t];
+    d.src_cat = ts[t];
+    d.item_base = (int)items.size();
+    for (int g = 0; g < lb[tl[t]].n_groups; ++g) items.push_back(make_int2(t, g));
+    const tpcf_result& o = outs[t];
+    want_lens[t] = (o.xi_E_marks || o.xi_B_marks || o.K_marks || o.w_marks || o.marks_weight || o.lens_sums) ? 1 : 0;
+    d.lens_acc_off = -1;
+    if (want_lens[t]) {
+      d.lens_acc_off = lens_acc_elems;
+      lens_acc_elems += (long long)kQ * nb * std::max(lb[tl[t]].n_valid, 1);
+    }
+  }
+  const int n_items = (int)items.size();
+  TaskDesc* d_tasks = (TaskDesc*)ws_alloc(c, sizeof(TaskDesc) * std::max(nT, 1));
+  LensDesc* d_lens = (LensDesc*)ws_alloc(c, sizeof(LensDesc) * std::max(nL, 1));
+  GridDesc* d_grids = (GridDesc*)ws_alloc(c, sizeof(GridDesc) * std::max(nS, 1));
+  check(cudaMemcpyAsync(d_tasks, tdesc.data(), sizeof(TaskDesc) * nT, cudaMemcpyHostToDevice, st), "H2D tasks");
+  check(cudaMemcpyAsync(d_lens, ldesc.data(), sizeof(LensDesc) * nL, cudaMemcpyHostToDevice, st), "H2D lens desc");
+  check(cudaMemcpyAsync(d_grids, grids.data(), sizeof(GridDesc) * nS, cudaMemcpyHostToDevice, st), "H2D grid desc");
+  double* item_sums = (double*)ws_alloc(c, sizeof(double) * kQ * nb * std::max(n_items, 1));
+  double* lens_acc = lens_acc_elems ? (double*)ws_alloc(c, sizeof(double) * lens_acc_elems) : nullptr;
+  int* head = (int*)ws_alloc(c, sizeof(int) * 4);
+  unsigned* err = (unsigned*)(head + 1);
+  double* d_e2 = (double*)ws_alloc(c, sizeof(double) * (nb + 1));
+  float* d_e2f = (float*)ws_alloc(c, sizeof(float) * (nb + 1));
+  std::vector<float> e2f(nb + 1);
+  for (int i = 0; i <= nb; ++i) e2f[i] = (float)e2[i];
+  check(cudaMemcpyAsync(d_e2, e2.data(), sizeof(double) * (nb + 1), cudaMemcpyHostToDevice, st), "H2D edges");
+  check(cudaMemcpyAsync(d_e2f, e2f.data(), sizeof(float) * (nb + 1), cudaMemcpyHostToDevice, st), "H2D edges f");
+  check(cudaMemsetAsync(head, 0, sizeof(int) * 4, st), "memset head");
+
+  int2* d_items = (int2*)ws_alloc(c, sizeof(int2) * std::max(n_items, 1));
+  int grid = 0;
+  if (n_items > 0) {
+    int2* d_items0 = (int2*)ws_alloc(c, sizeof(int2) * n_items);
+    check(cudaMemcpyAsync(d_items0, items.data(), sizeof(int2) * n_items, cudaMemcpyHostToDevice, st), "H2D items");
+    unsigned long long* ck0 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * n_items);
+    unsigned long long* ck1 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * n_items);
+    int* o0 = (int*)ws_alloc(c, sizeof(int) * n_items);
+    int* o1 = (int*)ws_alloc(c, sizeof(int) * n_items);
+    counted(c, launch_item_cost(d_items0, n_items, d_tasks, d_lens, d_grids, R, margin, ck0, o0, st), "item cost");
+    size_t tb = 0;
+    check(sort_pairs_u64_desc(nullptr, tb, ck0, ck1, o0, o1, n_items, st), "sort size");
+    void* tmp = ws_alloc(c, tb);
+    check(sort_pairs_u64_desc(tmp, tb, ck0, ck1, o0, o1, n_items, st), "sort items");
+    const int sc = c->opts.shard_count > 1 ? c->opts.shard_count : 1;
+    const int si = sc > 1 ? c->opts.shard_index : 0;
+    counted(c, launch_permute_items(d_items0, o1, n_items, si, sc, d_items, st), "permute items");
+    const int n_run = sc > 1 ? (n_items - si + sc - 1) / sc : n_items;
+    if (sc > 1) check(cudaMemsetAsync(item_sums, 0, sizeof(double) * kQ * nb * n_items, st), "memset items");
+    if (sc > 1 && lens_acc) check(cudaMemsetAsync(lens_acc, 0, sizeof(double) * lens_acc_elems, st), "memset lens");
+
+    PairParams P{};
+    P.tasks = d_tasks; P.lenses = d_lens; P.grids = d_grids; P.items = d_items; P.n_items = n_run;
+    P.nb = nb; P.queue_head = head; P.item_sums = item_sums; P.lens_acc = lens_acc; P.err = err;
+    P.e2 = d_e2; P.e2f = d_e2f; P.R = R; P.margin = margin;
+    if (logb) {
+      const double l0 = std::log2(e2[0]), l1 = std::log2(e2[nb]);
+      const double A = nb / (l1 - l0);
+      P.binA = (float)A;
+      P.binB = (float)(-l0 * A);
+      P.eps = 1.0f / 32768.0f;
+    } else {
+      P.binA = P.binB = 0.f;
+      P.eps = 4e-6f;
+    }
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    if (c->time_pairs) {
+      check(cudaEventCreate(&ev0), "event");
+      check(cudaEventCreate(&ev1), "event");
+      check(cudaEventRecord(ev0, st), "event record");
+    }
+    counted(c, launch_pairs(P, mode, has_m, has_z, logb, bt, c->num_sms, st, &grid), "pair kernel");
+    if (c->time_pairs) {
+      check(cudaEventRecord(ev1, st), "event record");
+      c->pending_ev0 = ev0;
+      c->pending_ev1 = ev1;
+    }
+  }
+  vlog(c, "mode=%d tasks=%d items=%d grid=%d bt=%d has_m=%d has_z=%d", mode, nT, n_items, grid, bt, (int)has_m,
+       (int)has_z);
+
+  // ---- per-patch sums and per-lens outputs
+  std::vector<std::vector<double>> hpatch(nT);
+  std::vector<double*> dpatch(nT);
+  for (int t = 0; t < nT; ++t) {
+    const LensBuilt& B = lb[tl[t]];
+    dpatch[t] = (double*)ws_alloc(c, sizeof(double) * kQ * nb * n_patch_eff);
+    if (n_items > 0 && B.n_groups > 0)
+      counted(c, launch_patch_reduce(item_sums, tdesc[t].item_base, B.d_patch_groups, n_patch_eff, nb, dpatch[t], st),
+              "patch reduce");
+    else
+      check(cudaMemsetAsync(dpatch[t], 0, sizeof(double) * kQ * nb * n_patch_eff, st), "memset patch");
+    hpatch[t].resize((size_t)kQ * nb * n_patch_eff);
+    check(cudaMemcpyAsync(hpatch[t].data(), dpatch[t], sizeof(double) * kQ * nb * n_patch_eff,
+                          cudaMemcpyDeviceToHost, st), "D2H patch");
+    if (want_lens[t]) {
+      const tpcf_result& o = outs[t];
+      const int64_t nA = lens[tl[t]].n;
+      auto dev_out = [&](void* user, size_t bytes) -> void* {
+        if (!user) return nullptr;
+        void* d = is_device_ptr(user) ? user : ws_alloc(c, bytes);
+        check(cudaMemsetAsync(d, 0, bytes, st), "memset lens out");
+        return d;
+      };
+      const size_t mb = sizeof(float) * nb * (size_t)std::max<int64_t>(nA, 0);
+      float* xE = (float*)dev_out(o.xi_E_marks, mb);
+      float* xB = (float*)dev_out(o.xi_B_marks, mb);
+      float* Km = (float*)dev_out(o.K_marks, mb);
+      float* wm = (float*)dev_out(o.w_marks, mb);
+      float* mw = (float*)dev_out(o.marks_weight, sizeof(float) * std::max<int64_t>(nA, 0));
+      double* ls = (double*)dev_out(o.lens_sums, sizeof(double) * 6 * nb * (size_t)std::max<int64_t>(nA, 0));
+      const bool marks_all = xE && xB && Km && wm;
+      if (!marks_all && (xE || xB || Km || wm))
+        throw Failure(TPCF_ERR_INVALID_ARG, "xi_E_marks, xi_B_marks, K_marks and w_marks go together");
+      if (B.n_valid > 0 && n_items > 0)
+        counted(c, launch_lens_outputs(lens_acc + tdesc[t].lens_acc_off, B.rec, B.perm, B.n_valid, nb, xE, xB, Km,
+                                       wm, mw, ls, st), "lens outputs");
+      if (xE && xE != (void*)o.xi_E_marks) copy_out(c, o.xi_E_marks, xE, mb);
+      if (xB && xB != (void*)o.xi_B_marks) copy_out(c, o.xi_B_marks, xB, mb);
+      if (Km && Km != (void*)o.K_marks) copy_out(c, o.K_marks, Km, mb);
+      if (wm && wm != (void*)o.w_marks) copy_out(c, o.w_marks, wm, mb);
+      if (mw && mw != (void*)o.marks_weight) copy_out(c, o.marks_weight, mw, sizeof(float) * nA);
+      if (ls && ls != (void*)o.lens_sums) copy_out(c, o.lens_sums, ls, sizeof(double) * 6 * nb * nA);
+    }
+  }
+  unsigned herr = 0;
+  check(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "D2H err");
+  check(cudaStreamSynchronize(st), "sync results");
+  if (herr & kErrTimeout) throw Failure(TPCF_ERR_TIMEOUT, "a bounded device wait timed out in the pair kernel");
+  if (herr) throw Failure(TPCF_ERR_CUDA, "device error flags " + std::to_string(herr));
+  if (c->pending_ev0) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->pending_ev0, c->pending_ev1);
+    c->last_pair_ms = ms;
+    cudaEventDestroy(c->pending_ev0);
+    cudaEventDestroy(c->pending_ev1);
+    c->pending_ev0 = c->pending_ev1 = nullptr;
+  }
+
+  // ---- totals and normalised outputs (host, fixed order)
+  std::vector<float> centers(nb);
+  bin_centers_f32(bins, centers.data());
+  static const int pub_row[6] = {QDW, QGT, QGX, QW, QK, QN};  // public row order (dw, gt, gx, w, K, n)
+  c->last_pairs = 0;
+  for (int t = 0; t < nT; ++t) {
+    tpcf_result& o = outs[t];
+    std::vector<double> tot((size_t)kQ * nb, 0.0);
+    for (int p = 0; p < n_patch_eff; ++p)
+      for (int q = 0; q < kQ * nb; ++q) tot[q] += hpatch[t][(size_t)p * kQ * nb + q];
+    std::vector<double> sdw(nb), sgt(nb), sgx(nb), sw(nb), sK(nb);
+    std::vector<int64_t> np(nb);
+    std::vector<float> mt(nb), gt(nb), gx(nb), ww(nb);
+    for (int b = 0; b < nb; ++b) {
+      sdw[b] = tot[QDW * nb + b]; sgt[b] = tot[QGT * nb + b]; sgx[b] = tot[QGX * nb + b];
+      sw[b] = tot[QW * nb + b]; sK[b] = tot[QK * nb + b]; np[b] = (int64_t)llround(tot[QN * nb + b]);
+      c->last_pairs += np[b];
+      mt[b] = (float)(sdw[b] / sw[b]);
+      gt[b] = sK[b] > 0 ? (float)(sgt[b] / sK[b]) : 0.f;
+      gx[b] = sK[b] > 0 ? (float)(sgx[b] / sK[b]) : 0.f;
+      ww[b] = (float)sw[b];
+    }
+    copy_out(c, o.sum_dw, sdw.data(), sizeof(double) * nb);
+    copy_out(c, o.sum_gt, sgt.data(), sizeof(double) * nb);
+    copy_out(c, o.sum_gx, sgx.data(), sizeof(double) * nb);
+    copy_out(c, o.sum_w, sw.data(), sizeof(double) * nb);
+    copy_out(c, o.sum_K, sK.data(), sizeof(double) * nb);
+    copy_out(c, o.n_pairs, np.data(), sizeof(int64_t) * nb);
+    copy_out(c, o.theta, centers.data(), sizeof(float) * nb);
+    if (!sharded) {
+      copy_out(c, o.mean_theta, mt.data(), sizeof(float) * nb);
+      copy_out(c, o.g_t, gt.data(), sizeof(float) * nb);
+      copy_out(c, o.g_x, gx.data(), sizeof(float) * nb);
+      copy_out(c, o.weights, ww.data(), sizeof(float) * nb);
+    }
+    if (o.patch_sums && use_patch_any) {
+      std::vector<double> ps((size_t)n_patch * 6 * nb);
+      for (int p = 0; p < n_patch; ++p)
+        for (int r = 0; r < 6; ++r)
+          for (int b = 0; b < nb; ++b)
+            ps[((size_t)p * 6 + r) * nb + b] = hpatch[t][(size_t)p * kQ * nb + pub_row[r] * nb + b];
+      copy_out(c, o.patch_sums, ps.data(), sizeof(double) * ps.size());
+    }
+    check(cudaStreamSynchronize(st), "sync outputs");  // host staging vectors are freed at scope exit
+  }
+  c->last_call_ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+  vlog(c, "call %.3f ms, pairs %lld", c->last_call_ms, (long long)c->last_pairs);
+  return TPCF_OK;
+}
+
+tpcf_status fail(tpcf_ctx* c, const Failure& f) {
+  if (c) c->err = f.msg;
+  return f.status;
+}
+
+}  // namespace
+
+// ============================================================== C ABI ======
+extern "C" {
+
+int32_t tpcf_abi_version(void) { return TPCF_ABI_VERSION; }
+
+tpcf_status tpcf_create(tpcf_ctx** out, int32_t device, const tpcf_opts* opts) {
+  if (!out) return TPCF_ERR_INVALID_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return TPCF_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= n) return TPCF_ERR_INVALID_ARG;
+  tpcf_ctx* c = new tpcf_ctx();
+  c->device = device;
+  if (opts) c->opts = *opts;
+  else {
+    std::memset(&c->opts, 0, sizeof(c->opts));
+    c->opts.use_grid = 1;
+  }
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return TPCF_ERR_CUDA;
+  }
+  c->stream = c->own_stream;
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  int major = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+  if (major < 10) {
+    cudaStreamDestroy(c->own_stream);
+    delete c;
+    return TPCF_ERR_NO_DEVICE;  // kernels are built for sm_100a only
+  }
+  *out = c;
+  return TPCF_OK;
+}
+
+tpcf_status tpcf_destroy(tpcf_ctx* c) {
+  if (!c) return TPCF_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto& s : c->slots)
+    if (s.ptr) cudaFree(s.ptr);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+  return TPCF_OK;
+}
+
+const char* tpcf_last_error(const tpcf_ctx* c) { return c ? c->err.c_str() : "no context"; }
+
+tpcf_status tpcf_set_stream(tpcf_ctx* c, void* s) {
+  if (!c) return TPCF_ERR_INVALID_ARG;
+  c->stream = s ? (cudaStream_t)s : c->own_stream;
+  return TPCF_OK;
+}
+
+int64_t tpcf_kernel_launches(const tpcf_ctx* c) { return c ? c->launches : 0; }
+
+tpcf_status tpcf_set_timing(tpcf_ctx* c, int32_t enable) {
+  if (!c) return TPCF_ERR_INVALID_ARG;
+  c->time_pairs = enable != 0;
+  return TPCF_OK;
+}
+
+tpcf_status tpcf_set_shard(tpcf_ctx* c, int32_t index, int32_t count) {
+  if (!c || count < 0 || (count > 1 && (index < 0 || index >= count))) return TPCF_ERR_INVALID_ARG;
+  c->opts.shard_index = index;
+  c->opts.shard_count = count;
+  return TPCF_OK;
+}
+
+tpcf_status tpcf_measure_fp32_peak(tpcf_ctx* c, double* tflops) {
+  if (!c || !tflops) return TPCF_ERR_INVALID_ARG;
+  try {
+    begin_call(c);
+    float* out = (float*)ws_alloc(c, 16);
+    const int threads = 256, blocks = c->num_sms * 8, iters = 1 << 16;
+    cudaEvent_t e0, e1;
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    counted(c, launch_ffma_peak(out, blocks, threads, 1024, c->stream), "ffma warm-up");
+    check(cudaEventRecord(e0, c->stream), "event record");
+    counted(c, launch_ffma_peak(out, blocks, threads, iters, c->stream), "ffma peak");
+    check(cudaEventRecord(e1, c->stream), "event record");
+    check(cudaEventSynchronize(e1), "event sync");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *tflops = 2.0 * 8.0 * (double)iters * threads * blocks / (ms * 1e-3) / 1e12;
+    return TPCF_OK;
+  } catch (const Failure& f) {
+    return fail(c, f);
+  }
+}
+
+tpcf_status tpcf_last_stats(const tpcf_ctx* c, tpcf_stats* s) {
+  if (!c || !s) return TPCF_ERR_INVALID_ARG;
+  s->pair_kernel_ms = c->time_pairs ? c->last_pair_ms : 0.0;
+  s->call_ms = c->last_call_ms;
+  s->n_pairs = c->last_pairs;
+  s->h2d_bytes = c->h2d_bytes;
+  s->kernel_launches = c->launches;
+  return TPCF_OK;
+}
+
+tpcf_status tpcf_canonical_edges(const tpcf_bins* bins, double* edges, double* edges_sq) {
+  if (!bins || !edges || !edges_sq) return TPCF_ERR_INVALID_ARG;
+  return canonical_edges(bins, edges, edges_sq);
+}
+
+tpcf_status tpcf_bin_centers(const tpcf_bins* bins, float* centers) {
+  if (!bins || !centers) return TPCF_ERR_INVALID_ARG;
+  std::vector<double> e(kMaxBins + 1), e2(kMaxBins + 1);
+  tpcf_status s = canonical_edges(bins, e.data(), e2.data());
+  if (s != TPCF_OK) return s;
+  bin_centers_f32(bins, centers);
+  return TPCF_OK;
+}
+
+tpcf_status tpcf_shear_scalar(tpcf_ctx* c, const float* xA, const float* yA, const float* zA, const float* valA,
+                              const float* wA, int64_t nA, const float* xB, const float* yB, const float* zB,
+                              const float* e1B, const float* e2B, const float* wB, const float* mB, int64_t nB,
+                              const tpcf_bins* bins, const int32_t* patchA, int32_t n_patch, tpcf_result* out) {
+  if (!c || !bins || !out) return TPCF_ERR_INVALID_ARG;
+  try {
+    std::vector<LensIn> L{{nA, xA, yA, zA, valA, wA, patchA}};
+    std::vector<SrcIn> S{{nB, xB, yB, zB, e1B, e2B, wB, mB}};
+    return run_batch(c, 0, L, S, {0}, {0}, bins, n_patch, out);
+  } catch (const Failure& f) {
+    return fail(c, f);
+  }
+}
+
+tpcf_status tpcf_scalar_scalar(tpcf_ctx* c, const float* xA, const float* yA, const float* valA, const float* wA,
+                               int64_t nA, const float* xB, const float* yB, const float* kE, const float* kB,
+                               const float* wB, int64_t nB, const tpcf_bins* bins, const int32_t* patchA,
+                               int32_t n_patch, tpcf_result* out) {
+  if (!c || !bins || !out) return TPCF_ERR_INVALID_ARG;
+  try {
+    std::vector<LensIn> L{{nA, xA, yA, nullptr, valA, wA, patchA}};
+    std::vector<SrcIn> S{{nB, xB, yB, nullptr, kE, kB, wB, nullptr}};
+    return run_batch(c, 1, L, S, {0}, {0}, bins, n_patch, out);
+  } catch (const Failure& f) {
+    return fail(c, f);
+  }
+}
+
+tpcf_status tpcf_batch_shear_scalar(tpcf_ctx* c, int32_t n_lens_cat, const tpcf_lens_catalog* lenses,
+                                    int32_t n_src_cat, const tpcf_shear_catalog* sources, int32_t n_task,
+                                    const int32_t* task_lens, const int32_t* task_src, const tpcf_bins* bins,
+                                    int32_t n_patch, tpcf_result* outs) {
+  if (!c || !bins || !outs || n_lens_cat < 1 || n_src_cat < 1 || n_task < 1 || !lenses || !sources || !task_lens ||
+      !task_src)
+    return TPCF_ERR_INVALID_ARG;
+  try {
+    std::vector<LensIn> L;
+    for (int i = 0; i < n_lens_cat; ++i) {
+      const tpcf_lens_catalog& l = lenses[i];
+      L.push_back({l.n, l.x, l.y, l.z, l.val, l.w, l.patch});
+    }
+    std::vector<SrcIn> S;
+    for (int i = 0; i < n_src_cat; ++i) {
+      const tpcf_shear_catalog& s = sources[i];
+      S.push_back({s.n, s.x, s.y, s.z, s.e1, s.e2, s.w, s.m});
+    }
+    std::vector<int> tl(task_lens, task_lens + n_task), ts(task_src, task_src + n_task);
+    return run_batch(c, 0, L, S, tl, ts, bins, n_patch, outs);
+  } catch (const Failure& f) {
+    return fail(c, f);
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,883 @@
+// pairs.cu -- the pair-summing kernels of libtpcf_b200 (sm_100a).
+//
+// Replaces the OpenMP pair loops of tangential_shear_tpcf
+// (src/tpcf.f90:261-363) and scalar_kappa_tpcf (src/tpcf.f90:451-535).
+//
+// One thread block = one lens group (one lens per thread) against every source
+// row the group's theta_max neighbourhood touches.  Sources stream through
+// shared memory in tiles moved by the bulk-copy engine (cp.async.bulk +
+// mbarrier, double-buffered); every thread reads the same source (broadcast)
+// and bins the pair into its own FP32 histogram column in shared memory.  The
+// histogram is laid out [bin][quantity][thread], so a warp's 32 read-modify-
+// writes fall in 32 distinct banks whatever bins the lanes pick, and no
+// atomics are needed.  Every ~1024 sources the FP32 columns are folded into
+// FP64: per block (times the lens factors val*w or w) and, when per-lens output
+// is requested, per lens.
+//
+// Binning.  The pair arithmetic is FP32.  For log spacing the bin comes from
+// t = log2(d2)*A + B (one MUFU.LG2 and one FFMA): bin = floor(t).  When t is
+// within `eps` of an integer the pair is re-binned in FP64 by the canonical
+// rule (squared FP64 edges, d2 from the FP32 inputs without contraction), so
+// n_pairs is identical to the FP64 rule of tpcf_canonical_edges.  Other
+// spacings binary-search the FP32 squared edges with a relative guard band.
+
+#include <cub/cub.cuh>
+#include <cstdio>
+
+#include "tpcf_internal.cuh"
+#include "tpcf_kernels.h"
+
+namespace tpcf {
+
+// ------------------------------------------------------------ PTX helpers --
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// 1-D bulk copy global -> shared, completion signalled on `bar`.  Both
+// addresses 16-byte aligned, bytes a multiple of 16 (SrcRec is 32 bytes).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: returns false after ~2^22 polls (each poll may suspend the
+// thread for a hardware-defined interval), never spins forever.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (uint32_t i = 0; i < (1u << 22); ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// ------------------------------------------------------- shared-memory map --
+struct PairSmem {
+  size_t tiles, hist, bsum, e2s, fvw, fw, e2f, span0, span1, tpref, mbar, misc, total;
+};
+__host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+__host__ __device__ inline PairSmem pair_smem_layout(int nb, int qa, int bt) {
+  PairSmem s;
+  size_t o = 0;
+  s.tiles = o; o += 2 * kTile * sizeof(SrcRec);
+  s.hist = o;  o += (size_t)nb * qa * bt * sizeof(float);
+  o = align_up(o, 16);
+  s.bsum = o;  o += (size_t)kQ * nb * sizeof(double);
+  s.e2s = o;   o += (size_t)(nb + 1) * sizeof(double);
+  s.fvw = o;   o += (size_t)bt * sizeof(double);
+  s.fw = o;    o += (size_t)bt * sizeof(double);
+  s.e2f = o;   o += (size_t)(nb + 1) * sizeof(float);
+  o = align_up(o, 16);
+  s.span0 = o; o += kMaxRows * sizeof(int);
+  s.span1 = o; o += kMaxRows * sizeof(int);
+  s.tpref = o; o += (kMaxRows + 1) * sizeof(int);
+  o = align_up(o, 16);
+  s.mbar = o;  o += 2 * sizeof(uint64_t);
+  s.misc = o;  o += 16;
+  s.total = align_up(o, 128);
+  return s;
+}
+
+// ------------------------------------------------------------ geometry ------
+__device__ __forceinline__ int clamp_floor(float v, int lo, int hi) {
+  v = floorf(v);
+  v = fminf(fmaxf(v, (float)lo), (float)hi);
+  return (int)v;
+}
+// Rows of cells within R of the box.
+__device__ __forceinline__ void row_range(const GridDesc& G, float4 box, float R, float m, int& cy0,
+                                          int& cy1) {
+  cy0 = clamp_floor((box.y - R - m - G.y0) * G.inv_cell, 0, G.ncy - 1);
+  cy1 = clamp_floor((box.w + R + m - G.y0) * G.inv_cell, 0, G.ncy - 1);
+}
+// The contiguous run of sources of row cy whose cells lie within R of the box.
+__device__ __forceinline__ int2 row_span(const GridDesc& G, float4 box, float R, float m, int cy) {
+  const float ylo = G.y0 + (float)cy * G.cell - m;
+  const float yhi = G.y0 + (float)(cy + 1) * G.cell + m;
+  const float dyr = fmaxf(0.f, fmaxf(ylo - box.w, box.y - yhi));
+  if (dyr > R) return make_int2(0, 0);
+  const float rx = sqrtf(fmaxf(R * R - dyr * dyr, 0.f)) + m;
+  const int cx0 = clamp_floor((box.x - rx - G.x0) * G.inv_cell, 0, G.ncx - 1);
+  const int cx1 = clamp_floor((box.z + rx - G.x0) * G.inv_cell, 0, G.ncx - 1);
+  const int base = cy * G.ncx;
+  return make_int2(G.cell_start[base + cx0], G.cell_start[base + cx1 + 1]);
+}
+
+// ------------------------------------------------------------ binning -------
+// Canonical FP64 bin of the pair (rare path: pairs inside the guard band).
+__device__ __noinline__ int slow_bin(float lx, float ly, float sx, float sy, const double* e2, int nb) {
+  const double dx = __dsub_rn((double)lx, (double)sx);
+  const double dy = __dsub_rn((double)ly, (double)sy);
+  const double d2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+  if (!(d2 >= e2[0]) || d2 > e2[nb]) return -1;
+  if (d2 == e2[nb]) return nb - 1;
+  int lo = 0, hi = nb;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (d2 >= e2[mid]) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+struct BinCtx {
+  float A, B, eps, one_m_eps;
+  float lo_g, hi_g;  // generic: fast reject bounds e2f[0]*(1-eps), e2f[nb]*(1+eps)
+  int nb;
+  const double* e2s;
+  const float* e2f;
+};
+
+template <bool LOGB>
+__device__ __forceinline__ int pair_bin(float d2, float lx, float ly, float sx, float sy, const BinCtx& C) {
+  if (LOGB) {
+    const float t = fmaf(__log2f(d2), C.A, C.B);
+    const float tf = floorf(t);
+    const float fr = t - tf;
+    int b = __float2int_rz(tf);
+    if (fr < C.eps || fr > C.one_m_eps) b = slow_bin(lx, ly, sx, sy, C.e2s, C.nb);
+    return b;
+  } else {
+    if (d2 < C.lo_g || d2 > C.hi_g) return -1;
+    int lo = 0, hi = C.nb;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (d2 >= C.e2f[mid]) lo = mid; else hi = mid;
+    }
+    const float el = C.e2f[lo], eh = C.e2f[lo + 1];
+    if (d2 <= el * (1.f + C.eps) || d2 >= eh * (1.f - C.eps)) lo = slow_bin(lx, ly, sx, sy, C.e2s, C.nb);
+    return lo;
+  }
+}
+
+// One pair: lens (lx, ly, lz) against source record (a, b).  hcol points at
+// this thread's histogram column; row (bin*QA + q) is at hcol[(bin*QA+q)*BT].
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int QA>
+__device__ __forceinline__ void do_pair(float lx, float ly, float lz, const float4 a, const float4 b,
+                                        float* __restrict__ hcol, const BinCtx& C) {
+  if (HAS_Z) {
+    if (lz > b.z) return;  // src/tpcf.f90:322
+  }
+  const float dx = lx - a.x;
+  const float dy = ly - a.y;
+  const float dx2 = dx * dx;
+  const float d2 = fmaf(dy, dy, dx2);
+  const int bin = pair_bin<LOGB>(d2, lx, ly, a.x, a.y, C);
+  if ((unsigned)bin >= (unsigned)C.nb) return;
+  // d and 1/d^2 from one MUFU.RSQ.  Generic spacings may have x_min = 0, where
+  // d2 = 0 is in range: there d = sqrt(0) = 0 exactly (as in the reference).
+  float d, r;
+  if (LOGB) {
+    const float rs = rsqrtf(d2);
+    d = d2 * rs;
+    r = rs * rs;
+  } else {
+    d = sqrtf(d2);
+    r = __frcp_rn(d2);
+  }
+  float* h = hcol + bin * (QA * BT);
+  if (MODE == 0) {
+    // cos 2phi = (dx^2 - dy^2)/d^2, sin 2phi = 2 dx dy / d^2 (src/tpcf.f90:343-344)
+    const float c2 = fmaf(-dy, dy, dx2) * r;
+    const float qq = dx * dy;
+    const float s2 = (qq + qq) * r;
+    // a.z = -e1*w, a.w = -e2*w:  g_t term = a.z*c2 + a.w*s2,  g_x term = a.w*c2 - a.z*s2
+    const float gt = fmaf(a.z, c2, a.w * s2);
+    const float gx = fmaf(a.w, c2, -(a.z * s2));
+    h[QGT * BT] += gt;
+    h[QGX * BT] += gx;
+  } else {
+    h[QGT * BT] += a.z;
+    h[QGX * BT] += a.w;
+  }
+  h[QW * BT] += b.x;
+  h[QDW * BT] = fmaf(d, b.x, h[QDW * BT]);
+  h[QN * BT] += 1.0f;
+  if (MODE == 0 && HAS_M) h[QK * BT] += b.y;
+}
+
+// Fold the FP32 histogram into FP64 (block sums and, optionally, per-lens
+// sums), then clear this thread's column.  Called by all threads.
+template <int QA, int BT>
+__device__ __forceinline__ void flush_hist(float* hist, double* bsum, const double* fvw, const double* fw,
+                                           int nb, double* lens_acc_col, size_t lens_stride, bool first,
+                                           bool active) {
+  const int tid = threadIdx.x;
+  __syncthreads();
+  float* hcol = hist + tid;
+  if (lens_acc_col && active) {
+    for (int q = 0; q < kQ; ++q) {
+      const int qa = (q == QK && QA == 5) ? QW : q;
+      for (int b = 0; b < nb; ++b) {
+        const double v = (double)hcol[(b * QA + qa) * BT];
+        double* p = lens_acc_col + (size_t)(q * nb + b) * lens_stride;
+        *p = first ? v : *p + v;
+      }
+    }
+  }
+  for (int e = tid; e < kQ * nb; e += BT) {
+    const int q = e / nb, b = e - q * nb;
+    if (q == QK && QA == 5) continue;  // K == w: copied from the w row at item end
+    const float* row = hist + (b * QA + q) * BT;
+    const double* f = (q == QGT || q == QGX) ? fvw : fw;
+    double s = 0.0;
+    if (q == QN) {
+      for (int l = 0; l < BT; ++l) s += (double)row[(l + tid) & (BT - 1)];
+    } else {
+      for (int l = 0; l < BT; ++l) {
+        const int c = (l + tid) & (BT - 1);
+        s = fma((double)row[c], f[c], s);
+      }
+    }
+    bsum[e] += s;
+  }
+  __syncthreads();
+  for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
+}
+
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT>
+__global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
+  constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
+  const int nb = P.nb;
+  const int tid = threadIdx.x;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const PairSmem L = pair_smem_layout(nb, QA, BT);
+  SrcRec* tiles = reinterpret_cast<SrcRec*>(smem + L.tiles);
+  float* hist = reinterpret_cast<float*>(smem + L.hist);
+  double* bsum = reinterpret_cast<double*>(smem + L.bsum);
+  double* e2s = reinterpret_cast<double*>(smem + L.e2s);
+  double* fvw = reinterpret_cast<double*>(smem + L.fvw);
+  double* fw = reinterpret_cast<double*>(smem + L.fw);
+  float* e2f = reinterpret_cast<float*>(smem + L.e2f);
+  int* span0 = reinterpret_cast<int*>(smem + L.span0);
+  int* span1 = reinterpret_cast<int*>(smem + L.span1);
+  int* tpref = reinterpret_cast<int*>(smem + L.tpref);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + L.mbar);
+  int* sh_item = reinterpret_cast<int*>(smem + L.misc);
+
+  if (tid == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    mbar_fence_init();
+  }
+  for (int i = tid; i <= nb; i += BT) {
+    e2s[i] = P.e2[i];
+    e2f[i] = P.e2f[i];
+  }
+  __syncthreads();
+  BinCtx C;
+  C.A = P.binA; C.B = P.binB; C.eps = P.eps; C.one_m_eps = 1.f - P.eps;
+  C.nb = nb; C.e2s = e2s; C.e2f = e2f;
+  C.lo_g = e2f[0] * (1.f - P.eps);
+  C.hi_g = e2f[nb] * (1.f + P.eps);
+
+  uint32_t phase = 0u;   // bit k: parity awaited next on buffer k
+  uint32_t tcount = 0u;  // tiles processed by this block so far
+  bool timed_out = false;
+  float* hcol = hist + tid;
+  for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
+
+  for (;;) {
+    if (tid == 0) *sh_item = atomicAdd(P.queue_head, 1);
+    __syncthreads();
+    const int item = *sh_item;
+    if (item >= P.n_items) break;
+    const int2 it = P.items[item];
+    const TaskDesc T = P.tasks[it.x];
+    const LensDesc LD = P.lenses[T.lens_cat];
+    const GridDesc G = P.grids[T.src_cat];
+    const int g = it.y;
+    const int gs = LD.group_start[g];
+    const int nl = LD.group_start[g + 1] - gs;
+    const bool active = tid < nl;
+    float lx = 0.f, ly = 0.f, lz = 0.f;
+    double vw = 0.0, w = 0.0;
+    if (active) {
+      const float4 r = LD.rec[gs + tid];
+      lx = r.x; ly = r.y;
+      vw = (double)r.z * (double)r.w;
+      w = (double)r.w;
+      if (HAS_Z) lz = LD.z[gs + tid];
+    }
+    fvw[tid] = vw;
+    fw[tid] = w;
+    for (int e = tid; e < kQ * nb; e += BT) bsum[e] = 0.0;
+    double* lens_col = nullptr;
+    size_t lens_stride = 0;
+    if (P.lens_acc && T.lens_acc_off >= 0) {
+      lens_col = P.lens_acc + T.lens_acc_off + gs + tid;
+      lens_stride = (size_t)LD.n_valid;
+    }
+    bool first_flush = true;
+    int since_flush = 0;
+    const float4 box = LD.group_box[g];
+    int cy0, cy1;
+    row_range(G, box, P.R, P.margin, cy0, cy1);
+
+    for (int c0 = cy0; c0 <= cy1; c0 += kMaxRows) {
+      const int nr = min(kMaxRows, cy1 - c0 + 1);
+      __syncthreads();
+      for (int r = tid; r < nr; r += BT) {
+        const int2 s = row_span(G, box, P.R, P.margin, c0 + r);
+        span0[r] = s.x;
+        span1[r] = s.y > s.x ? s.y : s.x;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        int acc = 0;
+        for (int r = 0; r < nr; ++r) {
+          tpref[r] = acc;
+          acc += (span1[r] - span0[r] + kTile - 1) / kTile;
+        }
+        tpref[nr] = acc;
+      }
+      __syncthreads();
+      const int ntiles = tpref[nr];
+      int rc = 0, ri = 0;
+      if (tid == 0 && ntiles > 0) {
+        while (tpref[ri + 1] <= 0) ++ri;
+        const int s0 = span0[ri];
+        const int n0 = min(kTile, span1[ri] - s0);
+        const int bb = tcount & 1u;
+        mbar_arrive_tx(&mbar[bb], (uint32_t)(n0 * sizeof(SrcRec)));
+        bulk_g2s(tiles + bb * kTile, G.rec + s0, (uint32_t)(n0 * sizeof(SrcRec)), &mbar[bb]);
+      }
+      for (int k = 0; k < ntiles; ++k) {
+        if (tid == 0 && k + 1 < ntiles) {
+          while (tpref[ri + 1] <= k + 1) ++ri;
+          const int s1 = span0[ri] + (k + 1 - tpref[ri]) * kTile;
+          const int n1 = min(kTile, span1[ri] - s1);
+          const int bb = (tcount + k + 1) & 1u;
+          mbar_arrive_tx(&mbar[bb], (uint32_t)(n1 * sizeof(SrcRec)));
+          bulk_g2s(tiles + bb * kTile, G.rec + s1, (uint32_t)(n1 * sizeof(SrcRec)), &mbar[bb]);
+        }
+        while (tpref[rc + 1] <= k) ++rc;
+        const int s = span0[rc] + (k - tpref[rc]) * kTile;
+        const int n = min(kTile, span1[rc] - s);
+        const int bb = (tcount + k) & 1u;
+        if (!mbar_wait_bounded(&mbar[bb], (phase >> bb) & 1u)) timed_out = true;
+        phase ^= (1u << bb);
+        if (active && !timed_out) {
+          const SrcRec* S = tiles + bb * kTile;
+#pragma unroll 4
+          for (int j = 0; j < n; ++j) {
+            const float4 a = S[j].a;
+            const float4 b = S[j].b;
+            do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, a, b, hcol, C);
+          }
+        }
+        since_flush += n;
+        if (since_flush >= 4 * kTile) {
+          flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush, active);
+          first_flush = false;
+          since_flush = 0;
+        }
+        __syncthreads();
+      }
+      tcount += (uint32_t)ntiles;
+    }
+    flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush, active);
+    __syncthreads();
+    double* out = P.item_sums + (size_t)(T.item_base + g) * kQ * nb;
+    for (int e = tid; e < kQ * nb; e += BT) {
+      const int q = e / nb;
+      out[e] = (q == QK && QA == 5) ? bsum[e - (QK - QW) * nb] : bsum[e];
+    }
+    __syncthreads();
+  }
+  if (timed_out) atomicOr(P.err, kErrTimeout);
+}
+
+// ------------------------------------------------------------ prep kernels --
+__device__ __forceinline__ int f2ord(float f) {
+  int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float ord2f(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+// Bounding box, z range and count of the valid objects of one catalogue.
+// box_ord = {minx, miny, maxx, maxy, minz, maxz} as order-preserving ints;
+// prange = {min, max} of the patch labels of valid lenses.
+// kind 0 = source (z < 0 masked, src/tpcf.f90:306); kind 1 = lens (w == 0
+// skipped, src/tpcf.f90:285; z < 0 masked).
+__global__ void k_bbox(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+                       const float* __restrict__ w, const int* __restrict__ patch, const float* __restrict__ m,
+                       long long n, int kind, int* box_ord, unsigned long long* count, int* prange) {
+  float mnx = INFINITY, mny = INFINITY, mxx = -INFINITY, mxy = -INFINITY, mnz = INFINITY, mxz = -INFINITY;
+  float mxm = 0.f;
+  int pmn = INT_MAX, pmx = INT_MIN;
+  unsigned long long c = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float xi = x[i], yi = y[i];
+    const float zi = z ? z[i] : 0.f;
+    bool v = isfinite(xi) && isfinite(yi) && zi >= 0.f;
+    if (kind == 1) {
+      if (w[i] == 0.f) v = false;
+      if (v && patch) { pmn = min(pmn, patch[i]); pmx = max(pmx, patch[i]); }
+    }
+    if (v) {
+      mnx = fminf(mnx, xi); mxx = fmaxf(mxx, xi);
+      mny = fminf(mny, yi); mxy = fmaxf(mxy, yi);
+      mnz = fminf(mnz, zi); mxz = fmaxf(mxz, zi);
+      if (m) mxm = fmaxf(mxm, fabsf(m[i]));
+      ++c;
+    }
+  }
+  typedef cub::BlockReduce<float, 256> BRf;
+  typedef cub::BlockReduce<unsigned long long, 256> BRu;
+  typedef cub::BlockReduce<int, 256> BRi;
+  __shared__ union {
+    typename BRf::TempStorage f;
+    typename BRu::TempStorage u;
+    typename BRi::TempStorage i;
+  } tmp;
+  const float mins[3] = {mnx, mny, mnz};
+  const float maxs[3] = {mxx, mxy, mxz};
+  const int slot_min[3] = {0, 1, 4};
+  const int slot_max[3] = {2, 3, 5};
+  for (int k = 0; k < 3; ++k) {
+    float r = BRf(tmp.f).Reduce(mins[k], cub::Min());
+    __syncthreads();
+    if (threadIdx.x == 0) atomicMin(&box_ord[slot_min[k]], f2ord(r));
+    r = BRf(tmp.f).Reduce(maxs[k], cub::Max());
+    __syncthreads();
+    if (threadIdx.x == 0) atomicMax(&box_ord[slot_max[k]], f2ord(r));
+  }
+  {
+    const float r = BRf(tmp.f).Reduce(mxm, cub::Max());
+    __syncthreads();
+    if (threadIdx.x == 0) atomicMax(&box_ord[6], f2ord(r));
+  }
+  const unsigned long long cs = BRu(tmp.u).Sum(c);
+  __syncthreads();
+  if (threadIdx.x == 0) atomicAdd(count, cs);
+  int pi = BRi(tmp.i).Reduce(pmn, cub::Min());
+  __syncthreads();
+  if (threadIdx.x == 0) atomicMin(&prange[0], pi);
+  pi = BRi(tmp.i).Reduce(pmx, cub::Max());
+  __syncthreads();
+  if (threadIdx.x == 0) atomicMax(&prange[1], pi);
+}
+
+__global__ void k_bbox_init(int* box_ord, unsigned long long* count, int* prange, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    box_ord[8 * i + 0] = f2ord(INFINITY);
+    box_ord[8 * i + 1] = f2ord(INFINITY);
+    box_ord[8 * i + 2] = f2ord(-INFINITY);
+    box_ord[8 * i + 3] = f2ord(-INFINITY);
+    box_ord[8 * i + 4] = f2ord(INFINITY);
+    box_ord[8 * i + 5] = f2ord(-INFINITY);
+    box_ord[8 * i + 6] = f2ord(0.f);
+    box_ord[8 * i + 7] = 0;
+    count[i] = 0;
+    prange[2 * i] = INT_MAX;
+    prange[2 * i + 1] = INT_MIN;
+  }
+}
+
+__global__ void k_bbox_finish(const int* box_ord, float* box, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) box[i] = ord2f(box_ord[i]);
+}
+
+// Cell key of each source (invalid -> ncells, sorts last).
+__global__ void k_src_keys(const float* __restrict__ x, const float* __restrict__ y,
+                           const float* __restrict__ z, long long n, float x0, float y0, float inv_cell,
+                           int ncx, int ncy, unsigned* keys, int* idx) {
+  const unsigned ncells = (unsigned)ncx * (unsigned)ncy;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float xi = x[i], yi = y[i];
+    bool v = isfinite(xi) && isfinite(yi);
+    if (z && z[i] < 0.f) v = false;
+    unsigned key = ncells;
+    if (v) {
+      const int cx = clamp_floor((xi - x0) * inv_cell, 0, ncx - 1);
+      const int cy = clamp_floor((yi - y0) * inv_cell, 0, ncy - 1);
+      key = (unsigned)cy * (unsigned)ncx + (unsigned)cx;
+    }
+    keys[i] = key;
+    idx[i] = (int)i;
+  }
+}
+
+// cell_start[c] = first sorted position with key >= c, for c in [0, ncells].
+__global__ void k_cell_start(const unsigned* __restrict__ keys, long long n, unsigned ncells, int* cell_start) {
+  const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > ncells) return;
+  long long lo = 0, hi = n;
+  while (lo < hi) {
+    const long long mid = (lo + hi) >> 1;
+    if (keys[mid] < c) lo = mid + 1; else hi = mid;
+  }
+  cell_start[c] = (int)lo;
+}
+
+// Packed, cell-sorted source records.  mode 0 shear, 1 scalar-scalar.
+__global__ void k_src_gather(const int* __restrict__ idx, int n_valid, int mode, const float* __restrict__ x,
+                             const float* __restrict__ y, const float* __restrict__ z,
+                             const float* __restrict__ f1, const float* __restrict__ f2,
+                             const float* __restrict__ w, const float* __restrict__ m, SrcRec* rec) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_valid) return;
+  const int i = idx[s];
+  const float wi = w[i];
+  SrcRec r;
+  if (mode == 0) {
+    r.a = make_float4(x[i], y[i], -(f1[i] * wi), -(f2[i] * wi));
+    const float mi = m ? m[i] : 0.f;
+    r.b = make_float4(wi, wi * (1.0f + mi), z ? z[i] : 0.f, 0.f);
+  } else {
+    r.a = make_float4(x[i], y[i], f1[i] * wi, f2[i] * wi);
+    r.b = make_float4(wi, wi, 0.f, 0.f);
+  }
+  rec[s] = r;
+}
+
+__device__ __forceinline__ unsigned spread16(unsigned v) {
+  v &= 0xffffu;
+  v = (v | (v << 8)) & 0x00ff00ffu;
+  v = (v | (v << 4)) & 0x0f0f0f0fu;
+  v = (v | (v << 2)) & 0x33333333u;
+  v = (v | (v << 1)) & 0x55555555u;
+  return v;
+}
+
+// Lens sort keys: (patch << 32) | Morton(x, y) on a 2^16 grid over the box;
+// invalid lenses get ~0 and sort last.
+__global__ void k_lens_keys(const float* __restrict__ x, const float* __restrict__ y,
+                            const float* __restrict__ z, const float* __restrict__ w,
+                            const int* __restrict__ patch, long long n, float4 box,
+                            unsigned long long* keys, int* idx) {
+  const float sx = 65535.f / fmaxf(box.z - box.x, 1e-30f);
+  const float sy = 65535.f / fmaxf(box.w - box.y, 1e-30f);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float xi = x[i], yi = y[i];
+    bool v = isfinite(xi) && isfinite(yi) && w[i] != 0.f;
+    if (z && z[i] < 0.f) v = false;
+    unsigned long long key = ~0ull;
+    if (v) {
+      const unsigned qx = (unsigned)clamp_floor((xi - box.x) * sx, 0, 65535);
+      const unsigned qy = (unsigned)clamp_floor((yi - box.y) * sy, 0, 65535);
+      const unsigned mort = spread16(qx) | (spread16(qy) << 1);
+      const unsigned long long p = patch ? (unsigned long long)(unsigned)patch[i] : 0ull;
+      key = (p << 32) | mort;
+    }
+    keys[i] = key;
+    idx[i] = (int)i;
+  }
+}
+
+__global__ void k_lens_gather(const int* __restrict__ idx, int n_valid, const float* __restrict__ x,
+                              const float* __restrict__ y, const float* __restrict__ z,
+                              const float* __restrict__ val, const float* __restrict__ w, float4* rec,
+                              float* zs, int* perm) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_valid) return;
+  const int i = idx[s];
+  rec[s] = make_float4(x[i], y[i], val[i], w[i]);
+  if (zs) zs[s] = z ? z[i] : 0.f;
+  perm[s] = i;
+}
+
+// off[p] = first sorted lens with patch >= p, for p in [0, n_patch].
+__global__ void k_patch_offsets(const unsigned long long* __restrict__ keys, int n_valid, int n_patch, int* off) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p > n_patch) return;
+  const unsigned long long t = (unsigned long long)(unsigned)p << 32;
+  int lo = 0, hi = n_valid;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (keys[mid] < t) lo = mid + 1; else hi = mid;
+  }
+  off[p] = lo;
+}
+
+// One warp per group: bounding box of its lenses.
+__global__ void k_group_box(const float4* __restrict__ rec, const int* __restrict__ gstart, int n_groups,
+                            float4* box) {
+  const int g = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (g >= n_groups) return;
+  float mnx = INFINITY, mny = INFINITY, mxx = -INFINITY, mxy = -INFINITY;
+  for (int i = gstart[g] + lane; i < gstart[g + 1]; i += 32) {
+    const float4 r = rec[i];
+    mnx = fminf(mnx, r.x); mxx = fmaxf(mxx, r.x);
+    mny = fminf(mny, r.y); mxy = fmaxf(mxy, r.y);
+  }
+  for (int o = 16; o; o >>= 1) {
+    mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+    mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+    mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+    mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+  }
+  if (lane == 0) box[g] = make_float4(mnx, mny, mxx, mxy);
+}
+
+// Estimated cost of each work item: lenses x sources in its rows.  Key for a
+// descending sort (longest items first).
+__global__ void k_item_cost(const int2* __restrict__ items, int n_items, const TaskDesc* __restrict__ tasks,
+                            const LensDesc* __restrict__ lenses, const GridDesc* __restrict__ grids, float R,
+                            float margin, unsigned long long* cost, int* order) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_items) return;
+  const int2 it = items[i];
+  const TaskDesc T = tasks[it.x];
+  const LensDesc L = lenses[T.lens_cat];
+  const GridDesc G = grids[T.src_cat];
+  const float4 box = L.group_box[it.y];
+  int cy0, cy1;
+  row_range(G, box, R, margin, cy0, cy1);
+  unsigned long long s = 0;
+  for (int cy = cy0; cy <= cy1; ++cy) {
+    const int2 sp = row_span(G, box, R, margin, cy);
+    if (sp.y > sp.x) s += (unsigned long long)(sp.y - sp.x);
+  }
+  const unsigned long long nl = (unsigned long long)(L.group_start[it.y + 1] - L.group_start[it.y]);
+  cost[i] = s * nl + 1;
+  order[i] = i;
+}
+
+// out[j] = items[order[j*count + index]]: shard `index` of `count`, taking every
+// count-th item of the cost-descending order (balanced shards).
+__global__ void k_permute_items(const int2* __restrict__ items, const int* __restrict__ order, int n, int index,
+                                int count, int2* out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long i = (long long)j * count + index;
+  if (i < n) out[j] = items[order[i]];
+}
+
+// FP32 FMA throughput probe: 8 independent FFMA chains per thread.
+__global__ void k_ffma_peak(float* out, int iters, float a, float b) {
+  float r[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r[k] = threadIdx.x * 1e-3f + k;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r[k] = fmaf(r[k], a, b);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += r[k];
+  if (s == 12345.678f) out[0] = s;  // keeps the loop alive, never true in practice
+}
+
+// Per-patch FP64 sums from item sums, fixed order (deterministic).
+// patch_groups[p] .. patch_groups[p+1] are the groups of patch p.
+__global__ void k_patch_reduce(const double* __restrict__ item_sums, int item_base, const int* __restrict__ patch_groups,
+                               int n_patch, int nb, double* patch_sums) {
+  const int p = blockIdx.x;
+  if (p >= n_patch) return;
+  const int g0 = patch_groups[p], g1 = patch_groups[p + 1];
+  for (int e = threadIdx.x; e < kQ * nb; e += blockDim.x) {
+    double s = 0.0;
+    for (int g = g0; g < g1; ++g) s += item_sums[(size_t)(item_base + g) * kQ * nb + e];
+    patch_sums[(size_t)p * kQ * nb + e] = s;
+  }
+}
+
+// Per-lens outputs in input order from per-lens FP64 sums [kQ][nb][n_valid]
+// (sorted order, no lens factors).  Outputs must be zeroed beforehand (masked
+// lenses keep 0, as in the reference).
+__global__ void k_lens_outputs(const double* __restrict__ acc, const float4* __restrict__ rec,
+                               const int* __restrict__ perm, int n_valid, int nb, float* xi_E, float* xi_B,
+                               float* K_m, float* w_m, float* marks_weight, double* lens_sums) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_valid) return;
+  const float4 r = rec[s];
+  const double vw = (double)r.z * (double)r.w, w = (double)r.w;
+  const size_t i = (size_t)perm[s];
+  double mw = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    const double gt = acc[(size_t)(QGT * nb + b) * n_valid + s] * vw;
+    const double gx = acc[(size_t)(QGX * nb + b) * n_valid + s] * vw;
+    const double ww = acc[(size_t)(QW * nb + b) * n_valid + s] * w;
+    const double dw = acc[(size_t)(QDW * nb + b) * n_valid + s] * w;
+    const double nn = acc[(size_t)(QN * nb + b) * n_valid + s];
+    const double kk = acc[(size_t)(QK * nb + b) * n_valid + s] * w;
+    if (xi_E) {
+      xi_E[i * nb + b] = (float)gt;
+      xi_B[i * nb + b] = (float)gx;
+      K_m[i * nb + b] = (float)kk;
+      w_m[i * nb + b] = (float)ww;
+    }
+    if (lens_sums) {
+      double* o = lens_sums + i * 6 * nb;
+      o[0 * nb + b] = dw;
+      o[1 * nb + b] = gt;
+      o[2 * nb + b] = gx;
+      o[3 * nb + b] = ww;
+      o[4 * nb + b] = kk;
+      o[5 * nb + b] = nn;
+    }
+    mw += ww;
+  }
+  if (marks_weight) marks_weight[i] = (float)mw;
+}
+
+// --------------------------------------------------------- host launchers --
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT>
+static cudaError_t launch_pairs_t(const PairParams& P, int num_sms, cudaStream_t st, int* grid_out) {
+  constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
+  const size_t smem = pair_smem_layout(P.nb, QA, BT).total;
+  auto kern = k_pairs<MODE, HAS_M, HAS_Z, LOGB, BT>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  int grid = per_sm * num_sms;
+  if (grid > P.n_items) grid = P.n_items;
+  if (grid < 1) grid = 1;
+  *grid_out = grid;
+  kern<<<grid, BT, smem, st>>>(P);
+  return cudaGetLastError();
+}
+
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB>
+static cudaError_t launch_pairs_bt(const PairParams& P, int bt, int num_sms, cudaStream_t st, int* grid) {
+  switch (bt) {
+    case 128: return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128>(P, num_sms, st, grid);
+    case 64: return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64>(P, num_sms, st, grid);
+    default: return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 32>(P, num_sms, st, grid);
+  }
+}
+
+size_t pair_smem_bytes(int nb, int qa, int bt) { return pair_smem_layout(nb, qa, bt).total; }
+
+cudaError_t launch_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int num_sms,
+                         cudaStream_t st, int* grid) {
+  if (mode == 1) {
+    return logb ? launch_pairs_bt<1, false, false, true>(P, bt, num_sms, st, grid)
+                : launch_pairs_bt<1, false, false, false>(P, bt, num_sms, st, grid);
+  }
+  if (has_m) {
+    if (has_z) return logb ? launch_pairs_bt<0, true, true, true>(P, bt, num_sms, st, grid)
+                           : launch_pairs_bt<0, true, true, false>(P, bt, num_sms, st, grid);
+    return logb ? launch_pairs_bt<0, true, false, true>(P, bt, num_sms, st, grid)
+                : launch_pairs_bt<0, true, false, false>(P, bt, num_sms, st, grid);
+  }
+  if (has_z) return logb ? launch_pairs_bt<0, false, true, true>(P, bt, num_sms, st, grid)
+                         : launch_pairs_bt<0, false, true, false>(P, bt, num_sms, st, grid);
+  return logb ? launch_pairs_bt<0, false, false, true>(P, bt, num_sms, st, grid)
+              : launch_pairs_bt<0, false, false, false>(P, bt, num_sms, st, grid);
+}
+
+static inline unsigned gdim(long long n, int b) {
+  long long g = (n + b - 1) / b;
+  if (g < 1) g = 1;
+  if (g > 148 * 32) g = 148 * 32;
+  return (unsigned)g;
+}
+
+cudaError_t launch_bbox(const float* x, const float* y, const float* z, const float* w, const int* patch,
+                        const float* m, long long n, int kind, int* box_ord, unsigned long long* count,
+                        int* prange, cudaStream_t st) {
+  if (n > 0) k_bbox<<<gdim(n, 256), 256, 0, st>>>(x, y, z, w, patch, m, n, kind, box_ord, count, prange);
+  return cudaGetLastError();
+}
+cudaError_t launch_bbox_init(int* box_ord, unsigned long long* count, int* prange, int n, cudaStream_t st) {
+  k_bbox_init<<<1, 1024, 0, st>>>(box_ord, count, prange, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_bbox_finish(const int* box_ord, float* box, int n, cudaStream_t st) {
+  k_bbox_finish<<<(n + 255) / 256, 256, 0, st>>>(box_ord, box, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_src_keys(const float* x, const float* y, const float* z, long long n, float x0, float y0,
+                            float inv_cell, int ncx, int ncy, unsigned* keys, int* idx, cudaStream_t st) {
+  if (n > 0) k_src_keys<<<gdim(n, 256), 256, 0, st>>>(x, y, z, n, x0, y0, inv_cell, ncx, ncy, keys, idx);
+  return cudaGetLastError();
+}
+cudaError_t launch_cell_start(const unsigned* keys, long long n, unsigned ncells, int* cell_start, cudaStream_t st) {
+  k_cell_start<<<(ncells + 1 + 255) / 256, 256, 0, st>>>(keys, n, ncells, cell_start);
+  return cudaGetLastError();
+}
+cudaError_t launch_src_gather(const int* idx, int n_valid, int mode, const float* x, const float* y, const float* z,
+                              const float* f1, const float* f2, const float* w, const float* m, SrcRec* rec,
+                              cudaStream_t st) {
+  if (n_valid > 0) k_src_gather<<<(n_valid + 255) / 256, 256, 0, st>>>(idx, n_valid, mode, x, y, z, f1, f2, w, m, rec);
+  return cudaGetLastError();
+}
+cudaError_t launch_lens_keys(const float* x, const float* y, const float* z, const float* w, const int* patch,
+                             long long n, float4 box, unsigned long long* keys, int* idx, cudaStream_t st) {
+  if (n > 0) k_lens_keys<<<gdim(n, 256), 256, 0, st>>>(x, y, z, w, patch, n, box, keys, idx);
+  return cudaGetLastError();
+}
+cudaError_t launch_lens_gather(const int* idx, int n_valid, const float* x, const float* y, const float* z,
+                               const float* val, const float* w, float4* rec, float* zs, int* perm, cudaStream_t st) {
+  if (n_valid > 0) k_lens_gather<<<(n_valid + 255) / 256, 256, 0, st>>>(idx, n_valid, x, y, z, val, w, rec, zs, perm);
+  return cudaGetLastError();
+}
+cudaError_t launch_patch_offsets(const unsigned long long* keys, int n_valid, int n_patch, int* off, cudaStream_t st) {
+  k_patch_offsets<<<(n_patch + 1 + 255) / 256, 256, 0, st>>>(keys, n_valid, n_patch, off);
+  return cudaGetLastError();
+}
+cudaError_t launch_group_box(const float4* rec, const int* gstart, int n_groups, float4* box, cudaStream_t st) {
+  if (n_groups > 0) k_group_box<<<(n_groups + 7) / 8, 256, 0, st>>>(rec, gstart, n_groups, box);
+  return cudaGetLastError();
+}
+cudaError_t launch_item_cost(const int2* items, int n_items, const TaskDesc* tasks, const LensDesc* lenses,
+                             const GridDesc* grids, float R, float margin, unsigned long long* cost, int* order,
+                             cudaStream_t st) {
+  if (n_items > 0)
+    k_item_cost<<<(n_items + 127) / 128, 128, 0, st>>>(items, n_items, tasks, lenses, grids, R, margin, cost, order);
+  return cudaGetLastError();
+}
+cudaError_t launch_permute_items(const int2* items, const int* order, int n, int index, int count, int2* out,
+                                 cudaStream_t st) {
+  if (n > 0) k_permute_items<<<(n + 255) / 256, 256, 0, st>>>(items, order, n, index, count, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_ffma_peak(float* out, int blocks, int threads, int iters, cudaStream_t st) {
+  k_ffma_peak<<<blocks, threads, 0, st>>>(out, iters, 0.999999f, 1e-7f);
+  return cudaGetLastError();
+}
+cudaError_t launch_patch_reduce(const double* item_sums, int item_base, const int* patch_groups, int n_patch, int nb,
+                                double* patch_sums, cudaStream_t st) {
+  if (n_patch > 0) k_patch_reduce<<<n_patch, 128, 0, st>>>(item_sums, item_base, patch_groups, n_patch, nb, patch_sums);
+  return cudaGetLastError();
+}
+cudaError_t launch_lens_outputs(const double* acc, const float4* rec, const int* perm, int n_valid, int nb,
+                                float* xi_E, float* xi_B, float* K_m, float* w_m, float* marks_weight,
+                                double* lens_sums, cudaStream_t st) {
+  if (n_valid > 0)
+    k_lens_outputs<<<(n_valid + 127) / 128, 128, 0, st>>>(acc, rec, perm, n_valid, nb, xi_E, xi_B, K_m, w_m,
+                                                          marks_weight, lens_sums);
+  return cudaGetLastError();
+}
+
+// CUB radix sorts (temp storage supplied by the caller).
+cudaError_t sort_pairs_u32(void* tmp, size_t& tmp_bytes, const unsigned* kin, unsigned* kout, const int* vin,
+                           int* vout, int n, int end_bit, cudaStream_t st) {
+  return cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, kin, kout, vin, vout, n, 0, end_bit, st);
+}
+cudaError_t sort_pairs_u64(void* tmp, size_t& tmp_bytes, const unsigned long long* kin, unsigned long long* kout,
+                           const int* vin, int* vout, int n, cudaStream_t st) {
+  return cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, kin, kout, vin, vout, n, 0, 64, st);
+}
+cudaError_t sort_pairs_u64_desc(void* tmp, size_t& tmp_bytes, const unsigned long long* kin,
+                                unsigned long long* kout, const int* vin, int* vout, int n, cudaStream_t st) {
+  return cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, kin, kout, vin, vout, n, 0, 64, st);
+}
+
+}  // namespace tpcf

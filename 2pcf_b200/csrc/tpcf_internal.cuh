@@ -1,0 +1,89 @@
+// tpcf_internal.cuh -- device-side data layout shared by the kernels and the
+// host orchestration of libtpcf_b200.
+//
+// Layout in HBM (one call, many catalogues):
+//   source catalogue  -> cell grid: records sorted by row-major cell index
+//                        (SrcRec, 32 B each), cell_start[ncx*ncy+1]
+//   lens catalogue    -> lenses sorted by (patch, Morton code); groups of at
+//                        most BT consecutive lenses that never straddle a
+//                        patch; one bounding box per group
+//   work item         -> (task, group): one lens group against every source
+//                        row that intersects the group box dilated by theta_max
+//   item_sums         -> FP64 [Q][n_bin] per (task, group), summed per patch
+//                        by k_patch_reduce in a fixed order (deterministic)
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tpcf {
+
+constexpr int kMaxBins = 128;
+constexpr int kMaxRows = 256;   // cell rows scanned per chunk of one work item
+constexpr int kTile = 256;      // sources per shared-memory tile
+constexpr int kFlushTiles = 4;  // FP32 histogram -> FP64 every 4 tiles (<= 1024 sources)
+constexpr int kQ = 6;           // quantities per bin in item/patch/lens sums
+
+// Quantity rows of every FP64 sum array (item, patch, lens and result sums).
+enum Quantity { QGT = 0, QGX = 1, QW = 2, QDW = 3, QN = 4, QK = 5 };
+
+// Device error bits, OR-ed into PairParams::err.
+enum ErrBits : unsigned {
+  kErrTimeout = 1u,   // a bounded mbarrier wait ran out
+  kErrRows = 2u,      // more cell rows than the row chunking expects
+  kErrBounds = 4u,    // an index check failed (skipped the access)
+};
+
+// A source in shared memory / HBM.  Shear: a = {x, y, -e1*w, -e2*w},
+// b = {w, (1+m)*w, z, 0}.  Scalar-scalar: a = {x, y, kE*w, kB*w}, b = {w, w, 0, 0}.
+struct __align__(16) SrcRec {
+  float4 a;
+  float4 b;
+};
+
+struct GridDesc {
+  float x0, y0, cell, inv_cell;
+  int ncx, ncy;
+  int n_valid;
+  int pad;
+  const int* cell_start;  // [ncx*ncy + 1]
+  const SrcRec* rec;      // [n_valid], sorted by cell
+};
+
+struct LensDesc {
+  const float4* rec;        // {x, y, val, w}, sorted
+  const float* z;           // sorted z, or nullptr
+  const int* group_start;   // [n_groups + 1] into the sorted lenses
+  const float4* group_box;  // {xmin, ymin, xmax, ymax}
+  int n_valid;
+  int n_groups;
+};
+
+struct TaskDesc {
+  int lens_cat;
+  int src_cat;
+  int item_base;            // row of (task, group 0) in item_sums
+  int pad;
+  long long lens_acc_off;   // element offset of this task's per-lens sums, -1 = none
+};
+
+struct PairParams {
+  const TaskDesc* tasks;
+  const LensDesc* lenses;
+  const GridDesc* grids;
+  const int2* items;        // (task, group) in processing order
+  int n_items;
+  int nb;
+  int* queue_head;
+  double* item_sums;        // [n_slots][kQ][nb]
+  double* lens_acc;         // per-lens FP64 [kQ][nb][n_valid] per task, or nullptr
+  unsigned* err;
+  const double* e2;         // canonical squared edges [nb+1]
+  const float* e2f;         // FP32 squared edges [nb+1] (generic spacing)
+  float R;                  // search radius: theta_max with a relative margin
+  float margin;             // absolute margin for cell-boundary rounding
+  float binA, binB;         // log spacing: t = lg2(d2)*binA + binB
+  float eps;                // guard band half-width in t units (log) or relative (generic)
+  int pad;
+};
+
+}  // namespace tpcf

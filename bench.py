@@ -1,0 +1,326 @@
+"""Benchmark: Gpairs/s of the shear-scalar (xi_t) pair sums at 10M objects.
+
+Workload (the tomography workload of synth.py, number 5): 5 shear bins of
+0.2/0.5/1.0/1.9/4.0 M sources x 5 scalar bins of 0.1/0.2/0.4/0.7/1.0 M lenses,
+10.0 M objects on a 1000 deg^2 flat patch (clustered: Gaussian blobs on a
+Poisson background), 25 cross-correlations in one persistent launch, 20 log
+bins from 1 to 300 arcmin, 100 lens patches (per-patch sums for the
+bootstrap).  Synthetic, seeded (numpy PCG64, seed 1005).
+
+One step = one tpcf_batch_shear_scalar call: grid and lens-group build on the
+device, the pair kernel over all 25 tasks, the per-patch reduction, outputs.
+``value`` uses inputs resident in HBM; ``e2e`` the same call with pinned host
+inputs (H2D copies and the result D2H inside the timed region).  Times are CUDA
+events on the stream the library launches on; for N > 1 ranks the work items
+are sharded (no data-path collective except one all-reduce of the per-patch
+sums) and the time is the max over ranks.
+
+--impl reference times the reference algorithm's CPU path (the FP32 OpenMP
+restatement of tangential_shear_tpcf with its kd-tree, oracle/) on the host
+cores on a bounded lens sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gpairs/s for xi_t at 10M objects, plain vs batched+adjoint form at 1e-6 rel. error"
+UNIT = "Gpairs/s"
+FLOP_PER_PAIR = 26  # shear-scalar, FMA = 2, MUFU = 1 (per binned pair)
+WORKLOAD_DESC = ("tomography: 5 shear bins (0.2,0.5,1.0,1.9,4.0 M) x 5 scalar bins "
+                 "(0.1,0.2,0.4,0.7,1.0 M) = 10.0 M objects, 25 cross-pairs in one launch, "
+                 "20 log bins 1-300 arcmin, 1000 deg^2 clustered, 100 lens patches")
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        for l in getattr(self, "lines", []):
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                               p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- workload --
+def workload(scale):
+    synth = importlib.import_module("2pcf_b200.synth")
+    return synth.make_workload(5, scale=scale)
+
+
+def cpu_baseline(w, seconds, nthreads, steps=1, warmup=0):
+    """Reference algorithm (FP32 restatement + kd-tree, OpenMP) on a lens sample:
+    every k-th lens of each scalar bin, concatenated, against each full shear
+    bin (the 25 task pairs).  Rate = binned pairs / pair-loop seconds (tree
+    builds excluded, which favours the CPU).  k is calibrated so one step takes
+    about ``seconds`` of pair-loop time."""
+    from oracle import oracle as O
+    lo, hi, nb = w["bins"]
+    lenses, shapes = w["lens_bins"], w["shape_bins"]
+
+    def sample(stride):
+        return {k: np.concatenate([L[k][::stride] for L in lenses]) for k in ("x", "y", "z", "val", "w")}
+
+    def run(stride):
+        Ls = sample(stride)
+        pairs, loop = 0, 0.0
+        for S in shapes:
+            r = O.ref_pairs(O.SHEAR, Ls, S, lo, hi, nb, num_threads=nthreads)
+            pairs += int(r["n_pairs"].sum())
+            loop += O.last_timing()[1]
+        return pairs, loop, len(Ls["x"])
+
+    p0, t0, _ = run(20000)                       # calibration (~120 lenses)
+    rate = p0 / max(t0, 1e-6)
+    pairs_per_lens = p0 / len(sample(20000)["x"])
+    n_tot = sum(len(L["x"]) for L in lenses)
+    want = max(1.0, seconds * rate / pairs_per_lens)
+    stride = max(1, int(n_tot / want))
+    for _ in range(warmup):
+        run(stride * 10)
+    tot_p, tot_t, nl = 0, 0.0, 0
+    for _ in range(steps):
+        p, t, nl = run(stride)
+        tot_p += p
+        tot_t += t
+    return {"value": tot_p / tot_t / 1e9, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"every {stride}-th lens of each scalar bin ({nl} lenses) against all "
+                      f"{sum(len(S['x']) for S in shapes) / 1e6:.1f} M sources, all 25 tasks; {tot_p:.3e} binned pairs; rate over the OpenMP pair "
+                      f"loop ({tot_t:.1f} s), kd-tree builds excluded",
+            "seconds": tot_t}
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    w = workload(args.scale)
+    nt = host_threads()
+    per_step = max(2.0, min(20.0, 120.0 / max(1, args.steps)))
+    cb = cpu_baseline(w, per_step, nt, steps=args.steps, warmup=args.warmup)
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": cb["seconds"] * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": WORKLOAD_DESC, "scale": args.scale},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------------- ours --
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="object-count scale of the workload")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    tpcf = importlib.import_module("2pcf_b200")
+
+    w = workload(args.scale)
+    bins = tpcf.create_bins(*w["bins"])
+    n_patch = w["n_patch"]
+    # lens patches: fixed-grid blocks of the field (one label per lens)
+    box = w["box"]
+    side = int(np.sqrt(n_patch))
+
+    def patches(L):
+        ix = np.minimum((L["x"] / box * side).astype(np.int32), side - 1)
+        iy = np.minimum((L["y"] / box * side).astype(np.int32), side - 1)
+        return (iy * side + ix).astype(np.int32)
+
+    lpatch = [patches(L) for L in w["lens_bins"]]
+    ctx = tpcf.Context(local)
+    ctx.set_timing(True)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    if world > 1:
+        ctx.set_shard(rank, world)
+
+    def cats(to):
+        L = [tpcf.LensCatalog(**{k: to(l[k]) for k in ("x", "y", "val", "w", "z")}) for l in w["lens_bins"]]
+        S = [tpcf.ShapeCatalog(**{k: to(s[k]) for k in ("x", "y", "e1", "e2", "w", "z", "m")})
+             for s in w["shape_bins"]]
+        return L, S
+
+    dev = lambda a: torch.from_numpy(a).cuda()
+    pin = lambda a: torch.from_numpy(a).pin_memory()
+    Ld, Sd = cats(dev)
+    Pd = [dev(p) for p in lpatch]
+    Lh, Sh = cats(pin)
+    Ph = [pin(p) for p in lpatch]
+    torch.cuda.synchronize()
+
+    def step(L, S, P):
+        outs = tpcf.batch_shear_2pcf(L, S, w["tasks"], bins, lens_patches=P, n_patch=n_patch, ctx=ctx)
+        if world > 1:
+            v = torch.tensor(np.stack([np.stack([o.sum_gt, o.sum_K, o.n_pairs.astype(np.float64)])
+                                       for o in outs]), device="cuda")
+            dist.all_reduce(v)
+            return int(v[:, 2].sum().item())
+        return sum(int(o.n_pairs.sum()) for o in outs)
+
+    def timed(L, S, P, n):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.kernel_launches
+        pair_ms = 0.0
+        pairs = 0
+        e0.record(stream)
+        for _ in range(n):
+            pairs = step(L, S, P)
+            pair_ms += ctx.stats()["pair_kernel_ms"]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms = e0.elapsed_time(e1) / n
+        t = torch.tensor([ms], device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.item(), pairs, pair_ms / n, ctx.kernel_launches - l0
+
+    for _ in range(args.warmup):
+        step(Ld, Sd, Pd)
+    with ClockSampler(local) as cs:
+        ms, pairs, pair_ms, launches = timed(Ld, Sd, Pd, args.steps)
+    clocks = cs.summary()
+    value = pairs / (ms * 1e-3) / 1e9
+
+    # end to end through the public API with pinned host inputs
+    for _ in range(1):
+        step(Lh, Sh, Ph)
+    ms_e2e, pairs_e2e, _, _ = timed(Lh, Sh, Ph, args.steps)
+    h2d = sum(a.numel() * a.element_size() for c in (Lh + Sh) for a in vars(c).values()
+              if hasattr(a, "numel")) + sum(p.numel() * 4 for p in Ph)
+    d2h = len(w["tasks"]) * bins.n_bin * (5 * 8 + 8 + 5 * 4 + n_patch * 6 * 8)
+
+    peak = ctx.measure_fp32_peak()
+    achieved = pairs * FLOP_PER_PAIR / (pair_ms * 1e-3) / 1e12
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "pairs_traffic.json")
+    if os.path.exists(tfile):
+        try:
+            t = json.load(open(tfile))
+            traffic = t["dram_bytes_per_pair"] * pairs
+        except Exception:
+            traffic = None
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "accumulate": "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD_DESC, "scale": args.scale, "global_batch": int(pairs),
+                   "parallelism": f"work items sharded over {world} rank(s)" if world > 1 else "single GPU",
+                   "l2": "inputs (280 MB of catalogues) larger than L2 (126 MB); no flush",
+                   "step": "grid build + 25-task pair kernel + per-patch sums (tpcf_batch_shear_scalar)"},
+        "e2e": {"value": pairs_e2e / (ms_e2e * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": "k_pairs",
+                     "flop_per_pair": FLOP_PER_PAIR, "kernel_ms": pair_ms,
+                     "peak_source": "measured in this run: FFMA loop (tpcf_measure_fp32_peak); "
+                                    "MEASURED_PEAKS.json has no FP32 figure"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        cb = cpu_baseline(w, args.cpu_seconds, host_threads())
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,230 @@
+/*
+ * tpcf_b200.h -- C ABI of libtpcf_b200.so, a B200 (sm_100a) implementation of
+ * the pair-summing path of tilmantroester/2pcf.
+ *
+ * Every entry point is plain C: scalars by value, arrays as pointers plus
+ * sizes, no C++ or torch types.  Each entry point names the reference routine
+ * it replaces (file:line inside the reference project).  A Fortran caller
+ * binds them through iso_c_binding (the interface module is given in
+ * INTEGRATION.md); Python binds them through ctypes.
+ *
+ * Conventions
+ *   - Arrays are 0-based structure-of-arrays, the memory layout of the
+ *     reference's contiguous 1-based `real` arrays passed with c_loc.
+ *   - 2-D outputs [n_A][n_bin] are row-major, which is the memory layout of the
+ *     reference's column-major (n_bin, n_A) marks arrays.
+ *   - Any input or output pointer may be host memory (pageable or pinned) or
+ *     device memory of the context's GPU; the library detects which and copies
+ *     only host arrays.
+ *   - Nullable pointers are marked.  Outputs are written only on TPCF_OK.
+ *   - The library never calls exit() or abort(): each call returns a
+ *     tpcf_status and tpcf_last_error(ctx) describes the last failure.  This
+ *     replaces the reference's `stop` / `error stop`.
+ *   - A context binds one device and one stream; use one context per host
+ *     thread.  There is no CPU fallback: without a usable GPU, tpcf_create
+ *     fails with TPCF_ERR_NO_DEVICE.
+ */
+#ifndef TPCF_B200_H
+#define TPCF_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TPCF_ABI_VERSION 1
+
+typedef enum tpcf_status {
+  TPCF_OK = 0,
+  TPCF_ERR_INVALID_ARG = 1,
+  TPCF_ERR_OOM = 2,
+  TPCF_ERR_OVERFLOW = 3,      /* a size limit of the library was exceeded      */
+  TPCF_ERR_TIMEOUT = 4,       /* a bounded device-side wait ran out            */
+  TPCF_ERR_CUDA = 5,          /* a CUDA runtime call failed                    */
+  TPCF_ERR_NOT_SUPPORTED = 6, /* e.g. spherical coordinates                    */
+  TPCF_ERR_NO_DEVICE = 7
+} tpcf_status;
+
+/* Bin spacings, same codes as lin_binning .. sqrt_binning (src/utils.f90:7). */
+enum { TPCF_LIN = 0, TPCF_LOG = 1, TPCF_IHS = 2, TPCF_SQRT = 3 };
+
+/* Replaces type(binning) (src/utils.f90:18-24) as built by
+ * create_bins(x_min, x_max, n_bin, p, spacing) (src/utils.f90:139-230).
+ * Edges are derived inside the library by the canonical FP64 rule (see
+ * tpcf_canonical_edges).  1 <= n_bin <= 128.                                   */
+typedef struct tpcf_bins {
+  int32_t n_bin;
+  int32_t spacing;
+  double x_min;
+  double x_max;
+  double ihs_theta; /* `p` of the ihs spacing; ignored otherwise              */
+} tpcf_bins;
+
+typedef struct tpcf_opts {
+  int32_t use_grid;      /* 1: cell-grid pruning at theta_max (replaces the
+                            kd-tree, use_kd_tree); 0: every lens against every
+                            source (the reference's --no-kd-tree)            */
+  int32_t verbose;       /* print phase timings to stderr                    */
+  double cell_size;      /* grid cell side in input units; 0 = autotuned     */
+  int32_t spherical;     /* must be 0: only flat coordinates are supported   */
+  int32_t shard_index;   /* with shard_count > 1, this call computes only the
+                            work items i with i % shard_count == shard_index
+                            (items ordered by estimated cost): per-bin,
+                            per-patch and per-lens sums are then partial and
+                            must be summed over shards (one all-reduce);
+                            normalised outputs are not written            */
+  int32_t shard_count;   /* 0 or 1: no sharding                              */
+  int32_t reserved[5];
+} tpcf_opts;
+
+/* Per-call results.  Replaces type(shear_2pcf_results) (src/tpcf.f90:17-22)
+ * plus the raw FP64 sums behind it.  Arrays are caller-allocated. */
+typedef struct tpcf_result {
+  /* FP64 per-bin sums, always written, [n_bin] each:
+   *   sum_dw = sum d*w_A*w_B        sum_gt = sum g_t terms (val_A-weighted)
+   *   sum_gx = sum g_x terms        sum_w  = sum w_A*w_B
+   *   sum_K  = sum w_A*w_B*(1+m_B)  (equals sum_w for scalar-scalar)         */
+  double* sum_dw;
+  double* sum_gt;
+  double* sum_gx;
+  double* sum_w;
+  double* sum_K;
+  int64_t* n_pairs;
+  /* Reference-normalised outputs (src/tpcf.f90:369-376), nullable, [n_bin]:
+   * theta = bin centres as create_bins computes them, mean_theta =
+   * sum_dw/sum_w (NaN when sum_w == 0, as in the reference), g_t, g_x =
+   * sum/K where K > 0 else 0, weights = sum_w.                              */
+  float* theta;
+  float* mean_theta;
+  float* g_t;
+  float* g_x;
+  float* weights;
+  /* Per-lens marks (src/tpcf.f90:354-358), nullable, [n_A][n_bin], lens order
+   * of the input; marks_weight is [n_A].                                    */
+  float* xi_E_marks;
+  float* xi_B_marks;
+  float* K_marks;
+  float* w_marks;
+  float* marks_weight;
+  /* Per-lens FP64 sums, nullable, [n_A][6][n_bin] with the six rows
+   * (sum_dw, sum_gt, sum_gx, sum_w, sum_K, n_pairs) of that lens.           */
+  double* lens_sums;
+  /* Per-patch FP64 sums, nullable, [n_patch][6][n_bin], same six rows, for
+   * lens patches given in the call (block sums of
+   * survey_marked_point_block_bootstrap, src/tpcf.f90:1130-1137).           */
+  double* patch_sums;
+} tpcf_result;
+
+/* Lens / scalar catalogue (lens_catalog, src/tpcf.f90:34-37).  z may be NULL
+ * (all 0).  patch may be NULL (one patch); otherwise values in [0, n_patch).  */
+typedef struct tpcf_lens_catalog {
+  int64_t n;
+  const float* x;
+  const float* y;
+  const float* z;
+  const float* val;
+  const float* w;
+  const int32_t* patch;
+} tpcf_lens_catalog;
+
+/* Shear catalogue (shape_catalog, src/tpcf.f90:24-27).  z may be NULL (all 0),
+ * m may be NULL (all 0). */
+typedef struct tpcf_shear_catalog {
+  int64_t n;
+  const float* x;
+  const float* y;
+  const float* z;
+  const float* e1;
+  const float* e2;
+  const float* w;
+  const float* m;
+} tpcf_shear_catalog;
+
+typedef struct tpcf_ctx tpcf_ctx;
+
+/* ---------------------------------------------------------------- context -- */
+int32_t tpcf_abi_version(void);
+tpcf_status tpcf_create(tpcf_ctx** ctx, int32_t device, const tpcf_opts* opts /* nullable */);
+tpcf_status tpcf_destroy(tpcf_ctx* ctx);
+const char* tpcf_last_error(const tpcf_ctx* ctx);
+/* Use a caller stream (a cudaStream_t passed as void*) instead of the
+ * context's own; NULL restores the context stream. */
+tpcf_status tpcf_set_stream(tpcf_ctx* ctx, void* cuda_stream);
+/* Number of kernels this context launched so far. */
+int64_t tpcf_kernel_launches(const tpcf_ctx* ctx);
+
+/* Statistics of the last pair-sum call.  pair_kernel_ms is measured with CUDA
+ * events recorded on the context stream around the pair kernel when timing
+ * is enabled (tpcf_set_timing), else 0. */
+typedef struct tpcf_stats {
+  double pair_kernel_ms;
+  double call_ms;
+  int64_t n_pairs;          /* sum of n_pairs over all bins and tasks       */
+  int64_t h2d_bytes;        /* bytes copied host->device by the last call   */
+  int64_t kernel_launches;  /* kernels launched by this context so far      */
+} tpcf_stats;
+tpcf_status tpcf_set_timing(tpcf_ctx* ctx, int32_t enable);
+tpcf_status tpcf_last_stats(const tpcf_ctx* ctx, tpcf_stats* stats);
+/* Change the sharding of later calls (see tpcf_opts.shard_index). */
+tpcf_status tpcf_set_shard(tpcf_ctx* ctx, int32_t shard_index, int32_t shard_count);
+
+/* Roofline helper with no counterpart in the reference: measures this GPU's
+ * FP32 FMA throughput (FLOP/s counting an FMA as 2) with a register-resident
+ * FFMA loop timed by CUDA events on the context stream. */
+tpcf_status tpcf_measure_fp32_peak(tpcf_ctx* ctx, double* tflops);
+
+/* Canonical FP64 edges [n_bin+1] and squared edges [n_bin+1]: the bin rule of
+ * every pair kernel.  A pair with d2 = dx*dx + dy*dy (FP64, from the FP32
+ * inputs, no contraction) is in bin i when edges_sq[i] <= d2 < edges_sq[i+1],
+ * in bin n_bin-1 when d2 == edges_sq[n_bin], and in no bin otherwise.  Host
+ * only; mirrors the edge formulas of create_bins (src/utils.f90:202-228). */
+tpcf_status tpcf_canonical_edges(const tpcf_bins* bins, double* edges, double* edges_sq);
+
+/* Bin centres as the reference computes them in FP32 (src/utils.f90:202-229). */
+tpcf_status tpcf_bin_centers(const tpcf_bins* bins, float* centers);
+
+/* ------------------------------------------------------------- pair sums -- */
+/* Replaces tangential_shear_tpcf (src/tpcf.f90:190-378), called from
+ * shear_2pcf (src/tpcf.f90:134-160).  Lenses with wA == 0 or zA < 0 and
+ * sources with zB < 0 take part in no pair; a pair is skipped when zA > zB
+ * (src/tpcf.f90:285, :306, :322).  zA, zB, mB and patchA may be NULL. */
+tpcf_status tpcf_shear_scalar(tpcf_ctx* ctx,
+                              const float* xA, const float* yA, const float* zA,
+                              const float* valA, const float* wA, int64_t nA,
+                              const float* xB, const float* yB, const float* zB,
+                              const float* e1B, const float* e2B, const float* wB,
+                              const float* mB, int64_t nB,
+                              const tpcf_bins* bins,
+                              const int32_t* patchA, int32_t n_patch,
+                              tpcf_result* out);
+
+/* Replaces scalar_kappa_tpcf (src/tpcf.f90:380-545), called from kappa_2pcf
+ * (src/tpcf.f90:162-188): sum_gt accumulates kE*wB*valA*wA and sum_gx
+ * kB*wB*valA*wA; K = weights. */
+tpcf_status tpcf_scalar_scalar(tpcf_ctx* ctx,
+                               const float* xA, const float* yA,
+                               const float* valA, const float* wA, int64_t nA,
+                               const float* xB, const float* yB,
+                               const float* kE, const float* kB, const float* wB, int64_t nB,
+                               const tpcf_bins* bins,
+                               const int32_t* patchA, int32_t n_patch,
+                               tpcf_result* out);
+
+/* Batched tomography: n_task (lens catalogue, source catalogue) pairs, all in
+ * one persistent launch.  Each task t correlates lenses[task_lens[t]] with
+ * sources[task_src[t]] exactly as tpcf_shear_scalar would, writing outs[t].
+ * Replaces the per-field loop around shear_2pcf (src/main.f90:585-617). */
+tpcf_status tpcf_batch_shear_scalar(tpcf_ctx* ctx,
+                                    int32_t n_lens_cat, const tpcf_lens_catalog* lenses,
+                                    int32_t n_src_cat, const tpcf_shear_catalog* sources,
+                                    int32_t n_task, const int32_t* task_lens,
+                                    const int32_t* task_src,
+                                    const tpcf_bins* bins, int32_t n_patch,
+                                    tpcf_result* outs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TPCF_B200_H */
