@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -465,7 +466,9 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
       check(cudaEventCreate(&ev1), "event");
       check(cudaEventRecord(ev0, st), "event record");
     }
-    counted(c, launch_pairs(P, mode, has_m, has_z, logb, bt, c->num_sms, st, &grid), "pair kernel");
+    const char* var_env = std::getenv("TPCF_PAIR_VARIANT");
+    const int variant = var_env ? std::atoi(var_env) : 0;
+    counted(c, launch_pairs(P, mode, has_m, has_z, logb, bt, variant, c->num_sms, st, &grid), "pair kernel");
     if (c->time_pairs) {
       check(cudaEventRecord(ev1, st), "event record");
       c->pending_ev0 = ev0;

@@ -76,6 +76,7 @@ struct PairSmem {
   size_t tiles, hist, bsum, e2s, fvw, fw, e2f, span0, span1, tpref, mbar, misc, total;
 };
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+// bt here is the number of histogram columns (threads x lenses per thread).
 __host__ __device__ inline PairSmem pair_smem_layout(int nb, int qa, int bt) {
   PairSmem s;
   size_t o = 0;
@@ -169,9 +170,17 @@ __device__ __forceinline__ int pair_bin(float d2, float lx, float ly, float sx, 
   }
 }
 
+// Add v to a histogram cell owned by this thread: a plain read-modify-write,
+// or a shared-memory reduction (no load-use dependency on the issuing thread).
+template <bool RED>
+__device__ __forceinline__ void hadd(float* p, float v) {
+  if (RED) atomicAdd(p, v);
+  else *p += v;
+}
+
 // One pair: lens (lx, ly, lz) against source record (a, b).  hcol points at
-// this thread's histogram column; row (bin*QA + q) is at hcol[(bin*QA+q)*BT].
-template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int QA>
+// this lens's histogram column; row (bin*QA + q) is at hcol[(bin*QA+q)*NC].
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int NC, int QA, bool RED>
 __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const float4 a, const float4 b,
                                         float* __restrict__ hcol, const BinCtx& C) {
   if (HAS_Z) {
@@ -194,7 +203,7 @@ __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const floa
     d = sqrtf(d2);
     r = __frcp_rn(d2);
   }
-  float* h = hcol + bin * (QA * BT);
+  float* h = hcol + bin * (QA * NC);
   if (MODE == 0) {
     // cos 2phi = (dx^2 - dy^2)/d^2, sin 2phi = 2 dx dy / d^2 (src/tpcf.f90:343-344)
     const float c2 = fmaf(-dy, dy, dx2) * r;
@@ -203,33 +212,38 @@ __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const floa
     // a.z = -e1*w, a.w = -e2*w:  g_t term = a.z*c2 + a.w*s2,  g_x term = a.w*c2 - a.z*s2
     const float gt = fmaf(a.z, c2, a.w * s2);
     const float gx = fmaf(a.w, c2, -(a.z * s2));
-    h[QGT * BT] += gt;
-    h[QGX * BT] += gx;
+    hadd<RED>(&h[QGT * NC], gt);
+    hadd<RED>(&h[QGX * NC], gx);
   } else {
-    h[QGT * BT] += a.z;
-    h[QGX * BT] += a.w;
+    hadd<RED>(&h[QGT * NC], a.z);
+    hadd<RED>(&h[QGX * NC], a.w);
   }
-  h[QW * BT] += b.x;
-  h[QDW * BT] = fmaf(d, b.x, h[QDW * BT]);
-  h[QN * BT] += 1.0f;
-  if (MODE == 0 && HAS_M) h[QK * BT] += b.y;
+  hadd<RED>(&h[QW * NC], b.x);
+  hadd<RED>(&h[QDW * NC], d * b.x);
+  hadd<RED>(&h[QN * NC], 1.0f);
+  if (MODE == 0 && HAS_M) hadd<RED>(&h[QK * NC], b.y);
 }
 
 // Fold the FP32 histogram into FP64 (block sums and, optionally, per-lens
 // sums), then clear this thread's column.  Called by all threads.
-template <int QA, int BT>
+// Histogram columns: NC = LPT*BT; thread t owns columns t, t+BT, ... (one per
+// lens it holds).  lens_acc_col[k] is the per-lens FP64 column of lens k or null.
+template <int QA, int BT, int LPT>
 __device__ __forceinline__ void flush_hist(float* hist, double* bsum, const double* fvw, const double* fw,
-                                           int nb, double* lens_acc_col, size_t lens_stride, bool first,
-                                           bool active) {
+                                           int nb, double* const* lens_acc_col, size_t lens_stride, bool first) {
+  constexpr int NC = BT * LPT;
   const int tid = threadIdx.x;
   __syncthreads();
-  float* hcol = hist + tid;
-  if (lens_acc_col && active) {
+#pragma unroll
+  for (int k = 0; k < LPT; ++k) {
+    double* col = lens_acc_col[k];
+    if (!col) continue;
+    const float* hcol = hist + tid + k * BT;
     for (int q = 0; q < kQ; ++q) {
       const int qa = (q == QK && QA == 5) ? QW : q;
       for (int b = 0; b < nb; ++b) {
-        const double v = (double)hcol[(b * QA + qa) * BT];
-        double* p = lens_acc_col + (size_t)(q * nb + b) * lens_stride;
+        const double v = (double)hcol[(b * QA + qa) * NC];
+        double* p = col + (size_t)(q * nb + b) * lens_stride;
         *p = first ? v : *p + v;
       }
     }
@@ -237,30 +251,35 @@ __device__ __forceinline__ void flush_hist(float* hist, double* bsum, const doub
   for (int e = tid; e < kQ * nb; e += BT) {
     const int q = e / nb, b = e - q * nb;
     if (q == QK && QA == 5) continue;  // K == w: copied from the w row at item end
-    const float* row = hist + (b * QA + q) * BT;
+    const float* row = hist + (b * QA + q) * NC;
     const double* f = (q == QGT || q == QGX) ? fvw : fw;
     double s = 0.0;
     if (q == QN) {
-      for (int l = 0; l < BT; ++l) s += (double)row[(l + tid) & (BT - 1)];
+      for (int l = 0; l < NC; ++l) s += (double)row[(l + tid) & (NC - 1)];
     } else {
-      for (int l = 0; l < BT; ++l) {
-        const int c = (l + tid) & (BT - 1);
+      for (int l = 0; l < NC; ++l) {
+        const int c = (l + tid) & (NC - 1);
         s = fma((double)row[c], f[c], s);
       }
     }
     bsum[e] += s;
   }
   __syncthreads();
-  for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
+#pragma unroll
+  for (int k = 0; k < LPT; ++k) {
+    float* hcol = hist + tid + k * BT;
+    for (int e = 0; e < nb * QA; ++e) hcol[e * NC] = 0.f;
+  }
 }
 
-template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT>
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int LPT, bool RED>
 __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
   constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
+  constexpr int NC = BT * LPT;  // histogram columns = lenses per group
   const int nb = P.nb;
   const int tid = threadIdx.x;
   extern __shared__ __align__(128) unsigned char smem[];
-  const PairSmem L = pair_smem_layout(nb, QA, BT);
+  const PairSmem L = pair_smem_layout(nb, QA, NC);
   SrcRec* tiles = reinterpret_cast<SrcRec*>(smem + L.tiles);
   float* hist = reinterpret_cast<float*>(smem + L.hist);
   double* bsum = reinterpret_cast<double*>(smem + L.bsum);
@@ -293,8 +312,9 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
   uint32_t phase = 0u;   // bit k: parity awaited next on buffer k
   uint32_t tcount = 0u;  // tiles processed by this block so far
   bool timed_out = false;
-  float* hcol = hist + tid;
-  for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
+#pragma unroll
+  for (int k = 0; k < LPT; ++k)
+    for (int e = 0; e < nb * QA; ++e) hist[tid + k * BT + e * NC] = 0.f;
 
   for (;;) {
     if (tid == 0) *sh_item = atomicAdd(P.queue_head, 1);
@@ -308,25 +328,29 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
     const int g = it.y;
     const int gs = LD.group_start[g];
     const int nl = LD.group_start[g + 1] - gs;
-    const bool active = tid < nl;
-    float lx = 0.f, ly = 0.f, lz = 0.f;
-    double vw = 0.0, w = 0.0;
-    if (active) {
-      const float4 r = LD.rec[gs + tid];
-      lx = r.x; ly = r.y;
-      vw = (double)r.z * (double)r.w;
-      w = (double)r.w;
-      if (HAS_Z) lz = LD.z[gs + tid];
+    float lx[LPT], ly[LPT], lz[LPT];
+    bool act[LPT];
+    double* lens_col[LPT];
+#pragma unroll
+    for (int k = 0; k < LPT; ++k) {
+      const int li = tid + k * BT;
+      act[k] = li < nl;
+      lx[k] = ly[k] = lz[k] = 0.f;
+      double vw = 0.0, w = 0.0;
+      lens_col[k] = nullptr;
+      if (act[k]) {
+        const float4 r = LD.rec[gs + li];
+        lx[k] = r.x; ly[k] = r.y;
+        vw = (double)r.z * (double)r.w;
+        w = (double)r.w;
+        if (HAS_Z) lz[k] = LD.z[gs + li];
+        if (P.lens_acc && T.lens_acc_off >= 0) lens_col[k] = P.lens_acc + T.lens_acc_off + gs + li;
+      }
+      fvw[li] = vw;
+      fw[li] = w;
     }
-    fvw[tid] = vw;
-    fw[tid] = w;
+    const size_t lens_stride = (size_t)LD.n_valid;
     for (int e = tid; e < kQ * nb; e += BT) bsum[e] = 0.0;
-    double* lens_col = nullptr;
-    size_t lens_stride = 0;
-    if (P.lens_acc && T.lens_acc_off >= 0) {
-      lens_col = P.lens_acc + T.lens_acc_off + gs + tid;
-      lens_stride = (size_t)LD.n_valid;
-    }
     bool first_flush = true;
     int since_flush = 0;
     const float4 box = LD.group_box[g];
@@ -337,9 +361,9 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
       const int nr = min(kMaxRows, cy1 - c0 + 1);
       __syncthreads();
       for (int r = tid; r < nr; r += BT) {
-        const int2 s = row_span(G, box, P.R, P.margin, c0 + r);
-        span0[r] = s.x;
-        span1[r] = s.y > s.x ? s.y : s.x;
+        const int2 sp = row_span(G, box, P.R, P.margin, c0 + r);
+        span0[r] = sp.x;
+        span1[r] = sp.y > sp.x ? sp.y : sp.x;
       }
       __syncthreads();
       if (tid == 0) {
@@ -376,18 +400,30 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
         const int bb = (tcount + k) & 1u;
         if (!mbar_wait_bounded(&mbar[bb], (phase >> bb) & 1u)) timed_out = true;
         phase ^= (1u << bb);
-        if (active && !timed_out) {
+        if (act[0] && !timed_out) {
           const SrcRec* S = tiles + bb * kTile;
+          if (LPT == 1 || !act[LPT - 1]) {
 #pragma unroll 4
-          for (int j = 0; j < n; ++j) {
-            const float4 a = S[j].a;
-            const float4 b = S[j].b;
-            do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, a, b, hcol, C);
+            for (int j = 0; j < n; ++j) {
+              const float4 a = S[j].a;
+              const float4 b = S[j].b;
+              do_pair<MODE, HAS_M, HAS_Z, LOGB, NC, QA, RED>(lx[0], ly[0], lz[0], a, b, hist + tid, C);
+            }
+          } else {
+#pragma unroll 2
+            for (int j = 0; j < n; ++j) {
+              const float4 a = S[j].a;
+              const float4 b = S[j].b;
+#pragma unroll
+              for (int kk = 0; kk < LPT; ++kk)
+                do_pair<MODE, HAS_M, HAS_Z, LOGB, NC, QA, RED>(lx[kk], ly[kk], lz[kk], a, b,
+                                                               hist + tid + kk * BT, C);
+            }
           }
         }
         since_flush += n;
         if (since_flush >= 4 * kTile) {
-          flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush, active);
+          flush_hist<QA, BT, LPT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
           first_flush = false;
           since_flush = 0;
         }
@@ -395,7 +431,7 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
       }
       tcount += (uint32_t)ntiles;
     }
-    flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush, active);
+    flush_hist<QA, BT, LPT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
     __syncthreads();
     double* out = P.item_sums + (size_t)(T.item_base + g) * kQ * nb;
     for (int e = tid; e < kQ * nb; e += BT) {
@@ -734,11 +770,11 @@ __global__ void k_lens_outputs(const double* __restrict__ acc, const float4* __r
 }
 
 // --------------------------------------------------------- host launchers --
-template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT>
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int LPT, bool RED>
 static cudaError_t launch_pairs_t(const PairParams& P, int num_sms, cudaStream_t st, int* grid_out) {
   constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
-  const size_t smem = pair_smem_layout(P.nb, QA, BT).total;
-  auto kern = k_pairs<MODE, HAS_M, HAS_Z, LOGB, BT>;
+  const size_t smem = pair_smem_layout(P.nb, QA, BT * LPT).total;
+  auto kern = k_pairs<MODE, HAS_M, HAS_Z, LOGB, BT, LPT, RED>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -754,32 +790,41 @@ static cudaError_t launch_pairs_t(const PairParams& P, int num_sms, cudaStream_t
 }
 
 template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB>
-static cudaError_t launch_pairs_bt(const PairParams& P, int bt, int num_sms, cudaStream_t st, int* grid) {
-  switch (bt) {
-    case 128: return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128>(P, num_sms, st, grid);
-    case 64: return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64>(P, num_sms, st, grid);
-    default: return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 32>(P, num_sms, st, grid);
+static cudaError_t launch_pairs_bt(const PairParams& P, int bt, int variant, int num_sms, cudaStream_t st,
+                                   int* grid) {
+  if (bt == 128) {
+    if (MODE == 0 && !HAS_M && !HAS_Z && LOGB) {  // variants of the main configuration
+      switch (variant) {
+        case 1: return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 1, true>(P, num_sms, st, grid);
+        case 2: return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64, 2, false>(P, num_sms, st, grid);
+        case 3: return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64, 2, true>(P, num_sms, st, grid);
+        default: break;
+      }
+    }
+    return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 1, false>(P, num_sms, st, grid);
   }
+  if (bt == 64) return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64, 1, false>(P, num_sms, st, grid);
+  return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 32, 1, false>(P, num_sms, st, grid);
 }
 
 size_t pair_smem_bytes(int nb, int qa, int bt) { return pair_smem_layout(nb, qa, bt).total; }
 
-cudaError_t launch_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int num_sms,
-                         cudaStream_t st, int* grid) {
+cudaError_t launch_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int variant,
+                         int num_sms, cudaStream_t st, int* grid) {
   if (mode == 1) {
-    return logb ? launch_pairs_bt<1, false, false, true>(P, bt, num_sms, st, grid)
-                : launch_pairs_bt<1, false, false, false>(P, bt, num_sms, st, grid);
+    return logb ? launch_pairs_bt<1, false, false, true>(P, bt, variant, num_sms, st, grid)
+                : launch_pairs_bt<1, false, false, false>(P, bt, variant, num_sms, st, grid);
   }
   if (has_m) {
-    if (has_z) return logb ? launch_pairs_bt<0, true, true, true>(P, bt, num_sms, st, grid)
-                           : launch_pairs_bt<0, true, true, false>(P, bt, num_sms, st, grid);
-    return logb ? launch_pairs_bt<0, true, false, true>(P, bt, num_sms, st, grid)
-                : launch_pairs_bt<0, true, false, false>(P, bt, num_sms, st, grid);
+    if (has_z) return logb ? launch_pairs_bt<0, true, true, true>(P, bt, variant, num_sms, st, grid)
+                           : launch_pairs_bt<0, true, true, false>(P, bt, variant, num_sms, st, grid);
+    return logb ? launch_pairs_bt<0, true, false, true>(P, bt, variant, num_sms, st, grid)
+                : launch_pairs_bt<0, true, false, false>(P, bt, variant, num_sms, st, grid);
   }
-  if (has_z) return logb ? launch_pairs_bt<0, false, true, true>(P, bt, num_sms, st, grid)
-                         : launch_pairs_bt<0, false, true, false>(P, bt, num_sms, st, grid);
-  return logb ? launch_pairs_bt<0, false, false, true>(P, bt, num_sms, st, grid)
-              : launch_pairs_bt<0, false, false, false>(P, bt, num_sms, st, grid);
+  if (has_z) return logb ? launch_pairs_bt<0, false, true, true>(P, bt, variant, num_sms, st, grid)
+                         : launch_pairs_bt<0, false, true, false>(P, bt, variant, num_sms, st, grid);
+  return logb ? launch_pairs_bt<0, false, false, true>(P, bt, variant, num_sms, st, grid)
+              : launch_pairs_bt<0, false, false, false>(P, bt, variant, num_sms, st, grid);
 }
 
 static inline unsigned gdim(long long n, int b) {

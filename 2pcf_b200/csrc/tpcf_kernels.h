@@ -9,8 +9,10 @@
 namespace tpcf {
 
 size_t pair_smem_bytes(int nb, int qa, int bt);
-cudaError_t launch_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int num_sms,
-                         cudaStream_t st, int* grid);
+// bt = lenses per group; `variant` picks the thread shape of the main
+// configuration (0: bt threads x 1 lens; others: see pairs.cu).
+cudaError_t launch_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int variant,
+                         int num_sms, cudaStream_t st, int* grid);
 
 cudaError_t launch_bbox_init(int* box_ord, unsigned long long* count, int* prange, int n, cudaStream_t st);
 // box_ord holds 8 order-preserving ints per catalogue: minx, miny, maxx, maxy,

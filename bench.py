@@ -55,7 +55,7 @@ def load_peaks():
 class ClockSampler:
     """nvidia-smi clock/throttle samples every 200 ms while running."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -83,12 +83,23 @@ class ClockSampler:
                 out = ""
             self.lines = [l for l in out.splitlines() if l.strip()]
 
+    def window(self, t0, t1):
+        """Restrict the summary to samples taken between wall times t0 and t1."""
+        self.t0, self.t1 = t0, t1
+
     def summary(self):
+        import datetime
         sm, mx, reasons = [], None, set()
         for l in getattr(self, "lines", []):
             p = [x.strip() for x in l.split(",")]
             if len(p) < 9:
                 continue
+            try:
+                ts = datetime.datetime.strptime(p[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                if hasattr(self, "t0") and not (self.t0 - 0.3 <= ts <= self.t1 + 0.3):
+                    continue
+            except ValueError:
+                pass
             try:
                 sm.append(float(p[1]))
                 mx = float(p[2])
@@ -185,6 +196,9 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="object-count scale of the workload")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--region", type=float, default=0.0,
+                    help="profiling: keep only objects with x, y < REGION arcmin (density unchanged)")
+    ap.add_argument("--task", type=int, default=-1, help="profiling: run only this task of the 25")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -203,6 +217,13 @@ def main():
     tpcf = importlib.import_module("2pcf_b200")
 
     w = workload(args.scale)
+    if args.region > 0:
+        for cat in w["lens_bins"] + w["shape_bins"]:
+            keep = (cat["x"] < args.region) & (cat["y"] < args.region)
+            for k in list(cat):
+                cat[k] = np.ascontiguousarray(cat[k][keep])
+    if args.task >= 0:
+        w["tasks"] = [w["tasks"][args.task]]
     bins = tpcf.create_bins(*w["bins"])
     n_patch = w["n_patch"]
     # lens patches: fixed-grid blocks of the field (one label per lens)
@@ -267,10 +288,12 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return t.item(), pairs, pair_ms / n, ctx.kernel_launches - l0
 
-    for _ in range(args.warmup):
-        step(Ld, Sd, Pd)
-    with ClockSampler(local) as cs:
+    with ClockSampler(local) as cs:  # started before the warm-up: its start-up stays outside the timing
+        for _ in range(args.warmup):
+            step(Ld, Sd, Pd)
+        t0 = time.time()
         ms, pairs, pair_ms, launches = timed(Ld, Sd, Pd, args.steps)
+        cs.window(t0, time.time())
     clocks = cs.summary()
     value = pairs / (ms * 1e-3) / 1e9
 
@@ -298,7 +321,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f32", "accumulate": "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD_DESC, "scale": args.scale, "global_batch": int(pairs),
+        "config": {"workload": WORKLOAD_DESC, "scale": args.scale, "region": args.region, "task": args.task,
+                   "global_batch": int(pairs),
                    "parallelism": f"work items sharded over {world} rank(s)" if world > 1 else "single GPU",
                    "l2": "inputs (280 MB of catalogues) larger than L2 (126 MB); no flush",
                    "step": "grid build + 25-task pair kernel + per-patch sums (tpcf_batch_shear_scalar)"},

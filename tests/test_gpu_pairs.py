@@ -141,7 +141,8 @@ def test_marks_and_lens_sums(tpcf, oracle, ctx):
     np.testing.assert_array_equal(got[:, 5], lens[:, 5])
     scale = np.abs(lens).sum(axis=2, keepdims=True) + 1e-300
     assert np.all(np.abs(got[:, :5] - lens[:, :5]) <= 1e-6 * scale[:, :5])
-    np.testing.assert_allclose(res.xi_E_marks[idx], lens[:, 1], rtol=2e-6, atol=1e-6 * scale[:, 1])
+    # marks are FP32 (as in the reference): within FP32 rounding of the FP64 sums
+    assert np.all(np.abs(res.xi_E_marks[idx] - lens[:, 1]) <= 2e-6 * scale[:, 1] + 1e-7 * np.abs(lens[:, 1]))
     np.testing.assert_allclose(res.w_marks[idx], lens[:, 3], rtol=2e-6)
     np.testing.assert_allclose(res.marks_weight[idx], lens[:, 3].sum(1), rtol=2e-6)
     assert np.all(res.xi_E_marks[::97] == 0) and np.all(res.marks_weight[::97] == 0)
