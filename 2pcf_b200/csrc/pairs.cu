@@ -401,14 +401,25 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
         if (!mbar_wait_bounded(&mbar[bb], (phase >> bb) & 1u)) timed_out = true;
         phase ^= (1u << bb);
         if (act[0] && !timed_out) {
-          const SrcRec* S = tiles + bb * kTile;
+          const SrcRec* __restrict__ S = tiles + bb * kTile;
           if (LPT == 1 || !act[LPT - 1]) {
-#pragma unroll 4
-            for (int j = 0; j < n; ++j) {
-              const float4 a = S[j].a;
-              const float4 b = S[j].b;
-              do_pair<MODE, HAS_M, HAS_Z, LOGB, NC, QA, RED>(lx[0], ly[0], lz[0], a, b, hist + tid, C);
+            float* __restrict__ hc = hist + tid;
+            int j = 0;
+            // four sources per step, loaded before any histogram store so the
+            // loads need not wait behind the previous read-modify-writes
+            for (; j + 4 <= n; j += 4) {
+              float4 a[4], b[4];
+#pragma unroll
+              for (int u = 0; u < 4; ++u) {
+                a[u] = S[j + u].a;
+                b[u] = S[j + u].b;
+              }
+#pragma unroll
+              for (int u = 0; u < 4; ++u)
+                do_pair<MODE, HAS_M, HAS_Z, LOGB, NC, QA, RED>(lx[0], ly[0], lz[0], a[u], b[u], hc, C);
             }
+            for (; j < n; ++j)
+              do_pair<MODE, HAS_M, HAS_Z, LOGB, NC, QA, RED>(lx[0], ly[0], lz[0], S[j].a, S[j].b, hc, C);
           } else {
 #pragma unroll 2
             for (int j = 0; j < n; ++j) {

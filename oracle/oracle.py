@@ -72,6 +72,8 @@ def lib():
                                           _f64p, _f64p, _f64p, _f64p]
         L.orc_covariance.argtypes = [C.c_int, C.c_int, _f64p, _f64p]
         L.orc_last_timing.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+        L.orc_philox4x32.argtypes = [_u32p, _u32p, _u32p]
         _lib = L
     return _lib
 
@@ -261,6 +263,13 @@ def qsort_arg_f32(a, reverse=False):
 
 
 # --------------------------------------------------------------- bootstrap --
+def philox4x32(ctr, key):
+    """One Philox4x32-10 block (Salmon et al., SC'11)."""
+    out = np.zeros(4, np.uint32)
+    lib().orc_philox4x32(np.ascontiguousarray(ctr, np.uint32), np.ascontiguousarray(key, np.uint32), out)
+    return out
+
+
 def bootstrap_multiplicity(seed, n_boot, n_patch, n_draw):
     mult = np.zeros((n_boot, n_patch), np.int32)
     lib().orc_bootstrap_multiplicity(seed, n_boot, n_patch, n_draw, mult)

@@ -940,6 +940,13 @@ int orc_kmeans_det(long n, const float* x, const float* y, const float* w, int k
 
 int orc_fixed_scale(long n, double vmax) { return det::fixed_scale(n, vmax); }
 
+// Raw Philox4x32-10 block, for known-answer tests.
+void orc_philox4x32(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+  uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+  det::philox4x32(c, key[0], key[1]);
+  for (int i = 0; i < 4; ++i) out[i] = c[i];
+}
+
 // Multiplicity matrix [n_boot][n_patch] from n_draw Philox draws per sample.
 int orc_bootstrap_multiplicity(uint64_t seed, int n_boot, int n_patch, int n_draw, int* mult) {
   std::fill(mult, mult + (size_t)n_boot * n_patch, 0);
