@@ -307,14 +307,16 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
       unsigned* k1 = (unsigned*)ws_alloc(c, sizeof(unsigned) * s.n);
       int* i0 = (int*)ws_alloc(c, sizeof(int) * s.n);
       int* i1 = (int*)ws_alloc(c, sizeof(int) * s.n);
-      counted(c, launch_src_keys(s.x, s.y, s.z, s.n, x0, y0, g.inv_cell, ncx, ncy, k0, i0, st), "src keys");
-      int end_bit = 1;
-      while (end_bit < 32 && (1ull << end_bit) <= (unsigned long long)ncells) ++end_bit;
+      int cell_bits = 1;
+      while (cell_bits < 32 && (1ull << cell_bits) <= (unsigned long long)ncells) ++cell_bits;
+      const int mb = std::min(16, (32 - cell_bits) & ~1);  // within-cell Morton bits
+      counted(c, launch_src_keys(s.x, s.y, s.z, s.n, x0, y0, g.inv_cell, ncx, ncy, mb, k0, i0, st), "src keys");
+      const int end_bit = cell_bits + mb;
       size_t tb = 0;
       check(sort_pairs_u32(nullptr, tb, k0, k1, i0, i1, (int)s.n, end_bit, st), "sort size");
       void* tmp = ws_alloc(c, tb);
       check(sort_pairs_u32(tmp, tb, k0, k1, i0, i1, (int)s.n, end_bit, st), "sort sources");
-      counted(c, launch_cell_start(k1, s.n, ncells, cs, st), "cell start");
+      counted(c, launch_cell_start(k1, s.n, ncells, mb, cs, st), "cell start");
       counted(c, launch_src_gather(i1, n_valid, mode, s.x, s.y, s.z, s.f1, s.f2, s.w, s.m, rec, st), "src gather");
     } else {
       check(cudaMemsetAsync(cs, 0, sizeof(int) * (ncells + 1), st), "memset cells");

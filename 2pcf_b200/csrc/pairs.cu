@@ -73,7 +73,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 // ------------------------------------------------------- shared-memory map --
 struct PairSmem {
-  size_t tiles, hist, bsum, e2s, fvw, fw, e2f, span0, span1, tpref, mbar, misc, total;
+  size_t tiles, hist, bsum, e2s, fvw, fw, e2f, span0, span1, tpref, subbox, mbar, misc, total;
 };
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // bt here is the number of histogram columns (threads x lenses per thread).
@@ -93,6 +93,7 @@ __host__ __device__ inline PairSmem pair_smem_layout(int nb, int qa, int bt) {
   s.span1 = o; o += kMaxRows * sizeof(int);
   s.tpref = o; o += (kMaxRows + 1) * sizeof(int);
   o = align_up(o, 16);
+  s.subbox = o; o += (kTile / 32) * sizeof(float4);
   s.mbar = o;  o += 2 * sizeof(uint64_t);
   s.misc = o;  o += 16;
   s.total = align_up(o, 128);
@@ -142,6 +143,7 @@ __device__ __noinline__ int slow_bin(float lx, float ly, float sx, float sy, con
 
 struct BinCtx {
   float A, B, eps, one_m_eps;
+  float eps_rel;     // relative guard on d2 around one FP32 edge (register paths)
   float lo_g, hi_g;  // generic: fast reject bounds e2f[0]*(1-eps), e2f[nb]*(1+eps)
   int nb;
   const double* e2s;
@@ -170,17 +172,9 @@ __device__ __forceinline__ int pair_bin(float d2, float lx, float ly, float sx, 
   }
 }
 
-// Add v to a histogram cell owned by this thread: a plain read-modify-write,
-// or a shared-memory reduction (no load-use dependency on the issuing thread).
-template <bool RED>
-__device__ __forceinline__ void hadd(float* p, float v) {
-  if (RED) atomicAdd(p, v);
-  else *p += v;
-}
-
 // One pair: lens (lx, ly, lz) against source record (a, b).  hcol points at
 // this lens's histogram column; row (bin*QA + q) is at hcol[(bin*QA+q)*NC].
-template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int NC, int QA, bool RED>
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int NC, int QA>
 __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const float4 a, const float4 b,
                                         float* __restrict__ hcol, const BinCtx& C) {
   if (HAS_Z) {
@@ -212,38 +206,196 @@ __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const floa
     // a.z = -e1*w, a.w = -e2*w:  g_t term = a.z*c2 + a.w*s2,  g_x term = a.w*c2 - a.z*s2
     const float gt = fmaf(a.z, c2, a.w * s2);
     const float gx = fmaf(a.w, c2, -(a.z * s2));
-    hadd<RED>(&h[QGT * NC], gt);
-    hadd<RED>(&h[QGX * NC], gx);
+    h[QGT * NC] += gt;
+    h[QGX * NC] += gx;
   } else {
-    hadd<RED>(&h[QGT * NC], a.z);
-    hadd<RED>(&h[QGX * NC], a.w);
+    h[QGT * NC] += a.z;
+    h[QGX * NC] += a.w;
   }
-  hadd<RED>(&h[QW * NC], b.x);
-  hadd<RED>(&h[QDW * NC], d * b.x);
-  hadd<RED>(&h[QN * NC], 1.0f);
-  if (MODE == 0 && HAS_M) hadd<RED>(&h[QK * NC], b.y);
+  h[QW * NC] += b.x;
+  h[QDW * NC] = fmaf(d, b.x, h[QDW * NC]);
+  h[QN * NC] += 1.0f;
+  if (MODE == 0 && HAS_M) h[QK * NC] += b.y;
+}
+
+// ---------------------------------------------------- sub-chunk fast paths --
+// A tile is cut into sub-chunks of 32 consecutive sources (spatially compact:
+// sources are sorted by cell, then Morton order inside the cell).  For each
+// lens and sub-chunk the bin range of the chunk's bounding box is bounded
+// conservatively (guard band eps on both ends):
+//   0  no pair of the chunk is in range        -> nothing to do
+//   1  every pair is in one bin `blo`           -> register sums, no binning
+//   2  pairs fall in bins blo and blo+1 only    -> register sums split at the
+//                                                  one edge, FP64 re-binning
+//                                                  inside its guard band
+//   3  anything else (or a z cut)               -> per-pair binning (do_pair)
+// The path is chosen per warp (the largest class of its lanes), so lanes never
+// diverge inside a source loop.  Every pair still lands in its canonical bin:
+// in classes 1 and 2 the box bounds prove which bins are possible.
+
+// Largest i in [0, nb] with e2f[i] <= v, or -1 (generic spacings).
+__device__ __forceinline__ int edge_index_f32(float v, const float* e2f, int nb) {
+  if (v < e2f[0]) return -1;
+  int lo = 0, hi = nb + 1;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (v >= e2f[mid]) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+template <bool LOGB, bool HAS_Z>
+__device__ __forceinline__ int classify(float lx, float ly, const float4 box, const BinCtx& C, int& blo) {
+  const float dxl = fmaxf(fmaxf(box.x - lx, lx - box.z), 0.f);
+  const float dyl = fmaxf(fmaxf(box.y - ly, ly - box.w), 0.f);
+  const float dxh = fmaxf(lx - box.x, box.z - lx);
+  const float dyh = fmaxf(ly - box.y, box.w - ly);
+  const float dmin2 = fmaf(dyl, dyl, dxl * dxl);
+  const float dmax2 = fmaf(dyh, dyh, dxh * dxh);
+  int b0, b1;
+  if (LOGB) {
+    b0 = __float2int_rd(fmaf(__log2f(dmin2), C.A, C.B) - C.eps);
+    b1 = __float2int_rd(fmaf(__log2f(dmax2), C.A, C.B) + C.eps);
+  } else {
+    b0 = edge_index_f32(dmin2 * (1.f - C.eps), C.e2f, C.nb);
+    b1 = edge_index_f32(dmax2 * (1.f + C.eps), C.e2f, C.nb);
+  }
+  if (b1 < 0 || b0 >= C.nb) return 0;
+  blo = b0;
+  if (HAS_Z) return 3;
+  if (b0 == b1) return 1;
+  if (b1 == b0 + 1) return 2;
+  return 3;
+}
+
+// Per-pair quantities shared by the register paths: g_t, g_x terms (shear) or
+// kE*w, kB*w (scalar-scalar), and d.
+template <int MODE, bool LOGB>
+__device__ __forceinline__ void pair_terms(float lx, float ly, const float4 a, float& d2, float& d, float& t1,
+                                           float& t2) {
+  const float dx = lx - a.x;
+  const float dy = ly - a.y;
+  const float dx2 = dx * dx;
+  d2 = fmaf(dy, dy, dx2);
+  float r;
+  if (LOGB) {
+    const float rs = rsqrtf(d2);
+    d = d2 * rs;
+    r = rs * rs;
+  } else {
+    d = sqrtf(d2);
+    r = __frcp_rn(d2);
+  }
+  if (MODE == 0) {
+    const float c2 = fmaf(-dy, dy, dx2) * r;
+    const float qq = dx * dy;
+    const float s2 = (qq + qq) * r;
+    t1 = fmaf(a.z, c2, a.w * s2);
+    t2 = fmaf(a.w, c2, -(a.z * s2));
+  } else {
+    t1 = a.z;
+    t2 = a.w;
+  }
+}
+
+template <int QA, int NC>
+__device__ __forceinline__ void hist_add(float* hcol, int bin, const float* v) {
+  float* h = hcol + bin * (QA * NC);
+#pragma unroll
+  for (int q = 0; q < QA; ++q) h[q * NC] += v[q];
+}
+
+// Class 1: every pair of the chunk is in bin `blo`.
+template <int MODE, bool HAS_M, bool LOGB, int NC, int QA>
+__device__ __forceinline__ void chunk_single(const SrcRec* __restrict__ S, int cnt, float lx, float ly, int cls,
+                                             int blo, float* __restrict__ hcol) {
+  float acc[QA];
+#pragma unroll
+  for (int q = 0; q < QA; ++q) acc[q] = 0.f;
+#pragma unroll 4
+  for (int j = 0; j < cnt; ++j) {
+    const float4 a = S[j].a;
+    const float4 b = S[j].b;
+    float d2, d, t1, t2;
+    pair_terms<MODE, LOGB>(lx, ly, a, d2, d, t1, t2);
+    acc[QGT] += t1;
+    acc[QGX] += t2;
+    acc[QW] += b.x;
+    acc[QDW] = fmaf(d, b.x, acc[QDW]);
+    if (MODE == 0 && HAS_M) acc[QK] += b.y;
+  }
+  acc[QN] = (float)cnt;
+  if (cls == 1) hist_add<QA, NC>(hcol, blo, acc);
+}
+
+// Class 2: pairs in bins blo and blo+1 (either may be out of range, then it is
+// dropped); the edge between them is e2f[blo+1].
+template <int MODE, bool HAS_M, bool LOGB, int NC, int QA>
+__device__ __forceinline__ void chunk_dual(const SrcRec* __restrict__ S, int cnt, float lx, float ly, int cls,
+                                           int blo, float* __restrict__ hcol, const BinCtx& C) {
+  float tot[QA], hi[QA];
+#pragma unroll
+  for (int q = 0; q < QA; ++q) tot[q] = hi[q] = 0.f;
+  // lanes of class 1 (or 0) keep an edge no pair reaches
+  const float E = (cls == 2) ? C.e2f[blo + 1] : 3.0e38f;
+  const float gE = (cls == 2) ? E * C.eps_rel : 0.f;
+#pragma unroll 2
+  for (int j = 0; j < cnt; ++j) {
+    const float4 a = S[j].a;
+    const float4 b = S[j].b;
+    float d2, d, t1, t2;
+    pair_terms<MODE, LOGB>(lx, ly, a, d2, d, t1, t2);
+    bool up = d2 >= E;
+    if (fabsf(d2 - E) <= gE) {
+      // canonical bin is blo or blo+1, or -1 on a side outside [x_min, x_max]
+      const int cb = slow_bin(lx, ly, a.x, a.y, C.e2s, C.nb);
+      up = (cb == blo + 1) || (cb < 0 && blo + 1 == C.nb);
+    }
+    const float dw = d * b.x;
+    tot[QGT] += t1;
+    tot[QGX] += t2;
+    tot[QW] += b.x;
+    tot[QDW] += dw;
+    if (MODE == 0 && HAS_M) tot[QK] += b.y;
+    if (up) {
+      hi[QGT] += t1;
+      hi[QGX] += t2;
+      hi[QW] += b.x;
+      hi[QDW] += dw;
+      hi[QN] += 1.f;
+      if (MODE == 0 && HAS_M) hi[QK] += b.y;
+    }
+  }
+  tot[QN] = (float)cnt;
+  if (cls == 0) return;
+  float lo[QA];
+#pragma unroll
+  for (int q = 0; q < QA; ++q) lo[q] = tot[q] - hi[q];
+  if (cls == 1) {
+    hist_add<QA, NC>(hcol, blo, tot);
+    return;
+  }
+  if (blo >= 0) hist_add<QA, NC>(hcol, blo, lo);
+  if (blo + 1 < C.nb) hist_add<QA, NC>(hcol, blo + 1, hi);
 }
 
 // Fold the FP32 histogram into FP64 (block sums and, optionally, per-lens
 // sums), then clear this thread's column.  Called by all threads.
-// Histogram columns: NC = LPT*BT; thread t owns columns t, t+BT, ... (one per
-// lens it holds).  lens_acc_col[k] is the per-lens FP64 column of lens k or null.
-template <int QA, int BT, int LPT>
+// Fold the FP32 histogram into FP64: the block sums (times the lens factors
+// val*w or w) and, when lens_col is set, this thread's per-lens FP64 column.
+// Then clear this thread's column.  Called by all threads.
+template <int QA, int BT>
 __device__ __forceinline__ void flush_hist(float* hist, double* bsum, const double* fvw, const double* fw,
-                                           int nb, double* const* lens_acc_col, size_t lens_stride, bool first) {
-  constexpr int NC = BT * LPT;
+                                           int nb, double* lens_col, size_t lens_stride, bool first) {
   const int tid = threadIdx.x;
   __syncthreads();
-#pragma unroll
-  for (int k = 0; k < LPT; ++k) {
-    double* col = lens_acc_col[k];
-    if (!col) continue;
-    const float* hcol = hist + tid + k * BT;
+  float* hcol = hist + tid;
+  if (lens_col) {
     for (int q = 0; q < kQ; ++q) {
       const int qa = (q == QK && QA == 5) ? QW : q;
       for (int b = 0; b < nb; ++b) {
-        const double v = (double)hcol[(b * QA + qa) * NC];
-        double* p = col + (size_t)(q * nb + b) * lens_stride;
+        const double v = (double)hcol[(b * QA + qa) * BT];
+        double* p = lens_col + (size_t)(q * nb + b) * lens_stride;
         *p = first ? v : *p + v;
       }
     }
@@ -251,35 +403,34 @@ __device__ __forceinline__ void flush_hist(float* hist, double* bsum, const doub
   for (int e = tid; e < kQ * nb; e += BT) {
     const int q = e / nb, b = e - q * nb;
     if (q == QK && QA == 5) continue;  // K == w: copied from the w row at item end
-    const float* row = hist + (b * QA + q) * NC;
+    const float* row = hist + (b * QA + q) * BT;
     const double* f = (q == QGT || q == QGX) ? fvw : fw;
     double s = 0.0;
     if (q == QN) {
-      for (int l = 0; l < NC; ++l) s += (double)row[(l + tid) & (NC - 1)];
+      for (int l = 0; l < BT; ++l) s += (double)row[(l + tid) & (BT - 1)];
     } else {
-      for (int l = 0; l < NC; ++l) {
-        const int c = (l + tid) & (NC - 1);
+      for (int l = 0; l < BT; ++l) {
+        const int c = (l + tid) & (BT - 1);
         s = fma((double)row[c], f[c], s);
       }
     }
     bsum[e] += s;
   }
   __syncthreads();
-#pragma unroll
-  for (int k = 0; k < LPT; ++k) {
-    float* hcol = hist + tid + k * BT;
-    for (int e = 0; e < nb * QA; ++e) hcol[e * NC] = 0.f;
-  }
+  for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
 }
 
-template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int LPT, bool RED>
+// PATH 0: sub-chunk classification with the register paths (default);
+// PATH 1: per-pair binning for every pair (kept for A/B measurement).
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int PATH>
 __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
   constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
-  constexpr int NC = BT * LPT;  // histogram columns = lenses per group
+  constexpr int NW = BT / 32;
   const int nb = P.nb;
   const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
   extern __shared__ __align__(128) unsigned char smem[];
-  const PairSmem L = pair_smem_layout(nb, QA, NC);
+  const PairSmem L = pair_smem_layout(nb, QA, BT);
   SrcRec* tiles = reinterpret_cast<SrcRec*>(smem + L.tiles);
   float* hist = reinterpret_cast<float*>(smem + L.hist);
   double* bsum = reinterpret_cast<double*>(smem + L.bsum);
@@ -290,6 +441,7 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
   int* span0 = reinterpret_cast<int*>(smem + L.span0);
   int* span1 = reinterpret_cast<int*>(smem + L.span1);
   int* tpref = reinterpret_cast<int*>(smem + L.tpref);
+  float4* subbox = reinterpret_cast<float4*>(smem + L.subbox);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + L.mbar);
   int* sh_item = reinterpret_cast<int*>(smem + L.misc);
 
@@ -306,15 +458,15 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
   BinCtx C;
   C.A = P.binA; C.B = P.binB; C.eps = P.eps; C.one_m_eps = 1.f - P.eps;
   C.nb = nb; C.e2s = e2s; C.e2f = e2f;
+  C.eps_rel = 4e-6f;
   C.lo_g = e2f[0] * (1.f - P.eps);
   C.hi_g = e2f[nb] * (1.f + P.eps);
 
   uint32_t phase = 0u;   // bit k: parity awaited next on buffer k
   uint32_t tcount = 0u;  // tiles processed by this block so far
   bool timed_out = false;
-#pragma unroll
-  for (int k = 0; k < LPT; ++k)
-    for (int e = 0; e < nb * QA; ++e) hist[tid + k * BT + e * NC] = 0.f;
+  float* __restrict__ hcol = hist + tid;
+  for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
 
   for (;;) {
     if (tid == 0) *sh_item = atomicAdd(P.queue_head, 1);
@@ -328,27 +480,20 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
     const int g = it.y;
     const int gs = LD.group_start[g];
     const int nl = LD.group_start[g + 1] - gs;
-    float lx[LPT], ly[LPT], lz[LPT];
-    bool act[LPT];
-    double* lens_col[LPT];
-#pragma unroll
-    for (int k = 0; k < LPT; ++k) {
-      const int li = tid + k * BT;
-      act[k] = li < nl;
-      lx[k] = ly[k] = lz[k] = 0.f;
-      double vw = 0.0, w = 0.0;
-      lens_col[k] = nullptr;
-      if (act[k]) {
-        const float4 r = LD.rec[gs + li];
-        lx[k] = r.x; ly[k] = r.y;
-        vw = (double)r.z * (double)r.w;
-        w = (double)r.w;
-        if (HAS_Z) lz[k] = LD.z[gs + li];
-        if (P.lens_acc && T.lens_acc_off >= 0) lens_col[k] = P.lens_acc + T.lens_acc_off + gs + li;
-      }
-      fvw[li] = vw;
-      fw[li] = w;
+    const bool act = tid < nl;
+    float lx = 0.f, ly = 0.f, lz = 0.f;
+    double vw = 0.0, w = 0.0;
+    double* lens_col = nullptr;
+    if (act) {
+      const float4 r = LD.rec[gs + tid];
+      lx = r.x; ly = r.y;
+      vw = (double)r.z * (double)r.w;
+      w = (double)r.w;
+      if (HAS_Z) lz = LD.z[gs + tid];
+      if (P.lens_acc && T.lens_acc_off >= 0) lens_col = P.lens_acc + T.lens_acc_off + gs + tid;
     }
+    fvw[tid] = vw;
+    fw[tid] = w;
     const size_t lens_stride = (size_t)LD.n_valid;
     for (int e = tid; e < kQ * nb; e += BT) bsum[e] = 0.0;
     bool first_flush = true;
@@ -398,15 +543,63 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
         const int s = span0[rc] + (k - tpref[rc]) * kTile;
         const int n = min(kTile, span1[rc] - s);
         const int bb = (tcount + k) & 1u;
-        if (!mbar_wait_bounded(&mbar[bb], (phase >> bb) & 1u)) timed_out = true;
+        const bool ok = mbar_wait_bounded(&mbar[bb], (phase >> bb) & 1u);
         phase ^= (1u << bb);
-        if (act[0] && !timed_out) {
-          const SrcRec* __restrict__ S = tiles + bb * kTile;
-          if (LPT == 1 || !act[LPT - 1]) {
-            float* __restrict__ hc = hist + tid;
+        const SrcRec* __restrict__ S = tiles + bb * kTile;
+        const int nsub = (n + 31) >> 5;
+        if (PATH == 0 && ok) {
+          // bounding box of each 32-source sub-chunk (one warp per sub-chunk)
+          for (int sc = warp; sc < nsub; sc += NW) {
+            const int j = sc * 32 + lane;
+            float mnx = INFINITY, mny = INFINITY, mxx = -INFINITY, mxy = -INFINITY;
+            if (j < n) {
+              const float4 a = S[j].a;
+              mnx = mxx = a.x;
+              mny = mxy = a.y;
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+              mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+              mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+              mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+              mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+            }
+            if (lane == 0) subbox[sc] = make_float4(mnx, mny, mxx, mxy);
+          }
+        }
+        if (__syncthreads_or(!ok)) timed_out = true;
+        if (!timed_out) {
+          if (PATH == 0) {
+            for (int sc = 0; sc < nsub; ++sc) {
+              const int base = sc * 32;
+              const int cnt = min(32, n - base);
+              int blo = 0;
+              const int cls = act ? classify<LOGB, HAS_Z>(lx, ly, subbox[sc], C, blo) : 0;
+              const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)cls);
+              if (m == 0) continue;
+              const SrcRec* __restrict__ Sc = S + base;
+              if (m == 1) {
+                chunk_single<MODE, HAS_M, LOGB, BT, QA>(Sc, cnt, lx, ly, cls, blo, hcol);
+              } else if (m == 2) {
+                chunk_dual<MODE, HAS_M, LOGB, BT, QA>(Sc, cnt, lx, ly, cls, blo, hcol, C);
+              } else if (act) {
+                int j = 0;
+                for (; j + 4 <= cnt; j += 4) {
+                  float4 a[4], b[4];
+#pragma unroll
+                  for (int u = 0; u < 4; ++u) {
+                    a[u] = Sc[j + u].a;
+                    b[u] = Sc[j + u].b;
+                  }
+#pragma unroll
+                  for (int u = 0; u < 4; ++u)
+                    do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, a[u], b[u], hcol, C);
+                }
+                for (; j < cnt; ++j) do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, Sc[j].a, Sc[j].b, hcol, C);
+              }
+            }
+          } else if (act) {
             int j = 0;
-            // four sources per step, loaded before any histogram store so the
-            // loads need not wait behind the previous read-modify-writes
             for (; j + 4 <= n; j += 4) {
               float4 a[4], b[4];
 #pragma unroll
@@ -415,26 +608,14 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
                 b[u] = S[j + u].b;
               }
 #pragma unroll
-              for (int u = 0; u < 4; ++u)
-                do_pair<MODE, HAS_M, HAS_Z, LOGB, NC, QA, RED>(lx[0], ly[0], lz[0], a[u], b[u], hc, C);
+              for (int u = 0; u < 4; ++u) do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, a[u], b[u], hcol, C);
             }
-            for (; j < n; ++j)
-              do_pair<MODE, HAS_M, HAS_Z, LOGB, NC, QA, RED>(lx[0], ly[0], lz[0], S[j].a, S[j].b, hc, C);
-          } else {
-#pragma unroll 2
-            for (int j = 0; j < n; ++j) {
-              const float4 a = S[j].a;
-              const float4 b = S[j].b;
-#pragma unroll
-              for (int kk = 0; kk < LPT; ++kk)
-                do_pair<MODE, HAS_M, HAS_Z, LOGB, NC, QA, RED>(lx[kk], ly[kk], lz[kk], a, b,
-                                                               hist + tid + kk * BT, C);
-            }
+            for (; j < n; ++j) do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, S[j].a, S[j].b, hcol, C);
           }
         }
         since_flush += n;
         if (since_flush >= 4 * kTile) {
-          flush_hist<QA, BT, LPT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
+          flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
           first_flush = false;
           since_flush = 0;
         }
@@ -442,7 +623,7 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
       }
       tcount += (uint32_t)ntiles;
     }
-    flush_hist<QA, BT, LPT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
+    flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
     __syncthreads();
     double* out = P.item_sums + (size_t)(T.item_base + g) * kQ * nb;
     for (int e = tid; e < kQ * nb; e += BT) {
@@ -451,7 +632,7 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
     }
     __syncthreads();
   }
-  if (timed_out) atomicOr(P.err, kErrTimeout);
+  if (timed_out && tid == 0) atomicOr(P.err, kErrTimeout);
 }
 
 // ------------------------------------------------------------ prep kernels --
@@ -546,34 +727,49 @@ __global__ void k_bbox_finish(const int* box_ord, float* box, int n) {
   if (i < n) box[i] = ord2f(box_ord[i]);
 }
 
-// Cell key of each source (invalid -> ncells, sorts last).
+__device__ __forceinline__ unsigned spread16(unsigned v);
+
+// Sort key of each source: (cell << mb) | Morton code of its position inside the
+// cell on a 2^(mb/2) grid, so that consecutive sources of one cell are spatially
+// compact (32-source sub-chunks get small bounding boxes).  Invalid sources get
+// ncells << mb and sort last.
 __global__ void k_src_keys(const float* __restrict__ x, const float* __restrict__ y,
                            const float* __restrict__ z, long long n, float x0, float y0, float inv_cell,
-                           int ncx, int ncy, unsigned* keys, int* idx) {
+                           int ncx, int ncy, int mb, unsigned* keys, int* idx) {
   const unsigned ncells = (unsigned)ncx * (unsigned)ncy;
+  const int half = mb >> 1;
+  const float q = (float)(1u << half);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const float xi = x[i], yi = y[i];
     bool v = isfinite(xi) && isfinite(yi);
     if (z && z[i] < 0.f) v = false;
-    unsigned key = ncells;
+    unsigned key = ncells << mb;
     if (v) {
-      const int cx = clamp_floor((xi - x0) * inv_cell, 0, ncx - 1);
-      const int cy = clamp_floor((yi - y0) * inv_cell, 0, ncy - 1);
-      key = (unsigned)cy * (unsigned)ncx + (unsigned)cx;
+      const float fx = (xi - x0) * inv_cell, fy = (yi - y0) * inv_cell;
+      const int cx = clamp_floor(fx, 0, ncx - 1);
+      const int cy = clamp_floor(fy, 0, ncy - 1);
+      key = ((unsigned)cy * (unsigned)ncx + (unsigned)cx) << mb;
+      if (half > 0) {
+        const unsigned qx = (unsigned)clamp_floor((fx - (float)cx) * q, 0, (1 << half) - 1);
+        const unsigned qy = (unsigned)clamp_floor((fy - (float)cy) * q, 0, (1 << half) - 1);
+        key |= spread16(qx) | (spread16(qy) << 1);
+      }
     }
     keys[i] = key;
     idx[i] = (int)i;
   }
 }
 
-// cell_start[c] = first sorted position with key >= c, for c in [0, ncells].
-__global__ void k_cell_start(const unsigned* __restrict__ keys, long long n, unsigned ncells, int* cell_start) {
+// cell_start[c] = first sorted position with key >= c << mb, for c in [0, ncells].
+__global__ void k_cell_start(const unsigned* __restrict__ keys, long long n, unsigned ncells, int mb,
+                             int* cell_start) {
   const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c > ncells) return;
+  const unsigned t = c << mb;
   long long lo = 0, hi = n;
   while (lo < hi) {
     const long long mid = (lo + hi) >> 1;
-    if (keys[mid] < c) lo = mid + 1; else hi = mid;
+    if (keys[mid] < t) lo = mid + 1; else hi = mid;
   }
   cell_start[c] = (int)lo;
 }
@@ -781,11 +977,11 @@ __global__ void k_lens_outputs(const double* __restrict__ acc, const float4* __r
 }
 
 // --------------------------------------------------------- host launchers --
-template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int LPT, bool RED>
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int PATH>
 static cudaError_t launch_pairs_t(const PairParams& P, int num_sms, cudaStream_t st, int* grid_out) {
   constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
-  const size_t smem = pair_smem_layout(P.nb, QA, BT * LPT).total;
-  auto kern = k_pairs<MODE, HAS_M, HAS_Z, LOGB, BT, LPT, RED>;
+  const size_t smem = pair_smem_layout(P.nb, QA, BT).total;
+  auto kern = k_pairs<MODE, HAS_M, HAS_Z, LOGB, BT, PATH>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -804,18 +1000,12 @@ template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB>
 static cudaError_t launch_pairs_bt(const PairParams& P, int bt, int variant, int num_sms, cudaStream_t st,
                                    int* grid) {
   if (bt == 128) {
-    if (MODE == 0 && !HAS_M && !HAS_Z && LOGB) {  // variants of the main configuration
-      switch (variant) {
-        case 1: return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 1, true>(P, num_sms, st, grid);
-        case 2: return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64, 2, false>(P, num_sms, st, grid);
-        case 3: return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64, 2, true>(P, num_sms, st, grid);
-        default: break;
-      }
-    }
-    return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 1, false>(P, num_sms, st, grid);
+    if (variant == 1 && MODE == 0 && !HAS_M && !HAS_Z && LOGB)  // per-pair path, for A/B measurement
+      return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 1>(P, num_sms, st, grid);
+    return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 0>(P, num_sms, st, grid);
   }
-  if (bt == 64) return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64, 1, false>(P, num_sms, st, grid);
-  return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 32, 1, false>(P, num_sms, st, grid);
+  if (bt == 64) return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64, 0>(P, num_sms, st, grid);
+  return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 32, 0>(P, num_sms, st, grid);
 }
 
 size_t pair_smem_bytes(int nb, int qa, int bt) { return pair_smem_layout(nb, qa, bt).total; }
@@ -860,12 +1050,13 @@ cudaError_t launch_bbox_finish(const int* box_ord, float* box, int n, cudaStream
   return cudaGetLastError();
 }
 cudaError_t launch_src_keys(const float* x, const float* y, const float* z, long long n, float x0, float y0,
-                            float inv_cell, int ncx, int ncy, unsigned* keys, int* idx, cudaStream_t st) {
-  if (n > 0) k_src_keys<<<gdim(n, 256), 256, 0, st>>>(x, y, z, n, x0, y0, inv_cell, ncx, ncy, keys, idx);
+                            float inv_cell, int ncx, int ncy, int mb, unsigned* keys, int* idx, cudaStream_t st) {
+  if (n > 0) k_src_keys<<<gdim(n, 256), 256, 0, st>>>(x, y, z, n, x0, y0, inv_cell, ncx, ncy, mb, keys, idx);
   return cudaGetLastError();
 }
-cudaError_t launch_cell_start(const unsigned* keys, long long n, unsigned ncells, int* cell_start, cudaStream_t st) {
-  k_cell_start<<<(ncells + 1 + 255) / 256, 256, 0, st>>>(keys, n, ncells, cell_start);
+cudaError_t launch_cell_start(const unsigned* keys, long long n, unsigned ncells, int mb, int* cell_start,
+                              cudaStream_t st) {
+  k_cell_start<<<(ncells + 1 + 255) / 256, 256, 0, st>>>(keys, n, ncells, mb, cell_start);
   return cudaGetLastError();
 }
 cudaError_t launch_src_gather(const int* idx, int n_valid, int mode, const float* x, const float* y, const float* z,
