@@ -100,6 +100,8 @@ def lib():
          [C.POINTER(Bins), vp, i32, C.POINTER(Result)])
     _sig(L, "tpcf_batch_shear_scalar", st, [vp, i32, C.POINTER(LensCat), i32, C.POINTER(ShearCat),
                                             i32, vp, vp, C.POINTER(Bins), i32, C.POINTER(Result)])
+    _sig(L, "tpcf_shear_scalar_noalloc", st, [vp] + [vp] * 5 + [i64] + [vp] * 7 + [i64] +
+         [C.POINTER(Bins), C.POINTER(Result)])
     _declare_extra(L)
     if L.tpcf_abi_version() != 1:
         raise ImportError("libtpcf_b200.so ABI version mismatch")

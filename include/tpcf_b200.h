@@ -223,6 +223,28 @@ tpcf_status tpcf_batch_shear_scalar(tpcf_ctx* ctx,
                                     const tpcf_bins* bins, int32_t n_patch,
                                     tpcf_result* outs);
 
+/* No counterpart in the reference.  The pair sum of tpcf_shear_scalar for
+ * callers that cannot allocate device memory: a framework's caching allocator
+ * or a fixed pool owns the GPU's memory (an extra cudaMalloc would fail or
+ * fragment it), or cudaMalloc/cudaFree, which may synchronise the whole device,
+ * is unaffordable in the caller's loop.  Every scratch buffer comes from one
+ * static 64 MiB device array that each GPU loading the library holds until the
+ * process exits; nothing is allocated.  The first call on each device looks up
+ * the array's address (cudaGetSymbolAddress) and must come before any stream
+ * capture.  All calls share the array and it keeps the last call's contents
+ * (what must start at zero is cleared by each call): calls that overlap on the
+ * GPU, from two host threads or two streams, race.  Patches and per-lens
+ * outputs are not available (those fields of `out` must be NULL).  A call that
+ * needs more than the 64 MiB (roughly 600 thousand objects in all) fails with
+ * TPCF_ERR_OVERFLOW before any pair work. */
+tpcf_status tpcf_shear_scalar_noalloc(tpcf_ctx* ctx,
+                                      const float* xA, const float* yA, const float* zA,
+                                      const float* valA, const float* wA, int64_t nA,
+                                      const float* xB, const float* yB, const float* zB,
+                                      const float* e1B, const float* e2B, const float* wB,
+                                      const float* mB, int64_t nB,
+                                      const tpcf_bins* bins, tpcf_result* out);
+
 #ifdef __cplusplus
 }
 #endif
