@@ -29,7 +29,8 @@ _SPACING = {"lin": 0, "log": 1, "ihs": 2, "sqrt": 3}
 __all__ = [
     "Binning", "create_bins", "Context", "ShapeCatalog", "LensCatalog", "KappaMap",
     "LensingSurveyField", "Shear2pcfResults", "shear_2pcf", "kappa_2pcf",
-    "tangential_shear_tpcf", "scalar_kappa_tpcf", "batch_shear_2pcf", "TPCFError",
+    "tangential_shear_tpcf", "scalar_kappa_tpcf", "batch_shear_2pcf", "partition_data",
+    "block_bootstrap", "TPCFError",
 ]
 
 
@@ -235,9 +236,10 @@ class Shear2pcfResults:
     marks_weight: Optional[np.ndarray] = None
     lens_sums: Optional[np.ndarray] = None
     patch_sums: Optional[np.ndarray] = None
+    lens_raw: Optional[np.ndarray] = None
 
 
-def _alloc_result(nb, nA, marks, lens_sums, n_patch):
+def _alloc_result(nb, nA, marks, lens_sums, n_patch, lens_raw=False):
     r = {k: np.zeros(nb) for k in ("sum_dw", "sum_gt", "sum_gx", "sum_w", "sum_K")}
     r["n_pairs"] = np.zeros(nb, np.int64)
     for k in ("theta", "mean_theta", "g_t", "g_x", "weights"):
@@ -250,6 +252,8 @@ def _alloc_result(nb, nA, marks, lens_sums, n_patch):
         r["lens_sums"] = np.zeros((nA, 6, nb))
     if n_patch and n_patch > 0:
         r["patch_sums"] = np.zeros((n_patch, 6, nb))
+    if lens_raw:
+        r["lens_raw"] = np.zeros((nA, 6, nb))
     cres = Result(**{k: (v.ctypes.data if v is not None else None) for k, v in r.items()})
     return r, cres
 
@@ -266,7 +270,7 @@ def _resolve_ctx(ctx):
 def tangential_shear_tpcf(x_A, y_A, z_A, val_A, weight_A, x_B, y_B, z_B, e1_B, e2_B, weight_B, m_B,
                           bins: Binning, spherical_coords=False, num_threads=None,
                           use_kd_tree=True, verbose=False, calculate_marks=True,
-                          patch_A=None, n_patch=0, lens_sums=False, ctx: Context = None):
+                          patch_A=None, n_patch=0, lens_sums=False, lens_raw=False, ctx: Context = None):
     """tangential_shear_tpcf (src/tpcf.f90:190-378) on the GPU.
 
     Returns a Shear2pcfResults: avg_theta is ``mean_theta``; the marks arrays
@@ -282,7 +286,8 @@ def tangential_shear_tpcf(x_A, y_A, z_A, val_A, weight_A, x_B, y_B, z_B, e1_B, e
     P = _Arr(patch_A, np.int32)
     nA, nB = A[0].n, B[0].n
     nb = bins.n_bin
-    r, cres = _alloc_result(nb, nA, calculate_marks, lens_sums, n_patch if patch_A is not None else 0)
+    r, cres = _alloc_result(nb, nA, calculate_marks, lens_sums, n_patch if patch_A is not None else 0,
+                            lens_raw)
     cb = bins.c_struct()
     st = lib().tpcf_shear_scalar(ctx.handle, *[a.ptr for a in A], nA, *[b.ptr for b in B], nB,
                                  C.byref(cb), P.ptr, int(n_patch), C.byref(cres))
@@ -362,3 +367,84 @@ def batch_shear_2pcf(lenses: Sequence[LensCatalog], shapes: Sequence[ShapeCatalo
                                        int(n_patch) if lens_patches is not None else 0, outs)
     _check(st, ctx.handle)
     return [_finish(r, nb) for r in pyouts]
+
+
+# ------------------------------------------------------ patches and errors ---
+def partition_data(x, y, weights, k, iterations=1000, reassignment_tol=0.0, ctx: Context = None):
+    """partition_data (src/kmeans.f90:12-263) for Voronoi blocks on the GPU.
+
+    Returns (labels [n] 0-based, centroids [k][2], iterations run).  Labels are
+    deterministic (fixed-point centroid sums)."""
+    ctx = _resolve_ctx(ctx)
+    X, Y, W = _Arr(x), _Arr(y), _Arr(weights)
+    n = X.n
+    lab = np.zeros(n, np.int32)
+    cen = np.zeros((k, 2), np.float32)
+    it = C.c_int32()
+    _check(lib().tpcf_kmeans(ctx.handle, X.ptr, Y.ptr, W.ptr, n, int(k), int(iterations),
+                             float(reassignment_tol), lab.ctypes.data, cen.ctypes.data, C.byref(it)),
+           ctx.handle)
+    return lab, cen, it.value
+
+
+def block_bootstrap(patch_sums, n_boot, seed=0, supersampling_factor=1.0, multiplicity=None,
+                    covariance=True, ctx: Context = None):
+    """Block bootstrap over lens patches for one or many tasks
+    (survey_marked_point_block_bootstrap's resampling, src/tpcf.f90:1166-1191).
+
+    ``patch_sums``: [n_patch][6][n_bin] (one task) or [n_task][n_patch][6][n_bin]
+    as returned in Shear2pcfResults.patch_sums.  Returns a dict with g_t, g_x
+    [n_boot][n_task][n_bin], weights [n_boot][n_task], multiplicity
+    [n_boot][n_patch] and, if asked, cov_g_t / cov_g_x over the joint vector."""
+    ctx = _resolve_ctx(ctx)
+    ps = np.ascontiguousarray(patch_sums, np.float64)
+    if ps.ndim == 3:
+        ps = ps[None]
+    n_task, n_patch, six, nb = ps.shape
+    assert six == 6
+    D = n_task * nb
+    gt = np.zeros((n_boot, n_task, nb))
+    gx = np.zeros((n_boot, n_task, nb))
+    W = np.zeros((n_boot, n_task))
+    mult = np.zeros((n_boot, n_patch), np.int32)
+    cgt = np.zeros((D, D)) if covariance else None
+    cgx = np.zeros((D, D)) if covariance else None
+    M = None if multiplicity is None else np.ascontiguousarray(multiplicity, np.int32)
+    p = lambda a: None if a is None else a.ctypes.data
+    _check(lib().tpcf_bootstrap(ctx.handle, ps.ctypes.data, n_task, n_patch, nb, p(M), int(seed), int(n_boot),
+                                float(supersampling_factor), gt.ctypes.data, gx.ctypes.data, W.ctypes.data,
+                                p(cgt), p(cgx), mult.ctypes.data), ctx.handle)
+    out = dict(g_t=gt, g_x=gx, weights=W, multiplicity=M if M is not None else mult)
+    if covariance:
+        out.update(cov_g_t=cgt, cov_g_x=cgx)
+    return out
+
+
+
+# ---------------------------------------------------------------- gradients --
+def tangential_shear_adjoint(x_A, y_A, z_A, val_A, weight_A, x_B, y_B, z_B, e1_B, e2_B, weight_B, m_B,
+                             bins: Binning, forward: Shear2pcfResults, dL_dg_t, dL_dg_x=None,
+                             ctx: Context = None):
+    """Gradient of L with dL/dg_t, dL/dg_x given per bin, through
+    tpcf_shear_scalar_adjoint.  ``forward`` is the Shear2pcfResults of the same
+    inputs computed with lens_raw=True.  Returns a dict of gradients w.r.t.
+    val_A, w_A, e1_B, e2_B, w_B, m_B (float32 arrays)."""
+    ctx = _resolve_ctx(ctx)
+    A = [_Arr(a) for a in (x_A, y_A, z_A, val_A, weight_A)]
+    B = [_Arr(a) for a in (x_B, y_B, z_B, e1_B, e2_B, weight_B, m_B)]
+    nA, nB = A[0].n, B[0].n
+    if forward.lens_raw is None:
+        raise ValueError("forward must be computed with lens_raw=True")
+    f64 = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
+    lt, lx = f64(dL_dg_t), f64(dL_dg_x)
+    raw = f64(forward.lens_raw)
+    g = {k: np.zeros(nA, np.float32) for k in ("val_A", "w_A")}
+    g.update({k: np.zeros(nB, np.float32) for k in ("e1_B", "e2_B", "w_B", "m_B")})
+    cb = bins.c_struct()
+    p = lambda a: None if a is None else a.ctypes.data
+    st = lib().tpcf_shear_scalar_adjoint(
+        ctx.handle, *[a.ptr for a in A], nA, *[b.ptr for b in B], nB, C.byref(cb),
+        p(f64(forward.sum_gt)), p(f64(forward.sum_gx)), p(f64(forward.sum_K)), p(raw), p(lt), p(lx),
+        *[g[k].ctypes.data for k in ("val_A", "w_A", "e1_B", "e2_B", "w_B", "m_B")])
+    _check(st, ctx.handle)
+    return g

@@ -39,7 +39,7 @@ class Result(C.Structure):
         "sum_dw", "sum_gt", "sum_gx", "sum_w", "sum_K", "n_pairs",
         "theta", "mean_theta", "g_t", "g_x", "weights",
         "xi_E_marks", "xi_B_marks", "K_marks", "w_marks", "marks_weight",
-        "lens_sums", "patch_sums")]
+        "lens_sums", "patch_sums", "lens_raw")]
 
 
 class LensCat(C.Structure):
@@ -102,6 +102,11 @@ def lib():
                                             i32, vp, vp, C.POINTER(Bins), i32, C.POINTER(Result)])
     _sig(L, "tpcf_shear_scalar_noalloc", st, [vp] + [vp] * 5 + [i64] + [vp] * 7 + [i64] +
          [C.POINTER(Bins), C.POINTER(Result)])
+    _sig(L, "tpcf_shear_scalar_adjoint", st, [vp] + [vp] * 5 + [i64] + [vp] * 7 + [i64] +
+         [C.POINTER(Bins)] + [vp] * 4 + [vp] * 2 + [vp] * 6)
+    _sig(L, "tpcf_kmeans", st, [vp, vp, vp, vp, i64, i32, i32, C.c_float, vp, vp, C.POINTER(i32)])
+    _sig(L, "tpcf_bootstrap", st, [vp, vp, i32, i32, i32, vp, C.c_uint64, i32, C.c_double,
+                                   vp, vp, vp, vp, vp, vp])
     _declare_extra(L)
     if L.tpcf_abi_version() != 1:
         raise ImportError("libtpcf_b200.so ABI version mismatch")

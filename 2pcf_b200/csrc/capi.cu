@@ -401,7 +401,8 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     d.item_base = (int)items.size();
     for (int g = 0; g < lb[tl[t]].n_groups; ++g) items.push_back(make_int2(t, g));
     const tpcf_result& o = outs[t];
-    want_lens[t] = (o.xi_E_marks || o.xi_B_marks || o.K_marks || o.w_marks || o.marks_weight || o.lens_sums) ? 1 : 0;
+    want_lens[t] =
+        (o.xi_E_marks || o.xi_B_marks || o.K_marks || o.w_marks || o.marks_weight || o.lens_sums || o.lens_raw) ? 1 : 0;
     d.lens_acc_off = -1;
     if (want_lens[t]) {
       d.lens_acc_off = lens_acc_elems;
@@ -510,18 +511,20 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
       float* wm = (float*)dev_out(o.w_marks, mb);
       float* mw = (float*)dev_out(o.marks_weight, sizeof(float) * std::max<int64_t>(nA, 0));
       double* ls = (double*)dev_out(o.lens_sums, sizeof(double) * 6 * nb * (size_t)std::max<int64_t>(nA, 0));
+      double* lr = (double*)dev_out(o.lens_raw, sizeof(double) * 6 * nb * (size_t)std::max<int64_t>(nA, 0));
       const bool marks_all = xE && xB && Km && wm;
       if (!marks_all && (xE || xB || Km || wm))
         throw Failure(TPCF_ERR_INVALID_ARG, "xi_E_marks, xi_B_marks, K_marks and w_marks go together");
       if (B.n_valid > 0 && n_items > 0)
         counted(c, launch_lens_outputs(lens_acc + tdesc[t].lens_acc_off, B.rec, B.perm, B.n_valid, nb, xE, xB, Km,
-                                       wm, mw, ls, st), "lens outputs");
+                                       wm, mw, ls, lr, st), "lens outputs");
       if (xE && xE != (void*)o.xi_E_marks) copy_out(c, o.xi_E_marks, xE, mb);
       if (xB && xB != (void*)o.xi_B_marks) copy_out(c, o.xi_B_marks, xB, mb);
       if (Km && Km != (void*)o.K_marks) copy_out(c, o.K_marks, Km, mb);
       if (wm && wm != (void*)o.w_marks) copy_out(c, o.w_marks, wm, mb);
       if (mw && mw != (void*)o.marks_weight) copy_out(c, o.marks_weight, mw, sizeof(float) * nA);
       if (ls && ls != (void*)o.lens_sums) copy_out(c, o.lens_sums, ls, sizeof(double) * 6 * nb * nA);
+      if (lr && lr != (void*)o.lens_raw) copy_out(c, o.lens_raw, lr, sizeof(double) * 6 * nb * nA);
     }
   }
   unsigned herr = 0;

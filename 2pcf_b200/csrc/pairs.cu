@@ -24,52 +24,11 @@
 #include <cub/cub.cuh>
 #include <cstdio>
 
+#include "tpcf_device.cuh"
 #include "tpcf_internal.cuh"
 #include "tpcf_kernels.h"
 
 namespace tpcf {
-
-// ------------------------------------------------------------ PTX helpers --
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-// 1-D bulk copy global -> shared, completion signalled on `bar`.  Both
-// addresses 16-byte aligned, bytes a multiple of 16 (SrcRec is 32 bytes).
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait: returns false after ~2^22 polls (each poll may suspend the
-// thread for a hardware-defined interval), never spins forever.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-  for (uint32_t i = 0; i < (1u << 22); ++i)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
 
 // ------------------------------------------------------- shared-memory map --
 struct PairSmem {
@@ -98,78 +57,6 @@ __host__ __device__ inline PairSmem pair_smem_layout(int nb, int qa, int bt) {
   s.misc = o;  o += 16;
   s.total = align_up(o, 128);
   return s;
-}
-
-// ------------------------------------------------------------ geometry ------
-__device__ __forceinline__ int clamp_floor(float v, int lo, int hi) {
-  v = floorf(v);
-  v = fminf(fmaxf(v, (float)lo), (float)hi);
-  return (int)v;
-}
-// Rows of cells within R of the box.
-__device__ __forceinline__ void row_range(const GridDesc& G, float4 box, float R, float m, int& cy0,
-                                          int& cy1) {
-  cy0 = clamp_floor((box.y - R - m - G.y0) * G.inv_cell, 0, G.ncy - 1);
-  cy1 = clamp_floor((box.w + R + m - G.y0) * G.inv_cell, 0, G.ncy - 1);
-}
-// The contiguous run of sources of row cy whose cells lie within R of the box.
-__device__ __forceinline__ int2 row_span(const GridDesc& G, float4 box, float R, float m, int cy) {
-  const float ylo = G.y0 + (float)cy * G.cell - m;
-  const float yhi = G.y0 + (float)(cy + 1) * G.cell + m;
-  const float dyr = fmaxf(0.f, fmaxf(ylo - box.w, box.y - yhi));
-  if (dyr > R) return make_int2(0, 0);
-  const float rx = sqrtf(fmaxf(R * R - dyr * dyr, 0.f)) + m;
-  const int cx0 = clamp_floor((box.x - rx - G.x0) * G.inv_cell, 0, G.ncx - 1);
-  const int cx1 = clamp_floor((box.z + rx - G.x0) * G.inv_cell, 0, G.ncx - 1);
-  const int base = cy * G.ncx;
-  return make_int2(G.cell_start[base + cx0], G.cell_start[base + cx1 + 1]);
-}
-
-// ------------------------------------------------------------ binning -------
-// Canonical FP64 bin of the pair (rare path: pairs inside the guard band).
-__device__ __noinline__ int slow_bin(float lx, float ly, float sx, float sy, const double* e2, int nb) {
-  const double dx = __dsub_rn((double)lx, (double)sx);
-  const double dy = __dsub_rn((double)ly, (double)sy);
-  const double d2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
-  if (!(d2 >= e2[0]) || d2 > e2[nb]) return -1;
-  if (d2 == e2[nb]) return nb - 1;
-  int lo = 0, hi = nb;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (d2 >= e2[mid]) lo = mid; else hi = mid;
-  }
-  return lo;
-}
-
-struct BinCtx {
-  float A, B, eps, one_m_eps;
-  float eps_rel;     // relative guard on d2 around one FP32 edge (register paths)
-  float lo_g, hi_g;  // generic: fast reject bounds e2f[0]*(1-eps), e2f[nb]*(1+eps)
-  int nb;
-  const double* e2s;
-  const float* e2f;
-};
-
-template <bool LOGB>
-__device__ __forceinline__ int pair_bin(float d2, float lx, float ly, float sx, float sy, const BinCtx& C) {
-  if (LOGB) {
-    const float t = fmaf(__log2f(d2), C.A, C.B);
-    const float tf = floorf(t);
-    const float fr = t - tf;
-    int b = __float2int_rz(tf);
-    if (fr < C.eps || fr > C.one_m_eps) b = slow_bin(lx, ly, sx, sy, C.e2s, C.nb);
-    return b;
-  } else {
-    if (d2 < C.lo_g || d2 > C.hi_g) return -1;
-    int lo = 0, hi = C.nb;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (d2 >= C.e2f[mid]) lo = mid; else hi = mid;
-    }
-    const float el = C.e2f[lo], eh = C.e2f[lo + 1];
-    if (d2 <= el * (1.f + C.eps) || d2 >= eh * (1.f - C.eps)) lo = slow_bin(lx, ly, sx, sy, C.e2s, C.nb);
-    return lo;
-  }
 }
 
 // One pair: lens (lx, ly, lz) against source record (a, b).  hcol points at
@@ -232,41 +119,6 @@ __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const floa
 // The path is chosen per warp (the largest class of its lanes), so lanes never
 // diverge inside a source loop.  Every pair still lands in its canonical bin:
 // in classes 1 and 2 the box bounds prove which bins are possible.
-
-// Largest i in [0, nb] with e2f[i] <= v, or -1 (generic spacings).
-__device__ __forceinline__ int edge_index_f32(float v, const float* e2f, int nb) {
-  if (v < e2f[0]) return -1;
-  int lo = 0, hi = nb + 1;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (v >= e2f[mid]) lo = mid; else hi = mid;
-  }
-  return lo;
-}
-
-template <bool LOGB, bool HAS_Z>
-__device__ __forceinline__ int classify(float lx, float ly, const float4 box, const BinCtx& C, int& blo) {
-  const float dxl = fmaxf(fmaxf(box.x - lx, lx - box.z), 0.f);
-  const float dyl = fmaxf(fmaxf(box.y - ly, ly - box.w), 0.f);
-  const float dxh = fmaxf(lx - box.x, box.z - lx);
-  const float dyh = fmaxf(ly - box.y, box.w - ly);
-  const float dmin2 = fmaf(dyl, dyl, dxl * dxl);
-  const float dmax2 = fmaf(dyh, dyh, dxh * dxh);
-  int b0, b1;
-  if (LOGB) {
-    b0 = __float2int_rd(fmaf(__log2f(dmin2), C.A, C.B) - C.eps);
-    b1 = __float2int_rd(fmaf(__log2f(dmax2), C.A, C.B) + C.eps);
-  } else {
-    b0 = edge_index_f32(dmin2 * (1.f - C.eps), C.e2f, C.nb);
-    b1 = edge_index_f32(dmax2 * (1.f + C.eps), C.e2f, C.nb);
-  }
-  if (b1 < 0 || b0 >= C.nb) return 0;
-  blo = b0;
-  if (HAS_Z) return 3;
-  if (b0 == b1) return 1;
-  if (b1 == b0 + 1) return 2;
-  return 3;
-}
 
 // Per-pair quantities shared by the register paths: g_t, g_x terms (shear) or
 // kE*w, kB*w (scalar-scalar), and d.
@@ -942,7 +794,7 @@ __global__ void k_patch_reduce(const double* __restrict__ item_sums, int item_ba
 // lenses keep 0, as in the reference).
 __global__ void k_lens_outputs(const double* __restrict__ acc, const float4* __restrict__ rec,
                                const int* __restrict__ perm, int n_valid, int nb, float* xi_E, float* xi_B,
-                               float* K_m, float* w_m, float* marks_weight, double* lens_sums) {
+                               float* K_m, float* w_m, float* marks_weight, double* lens_sums, double* lens_raw) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_valid) return;
   const float4 r = rec[s];
@@ -969,6 +821,15 @@ __global__ void k_lens_outputs(const double* __restrict__ acc, const float4* __r
       o[2 * nb + b] = gx;
       o[3 * nb + b] = ww;
       o[4 * nb + b] = kk;
+      o[5 * nb + b] = nn;
+    }
+    if (lens_raw) {
+      double* o = lens_raw + i * 6 * nb;
+      o[0 * nb + b] = acc[(size_t)(QDW * nb + b) * n_valid + s];
+      o[1 * nb + b] = acc[(size_t)(QGT * nb + b) * n_valid + s];
+      o[2 * nb + b] = acc[(size_t)(QGX * nb + b) * n_valid + s];
+      o[3 * nb + b] = acc[(size_t)(QW * nb + b) * n_valid + s];
+      o[4 * nb + b] = acc[(size_t)(QK * nb + b) * n_valid + s];
       o[5 * nb + b] = nn;
     }
     mw += ww;
@@ -1106,10 +967,10 @@ cudaError_t launch_patch_reduce(const double* item_sums, int item_base, const in
 }
 cudaError_t launch_lens_outputs(const double* acc, const float4* rec, const int* perm, int n_valid, int nb,
                                 float* xi_E, float* xi_B, float* K_m, float* w_m, float* marks_weight,
-                                double* lens_sums, cudaStream_t st) {
+                                double* lens_sums, double* lens_raw, cudaStream_t st) {
   if (n_valid > 0)
     k_lens_outputs<<<(n_valid + 127) / 128, 128, 0, st>>>(acc, rec, perm, n_valid, nb, xi_E, xi_B, K_m, w_m,
-                                                          marks_weight, lens_sums);
+                                                          marks_weight, lens_sums, lens_raw);
   return cudaGetLastError();
 }
 

@@ -47,7 +47,7 @@ cudaError_t launch_patch_reduce(const double* item_sums, int item_base, const in
                                 int nb, double* patch_sums, cudaStream_t st);
 cudaError_t launch_lens_outputs(const double* acc, const float4* rec, const int* perm, int n_valid, int nb,
                                 float* xi_E, float* xi_B, float* K_m, float* w_m, float* marks_weight,
-                                double* lens_sums, cudaStream_t st);
+                                double* lens_sums, double* lens_raw, cudaStream_t st);
 
 cudaError_t sort_pairs_u32(void* tmp, size_t& tmp_bytes, const unsigned* kin, unsigned* kout, const int* vin,
                            int* vout, int n, int end_bit, cudaStream_t st);

@@ -114,6 +114,10 @@ typedef struct tpcf_result {
    * lens patches given in the call (block sums of
    * survey_marked_point_block_bootstrap, src/tpcf.f90:1130-1137).           */
   double* patch_sums;
+  /* Per-lens FP64 sums without the lens factors, nullable, [n_A][6][n_bin]:
+   * the same six rows with val_A*w_A (g rows) or w_A (d*w, w, K rows) left
+   * out.  Input of tpcf_shear_scalar_adjoint.                               */
+  double* lens_raw;
 } tpcf_result;
 
 /* Lens / scalar catalogue (lens_catalog, src/tpcf.f90:34-37).  z may be NULL
@@ -222,6 +226,61 @@ tpcf_status tpcf_batch_shear_scalar(tpcf_ctx* ctx,
                                     const int32_t* task_src,
                                     const tpcf_bins* bins, int32_t n_patch,
                                     tpcf_result* outs);
+
+/* ------------------------------------------------------------ gradients -- */
+/* No counterpart in the reference (it has no gradients).  Adjoint of
+ * tpcf_shear_scalar: given dL/dg_t and dL/dg_x per bin (g = the normalised
+ * xi of the forward call, nullable dL_dgx = 0), writes dL/dval_A, dL/dw_A
+ * [nA] and dL/de1_B, dL/de2_B, dL/dw_B, dL/dm_B [nB] (each nullable).  The
+ * inputs are those of the forward call plus its sum_gt, sum_gx, sum_K [n_bin]
+ * and lens_raw [nA][6][n_bin] outputs (lens_raw is only read for the lens
+ * gradients).  Pairs are binned exactly as in the forward call; the lens
+ * gradients come from lens_raw, the source gradients from one pass over all
+ * pairs with sources as owners.  Lenses and sources that take part in no pair
+ * get 0. */
+tpcf_status tpcf_shear_scalar_adjoint(tpcf_ctx* ctx,
+                                      const float* xA, const float* yA, const float* zA,
+                                      const float* valA, const float* wA, int64_t nA,
+                                      const float* xB, const float* yB, const float* zB,
+                                      const float* e1B, const float* e2B, const float* wB,
+                                      const float* mB, int64_t nB,
+                                      const tpcf_bins* bins,
+                                      const double* sum_gt, const double* sum_gx, const double* sum_K,
+                                      const double* lens_raw,
+                                      const double* dL_dgt, const double* dL_dgx,
+                                      float* grad_valA, float* grad_wA,
+                                      float* grad_e1B, float* grad_e2B, float* grad_wB, float* grad_mB);
+
+/* -------------------------------------------------- patches and errors -- */
+/* Replaces partition_data (src/kmeans.f90:12-263) as called for Voronoi
+ * blocks (equal_size = .false., weight_equalizer_scaling = 0,
+ * src/tpcf.f90:1117-1124): fixed-grid initial centroids
+ * (src/kmeans.f90:85-112), Lloyd iterations on the device until no label
+ * changes, the changed fraction drops below reassign_tol, or max_iter + 1
+ * passes.  Distances are FP32 sqrt(dx*dx+dy*dy) with IEEE rounding; centroid
+ * sums are 64-bit fixed point, so the labels are the same on every run.
+ * labels_out [n] are 0-based; centroids_out [k][2] is nullable.  The
+ * reference's equal-weight mode (distance penalty and rebalancing pass) is not
+ * provided. */
+tpcf_status tpcf_kmeans(tpcf_ctx* ctx, const float* x, const float* y, const float* w, int64_t n,
+                        int32_t k, int32_t max_iter, float reassign_tol,
+                        int32_t* labels_out, float* centroids_out, int32_t* n_iter_out);
+
+/* Replaces the resampling loop of survey_marked_point_block_bootstrap
+ * (src/tpcf.f90:1166-1191) and covariance_matrix (src/utils.f90:745-764) for
+ * n_task tasks at once.  patch_sums is [n_task][n_patch][6][n_bin] as the pair
+ * calls write it (tpcf_result.patch_sums).  multiplicity [n_boot][n_patch]
+ * may be NULL: then each resample draws int(n_patch*supersampling) patches
+ * with replacement from Philox4x32-10 keyed by `seed` (a pure function of
+ * seed, resample and draw; mult_out, nullable, receives the counts).
+ * Outputs: g_t, g_x [n_boot][n_task][n_bin] (0 where K <= 0, as the
+ * reference), weights [n_boot][n_task] (nullable), and the unbiased
+ * covariances of g_t and g_x over the joint data vector, [D][D] with
+ * D = n_task*n_bin (nullable). */
+tpcf_status tpcf_bootstrap(tpcf_ctx* ctx, const double* patch_sums, int32_t n_task, int32_t n_patch,
+                           int32_t n_bin, const int32_t* multiplicity, uint64_t seed, int32_t n_boot,
+                           double supersampling, double* g_t, double* g_x, double* weights,
+                           double* cov_gt, double* cov_gx, int32_t* mult_out);
 
 /* No counterpart in the reference.  The pair sum of tpcf_shear_scalar for
  * callers that cannot allocate device memory: a framework's caching allocator

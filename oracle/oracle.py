@@ -72,6 +72,8 @@ def lib():
                                           _f64p, _f64p, _f64p, _f64p]
         L.orc_covariance.argtypes = [C.c_int, C.c_int, _f64p, _f64p]
         L.orc_last_timing.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.orc_canon_adjoint.argtypes = ([C.c_long] + [vp] * 5 + [C.c_long] + [vp] * 7 +
+                                        [_f64p, C.c_int, _f64p, _f64p, C.c_int] + [_f64p] * 6)
         _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
         L.orc_philox4x32.argtypes = [_u32p, _u32p, _u32p]
         _lib = L
@@ -196,6 +198,23 @@ def canon_pairs(mode, lens, src, edges_sq, num_threads=None, lens_idx=None):
     if lens_out is not None:
         out["lens"] = lens_out
     return out
+
+
+def canon_adjoint(lens, src, edges_sq, lam_t, lam_x=None, num_threads=None):
+    """FP64 brute-force gradient of L = sum_b lam_t[b] xi_t,b + lam_x[b] xi_x,b
+    (shear-scalar, canonical bins) w.r.t. val_A, w_A, e1_B, e2_B, w_B, m_B."""
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+    nA, nB = len(lens["x"]), len(src["x"])
+    nb = len(edges_sq) - 1
+    A = [f(lens[k]) for k in ("x", "y", "z", "val", "w")]
+    B = [f(src[k]) for k in ("x", "y", "z", "e1", "e2", "w", "m")]
+    lt = np.ascontiguousarray(lam_t, np.float64)
+    lx = np.zeros(nb) if lam_x is None else np.ascontiguousarray(lam_x, np.float64)
+    out = [np.zeros(nA), np.zeros(nA)] + [np.zeros(nB) for _ in range(4)]
+    lib().orc_canon_adjoint(nA, *[_ptr(a) for a in A], nB, *[_ptr(b) for b in B],
+                            np.ascontiguousarray(edges_sq, np.float64), nb, lt, lx,
+                            num_threads or os.cpu_count() or 1, *out)
+    return dict(zip(("val_A", "w_A", "e1_B", "e2_B", "w_B", "m_B"), out))
 
 
 def normalise(s):

@@ -842,6 +842,76 @@ int orc_canon_pairs(int mode, long nA, const float* xA, const float* yA, const f
   return 0;
 }
 
+// FP64 brute-force gradient of L = sum_b lt[b]*xi_t,b + lx[b]*xi_x,b of the
+// shear-scalar estimator (canonical bins), with respect to val_A, w_A (per
+// lens) and e1_B, e2_B, w_B, m_B (per source).  xi = G/K where K > 0, else 0.
+int orc_canon_adjoint(long nA, const float* xA, const float* yA, const float* zA, const float* valA,
+                      const float* wA, long nB, const float* xB, const float* yB, const float* zB,
+                      const float* e1B, const float* e2B, const float* wB, const float* mB, const double* e2,
+                      int nb, const double* lt, const double* lx, int num_threads, double* g_val, double* g_wA,
+                      double* g_e1, double* g_e2, double* g_wB, double* g_m) {
+  std::vector<double> sums((size_t)canon::NQ * nb, 0.0);
+  orc_canon_pairs(0, nA, xA, yA, zA, valA, wA, nB, xB, yB, zB, e1B, e2B, wB, mB, e2, nb, num_threads,
+                  sums.data(), nullptr, 0, nullptr);
+  std::vector<double> mu(nb, 0.0), mux(nb, 0.0), nu(nb, 0.0);
+  for (int b = 0; b < nb; ++b) {
+    const double K = sums[canon::Q_K * nb + b];
+    if (K > 0) {
+      mu[b] = lt[b] / K;
+      mux[b] = lx[b] / K;
+      nu[b] = (lt[b] * (sums[canon::Q_GT * nb + b] / K) + lx[b] * (sums[canon::Q_GX * nb + b] / K)) / K;
+    }
+  }
+  auto pair = [&](long i, long j, int& b, double& c2, double& s2) -> bool {
+    if (wA[i] == 0.0f || zA[i] < 0.0f || zB[j] < 0.0f || zA[i] > zB[j]) return false;
+    const double d2 = canon::d2_of(xA[i], yA[i], xB[j], yB[j]);
+    b = canon::bin_of(d2, e2, nb);
+    if (b < 0) return false;
+    const double dx = (double)xA[i] - (double)xB[j], dy = (double)yA[i] - (double)yB[j];
+    const double d = sqrt(d2);
+    c2 = 2.0 * ((dx / d) * (dx / d)) - 1.0;
+    s2 = 2.0 * dx * dy / d2;
+    return true;
+  };
+#pragma omp parallel for schedule(dynamic, 16) num_threads(num_threads)
+  for (long i = 0; i < nA; ++i) {
+    double gv = 0, gw = 0;
+    for (long j = 0; j < nB; ++j) {
+      int b;
+      double c2, s2;
+      if (!pair(i, j, b, c2, s2)) continue;
+      const double e1 = e1B[j], ee2 = e2B[j], w = wB[j], m = mB ? mB[j] : 0.0;
+      const double t = -(e1 * c2 + ee2 * s2), x = -(-e1 * s2 + ee2 * c2);
+      const double a = mu[b] * t + mux[b] * x;
+      gv += a * w * (double)wA[i];
+      gw += a * w * (double)valA[i] - nu[b] * w * (1.0 + m);
+    }
+    g_val[i] = gv;
+    g_wA[i] = gw;
+  }
+#pragma omp parallel for schedule(dynamic, 16) num_threads(num_threads)
+  for (long j = 0; j < nB; ++j) {
+    double ge1 = 0, ge2 = 0, gw = 0, gm = 0;
+    const double e1 = e1B[j], ee2 = e2B[j], w = wB[j], m = mB ? mB[j] : 0.0;
+    for (long i = 0; i < nA; ++i) {
+      int b;
+      double c2, s2;
+      if (!pair(i, j, b, c2, s2)) continue;
+      const double vw = (double)valA[i] * (double)wA[i];
+      const double t = -(e1 * c2 + ee2 * s2), x = -(-e1 * s2 + ee2 * c2);
+      ge1 += (mu[b] * (-c2) + mux[b] * s2) * w * vw;
+      ge2 += (mu[b] * (-s2) + mux[b] * (-c2)) * w * vw;
+      gw += (mu[b] * t + mux[b] * x) * vw - nu[b] * (1.0 + m) * (double)wA[i];
+      gm += -nu[b] * w * (double)wA[i];
+    }
+    g_e1[j] = ge1;
+    g_e2[j] = ge2;
+    g_wB[j] = gw;
+    g_m[j] = gm;
+  }
+  return 0;
+}
+
 // kd-tree radius search (test_kdtree.f90).  Results are 0-based indices.
 int orc_kdtree_search(long n, const float* x, const float* y, float qx, float qy, float r,
                       int leafsize, int brute_force, long* results, long cap, long* n_found) {
