@@ -272,6 +272,14 @@ __device__ __forceinline__ void flush_hist(float* hist, double* bsum, const doub
   for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
 }
 
+#ifdef TPCF_MODE_STATS
+// Diagnostic build only: warp-level path counts [4] and lane-pairs per path [4].
+__device__ unsigned long long g_mode_stats[8];
+extern "C" int tpcf_debug_mode_stats(unsigned long long* out) {
+  return (int)cudaMemcpyFromSymbol(out, g_mode_stats, sizeof(g_mode_stats));
+}
+#endif
+
 // PATH 0: sub-chunk classification with the register paths (default);
 // PATH 1: per-pair binning for every pair (kept for A/B measurement).
 template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int PATH>
@@ -318,6 +326,11 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
   uint32_t tcount = 0u;  // tiles processed by this block so far
   bool timed_out = false;
   float* __restrict__ hcol = hist + tid;
+#ifdef TPCF_MODE_STATS
+  __shared__ unsigned long long sh_stats[8];
+  if (tid < 8) sh_stats[tid] = 0ull;
+  __syncthreads();
+#endif
   for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
 
   for (;;) {
@@ -428,6 +441,15 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
               int blo = 0;
               const int cls = act ? classify<LOGB, HAS_Z>(lx, ly, subbox[sc], C, blo) : 0;
               const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)cls);
+#ifdef TPCF_MODE_STATS
+              {
+                const unsigned nact = __popc(__ballot_sync(0xffffffffu, act));
+                if (lane == 0) {
+                  atomicAdd(&sh_stats[m], 1ull);
+                  atomicAdd(&sh_stats[4 + m], (unsigned long long)(cnt * nact));
+                }
+              }
+#endif
               if (m == 0) continue;
               const SrcRec* __restrict__ Sc = S + base;
               if (m == 1) {
@@ -485,6 +507,10 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
     __syncthreads();
   }
   if (timed_out && tid == 0) atomicOr(P.err, kErrTimeout);
+#ifdef TPCF_MODE_STATS
+  __syncthreads();
+  if (tid < 8) atomicAdd(&g_mode_stats[tid], sh_stats[tid]);
+#endif
 }
 
 // ------------------------------------------------------------ prep kernels --

@@ -163,6 +163,72 @@ def cpu_baseline(w, seconds, nthreads, steps=1, warmup=0):
             "seconds": tot_t}
 
 
+def adjoint_timing(w, ctx, bins, step_ms, pair_ms, stream):
+    """Forward with device-resident raw per-lens sums plus the adjoint (the
+    torch.autograd path: xi_t for every task, chi^2 against a seeded target,
+    backward) over all 25 tasks, against the plain batched forward."""
+    import torch
+    ag = importlib.import_module("2pcf_b200.autograd")
+    d = lambda a: torch.from_numpy(a).cuda()
+    rng = np.random.default_rng(1004)
+    t_fwd = t_all = 0.0
+    pairs = 0
+    for (i, j) in w["tasks"]:
+        L, S = w["lens_bins"][i], w["shape_bins"][j]
+        geo = dict(x_A=d(L["x"]), y_A=d(L["y"]), z_A=d(L["z"]), x_B=d(S["x"]), y_B=d(S["y"]),
+                   z_B=d(S["z"]), m_B=d(S["m"]))
+        leaves = [d(a).requires_grad_(True) for a in (L["val"], L["w"], S["e1"], S["e2"], S["w"])]
+        target = torch.from_numpy(rng.normal(0, 1e-4, bins.n_bin)).cuda()
+        torch.cuda.synchronize()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        xi_t, _ = ag.xi_shear(*leaves, geo, bins, ctx)
+        e1.record(stream)
+        loss = (((xi_t - target) / 1e-3) ** 2).sum()
+        loss.backward()
+        e2.record(stream)
+        torch.cuda.synchronize()
+        t_fwd += e0.elapsed_time(e1)
+        t_all += e0.elapsed_time(e2)
+        pairs += int(ctx.stats()["n_pairs"])
+        del geo, leaves, xi_t, loss
+    return {"value": pairs / (t_all * 1e-3) / 1e9, "unit": UNIT,
+            "forward_ms": t_fwd, "forward_plus_adjoint_ms": t_all,
+            "fwd_adj_over_plain_fwd": t_all / pair_ms,
+            "fwd_adj_over_fwd": t_all / t_fwd,
+            "note": "25 tasks, one differentiable call each (forward keeps raw per-lens sums on the "
+                    "device, backward = tpcf_shear_scalar_adjoint); plain forward = the pair kernel "
+                    "of the batched step"}
+
+
+def path_stats(tpcf, args):
+    """One batched call on the diagnostic build; prints the share of warp
+    sub-chunks and lane-pairs per path of k_pairs."""
+    import ctypes as C
+    import torch
+    tpcf._lib.LIB_PATH = os.path.join(ROOT, "2pcf_b200", "libtpcf_b200_stats.so")
+    w = workload(args.scale)
+    bins = tpcf.create_bins(*w["bins"])
+    dev = lambda a: torch.from_numpy(a).cuda()
+    L = [tpcf.LensCatalog(**{k: dev(l[k]) for k in ("x", "y", "val", "w", "z")}) for l in w["lens_bins"]]
+    S = [tpcf.ShapeCatalog(**{k: dev(s[k]) for k in ("x", "y", "e1", "e2", "w", "z", "m")})
+         for s in w["shape_bins"]]
+    ctx = tpcf.Context(0)
+    lib = tpcf._lib.lib()
+    st = (C.c_ulonglong * 8)()
+    lib.tpcf_debug_mode_stats(st)
+    base = np.array(st[:])
+    outs = tpcf.batch_shear_2pcf(L, S, w["tasks"], bins, ctx=ctx)
+    lib.tpcf_debug_mode_stats(st)
+    v = np.array(st[:]) - base
+    binned = sum(int(o.n_pairs.sum()) for o in outs)
+    res = {"binned_pairs": binned}
+    for i, name in enumerate(("skip", "single_bin", "one_edge", "per_pair")):
+        res[name] = {"warp_chunks": float(v[i] / v[:4].sum()), "lane_pairs": float(v[4 + i] / v[4:].sum())}
+    res["computed_lane_pairs_per_binned_pair"] = float(v[5:].sum() / binned)
+    print(json.dumps(res), flush=True)
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -196,6 +262,10 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0, help="object-count scale of the workload")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the batched+adjoint measurement")
+    ap.add_argument("--path-stats", action="store_true",
+                    help="diagnostic: load the counting build (make -C 2pcf_b200/csrc stats) and print the "
+                         "pair kernel's path mix for one batched call instead of benchmarking")
     ap.add_argument("--region", type=float, default=0.0,
                     help="profiling: keep only objects with x, y < REGION arcmin (density unchanged)")
     ap.add_argument("--task", type=int, default=-1, help="profiling: run only this task of the 25")
@@ -215,6 +285,8 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     tpcf = importlib.import_module("2pcf_b200")
+    if args.path_stats:
+        return path_stats(tpcf, args)
 
     w = workload(args.scale)
     if args.region > 0:
@@ -226,22 +298,13 @@ def main():
         w["tasks"] = [w["tasks"][args.task]]
     bins = tpcf.create_bins(*w["bins"])
     n_patch = w["n_patch"]
-    # lens patches: fixed-grid blocks of the field (one label per lens)
-    box = w["box"]
-    side = int(np.sqrt(n_patch))
-
-    def patches(L):
-        ix = np.minimum((L["x"] / box * side).astype(np.int32), side - 1)
-        iy = np.minimum((L["y"] / box * side).astype(np.int32), side - 1)
-        return (iy * side + ix).astype(np.int32)
-
-    lpatch = [patches(L) for L in w["lens_bins"]]
     ctx = tpcf.Context(local)
     ctx.set_timing(True)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     if world > 1:
         ctx.set_shard(rank, world)
+    n_boot = w["n_boot"]
 
     def cats(to):
         L = [tpcf.LensCatalog(**{k: to(l[k]) for k in ("x", "y", "val", "w", "z")}) for l in w["lens_bins"]]
@@ -252,21 +315,34 @@ def main():
     dev = lambda a: torch.from_numpy(a).cuda()
     pin = lambda a: torch.from_numpy(a).pin_memory()
     Ld, Sd = cats(dev)
-    Pd = [dev(p) for p in lpatch]
     Lh, Sh = cats(pin)
-    Ph = [pin(p) for p in lpatch]
+    # k-means input: all lens positions with the reference's weights 0.01 + w/max(w)
+    # (src/tpcf.f90:1104), one patch set shared by the 5 scalar bins
+    ux = np.concatenate([l["x"] for l in w["lens_bins"]])
+    uy = np.concatenate([l["y"] for l in w["lens_bins"]])
+    uw = np.concatenate([l["w"] for l in w["lens_bins"]])
+    uw = (0.01 + uw / uw.max()).astype(np.float32)
+    U_d = [dev(a) for a in (ux, uy, uw)]
+    U_h = [pin(a) for a in (ux, uy, uw)]
+    offs = np.cumsum([0] + [len(l["x"]) for l in w["lens_bins"]])
     torch.cuda.synchronize()
 
-    def step(L, S, P):
-        outs = tpcf.batch_shear_2pcf(L, S, w["tasks"], bins, lens_patches=P, n_patch=n_patch, ctx=ctx)
-        if world > 1:
-            v = torch.tensor(np.stack([np.stack([o.sum_gt, o.sum_K, o.n_pairs.astype(np.float64)])
-                                       for o in outs]), device="cuda")
-            dist.all_reduce(v)
-            return int(v[:, 2].sum().item())
-        return sum(int(o.n_pairs.sum()) for o in outs)
+    ctx_pair_ms = [0.0]
 
-    def timed(L, S, P, n):
+    def step(L, S, U):
+        lab, _, _ = tpcf.partition_data(U[0], U[1], U[2], n_patch, ctx=ctx)
+        P = [lab[offs[i]:offs[i + 1]] for i in range(len(L))]
+        outs = tpcf.batch_shear_2pcf(L, S, w["tasks"], bins, lens_patches=P, n_patch=n_patch, ctx=ctx)
+        ctx_pair_ms[0] = ctx.stats()["pair_kernel_ms"]  # the pair kernel's own CUDA-event time
+        ps = np.stack([o.patch_sums for o in outs])
+        if world > 1:
+            t = torch.from_numpy(ps).cuda()
+            dist.all_reduce(t)
+            ps = t.cpu().numpy()
+        boot = tpcf.block_bootstrap(ps, n_boot, seed=1005, ctx=ctx)
+        return int(ps[:, :, 5].sum()), boot
+
+    def timed(L, S, U, n):
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -276,8 +352,8 @@ def main():
         pairs = 0
         e0.record(stream)
         for _ in range(n):
-            pairs = step(L, S, P)
-            pair_ms += ctx.stats()["pair_kernel_ms"]
+            pairs, _ = step(L, S, U)
+            pair_ms += ctx_pair_ms[0]
         e1.record(stream)
         torch.cuda.synchronize()
         if world > 1:
@@ -290,21 +366,24 @@ def main():
 
     with ClockSampler(local) as cs:  # started before the warm-up: its start-up stays outside the timing
         for _ in range(args.warmup):
-            step(Ld, Sd, Pd)
+            step(Ld, Sd, U_d)
         t0 = time.time()
-        ms, pairs, pair_ms, launches = timed(Ld, Sd, Pd, args.steps)
+        ms, pairs, pair_ms, launches = timed(Ld, Sd, U_d, args.steps)
         cs.window(t0, time.time())
     clocks = cs.summary()
     value = pairs / (ms * 1e-3) / 1e9
 
     # end to end through the public API with pinned host inputs
-    for _ in range(1):
-        step(Lh, Sh, Ph)
-    ms_e2e, pairs_e2e, _, _ = timed(Lh, Sh, Ph, args.steps)
+    step(Lh, Sh, U_h)
+    ms_e2e, pairs_e2e, _, _ = timed(Lh, Sh, U_h, args.steps)
     h2d = sum(a.numel() * a.element_size() for c in (Lh + Sh) for a in vars(c).values()
-              if hasattr(a, "numel")) + sum(p.numel() * 4 for p in Ph)
-    d2h = len(w["tasks"]) * bins.n_bin * (5 * 8 + 8 + 5 * 4 + n_patch * 6 * 8)
+              if hasattr(a, "numel")) + sum(a.numel() * 4 for a in U_h)
+    d2h = (int(ux.size) * 4 + len(w["tasks"]) * bins.n_bin * (5 * 8 + 8 + 5 * 4 + n_patch * 6 * 8)
+           + 2 * n_boot * len(w["tasks"]) * bins.n_bin * 8 + 2 * (len(w["tasks"]) * bins.n_bin) ** 2 * 8)
 
+    adjoint = None
+    if world == 1 and not args.no_adjoint:
+        adjoint = adjoint_timing(w, ctx, bins, ms, pair_ms, stream)
     peak = ctx.measure_fp32_peak()
     achieved = pairs * FLOP_PER_PAIR / (pair_ms * 1e-3) / 1e12
     traffic = None
@@ -325,7 +404,9 @@ def main():
                    "global_batch": int(pairs),
                    "parallelism": f"work items sharded over {world} rank(s)" if world > 1 else "single GPU",
                    "l2": "inputs (280 MB of catalogues) larger than L2 (126 MB); no flush",
-                   "step": "grid build + 25-task pair kernel + per-patch sums (tpcf_batch_shear_scalar)"},
+                   "step": "k-means (100 patches, all 2.4 M lens positions) + grid build + one 25-task "
+                           "pair launch + per-patch sums + 1000-resample bootstrap with the joint "
+                           "500x500 covariance"},
         "e2e": {"value": pairs_e2e / (ms_e2e * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -334,6 +415,7 @@ def main():
                      "peak_source": "measured in this run: FFMA loop (tpcf_measure_fp32_peak); "
                                     "MEASURED_PEAKS.json has no FP32 figure"},
         "gpu_launches": int(launches),
+        "batched_adjoint": adjoint,
         "clocks": clocks,
     }
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
