@@ -114,6 +114,7 @@ class Context:
         o = Opts(int(use_grid), int(verbose), float(cell_size), 0, 0, 0, (C.c_int32 * 5)())
         _check(lib().tpcf_create(C.byref(self._h), int(device), C.byref(o)))
         self.device = device
+        self.cell_size = float(cell_size)
 
     @property
     def handle(self):
@@ -135,6 +136,11 @@ class Context:
 
     def set_timing(self, enable: bool):
         _check(lib().tpcf_set_timing(self._h, int(enable)), self._h)
+
+    def set_cell_size(self, cell_size: float):
+        """Grid cell side for later calls (0 = theta_max/16)."""
+        _check(lib().tpcf_set_cell_size(self._h, float(cell_size)), self._h)
+        self.cell_size = float(cell_size)
 
     def set_shard(self, index: int, count: int):
         """Compute only work items i % count == index (sums become partial)."""

@@ -91,6 +91,7 @@ def lib():
     _sig(L, "tpcf_set_timing", st, [vp, i32])
     _sig(L, "tpcf_last_stats", st, [vp, C.POINTER(Stats)])
     _sig(L, "tpcf_set_shard", st, [vp, i32, i32])
+    _sig(L, "tpcf_set_cell_size", st, [vp, C.c_double])
     _sig(L, "tpcf_measure_fp32_peak", st, [vp, C.POINTER(C.c_double)])
     _sig(L, "tpcf_canonical_edges", st, [C.POINTER(Bins), vp, vp])
     _sig(L, "tpcf_bin_centers", st, [C.POINTER(Bins), vp])

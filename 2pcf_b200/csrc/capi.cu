@@ -665,6 +665,12 @@ tpcf_status tpcf_set_timing(tpcf_ctx* c, int32_t enable) {
   return TPCF_OK;
 }
 
+tpcf_status tpcf_set_cell_size(tpcf_ctx* c, double cell_size) {
+  if (!c || !(cell_size >= 0) || !std::isfinite(cell_size)) return TPCF_ERR_INVALID_ARG;
+  c->opts.cell_size = cell_size;
+  return TPCF_OK;
+}
+
 tpcf_status tpcf_set_shard(tpcf_ctx* c, int32_t index, int32_t count) {
   if (!c || count < 0 || (count > 1 && (index < 0 || index >= count))) return TPCF_ERR_INVALID_ARG;
   c->opts.shard_index = index;

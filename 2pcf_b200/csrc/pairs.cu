@@ -120,16 +120,18 @@ __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const floa
 // diverge inside a source loop.  Every pair still lands in its canonical bin:
 // in classes 1 and 2 the box bounds prove which bins are possible.
 
-// Per-pair quantities shared by the register paths: g_t, g_x terms (shear) or
-// kE*w, kB*w (scalar-scalar), and d.
+// Per-pair quantities shared by the register paths.  Shear: with
+// P = dx^2 - dy^2, u = 2 dx dy and r = 1/d^2, cos 2phi = P r, sin 2phi = u r
+// (src/tpcf.f90:343-344), so the g_t, g_x terms are r*X and r*Y with
+// X = p P + q u, Y = q P - p u  (p = -e1 w, q = -e2 w).  Scalar-scalar:
+// X = kE w, Y = kB w, r = 1.
 template <int MODE, bool LOGB>
-__device__ __forceinline__ void pair_terms(float lx, float ly, const float4 a, float& d2, float& d, float& t1,
-                                           float& t2) {
+__device__ __forceinline__ void pair_terms(float lx, float ly, const float4 a, float& d2, float& d, float& r,
+                                           float& X, float& Y) {
   const float dx = lx - a.x;
   const float dy = ly - a.y;
   const float dx2 = dx * dx;
   d2 = fmaf(dy, dy, dx2);
-  float r;
   if (LOGB) {
     const float rs = rsqrtf(d2);
     d = d2 * rs;
@@ -139,14 +141,15 @@ __device__ __forceinline__ void pair_terms(float lx, float ly, const float4 a, f
     r = __frcp_rn(d2);
   }
   if (MODE == 0) {
-    const float c2 = fmaf(-dy, dy, dx2) * r;
+    const float P = fmaf(-dy, dy, dx2);
     const float qq = dx * dy;
-    const float s2 = (qq + qq) * r;
-    t1 = fmaf(a.z, c2, a.w * s2);
-    t2 = fmaf(a.w, c2, -(a.z * s2));
+    const float u = qq + qq;
+    X = fmaf(a.z, P, a.w * u);
+    Y = fmaf(a.w, P, -(a.z * u));
   } else {
-    t1 = a.z;
-    t2 = a.w;
+    r = 1.f;
+    X = a.z;
+    Y = a.w;
   }
 }
 
@@ -168,10 +171,10 @@ __device__ __forceinline__ void chunk_single(const SrcRec* __restrict__ S, int c
   for (int j = 0; j < cnt; ++j) {
     const float4 a = S[j].a;
     const float4 b = S[j].b;
-    float d2, d, t1, t2;
-    pair_terms<MODE, LOGB>(lx, ly, a, d2, d, t1, t2);
-    acc[QGT] += t1;
-    acc[QGX] += t2;
+    float d2, d, r, X, Y;
+    pair_terms<MODE, LOGB>(lx, ly, a, d2, d, r, X, Y);
+    acc[QGT] = fmaf(r, X, acc[QGT]);
+    acc[QGX] = fmaf(r, Y, acc[QGX]);
     acc[QW] += b.x;
     acc[QDW] = fmaf(d, b.x, acc[QDW]);
     if (MODE == 0 && HAS_M) acc[QK] += b.y;
@@ -195,8 +198,9 @@ __device__ __forceinline__ void chunk_dual(const SrcRec* __restrict__ S, int cnt
   for (int j = 0; j < cnt; ++j) {
     const float4 a = S[j].a;
     const float4 b = S[j].b;
-    float d2, d, t1, t2;
-    pair_terms<MODE, LOGB>(lx, ly, a, d2, d, t1, t2);
+    float d2, d, r, X, Y;
+    pair_terms<MODE, LOGB>(lx, ly, a, d2, d, r, X, Y);
+    const float t1 = r * X, t2 = r * Y;
     bool up = d2 >= E;
     if (fabsf(d2 - E) <= gE) {
       // canonical bin is blo or blo+1, or -1 on a side outside [x_min, x_max]

@@ -302,6 +302,12 @@ def main():
     ctx.set_timing(True)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
+    # cell side picked by the autotuner (trial calls on a density-preserving corner)
+    at = importlib.import_module("2pcf_b200.autotune")
+    tune = at.autotune_cell_size(
+        [tpcf.LensCatalog(**{k: l[k] for k in ("x", "y", "val", "w", "z")}) for l in w["lens_bins"]],
+        [tpcf.ShapeCatalog(**{k: s_[k] for k in ("x", "y", "e1", "e2", "w", "z", "m")}) for s_ in w["shape_bins"]],
+        w["tasks"], bins, ctx)
     if world > 1:
         ctx.set_shard(rank, world)
     n_boot = w["n_boot"]
@@ -404,6 +410,8 @@ def main():
                    "global_batch": int(pairs),
                    "parallelism": f"work items sharded over {world} rank(s)" if world > 1 else "single GPU",
                    "l2": "inputs (280 MB of catalogues) larger than L2 (126 MB); no flush",
+                   "cell_size": ctx.cell_size,
+                   "autotune_ms_per_gpair": {f"theta_max/{d}": round(v, 2) for d, v in tune.items()},
                    "step": "k-means (100 patches, all 2.4 M lens positions) + grid build + one 25-task "
                            "pair launch + per-patch sums + 1000-resample bootstrap with the joint "
                            "500x500 covariance"},

@@ -170,6 +170,9 @@ typedef struct tpcf_stats {
 } tpcf_stats;
 tpcf_status tpcf_set_timing(tpcf_ctx* ctx, int32_t enable);
 tpcf_status tpcf_last_stats(const tpcf_ctx* ctx, tpcf_stats* stats);
+/* Change the grid cell side of later calls (tpcf_opts.cell_size; 0 = theta_max/16).
+ * 2pcf_b200.autotune picks it by timing trial calls. */
+tpcf_status tpcf_set_cell_size(tpcf_ctx* ctx, double cell_size);
 /* Change the sharding of later calls (see tpcf_opts.shard_index). */
 tpcf_status tpcf_set_shard(tpcf_ctx* ctx, int32_t shard_index, int32_t shard_count);
 

@@ -203,3 +203,20 @@ def test_batch_matches_single_calls(tpcf, oracle, ctx):
     for (i, j), r in zip(tasks, outs):
         can = canon(oracle, oracle.SHEAR, cats[i][0], cats[j][1], bins)
         assert_parity(r, can)
+
+
+def test_cell_size_autotune_keeps_results(tpcf, oracle):
+    at = __import__("importlib").import_module("2pcf_b200.autotune")
+    L, S = uniform_shear(3000, 4000, 400.0, 88)
+    lens = [tpcf.LensCatalog(x=L["x"], y=L["y"], val=L["val"], w=L["w"], z=L["z"])]
+    shp = [tpcf.ShapeCatalog(x=S["x"], y=S["y"], e1=S["e1"], e2=S["e2"], w=S["w"], z=S["z"], m=S["m"])]
+    bins = tpcf.create_bins(1.0, 80.0, 12)
+    ctx = tpcf.Context(0)
+    timing = at.autotune_cell_size(lens, shp, [(0, 0)], bins, ctx, divisors=(8, 16, 48))
+    assert set(timing) == {8, 16, 48} and ctx.cell_size == bins.x_max / min(timing, key=timing.get)
+    can = oracle.canon_pairs(oracle.SHEAR, L, S, bins.bin_edges_sq)
+    for d in (5, 16, 64):
+        ctx.set_cell_size(bins.x_max / d)
+        r = tpcf.batch_shear_2pcf(lens, shp, [(0, 0)], bins, ctx=ctx)[0]
+        assert_parity(r, can)
+    ctx.close()
