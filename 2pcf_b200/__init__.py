@@ -87,6 +87,15 @@ class Binning:
         return Bins(int(self.n_bin), int(self.spacing), float(self.x_min), float(self.x_max),
                     float(self.ihs_theta))
 
+    @property
+    def chord_edges_sq(self) -> np.ndarray:
+        """Squared chords (2 sin(e/2))^2 of the edges (radians): the bin rule
+        of the spherical kernels (tpcf_chord_edges)."""
+        out = np.zeros(self.n_bin + 1)
+        cb = self.c_struct()
+        _check(lib().tpcf_chord_edges(C.byref(cb), out.ctypes.data))
+        return out
+
 
 def create_bins(x_min, x_max, n_bin, spacing=LOG_BINNING, p=1.0) -> Binning:
     """create_bins(x_min, x_max, n_bin, p, spacing) of src/utils.f90:139-230."""
@@ -115,6 +124,7 @@ class Context:
         _check(lib().tpcf_create(C.byref(self._h), int(device), C.byref(o)))
         self.device = device
         self.cell_size = float(cell_size)
+        self.spherical = False
 
     @property
     def handle(self):
@@ -141,6 +151,11 @@ class Context:
         """Grid cell side for later calls (0 = theta_max/16)."""
         _check(lib().tpcf_set_cell_size(self._h, float(cell_size)), self._h)
         self.cell_size = float(cell_size)
+
+    def set_spherical(self, on: bool):
+        """Positions (longitude, latitude) and bins in radians for later calls."""
+        _check(lib().tpcf_set_spherical(self._h, int(bool(on))), self._h)
+        self.spherical = bool(on)
 
     def set_shard(self, index: int, count: int):
         """Compute only work items i % count == index (sums become partial)."""
@@ -272,6 +287,24 @@ def _resolve_ctx(ctx):
     return ctx if ctx is not None else default_context(0)
 
 
+def _coords(ctx, spherical_coords):
+    """spherical_coords of the reference's calls: x, y are longitude and
+    latitude in radians, the bins angles in radians."""
+    if bool(spherical_coords) != ctx.spherical:
+        ctx.set_spherical(bool(spherical_coords))
+
+
+def unit_vectors(lam, phi, ctx: Context = None):
+    """(hi, lo) [n][3] FP32 parts of the unit vectors the spherical kernels use
+    (tpcf_unit_vectors)."""
+    ctx = _resolve_ctx(ctx)
+    a, b = _Arr(lam), _Arr(phi)
+    hi = np.zeros((a.n, 3), np.float32)
+    lo = np.zeros((a.n, 3), np.float32)
+    _check(lib().tpcf_unit_vectors(ctx.handle, a.ptr, b.ptr, a.n, hi.ctypes.data, lo.ctypes.data), ctx.handle)
+    return hi, lo
+
+
 # -------------------------------------------------------------- pair sums ----
 def tangential_shear_tpcf(x_A, y_A, z_A, val_A, weight_A, x_B, y_B, z_B, e1_B, e2_B, weight_B, m_B,
                           bins: Binning, spherical_coords=False, num_threads=None,
@@ -283,10 +316,9 @@ def tangential_shear_tpcf(x_A, y_A, z_A, val_A, weight_A, x_B, y_B, z_B, e1_B, e
     are [n_A][n_bin] (the memory layout of the reference's (n_bin, n_A)).
     ``num_threads`` is accepted and ignored; ``use_kd_tree`` selects the cell
     grid (True) or the all-pairs scan (False) when ``ctx`` is not given."""
-    if spherical_coords:
-        raise TPCFError(6, "spherical coordinates are not supported")
     if ctx is None:
         ctx = default_context(0) if use_kd_tree else Context(0, use_grid=False, verbose=verbose)
+    _coords(ctx, spherical_coords)
     A = [_Arr(a) for a in (x_A, y_A, z_A, val_A, weight_A)]
     B = [_Arr(a) for a in (x_B, y_B, z_B, e1_B, e2_B, weight_B, m_B)]
     P = _Arr(patch_A, np.int32)
@@ -306,10 +338,9 @@ def scalar_kappa_tpcf(x_A, y_A, val_A, w_A, x_B, y_B, kappa_E, kappa_B, w_B, bin
                       calculate_marks=True, patch_A=None, n_patch=0, lens_sums=False,
                       ctx: Context = None):
     """scalar_kappa_tpcf (src/tpcf.f90:380-545) on the GPU."""
-    if spherical_coords:
-        raise TPCFError(6, "spherical coordinates are not supported")
     if ctx is None:
         ctx = default_context(0) if use_kd_tree else Context(0, use_grid=False, verbose=verbose)
+    _coords(ctx, spherical_coords)
     A = [_Arr(a) for a in (x_A, y_A, val_A, w_A)]
     B = [_Arr(a) for a in (x_B, y_B, kappa_E, kappa_B, w_B)]
     P = _Arr(patch_A, np.int32)
@@ -341,10 +372,11 @@ def kappa_2pcf(field: LensingSurveyField, bins: Binning, spherical_coords=False,
 
 def batch_shear_2pcf(lenses: Sequence[LensCatalog], shapes: Sequence[ShapeCatalog],
                      tasks: Sequence[tuple], bins: Binning, lens_patches=None, n_patch=0,
-                     marks=False, lens_sums=False, ctx: Context = None):
+                     marks=False, lens_sums=False, spherical_coords=False, ctx: Context = None):
     """All (lens catalogue, shape catalogue) tasks in one persistent launch
     (tpcf_batch_shear_scalar).  ``lens_patches[i]`` labels lens catalogue i."""
     ctx = _resolve_ctx(ctx)
+    _coords(ctx, spherical_coords)
     keep = []
     lc = (LensCat * len(lenses))()
     for i, L in enumerate(lenses):
@@ -436,6 +468,7 @@ def tangential_shear_adjoint(x_A, y_A, z_A, val_A, weight_A, x_B, y_B, z_B, e1_B
     inputs computed with lens_raw=True.  Returns a dict of gradients w.r.t.
     val_A, w_A, e1_B, e2_B, w_B, m_B (float32 arrays)."""
     ctx = _resolve_ctx(ctx)
+    _coords(ctx, False)
     A = [_Arr(a) for a in (x_A, y_A, z_A, val_A, weight_A)]
     B = [_Arr(a) for a in (x_B, y_B, z_B, e1_B, e2_B, weight_B, m_B)]
     nA, nB = A[0].n, B[0].n

@@ -95,6 +95,9 @@ def lib():
     _sig(L, "tpcf_measure_fp32_peak", st, [vp, C.POINTER(C.c_double)])
     _sig(L, "tpcf_canonical_edges", st, [C.POINTER(Bins), vp, vp])
     _sig(L, "tpcf_bin_centers", st, [C.POINTER(Bins), vp])
+    _sig(L, "tpcf_set_spherical", st, [vp, i32])
+    _sig(L, "tpcf_chord_edges", st, [C.POINTER(Bins), vp])
+    _sig(L, "tpcf_unit_vectors", st, [vp, vp, vp, i64, vp, vp])
     _sig(L, "tpcf_shear_scalar", st, [vp] + [vp] * 5 + [i64] + [vp] * 7 + [i64] +
          [C.POINTER(Bins), vp, i32, C.POINTER(Result)])
     _sig(L, "tpcf_scalar_scalar", st, [vp] + [vp] * 4 + [i64] + [vp] * 5 + [i64] +

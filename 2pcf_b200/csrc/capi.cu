@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "sph_canon.cuh"
 #include "tpcf_b200.h"
 #include "tpcf_internal.cuh"
 #include "tpcf_kernels.h"
@@ -207,7 +208,12 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
   std::vector<double> e(nb + 1), e2(nb + 1);
   tpcf_status bs = canonical_edges(bins, e.data(), e2.data());
   if (bs != TPCF_OK) throw Failure(bs, "invalid binning");
-  if (c->opts.spherical) throw Failure(TPCF_ERR_NOT_SUPPORTED, "spherical coordinates are not supported");
+  const bool sph = c->opts.spherical != 0;
+  if (sph) {  // squared chords (2 sin(e/2))^2: the same bins on the unit sphere
+    for (int i = 0; i <= nb; ++i) e2[i] = canon_chord2(e[i]);
+    for (int i = 0; i < nb; ++i)
+      if (!(e2[i + 1] > e2[i]) || !(e[nb] <= 3.14159265358979)) throw Failure(TPCF_ERR_INVALID_ARG, "invalid binning");
+  }
   if (c->opts.shard_count > 1 && (c->opts.shard_index < 0 || c->opts.shard_index >= c->opts.shard_count))
     throw Failure(TPCF_ERR_INVALID_ARG, "shard_index outside [0, shard_count)");
   const bool sharded = c->opts.shard_count > 1;
@@ -236,6 +242,26 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     s.f1 = stage(c, s.f1, s.n); s.f2 = stage(c, s.f2, s.n); s.w = stage(c, s.w, s.n); s.m = stage(c, s.m, s.n);
   }
 
+  // ---- sphere: keep the input longitudes for the unit vectors; the grid and
+  // the lens order use longitudes reduced to [0, 2 pi)
+  std::vector<const float*> lamL(nL, nullptr), lamS(nS, nullptr);
+  if (sph) {
+    for (int i = 0; i < nL; ++i) {
+      lamL[i] = lens[i].x;
+      if (lens[i].n <= 0) continue;
+      float* xr = (float*)ws_alloc(c, sizeof(float) * lens[i].n);
+      counted(c, launch_wrap_lambda(lens[i].x, lens[i].n, xr, st), "wrap lambda");
+      lens[i].x = xr;
+    }
+    for (int i = 0; i < nS; ++i) {
+      lamS[i] = srcs[i].x;
+      if (srcs[i].n <= 0) continue;
+      float* xr = (float*)ws_alloc(c, sizeof(float) * srcs[i].n);
+      counted(c, launch_wrap_lambda(srcs[i].x, srcs[i].n, xr, st), "wrap lambda");
+      srcs[i].x = xr;
+    }
+  }
+
   // ---- bounding boxes, z ranges, max |m|, counts, patch ranges (one sync)
   const int ncat = nL + nS;
   int* box_ord = (int*)ws_alloc(c, sizeof(int) * 8 * ncat);
@@ -261,6 +287,11 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     if (lens[i].patch && hcnt[i] > 0 && (hpr[2 * i] < 0 || hpr[2 * i + 1] >= n_patch))
       throw Failure(TPCF_ERR_INVALID_ARG, "patch label outside [0, n_patch)");
 
+  if (sph)
+    for (int i = 0; i < ncat; ++i)
+      if (hcnt[i] > 0 && (hbox[8 * i + 1] < -1.57079637f || hbox[8 * i + 3] > 1.57079637f))
+        throw Failure(TPCF_ERR_INVALID_ARG, "latitude outside [-pi/2, pi/2] (spherical positions are radians)");
+
   // ---- kernel configuration
   bool has_m = false, has_z = false;
   for (int i = 0; i < nS; ++i)  // K differs from w only where some m != 0
@@ -272,7 +303,8 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
       if (lz_max > sz_min) has_z = true;
     }
   }
-  const bool logb = bins->spacing == TPCF_LOG;
+  // On the sphere log binning maps theta^2 by a series valid for chords <= 0.25.
+  const bool logb = bins->spacing == TPCF_LOG && (!sph || e2[nb] <= 0.0625);
   const int qa = has_m ? 6 : 5;
   int bt = 128;
   while (bt > 32 && (size_t)nb * qa * bt * 4 > 100 * 1024) bt /= 2;
@@ -289,6 +321,10 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     const int n_valid = (int)hcnt[nL + i];
     float x0 = n_valid ? b[0] : 0.f, y0 = n_valid ? b[1] : 0.f;
     float ex = n_valid ? b[2] - b[0] : 0.f, ey = n_valid ? b[3] - b[1] : 0.f;
+    if (sph) {  // longitude cells cover the whole circle
+      x0 = 0.f;
+      ex = 6.28318548f;
+    }
     double cell = c->opts.cell_size > 0 ? c->opts.cell_size : Rd / 16.0;
     const double span = std::max((double)ex, (double)ey);
     if (!c->opts.use_grid) cell = span * 2.0 + 1.0;
@@ -301,7 +337,8 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     g.x0 = x0; g.y0 = y0; g.cell = (float)cell; g.inv_cell = (float)(1.0 / cell);
     g.ncx = ncx; g.ncy = ncy; g.n_valid = n_valid;
     int* cs = (int*)ws_alloc(c, sizeof(int) * (ncells + 1));
-    SrcRec* rec = (SrcRec*)ws_alloc(c, sizeof(SrcRec) * std::max(n_valid, 1));
+    SrcRec* rec = sph ? nullptr : (SrcRec*)ws_alloc(c, sizeof(SrcRec) * std::max(n_valid, 1));
+    SrcRecS* recs = sph ? (SrcRecS*)ws_alloc(c, sizeof(SrcRecS) * std::max(n_valid, 1)) : nullptr;
     if (s.n > 0) {
       unsigned* k0 = (unsigned*)ws_alloc(c, sizeof(unsigned) * s.n);
       unsigned* k1 = (unsigned*)ws_alloc(c, sizeof(unsigned) * s.n);
@@ -317,12 +354,17 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
       void* tmp = ws_alloc(c, tb);
       check(sort_pairs_u32(tmp, tb, k0, k1, i0, i1, (int)s.n, end_bit, st), "sort sources");
       counted(c, launch_cell_start(k1, s.n, ncells, mb, cs, st), "cell start");
-      counted(c, launch_src_gather(i1, n_valid, mode, s.x, s.y, s.z, s.f1, s.f2, s.w, s.m, rec, st), "src gather");
+      if (sph)
+        counted(c, launch_src_gather_sph(i1, n_valid, mode, lamS[i], s.y, s.z, s.f1, s.f2, s.w, s.m, recs, st),
+                "src gather");
+      else
+        counted(c, launch_src_gather(i1, n_valid, mode, s.x, s.y, s.z, s.f1, s.f2, s.w, s.m, rec, st), "src gather");
     } else {
       check(cudaMemsetAsync(cs, 0, sizeof(int) * (ncells + 1), st), "memset cells");
     }
     g.cell_start = cs;
     g.rec = rec;
+    g.recs = recs;
   }
   float margin = 0.f;
   for (int i = 0; i < ncat; ++i) {
@@ -332,6 +374,7 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
   }
   float maxcell = 0.f;
   for (auto& g : grids) maxcell = std::max(maxcell, g.cell);
+  if (sph) margin = (float)(2.0 * M_PI + M_PI);  // reduced longitudes and latitudes
   margin = (float)(1e-5 * (margin + Rd) + 1e-4 * maxcell);
 
   // ---- lens catalogues: sort by (patch, Morton), groups of <= bt lenses
@@ -381,12 +424,18 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     B.d_patch_groups = (int*)ws_alloc(c, sizeof(int) * (n_patch_eff + 1));
     check(cudaMemcpyAsync(B.d_patch_groups, B.patch_groups.data(), sizeof(int) * (n_patch_eff + 1),
                           cudaMemcpyHostToDevice, st), "H2D patch groups");
+    float4* pos = nullptr;
+    if (sph) {
+      pos = (float4*)ws_alloc(c, sizeof(float4) * 2 * std::max(B.n_valid, 1));
+      if (B.n_valid > 0) counted(c, launch_lens_pos_sph(B.perm, B.n_valid, lamL[i], l.y, pos, st), "lens pos");
+    }
     B.group_box = (float4*)ws_alloc(c, sizeof(float4) * std::max(B.n_groups, 1));
     counted(c, launch_group_box(B.rec, B.group_start, B.n_groups, B.group_box, st), "group box");
     check(cudaStreamSynchronize(st), "sync groups");  // host vectors above must outlive the async copies
     LensDesc& d = ldesc[i];
     d.rec = B.rec; d.z = B.zs; d.group_start = B.group_start; d.group_box = B.group_box;
     d.n_valid = B.n_valid; d.n_groups = B.n_groups;
+    d.pos = pos;
   }
 
   // ---- tasks and work items
@@ -437,7 +486,11 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     unsigned long long* ck1 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * n_items);
     int* o0 = (int*)ws_alloc(c, sizeof(int) * n_items);
     int* o1 = (int*)ws_alloc(c, sizeof(int) * n_items);
-    counted(c, launch_item_cost(d_items0, n_items, d_tasks, d_lens, d_grids, R, margin, ck0, o0, st), "item cost");
+    if (sph)
+      counted(c, launch_item_cost_sph(d_items0, n_items, d_tasks, d_lens, d_grids, R, margin, ck0, o0, st),
+              "item cost");
+    else
+      counted(c, launch_item_cost(d_items0, n_items, d_tasks, d_lens, d_grids, R, margin, ck0, o0, st), "item cost");
     size_t tb = 0;
     check(sort_pairs_u64_desc(nullptr, tb, ck0, ck1, o0, o1, n_items, st), "sort size");
     void* tmp = ws_alloc(c, tb);
@@ -453,8 +506,8 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     P.tasks = d_tasks; P.lenses = d_lens; P.grids = d_grids; P.items = d_items; P.n_items = n_run;
     P.nb = nb; P.queue_head = head; P.item_sums = item_sums; P.lens_acc = lens_acc; P.err = err;
     P.e2 = d_e2; P.e2f = d_e2f; P.R = R; P.margin = margin;
-    if (logb) {
-      const double l0 = std::log2(e2[0]), l1 = std::log2(e2[nb]);
+    if (logb) {  // t = log2(theta^2) A + B (planar: theta^2 = d2)
+      const double l0 = std::log2(e[0] * e[0]), l1 = std::log2(e[nb] * e[nb]);
       const double A = nb / (l1 - l0);
       P.binA = (float)A;
       P.binB = (float)(-l0 * A);
@@ -471,7 +524,10 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     }
     const char* var_env = std::getenv("TPCF_PAIR_VARIANT");
     const int variant = var_env ? std::atoi(var_env) : 0;
-    counted(c, launch_pairs(P, mode, has_m, has_z, logb, bt, variant, c->num_sms, st, &grid), "pair kernel");
+    if (sph)
+      counted(c, launch_pairs_sph(P, mode, has_m, has_z, logb, bt, c->num_sms, st, &grid), "pair kernel");
+    else
+      counted(c, launch_pairs(P, mode, has_m, has_z, logb, bt, variant, c->num_sms, st, &grid), "pair kernel");
     if (c->time_pairs) {
       check(cudaEventRecord(ev1, st), "event record");
       c->pending_ev0 = ev0;
@@ -669,6 +725,41 @@ tpcf_status tpcf_set_cell_size(tpcf_ctx* c, double cell_size) {
   if (!c || !(cell_size >= 0) || !std::isfinite(cell_size)) return TPCF_ERR_INVALID_ARG;
   c->opts.cell_size = cell_size;
   return TPCF_OK;
+}
+
+tpcf_status tpcf_set_spherical(tpcf_ctx* c, int32_t on) {
+  if (!c || (on != 0 && on != 1)) return TPCF_ERR_INVALID_ARG;
+  c->opts.spherical = on;
+  return TPCF_OK;
+}
+
+tpcf_status tpcf_chord_edges(const tpcf_bins* bins, double* chord_sq) {
+  if (!bins || !chord_sq) return TPCF_ERR_INVALID_ARG;
+  std::vector<double> e(kMaxBins + 1), e2(kMaxBins + 1);
+  tpcf_status s = canonical_edges(bins, e.data(), e2.data());
+  if (s != TPCF_OK) return s;
+  if (!(e[bins->n_bin] <= 3.14159265358979)) return TPCF_ERR_INVALID_ARG;
+  for (int i = 0; i <= bins->n_bin; ++i) chord_sq[i] = canon_chord2(e[i]);
+  return TPCF_OK;
+}
+
+tpcf_status tpcf_unit_vectors(tpcf_ctx* c, const float* lam, const float* phi, int64_t n, float* hi, float* lo) {
+  if (!c || n < 0 || (n > 0 && (!lam || !phi || !hi || !lo))) return TPCF_ERR_INVALID_ARG;
+  try {
+    begin_call(c);
+    if (n == 0) return TPCF_OK;
+    const float* dl = stage(c, lam, n);
+    const float* dp = stage(c, phi, n);
+    float* dh = is_device_ptr(hi) ? hi : (float*)ws_alloc(c, sizeof(float) * 3 * (size_t)n);
+    float* dlo = is_device_ptr(lo) ? lo : (float*)ws_alloc(c, sizeof(float) * 3 * (size_t)n);
+    counted(c, launch_unit_vectors(dl, dp, n, dh, dlo, c->stream), "unit vectors");
+    if (dh != hi) copy_out(c, hi, dh, sizeof(float) * 3 * (size_t)n);
+    if (dlo != lo) copy_out(c, lo, dlo, sizeof(float) * 3 * (size_t)n);
+    check(cudaStreamSynchronize(c->stream), "sync unit vectors");
+    return TPCF_OK;
+  } catch (const Failure& f) {
+    return fail(c, f);
+  }
 }
 
 tpcf_status tpcf_set_shard(tpcf_ctx* c, int32_t index, int32_t count) {

@@ -24,6 +24,7 @@
 #include <cub/cub.cuh>
 #include <cstdio>
 
+#include "pair_hist.cuh"
 #include "tpcf_device.cuh"
 #include "tpcf_internal.cuh"
 #include "tpcf_kernels.h"
@@ -153,13 +154,6 @@ __device__ __forceinline__ void pair_terms(float lx, float ly, const float4 a, f
   }
 }
 
-template <int QA, int NC>
-__device__ __forceinline__ void hist_add(float* hcol, int bin, const float* v) {
-  float* h = hcol + bin * (QA * NC);
-#pragma unroll
-  for (int q = 0; q < QA; ++q) h[q * NC] += v[q];
-}
-
 // Class 1: every pair of the chunk is in bin `blo`.
 template <int MODE, bool HAS_M, bool LOGB, int NC, int QA>
 __device__ __forceinline__ void chunk_single(const SrcRec* __restrict__ S, int cnt, float lx, float ly, int cls,
@@ -233,47 +227,6 @@ __device__ __forceinline__ void chunk_dual(const SrcRec* __restrict__ S, int cnt
   }
   if (blo >= 0) hist_add<QA, NC>(hcol, blo, lo);
   if (blo + 1 < C.nb) hist_add<QA, NC>(hcol, blo + 1, hi);
-}
-
-// Fold the FP32 histogram into FP64 (block sums and, optionally, per-lens
-// sums), then clear this thread's column.  Called by all threads.
-// Fold the FP32 histogram into FP64: the block sums (times the lens factors
-// val*w or w) and, when lens_col is set, this thread's per-lens FP64 column.
-// Then clear this thread's column.  Called by all threads.
-template <int QA, int BT>
-__device__ __forceinline__ void flush_hist(float* hist, double* bsum, const double* fvw, const double* fw,
-                                           int nb, double* lens_col, size_t lens_stride, bool first) {
-  const int tid = threadIdx.x;
-  __syncthreads();
-  float* hcol = hist + tid;
-  if (lens_col) {
-    for (int q = 0; q < kQ; ++q) {
-      const int qa = (q == QK && QA == 5) ? QW : q;
-      for (int b = 0; b < nb; ++b) {
-        const double v = (double)hcol[(b * QA + qa) * BT];
-        double* p = lens_col + (size_t)(q * nb + b) * lens_stride;
-        *p = first ? v : *p + v;
-      }
-    }
-  }
-  for (int e = tid; e < kQ * nb; e += BT) {
-    const int q = e / nb, b = e - q * nb;
-    if (q == QK && QA == 5) continue;  // K == w: copied from the w row at item end
-    const float* row = hist + (b * QA + q) * BT;
-    const double* f = (q == QGT || q == QGX) ? fvw : fw;
-    double s = 0.0;
-    if (q == QN) {
-      for (int l = 0; l < BT; ++l) s += (double)row[(l + tid) & (BT - 1)];
-    } else {
-      for (int l = 0; l < BT; ++l) {
-        const int c = (l + tid) & (BT - 1);
-        s = fma((double)row[c], f[c], s);
-      }
-    }
-    bsum[e] += s;
-  }
-  __syncthreads();
-  for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
 }
 
 #ifdef TPCF_MODE_STATS

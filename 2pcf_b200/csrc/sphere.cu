@@ -1,0 +1,727 @@
+// sphere.cu -- pair sums on the sphere: the spherical_coords branch of
+// tangential_shear_tpcf / scalar_kappa_tpcf (src/tpcf.f90:297-359, with
+// distance_sphere src/utils.f90:512-528 and angles_sphere :618-639).
+//
+// Positions are FP32 (lambda, phi) in radians.  Each object becomes its unit
+// vector u, computed in FP64 by canon_sincos (sph_canon.cuh) and split into
+// FP32 hi + lo parts.  For a pair (lens A, source B):
+//   chord^2  c^2 = |u_B - u_A|^2, binned against (2 sin(e_i/2))^2 of the FP64
+//            angle edges e_i (monotone in the angle, so the same bins);
+//   angle    theta = 2 asin(c/2) (the reference's acos of the dot product);
+//   position angle at the lens, A = (u_B - u_A).east_A and
+//            B = (u_B - u_A).north_A.  These are the numerators of
+//            angles_sphere, so cos 2phi = (A^2 - B^2)/(A^2 + B^2) and
+//            sin 2phi = 2AB/(A^2 + B^2), the same as 2 cs1^2 - 1, 2 cs1 cs2.
+// The pair arithmetic is FP32 on hi + lo differences (relative error ~1e-7
+// at any separation).  The FP64 guard band re-bins a pair by the canonical
+// rule: u = hi + lo in FP64, c^2 = (dx^2 + dy^2) + dz^2 rounded as written.
+//
+// Pruning: a cell grid over (lambda reduced to [0, 2 pi), phi).  The rows of a
+// work item are the phi rows within R of the lens box (angular distance
+// >= |dphi|).  In each row the cells lie within the lambda reach
+// asin(sin R / cos phi*) of the box, phi* being its largest |phi|, taken
+// modulo 2 pi as up to three disjoint cell runs.  A pole within reach scans
+// the whole row.  The reference aborts near poles and the prime meridian
+// (src/kdtree.f90:398-413); here every position is valid.
+
+#include <cstdio>
+
+#include "pair_hist.cuh"
+#include "sph_canon.cuh"
+#include "tpcf_device.cuh"
+#include "tpcf_internal.cuh"
+#include "tpcf_kernels.h"
+
+namespace tpcf {
+
+// --------------------------------------------------- canonical unit vector --
+// u = (cos phi cos lambda, cos phi sin lambda, sin phi), hi = fl32(u),
+// lo = fl32(u - hi).
+__device__ __forceinline__ void canon_unit(float lam, float phi, float4& hi, float4& lo) {
+  double sl, cl, sp, cp;
+  canon_sincos((double)lam, sl, cl);
+  canon_sincos((double)phi, sp, cp);
+  const double ux = __dmul_rn(cp, cl), uy = __dmul_rn(cp, sl), uz = sp;
+  hi = make_float4(__double2float_rn(ux), __double2float_rn(uy), __double2float_rn(uz), 0.f);
+  lo = make_float4(__double2float_rn(__dsub_rn(ux, (double)hi.x)), __double2float_rn(__dsub_rn(uy, (double)hi.y)),
+                   __double2float_rn(__dsub_rn(uz, (double)hi.z)), 0.f);
+}
+
+// Canonical FP64 bin of a pair on the sphere (the guard-band path).
+__device__ __forceinline__ int slow_bin_s(float4 ha, float4 la, float4 hb, float4 lb, const double* e2,
+                                              int nb) {
+  const double dx = __dsub_rn(__dadd_rn((double)hb.x, (double)lb.x), __dadd_rn((double)ha.x, (double)la.x));
+  const double dy = __dsub_rn(__dadd_rn((double)hb.y, (double)lb.y), __dadd_rn((double)ha.y, (double)la.y));
+  const double dz = __dsub_rn(__dadd_rn((double)hb.z, (double)lb.z), __dadd_rn((double)ha.z, (double)la.z));
+  const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+  if (!(d2 >= e2[0]) || d2 > e2[nb]) return -1;
+  if (d2 == e2[nb]) return nb - 1;
+  int lo = 0, hi = nb;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (d2 >= e2[mid]) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// ------------------------------------------------------------ pair terms ----
+// One lens: unit vector hi/lo and its local east/north basis.
+struct LensS {
+  float4 h, l;
+  float ex, ey, nx, ny, nz;
+};
+
+__device__ __forceinline__ LensS lens_frame(float4 h, float4 l) {
+  LensS L;
+  L.h = h;
+  L.l = l;
+  const double ux = (double)h.x + (double)l.x, uy = (double)h.y + (double)l.y, uz = (double)h.z + (double)l.z;
+  const double rho = sqrt(ux * ux + uy * uy);
+  if (rho > 0.0) {
+    L.ex = (float)(-uy / rho); L.ey = (float)(ux / rho);
+    L.nx = (float)(-uz * ux / rho); L.ny = (float)(-uz * uy / rho); L.nz = (float)rho;
+  } else {  // exactly on a pole: any tangent basis
+    L.ex = 0.f; L.ey = 1.f; L.nx = uz > 0 ? -1.f : 1.f; L.ny = 0.f; L.nz = 0.f;
+  }
+  return L;
+}
+
+// theta = 2 asin(c/2) from c^2 and c.  SMALL (c <= 0.25): the series
+// c (1 + c^2/24 + 3 c^4/640 + 5 c^6/7168), truncation < 2e-9 relative.
+template <bool SMALL>
+__device__ __forceinline__ float chord_theta(float d2, float c) {
+  if (SMALL) return c * fmaf(d2, fmaf(d2, fmaf(d2, 6.9754464e-4f, 4.6875e-3f), 4.16666679e-2f), 1.f);
+  return 2.f * asinf(fminf(0.5f * c, 1.f));
+}
+// theta^2 / c^2 by the same series (log-spaced binning in theta^2).
+__device__ __forceinline__ float chord_theta2(float d2) {
+  const float g = fmaf(d2, fmaf(d2, fmaf(d2, 6.9754464e-4f, 4.6875e-3f), 4.16666679e-2f), 1.f);
+  return d2 * g * g;
+}
+
+// d2 = c^2, th = theta, r = 1/(A^2+B^2), X = p P + q U, Y = q P - p U with
+// P = A^2 - B^2, U = 2AB (shear); scalar: r = 1, X = p, Y = q.
+template <int MODE, bool SMALL>
+__device__ __forceinline__ void sph_terms(const LensS& L, const float4 a, const float4 b, float& d2, float& th,
+                                          float& r, float& X, float& Y) {
+  const float dx = (a.x - L.h.x) + (b.x - L.l.x);
+  const float dy = (a.y - L.h.y) + (b.y - L.l.y);
+  const float dz = (a.z - L.h.z) + (b.z - L.l.z);
+  d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+  // series path: binned pairs have d2 > 0; otherwise c = 0 exactly at d2 = 0
+  const float c = SMALL ? d2 * rsqrtf(d2) : sqrtf(d2);
+  th = chord_theta<SMALL>(d2, c);
+  if (MODE == 0) {
+    const float A = fmaf(dy, L.ey, dx * L.ex);
+    const float B = fmaf(dz, L.nz, fmaf(dy, L.ny, dx * L.nx));
+    const float A2 = A * A;
+    const float P = fmaf(-B, B, A2);
+    const float s = fmaf(B, B, A2);
+    const float ab = A * B;
+    const float U = ab + ab;
+    r = __fdividef(1.f, s);
+    X = fmaf(a.w, P, b.w * U);
+    Y = fmaf(b.w, P, -(a.w * U));
+  } else {
+    r = 1.f;
+    X = a.w;
+    Y = b.w;
+  }
+}
+
+template <bool LOGB>
+__device__ __forceinline__ int pair_bin_s(float d2, const LensS& L, const float4 a, const float4 b,
+                                          const BinCtx& C) {
+  if (LOGB) {
+    const float t = fmaf(__log2f(chord_theta2(d2)), C.A, C.B);
+    const float tf = floorf(t);
+    const float fr = t - tf;
+    int bin = __float2int_rz(tf);
+    if (fr < C.eps || fr > C.one_m_eps) bin = slow_bin_s(L.h, L.l, a, b, C.e2s, C.nb);
+    return bin;
+  } else {
+    if (d2 < C.lo_g || d2 > C.hi_g) return -1;
+    int lo = 0, hi = C.nb;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (d2 >= C.e2f[mid]) lo = mid; else hi = mid;
+    }
+    const float el = C.e2f[lo], eh = C.e2f[lo + 1];
+    if (d2 <= el * (1.f + C.eps) || d2 >= eh * (1.f - C.eps)) lo = slow_bin_s(L.h, L.l, a, b, C.e2s, C.nb);
+    return lo;
+  }
+}
+
+// Conservative bin class of a 3-D box (min mn, max mx of the chunk's hi parts,
+// already widened by the hi/lo split error) for one lens; classes as in the
+// planar kernel.
+template <bool LOGB, bool HAS_Z>
+__device__ __forceinline__ int classify_s(const LensS& L, const float4 mn, const float4 mx, const BinCtx& C,
+                                          int& blo) {
+  const float dxl = fmaxf(fmaxf(mn.x - L.h.x, L.h.x - mx.x), 0.f);
+  const float dyl = fmaxf(fmaxf(mn.y - L.h.y, L.h.y - mx.y), 0.f);
+  const float dzl = fmaxf(fmaxf(mn.z - L.h.z, L.h.z - mx.z), 0.f);
+  const float dxh = fmaxf(L.h.x - mn.x, mx.x - L.h.x);
+  const float dyh = fmaxf(L.h.y - mn.y, mx.y - L.h.y);
+  const float dzh = fmaxf(L.h.z - mn.z, mx.z - L.h.z);
+  const float dmin2 = fmaf(dzl, dzl, fmaf(dyl, dyl, dxl * dxl));
+  const float dmax2 = fmaf(dzh, dzh, fmaf(dyh, dyh, dxh * dxh));
+  int b0, b1;
+  if (LOGB) {
+    b0 = __float2int_rd(fmaf(__log2f(chord_theta2(dmin2)), C.A, C.B) - C.eps);
+    b1 = __float2int_rd(fmaf(__log2f(chord_theta2(dmax2)), C.A, C.B) + C.eps);
+  } else {
+    b0 = edge_index_f32(dmin2 * (1.f - C.eps), C.e2f, C.nb);
+    b1 = edge_index_f32(dmax2 * (1.f + C.eps), C.e2f, C.nb);
+  }
+  if (b1 < 0 || b0 >= C.nb) return 0;
+  blo = b0;
+  if (HAS_Z) return 3;
+  if (b0 == b1) return 1;
+  if (b1 == b0 + 1) return 2;
+  return 3;
+}
+
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, bool SMALL, int NC, int QA>
+__device__ __forceinline__ void do_pair_s(const LensS& L, float lz, const SrcRecS& s, float* __restrict__ hcol,
+                                          const BinCtx& C) {
+  if (HAS_Z) {
+    if (lz > s.c.z) return;  // src/tpcf.f90:322
+  }
+  float d2, th, r, X, Y;
+  sph_terms<MODE, SMALL>(L, s.a, s.b, d2, th, r, X, Y);
+  const int bin = pair_bin_s<LOGB>(d2, L, s.a, s.b, C);
+  if ((unsigned)bin >= (unsigned)C.nb) return;
+  float* h = hcol + bin * (QA * NC);
+  h[QGT * NC] = fmaf(r, X, h[QGT * NC]);
+  h[QGX * NC] = fmaf(r, Y, h[QGX * NC]);
+  h[QW * NC] += s.c.x;
+  h[QDW * NC] = fmaf(th, s.c.x, h[QDW * NC]);
+  h[QN * NC] += 1.0f;
+  if (MODE == 0 && HAS_M) h[QK * NC] += s.c.y;
+}
+
+template <int MODE, bool HAS_M, bool SMALL, int NC, int QA>
+__device__ __forceinline__ void chunk_single_s(const SrcRecS* __restrict__ S, int cnt, const LensS& L, int cls,
+                                               int blo, float* __restrict__ hcol) {
+  float acc[QA];
+#pragma unroll
+  for (int q = 0; q < QA; ++q) acc[q] = 0.f;
+#pragma unroll 2
+  for (int j = 0; j < cnt; ++j) {
+    const float4 a = S[j].a, b = S[j].b, cc = S[j].c;
+    float d2, th, r, X, Y;
+    sph_terms<MODE, SMALL>(L, a, b, d2, th, r, X, Y);
+    acc[QGT] = fmaf(r, X, acc[QGT]);
+    acc[QGX] = fmaf(r, Y, acc[QGX]);
+    acc[QW] += cc.x;
+    acc[QDW] = fmaf(th, cc.x, acc[QDW]);
+    if (MODE == 0 && HAS_M) acc[QK] += cc.y;
+  }
+  acc[QN] = (float)cnt;
+  if (cls == 1) hist_add<QA, NC>(hcol, blo, acc);
+}
+
+template <int MODE, bool HAS_M, bool SMALL, int NC, int QA>
+__device__ __forceinline__ void chunk_dual_s(const SrcRecS* __restrict__ S, int cnt, const LensS& L, int cls,
+                                             int blo, float* __restrict__ hcol, const BinCtx& C) {
+  float tot[QA], hi[QA];
+#pragma unroll
+  for (int q = 0; q < QA; ++q) tot[q] = hi[q] = 0.f;
+  const float E = (cls == 2) ? C.e2f[blo + 1] : 3.0e38f;
+  const float gE = (cls == 2) ? E * C.eps_rel : 0.f;
+#pragma unroll 2
+  for (int j = 0; j < cnt; ++j) {
+    const float4 a = S[j].a, b = S[j].b, cc = S[j].c;
+    float d2, th, r, X, Y;
+    sph_terms<MODE, SMALL>(L, a, b, d2, th, r, X, Y);
+    const float t1 = r * X, t2 = r * Y;
+    bool up = d2 >= E;
+    if (fabsf(d2 - E) <= gE) {
+      const int cb = slow_bin_s(L.h, L.l, a, b, C.e2s, C.nb);
+      up = (cb == blo + 1) || (cb < 0 && blo + 1 == C.nb);
+    }
+    const float dw = th * cc.x;
+    tot[QGT] += t1;
+    tot[QGX] += t2;
+    tot[QW] += cc.x;
+    tot[QDW] += dw;
+    if (MODE == 0 && HAS_M) tot[QK] += cc.y;
+    if (up) {
+      hi[QGT] += t1;
+      hi[QGX] += t2;
+      hi[QW] += cc.x;
+      hi[QDW] += dw;
+      hi[QN] += 1.f;
+      if (MODE == 0 && HAS_M) hi[QK] += cc.y;
+    }
+  }
+  tot[QN] = (float)cnt;
+  if (cls == 0) return;
+  float lo[QA];
+#pragma unroll
+  for (int q = 0; q < QA; ++q) lo[q] = tot[q] - hi[q];
+  if (cls == 1) {
+    hist_add<QA, NC>(hcol, blo, tot);
+    return;
+  }
+  if (blo >= 0) hist_add<QA, NC>(hcol, blo, lo);
+  if (blo + 1 < C.nb) hist_add<QA, NC>(hcol, blo + 1, hi);
+}
+
+// ------------------------------------------------------------ cell runs -----
+constexpr float kTwoPiF = 6.28318548f;      // 2 pi rounded up to FP32
+constexpr int kRowsS = kMaxRows / 4;        // rows per chunk: 3 runs each fit kMaxRows
+
+// Lambda reach of a work item: full = every cell of a row, else the interval
+// [box.x - dl, box.z + dl] modulo 2 pi.
+__device__ __forceinline__ void sph_reach(const GridDesc& G, float4 box, float R, float m, float& dl, bool& full) {
+  const float ps = fmaxf(fabsf(box.y), fabsf(box.w)) + m;
+  full = false;
+  dl = 0.f;
+  if (ps + R >= 1.5707f) { full = true; return; }
+  const float sr = sinf(R) / cosf(ps);
+  if (!(sr < 0.999f)) { full = true; return; }
+  dl = asinf(sr) * 1.0001f + m;
+  if ((box.z - box.x) + 2.f * dl + 2.f * G.cell + 4.f * m >= 6.2831f) full = true;
+}
+
+// The runs of sorted sources in row cy whose cells may hold a source within R
+// of the box; returns how many (0..3).  The shifted intervals are more than
+// two cells apart, so no cell appears in two runs.
+__device__ __forceinline__ int sph_row_spans(const GridDesc& G, float4 box, float R, float m, int cy, float dl,
+                                             bool full, int2* out) {
+  const float ylo = G.y0 + (float)cy * G.cell - m;
+  const float yhi = G.y0 + (float)(cy + 1) * G.cell + m;
+  const float dyr = fmaxf(0.f, fmaxf(ylo - box.w, box.y - yhi));
+  if (dyr > R) return 0;
+  const int base = cy * G.ncx;
+  if (full) {
+    out[0] = make_int2(G.cell_start[base], G.cell_start[base + G.ncx]);
+    return 1;
+  }
+  const float a = box.x - dl, b = box.z + dl;
+  const float xmax = G.x0 + (float)G.ncx * G.cell;
+  int n = 0;
+#pragma unroll
+  for (int k = -1; k <= 1; ++k) {
+    const float s = (float)k * kTwoPiF;
+    if (b + s < G.x0 - m || a + s > xmax + m) continue;
+    const int cx0 = clamp_floor((a + s - G.x0) * G.inv_cell, 0, G.ncx - 1);
+    const int cx1 = clamp_floor((b + s - G.x0) * G.inv_cell, 0, G.ncx - 1);
+    out[n++] = make_int2(G.cell_start[base + cx0], G.cell_start[base + cx1 + 1]);
+  }
+  return n;
+}
+
+// ------------------------------------------------------------ the kernel ----
+struct SphSmem {
+  size_t tiles, hist, bsum, e2s, fvw, fw, e2f, span0, span1, tpref, subbox, mbar, misc, total;
+};
+__host__ __device__ inline size_t align_up_s(size_t v, size_t a) { return (v + a - 1) / a * a; }
+__host__ __device__ inline SphSmem sph_smem_layout(int nb, int qa, int bt) {
+  SphSmem s;
+  size_t o = 0;
+  s.tiles = o; o += 2 * kTile * sizeof(SrcRecS);
+  s.hist = o;  o += (size_t)nb * qa * bt * sizeof(float);
+  o = align_up_s(o, 16);
+  s.bsum = o;  o += (size_t)kQ * nb * sizeof(double);
+  s.e2s = o;   o += (size_t)(nb + 1) * sizeof(double);
+  s.fvw = o;   o += (size_t)bt * sizeof(double);
+  s.fw = o;    o += (size_t)bt * sizeof(double);
+  s.e2f = o;   o += (size_t)(nb + 1) * sizeof(float);
+  o = align_up_s(o, 16);
+  s.span0 = o; o += kMaxRows * sizeof(int);
+  s.span1 = o; o += kMaxRows * sizeof(int);
+  s.tpref = o; o += (kMaxRows + 1) * sizeof(int);
+  o = align_up_s(o, 16);
+  s.subbox = o; o += 2 * (kTile / 32) * sizeof(float4);
+  s.mbar = o;  o += 2 * sizeof(uint64_t);
+  s.misc = o;  o += 16;
+  s.total = align_up_s(o, 128);
+  return s;
+}
+
+// Persistent: each block takes (task, lens group) items from the queue and
+// streams the item's source runs through shared memory (bulk copies,
+// double-buffered, bounded waits), as the planar kernel does.
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT>
+__global__ void __launch_bounds__(BT) k_pairs_sph(const PairParams P) {
+  constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
+  constexpr int NW = BT / 32;
+  constexpr bool SMALL = LOGB;  // log spacing on the sphere is only chosen with chord(x_max) <= 0.25
+  const int nb = P.nb;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const SphSmem Ls = sph_smem_layout(nb, QA, BT);
+  SrcRecS* tiles = reinterpret_cast<SrcRecS*>(smem + Ls.tiles);
+  float* hist = reinterpret_cast<float*>(smem + Ls.hist);
+  double* bsum = reinterpret_cast<double*>(smem + Ls.bsum);
+  double* e2s = reinterpret_cast<double*>(smem + Ls.e2s);
+  double* fvw = reinterpret_cast<double*>(smem + Ls.fvw);
+  double* fw = reinterpret_cast<double*>(smem + Ls.fw);
+  float* e2f = reinterpret_cast<float*>(smem + Ls.e2f);
+  int* span0 = reinterpret_cast<int*>(smem + Ls.span0);
+  int* span1 = reinterpret_cast<int*>(smem + Ls.span1);
+  int* tpref = reinterpret_cast<int*>(smem + Ls.tpref);
+  float4* subbox = reinterpret_cast<float4*>(smem + Ls.subbox);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + Ls.mbar);
+  int* sh_item = reinterpret_cast<int*>(smem + Ls.misc);
+
+  if (tid == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    mbar_fence_init();
+  }
+  for (int i = tid; i <= nb; i += BT) {
+    e2s[i] = P.e2[i];
+    e2f[i] = P.e2f[i];
+  }
+  __syncthreads();
+  BinCtx C;
+  C.A = P.binA; C.B = P.binB; C.eps = P.eps; C.one_m_eps = 1.f - P.eps;
+  C.nb = nb; C.e2s = e2s; C.e2f = e2f;
+  C.eps_rel = 4e-6f;
+  C.lo_g = e2f[0] * (1.f - P.eps);
+  C.hi_g = e2f[nb] * (1.f + P.eps);
+
+  uint32_t phase = 0u;
+  uint32_t tcount = 0u;
+  bool timed_out = false;
+  float* __restrict__ hcol = hist + tid;
+  for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
+
+  for (;;) {
+    if (tid == 0) *sh_item = atomicAdd(P.queue_head, 1);
+    __syncthreads();
+    const int item = *sh_item;
+    if (item >= P.n_items) break;
+    const int2 it = P.items[item];
+    const TaskDesc T = P.tasks[it.x];
+    const LensDesc LD = P.lenses[T.lens_cat];
+    const GridDesc G = P.grids[T.src_cat];
+    const int g = it.y;
+    const int gs = LD.group_start[g];
+    const int nl = LD.group_start[g + 1] - gs;
+    const bool act = tid < nl;
+    LensS Lf;
+    float lz = 0.f;
+    double vw = 0.0, w = 0.0;
+    double* lens_col = nullptr;
+    if (act) {
+      const float4 r = LD.rec[gs + tid];
+      Lf = lens_frame(LD.pos[2 * (gs + tid)], LD.pos[2 * (gs + tid) + 1]);
+      vw = (double)r.z * (double)r.w;
+      w = (double)r.w;
+      if (HAS_Z) lz = LD.z[gs + tid];
+      if (P.lens_acc && T.lens_acc_off >= 0) lens_col = P.lens_acc + T.lens_acc_off + gs + tid;
+    } else {
+      Lf = lens_frame(make_float4(1.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f));
+    }
+    fvw[tid] = vw;
+    fw[tid] = w;
+    const size_t lens_stride = (size_t)LD.n_valid;
+    for (int e = tid; e < kQ * nb; e += BT) bsum[e] = 0.0;
+    bool first_flush = true;
+    int since_flush = 0;
+    const float4 box = LD.group_box[g];
+    int cy0, cy1;
+    row_range(G, box, P.R, P.margin, cy0, cy1);
+    float dl;
+    bool full;
+    sph_reach(G, box, P.R, P.margin, dl, full);
+
+    for (int c0 = cy0; c0 <= cy1; c0 += kRowsS) {
+      const int nr = min(kRowsS, cy1 - c0 + 1);
+      const int ns = 3 * nr;
+      __syncthreads();
+      for (int r = tid; r < nr; r += BT) {
+        int2 sp[3];
+        const int k = sph_row_spans(G, box, P.R, P.margin, c0 + r, dl, full, sp);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const int2 v = j < k ? sp[j] : make_int2(0, 0);
+          span0[3 * r + j] = v.x;
+          span1[3 * r + j] = v.y > v.x ? v.y : v.x;
+        }
+      }
+      __syncthreads();
+      if (tid == 0) {
+        int acc = 0;
+        for (int r = 0; r < ns; ++r) {
+          tpref[r] = acc;
+          acc += (span1[r] - span0[r] + kTile - 1) / kTile;
+        }
+        tpref[ns] = acc;
+      }
+      __syncthreads();
+      const int ntiles = tpref[ns];
+      int rc = 0, ri = 0;
+      if (tid == 0 && ntiles > 0) {
+        while (tpref[ri + 1] <= 0) ++ri;
+        const int s0 = span0[ri];
+        const int n0 = min(kTile, span1[ri] - s0);
+        const int bb = tcount & 1u;
+        mbar_arrive_tx(&mbar[bb], (uint32_t)(n0 * sizeof(SrcRecS)));
+        bulk_g2s(tiles + bb * kTile, G.recs + s0, (uint32_t)(n0 * sizeof(SrcRecS)), &mbar[bb]);
+      }
+      for (int k = 0; k < ntiles; ++k) {
+        if (tid == 0 && k + 1 < ntiles) {
+          while (tpref[ri + 1] <= k + 1) ++ri;
+          const int s1 = span0[ri] + (k + 1 - tpref[ri]) * kTile;
+          const int n1 = min(kTile, span1[ri] - s1);
+          const int bb = (tcount + k + 1) & 1u;
+          mbar_arrive_tx(&mbar[bb], (uint32_t)(n1 * sizeof(SrcRecS)));
+          bulk_g2s(tiles + bb * kTile, G.recs + s1, (uint32_t)(n1 * sizeof(SrcRecS)), &mbar[bb]);
+        }
+        while (tpref[rc + 1] <= k) ++rc;
+        const int s = span0[rc] + (k - tpref[rc]) * kTile;
+        const int n = min(kTile, span1[rc] - s);
+        const int bb = (tcount + k) & 1u;
+        const bool ok = mbar_wait_bounded(&mbar[bb], (phase >> bb) & 1u);
+        phase ^= (1u << bb);
+        const SrcRecS* __restrict__ S = tiles + bb * kTile;
+        const int nsub = (n + 31) >> 5;
+        if (ok) {
+          // 3-D box of each 32-source sub-chunk, widened by 2^-23 per side:
+          // the hi/lo split of both ends moves u_B - u_A by at most 2^-24.
+          for (int sc = warp; sc < nsub; sc += NW) {
+            const int j = sc * 32 + lane;
+            float mnx = INFINITY, mny = INFINITY, mnz = INFINITY, mxx = -INFINITY, mxy = -INFINITY,
+                  mxz = -INFINITY;
+            if (j < n) {
+              const float4 a = S[j].a;
+              mnx = mxx = a.x;
+              mny = mxy = a.y;
+              mnz = mxz = a.z;
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+              mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+              mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+              mnz = fminf(mnz, __shfl_xor_sync(0xffffffffu, mnz, o));
+              mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+              mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+              mxz = fmaxf(mxz, __shfl_xor_sync(0xffffffffu, mxz, o));
+            }
+            if (lane == 0) {
+              const float d = 1.1920929e-7f;
+              subbox[2 * sc] = make_float4(mnx - d, mny - d, mnz - d, 0.f);
+              subbox[2 * sc + 1] = make_float4(mxx + d, mxy + d, mxz + d, 0.f);
+            }
+          }
+        }
+        if (__syncthreads_or(!ok)) timed_out = true;
+        if (!timed_out) {
+          for (int sc = 0; sc < nsub; ++sc) {
+            const int base = sc * 32;
+            const int cnt = min(32, n - base);
+            int blo = 0;
+            const int cls = act ? classify_s<LOGB, HAS_Z>(Lf, subbox[2 * sc], subbox[2 * sc + 1], C, blo) : 0;
+            const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)cls);
+            if (m == 0) continue;
+            const SrcRecS* __restrict__ Sc = S + base;
+            if (m == 1) {
+              chunk_single_s<MODE, HAS_M, SMALL, BT, QA>(Sc, cnt, Lf, cls, blo, hcol);
+            } else if (m == 2) {
+              chunk_dual_s<MODE, HAS_M, SMALL, BT, QA>(Sc, cnt, Lf, cls, blo, hcol, C);
+            } else if (act) {
+              for (int j = 0; j < cnt; ++j) do_pair_s<MODE, HAS_M, HAS_Z, LOGB, SMALL, BT, QA>(Lf, lz, Sc[j], hcol, C);
+            }
+          }
+        }
+        since_flush += n;
+        if (since_flush >= 4 * kTile) {
+          flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
+          first_flush = false;
+          since_flush = 0;
+        }
+        __syncthreads();
+      }
+      tcount += (uint32_t)ntiles;
+    }
+    flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
+    __syncthreads();
+    double* out = P.item_sums + (size_t)(T.item_base + g) * kQ * nb;
+    for (int e = tid; e < kQ * nb; e += BT) {
+      const int q = e / nb;
+      out[e] = (q == QK && QA == 5) ? bsum[e - (QK - QW) * nb] : bsum[e];
+    }
+    __syncthreads();
+  }
+  if (timed_out && tid == 0) atomicOr(P.err, kErrTimeout);
+}
+
+// ------------------------------------------------------------ prep kernels --
+// lambda reduced to [0, 2 pi) (FP32; used only for the cell grid and the
+// lens ordering, never in the pair arithmetic).
+__global__ void k_wrap_lambda(const float* __restrict__ x, long long n, float* out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float v = x[i];
+    float t = v - kTwoPiF * floorf(v * 0.159154937f);
+    if (t < 0.f) t += kTwoPiF;
+    if (t >= kTwoPiF) t -= kTwoPiF;
+    out[i] = t;
+  }
+}
+
+__global__ void k_src_gather_sph(const int* __restrict__ idx, int n_valid, int mode, const float* __restrict__ lam,
+                                 const float* __restrict__ phi, const float* __restrict__ z,
+                                 const float* __restrict__ f1, const float* __restrict__ f2,
+                                 const float* __restrict__ w, const float* __restrict__ m, SrcRecS* rec) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_valid) return;
+  const int i = idx[s];
+  const float wi = w[i];
+  float4 hi, lo;
+  canon_unit(lam[i], phi[i], hi, lo);
+  SrcRecS r;
+  if (mode == 0) {
+    hi.w = -(f1[i] * wi);
+    lo.w = -(f2[i] * wi);
+    const float mi = m ? m[i] : 0.f;
+    r.c = make_float4(wi, wi * (1.0f + mi), z ? z[i] : 0.f, 0.f);
+  } else {
+    hi.w = f1[i] * wi;
+    lo.w = f2[i] * wi;
+    r.c = make_float4(wi, wi, 0.f, 0.f);
+  }
+  r.a = hi;
+  r.b = lo;
+  rec[s] = r;
+}
+
+// Unit vectors (hi, lo) of the sorted lenses; perm[s] = input index.
+__global__ void k_lens_pos_sph(const int* __restrict__ perm, int n_valid, const float* __restrict__ lam,
+                               const float* __restrict__ phi, float4* pos) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_valid) return;
+  const int i = perm[s];
+  float4 hi, lo;
+  canon_unit(lam[i], phi[i], hi, lo);
+  pos[2 * s] = hi;
+  pos[2 * s + 1] = lo;
+}
+
+// Unit vectors (hi, lo) in input order (tests and diagnostics).
+__global__ void k_unit_vectors(const float* __restrict__ lam, const float* __restrict__ phi, long long n,
+                               float* hi, float* lo) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    float4 h, l;
+    canon_unit(lam[i], phi[i], h, l);
+    hi[3 * i] = h.x; hi[3 * i + 1] = h.y; hi[3 * i + 2] = h.z;
+    lo[3 * i] = l.x; lo[3 * i + 1] = l.y; lo[3 * i + 2] = l.z;
+  }
+}
+
+__global__ void k_item_cost_sph(const int2* __restrict__ items, int n_items, const TaskDesc* __restrict__ tasks,
+                                const LensDesc* __restrict__ lenses, const GridDesc* __restrict__ grids, float R,
+                                float margin, unsigned long long* cost, int* order) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_items) return;
+  const int2 it = items[i];
+  const TaskDesc T = tasks[it.x];
+  const LensDesc L = lenses[T.lens_cat];
+  const GridDesc G = grids[T.src_cat];
+  const float4 box = L.group_box[it.y];
+  int cy0, cy1;
+  row_range(G, box, R, margin, cy0, cy1);
+  float dl;
+  bool full;
+  sph_reach(G, box, R, margin, dl, full);
+  unsigned long long s = 0;
+  for (int cy = cy0; cy <= cy1; ++cy) {
+    int2 sp[3];
+    const int k = sph_row_spans(G, box, R, margin, cy, dl, full, sp);
+    for (int j = 0; j < k; ++j)
+      if (sp[j].y > sp[j].x) s += (unsigned long long)(sp[j].y - sp[j].x);
+  }
+  const unsigned long long nl = (unsigned long long)(L.group_start[it.y + 1] - L.group_start[it.y]);
+  cost[i] = s * nl + 1;
+  order[i] = i;
+}
+
+// --------------------------------------------------------- host launchers --
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT>
+static cudaError_t launch_sph_t(const PairParams& P, int num_sms, cudaStream_t st, int* grid_out) {
+  constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
+  const size_t smem = sph_smem_layout(P.nb, QA, BT).total;
+  auto kern = k_pairs_sph<MODE, HAS_M, HAS_Z, LOGB, BT>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  int grid = per_sm * num_sms;
+  if (grid > P.n_items) grid = P.n_items;
+  if (grid < 1) grid = 1;
+  *grid_out = grid;
+  kern<<<grid, BT, smem, st>>>(P);
+  return cudaGetLastError();
+}
+
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB>
+static cudaError_t launch_sph_bt(const PairParams& P, int bt, int num_sms, cudaStream_t st, int* grid) {
+  if (bt == 128) return launch_sph_t<MODE, HAS_M, HAS_Z, LOGB, 128>(P, num_sms, st, grid);
+  if (bt == 64) return launch_sph_t<MODE, HAS_M, HAS_Z, LOGB, 64>(P, num_sms, st, grid);
+  return launch_sph_t<MODE, HAS_M, HAS_Z, LOGB, 32>(P, num_sms, st, grid);
+}
+
+cudaError_t launch_pairs_sph(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int num_sms,
+                             cudaStream_t st, int* grid) {
+  if (mode == 1) {
+    return logb ? launch_sph_bt<1, false, false, true>(P, bt, num_sms, st, grid)
+                : launch_sph_bt<1, false, false, false>(P, bt, num_sms, st, grid);
+  }
+  if (has_m) {
+    if (has_z) return logb ? launch_sph_bt<0, true, true, true>(P, bt, num_sms, st, grid)
+                           : launch_sph_bt<0, true, true, false>(P, bt, num_sms, st, grid);
+    return logb ? launch_sph_bt<0, true, false, true>(P, bt, num_sms, st, grid)
+                : launch_sph_bt<0, true, false, false>(P, bt, num_sms, st, grid);
+  }
+  if (has_z) return logb ? launch_sph_bt<0, false, true, true>(P, bt, num_sms, st, grid)
+                         : launch_sph_bt<0, false, true, false>(P, bt, num_sms, st, grid);
+  return logb ? launch_sph_bt<0, false, false, true>(P, bt, num_sms, st, grid)
+              : launch_sph_bt<0, false, false, false>(P, bt, num_sms, st, grid);
+}
+
+static inline unsigned gdim_s(long long n, int b) {
+  long long g = (n + b - 1) / b;
+  if (g < 1) g = 1;
+  if (g > 148 * 32) g = 148 * 32;
+  return (unsigned)g;
+}
+
+cudaError_t launch_wrap_lambda(const float* x, long long n, float* out, cudaStream_t st) {
+  if (n > 0) k_wrap_lambda<<<gdim_s(n, 256), 256, 0, st>>>(x, n, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_src_gather_sph(const int* idx, int n_valid, int mode, const float* lam, const float* phi,
+                                  const float* z, const float* f1, const float* f2, const float* w, const float* m,
+                                  SrcRecS* rec, cudaStream_t st) {
+  if (n_valid > 0)
+    k_src_gather_sph<<<(n_valid + 255) / 256, 256, 0, st>>>(idx, n_valid, mode, lam, phi, z, f1, f2, w, m, rec);
+  return cudaGetLastError();
+}
+cudaError_t launch_lens_pos_sph(const int* perm, int n_valid, const float* lam, const float* phi, float4* pos,
+                                cudaStream_t st) {
+  if (n_valid > 0) k_lens_pos_sph<<<(n_valid + 255) / 256, 256, 0, st>>>(perm, n_valid, lam, phi, pos);
+  return cudaGetLastError();
+}
+cudaError_t launch_unit_vectors(const float* lam, const float* phi, long long n, float* hi, float* lo,
+                                cudaStream_t st) {
+  if (n > 0) k_unit_vectors<<<gdim_s(n, 256), 256, 0, st>>>(lam, phi, n, hi, lo);
+  return cudaGetLastError();
+}
+cudaError_t launch_item_cost_sph(const int2* items, int n_items, const TaskDesc* tasks, const LensDesc* lenses,
+                                 const GridDesc* grids, float R, float margin, unsigned long long* cost, int* order,
+                                 cudaStream_t st) {
+  if (n_items > 0)
+    k_item_cost_sph<<<(n_items + 127) / 128, 128, 0, st>>>(items, n_items, tasks, lenses, grids, R, margin, cost,
+                                                            order);
+  return cudaGetLastError();
+}
+
+}  // namespace tpcf

@@ -40,22 +40,37 @@ struct __align__(16) SrcRec {
   float4 b;
 };
 
+// A source on the sphere: the unit vector u of (lambda, phi) split into FP32
+// hi + lo parts (u = hi + lo to ~2^-48), so that u_B - u_A keeps full FP32
+// relative precision at small separations.  Shear: a = {hi, -e1*w},
+// b = {lo, -e2*w}, c = {w, (1+m)*w, z, 0}; scalar-scalar: a = {hi, kE*w},
+// b = {lo, kB*w}, c = {w, w, 0, 0}.
+struct __align__(16) SrcRecS {
+  float4 a;
+  float4 b;
+  float4 c;
+};
+
+// Cell grid of one source catalogue.  Planar: cells over (x, y).  Sphere:
+// cells over (lambda reduced to [0, 2 pi), phi), records in `recs`.
 struct GridDesc {
   float x0, y0, cell, inv_cell;
   int ncx, ncy;
   int n_valid;
   int pad;
   const int* cell_start;  // [ncx*ncy + 1]
-  const SrcRec* rec;      // [n_valid], sorted by cell
+  const SrcRec* rec;      // [n_valid], sorted by cell (planar)
+  const SrcRecS* recs;    // [n_valid], sorted by cell (sphere), else nullptr
 };
 
 struct LensDesc {
-  const float4* rec;        // {x, y, val, w}, sorted
+  const float4* rec;        // {x, y, val, w}, sorted (sphere: x = lambda in [0, 2 pi))
   const float* z;           // sorted z, or nullptr
   const int* group_start;   // [n_groups + 1] into the sorted lenses
   const float4* group_box;  // {xmin, ymin, xmax, ymax}
   int n_valid;
   int n_groups;
+  const float4* pos;        // sphere: {hi.xyz, 0}, {lo.xyz, 0} per sorted lens, else nullptr
 };
 
 struct TaskDesc {

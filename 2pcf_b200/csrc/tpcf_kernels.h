@@ -14,6 +14,21 @@ size_t pair_smem_bytes(int nb, int qa, int bt);
 cudaError_t launch_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int variant,
                          int num_sms, cudaStream_t st, int* grid);
 
+// Spherical pair kernel (sphere.cu); P.grids[*].recs and P.lenses[*].pos set.
+cudaError_t launch_pairs_sph(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int num_sms,
+                             cudaStream_t st, int* grid);
+cudaError_t launch_wrap_lambda(const float* x, long long n, float* out, cudaStream_t st);
+cudaError_t launch_src_gather_sph(const int* idx, int n_valid, int mode, const float* lam, const float* phi,
+                                  const float* z, const float* f1, const float* f2, const float* w, const float* m,
+                                  SrcRecS* rec, cudaStream_t st);
+cudaError_t launch_lens_pos_sph(const int* perm, int n_valid, const float* lam, const float* phi, float4* pos,
+                                cudaStream_t st);
+cudaError_t launch_unit_vectors(const float* lam, const float* phi, long long n, float* hi, float* lo,
+                                cudaStream_t st);
+cudaError_t launch_item_cost_sph(const int2* items, int n_items, const TaskDesc* tasks, const LensDesc* lenses,
+                                 const GridDesc* grids, float R, float margin, unsigned long long* cost, int* order,
+                                 cudaStream_t st);
+
 cudaError_t launch_bbox_init(int* box_ord, unsigned long long* count, int* prange, int n, cudaStream_t st);
 // box_ord holds 8 order-preserving ints per catalogue: minx, miny, maxx, maxy,
 // minz, maxz, max|m|, unused.

@@ -42,7 +42,7 @@ typedef enum tpcf_status {
   TPCF_ERR_OVERFLOW = 3,      /* a size limit of the library was exceeded      */
   TPCF_ERR_TIMEOUT = 4,       /* a bounded device-side wait ran out            */
   TPCF_ERR_CUDA = 5,          /* a CUDA runtime call failed                    */
-  TPCF_ERR_NOT_SUPPORTED = 6, /* e.g. spherical coordinates                    */
+  TPCF_ERR_NOT_SUPPORTED = 6, /* e.g. the adjoint with spherical coordinates   */
   TPCF_ERR_NO_DEVICE = 7
 } tpcf_status;
 
@@ -67,7 +67,9 @@ typedef struct tpcf_opts {
                             source (the reference's --no-kd-tree)            */
   int32_t verbose;       /* print phase timings to stderr                    */
   double cell_size;      /* grid cell side in input units; 0 = autotuned     */
-  int32_t spherical;     /* must be 0: only flat coordinates are supported   */
+  int32_t spherical;     /* 1: x, y are longitude, latitude in radians and the
+                            bins are angles in radians (spherical_coords,
+                            src/tpcf.f90:297-359); |latitude| <= pi/2 */
   int32_t shard_index;   /* with shard_count > 1, this call computes only the
                             work items i with i % shard_count == shard_index
                             (items ordered by estimated cost): per-bin,
@@ -190,6 +192,29 @@ tpcf_status tpcf_canonical_edges(const tpcf_bins* bins, double* edges, double* e
 
 /* Bin centres as the reference computes them in FP32 (src/utils.f90:202-229). */
 tpcf_status tpcf_bin_centers(const tpcf_bins* bins, float* centers);
+
+/* Spherical coordinates for later calls of this context (sets
+ * tpcf_opts.spherical).  No reference counterpart: the reference passes
+ * spherical_coords to each call (src/tpcf.f90:190). */
+tpcf_status tpcf_set_spherical(tpcf_ctx* ctx, int32_t on);
+
+/* Squared canonical chords (2 sin(e_i/2))^2 [n_bin+1] of the canonical edges
+ * e_i (radians): the bin rule on the sphere.  A pair is binned by its
+ * squared chord |u_B - u_A|^2 exactly as tpcf_canonical_edges bins d2, with
+ * u = hi + lo of tpcf_unit_vectors in FP64 and the chord squared as
+ * (dx*dx + dy*dy) + dz*dz.  The sine is the library's own fixed FP64
+ * sequence (no libm), so the edges are the same on every host.  Host only;
+ * no reference counterpart (the reference bins acos of the dot product in
+ * FP32, src/utils.f90:512-528). */
+tpcf_status tpcf_chord_edges(const tpcf_bins* bins, double* chord_sq);
+
+/* Unit vectors of n points (lambda, phi in radians) as the spherical kernels
+ * use them: u in FP64 by the library's fixed sine/cosine sequence, then
+ * hi = fl32(u), lo = fl32(u - hi); hi and lo are [n][3].  Inputs and
+ * outputs may be host or device pointers.  Diagnostics; no reference
+ * counterpart. */
+tpcf_status tpcf_unit_vectors(tpcf_ctx* ctx, const float* lam, const float* phi, int64_t n, float* hi,
+                              float* lo);
 
 /* ------------------------------------------------------------- pair sums -- */
 /* Replaces tangential_shear_tpcf (src/tpcf.f90:190-378), called from

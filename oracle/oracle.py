@@ -74,6 +74,13 @@ def lib():
         L.orc_last_timing.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_canon_adjoint.argtypes = ([C.c_long] + [vp] * 5 + [C.c_long] + [vp] * 7 +
                                         [_f64p, C.c_int, _f64p, _f64p, C.c_int] + [_f64p] * 6)
+        L.orc_ref_sphere_f32.argtypes = ([C.c_int, C.c_long] + [vp] * 5 + [C.c_long] + [vp] * 7 +
+                                         [C.c_float, C.c_float, C.c_int, C.c_int, C.c_float, C.c_int] +
+                                         [vp] * 4)
+        L.orc_canon_sphere.argtypes = ([C.c_int, C.c_long] + [vp] * 5 + [C.c_long] + [vp] * 7 +
+                                       [_f64p, C.c_int, C.c_int, _f64p])
+        L.orc_sphere_edges_sq.argtypes = [_f64p, C.c_int, _f64p]
+        L.orc_unit_vectors.argtypes = [C.c_long, vp, vp, vp, vp]
         _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
         L.orc_philox4x32.argtypes = [_u32p, _u32p, _u32p]
         _lib = L
@@ -215,6 +222,68 @@ def canon_adjoint(lens, src, edges_sq, lam_t, lam_x=None, num_threads=None):
                             np.ascontiguousarray(edges_sq, np.float64), nb, lt, lx,
                             num_threads or os.cpu_count() or 1, *out)
     return dict(zip(("val_A", "w_A", "e1_B", "e2_B", "w_B", "m_B"), out))
+
+
+def sphere_edges_sq(edges):
+    """Squared canonical chords (2 sin(e/2))^2 of FP64 angle edges (radians)."""
+    e = np.ascontiguousarray(edges, np.float64)
+    out = np.zeros_like(e)
+    lib().orc_sphere_edges_sq(e, len(e) - 1, out)
+    return out
+
+
+def unit_vectors(lam, phi):
+    """Canonical unit vectors (hi, lo) [n][3] of FP32 (lambda, phi) radians."""
+    lam = np.ascontiguousarray(lam, np.float32)
+    phi = np.ascontiguousarray(phi, np.float32)
+    hi = np.zeros((len(lam), 3), np.float32)
+    lo = np.zeros((len(lam), 3), np.float32)
+    lib().orc_unit_vectors(len(lam), _ptr(lam), _ptr(phi), _ptr(hi), _ptr(lo))
+    return hi, lo
+
+
+def canon_sphere(mode, lens, src, edges_sq_chord, num_threads=None):
+    """Canonical FP64 pair sums on the sphere (positions in radians)."""
+    f = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
+    nA, nB = len(lens["x"]), len(src["x"])
+    e2 = np.ascontiguousarray(edges_sq_chord, np.float64)
+    nb = len(e2) - 1
+    xA, yA, vA, wA = (f(lens[k]) for k in ("x", "y", "val", "w"))
+    zA = f(lens.get("z")) if mode == SHEAR else None
+    if mode == SHEAR:
+        xB, yB, zB, e1, e2b, wB, mB = (f(src[k]) for k in ("x", "y", "z", "e1", "e2", "w", "m"))
+    else:
+        xB, yB, e1, e2b, wB = (f(src[k]) for k in ("x", "y", "kappa_E", "kappa_B", "w"))
+        zB = mB = None
+    sums = np.zeros(8 * nb)
+    lib().orc_canon_sphere(mode, nA, _ptr(xA), _ptr(yA), _ptr(zA), _ptr(vA), _ptr(wA), nB, _ptr(xB),
+                           _ptr(yB), _ptr(zB), _ptr(e1), _ptr(e2b), _ptr(wB), _ptr(mB), e2, nb,
+                           num_threads or os.cpu_count() or 1, sums)
+    sums = sums.reshape(8, nb)
+    return {k: sums[i].copy() for i, k in enumerate(CANON_Q)}
+
+
+def ref_sphere_f32(mode, lens, src, x_min, x_max, n_bin, spacing=LOG, p=1.0, num_threads=1):
+    """The reference's spherical pair loop in FP32 (distance_sphere with acos,
+    angles_sphere), all pairs."""
+    f = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
+    nA, nB = len(lens["x"]), len(src["x"])
+    xA, yA, vA, wA = (f(lens[k]) for k in ("x", "y", "val", "w"))
+    zA = f(lens.get("z")) if mode == SHEAR else None
+    if mode == SHEAR:
+        xB, yB, zB, e1, e2b, wB, mB = (f(src[k]) for k in ("x", "y", "z", "e1", "e2", "w", "m"))
+    else:
+        xB, yB, e1, e2b, wB = (f(src[k]) for k in ("x", "y", "kappa_E", "kappa_B", "w"))
+        zB = mB = None
+    out = {k: np.zeros(n_bin, np.float32) for k in ("g_t", "g_x", "weights")}
+    out["n_pairs"] = np.zeros(n_bin, np.int64)
+    rc = lib().orc_ref_sphere_f32(mode, nA, _ptr(xA), _ptr(yA), _ptr(zA), _ptr(vA), _ptr(wA), nB, _ptr(xB),
+                                  _ptr(yB), _ptr(zB), _ptr(e1), _ptr(e2b), _ptr(wB), _ptr(mB), x_min, x_max,
+                                  n_bin, spacing, p, num_threads, _ptr(out["g_t"]), _ptr(out["g_x"]),
+                                  _ptr(out["weights"]), _ptr(out["n_pairs"]))
+    if rc:
+        raise RuntimeError("bad binning")
+    return out
 
 
 def normalise(s):

@@ -912,6 +912,213 @@ int orc_canon_adjoint(long nA, const float* xA, const float* yA, const float* zA
   return 0;
 }
 
+// ------------------------------------------------------------ spherical --
+// Reference restatement in FP32 (src/utils.f90:512-528 distance_sphere,
+// :618-639 angles_sphere; pair loop src/tpcf.f90:297-359 with
+// spherical_coords, all pairs, no kd-tree), and the canonical FP64 rule the
+// library uses on the sphere: chord^2 = |u_B - u_A|^2 of unit vectors from
+// FP64 sin/cos of the FP32 (lambda, phi) in radians, against squared chords
+// (2 sin(e/2))^2 of the FP64 edges; position angle from A = du.east_A,
+// B = du.north_A (the numerators of angles_sphere).
+static inline float distance_sphere_f32(float l1, float p1, float l2, float p2) {
+  float cos_d = sinf(p1) * sinf(p2) + cosf(p1) * cosf(p2) * cosf(l2 - l1);
+  if (cos_d >= 1.0f) return 0.0f;
+  if (cos_d <= -1.0f) return 3.141592653589793f;
+  return acosf(cos_d);
+}
+
+int orc_ref_sphere_f32(int mode, long nA, const float* xA, const float* yA, const float* zA, const float* valA,
+                       const float* wA, long nB, const float* xB, const float* yB, const float* zB,
+                       const float* e1B, const float* e2B, const float* wB, const float* mB, float x_min,
+                       float x_max, int n_bin, int spacing, float p, int num_threads, float* g_t, float* g_x,
+                       float* weights, long long* n_pairs) {
+  ref::Binning<float> b;
+  if (ref::create_bins<float>(x_min, x_max, n_bin, spacing, p, b)) return 10;
+  std::vector<float> gt(n_bin, 0), gx(n_bin, 0), W(n_bin, 0), K(n_bin, 0);
+  std::vector<long long> np(n_bin, 0);
+#pragma omp parallel num_threads(num_threads)
+  {
+    std::vector<float> lgt(n_bin, 0), lgx(n_bin, 0), lw(n_bin, 0), lK(n_bin, 0);
+    std::vector<long long> lnp(n_bin, 0);
+#pragma omp for schedule(static)
+    for (long i = 0; i < nA; ++i) {
+      const float l1 = xA[i], p1 = yA[i], vf = valA[i], wf = wA[i];
+      const float zf = mode == 0 ? zA[i] : 0.0f;
+      if (wf == 0.0f) continue;
+      for (long j = 0; j < nB; ++j) {
+        if (mode == 0 && (zf < 0.0f || zB[j] < 0.0f || zf > zB[j])) continue;
+        const float l2 = xB[j], p2 = yB[j];
+        const float dist = distance_sphere_f32(l1, p1, l2, p2);
+        const int bi = ref::find_bin_index(dist, b);
+        if (bi < 0) continue;
+        const float w = wB[j];
+        if (mode == 0) {
+          const float sin_d = sinf(dist), cos_p2 = cosf(p2);
+          const float cs1 = cos_p2 / sin_d * sinf(l2 - l1);
+          const float cs2 = (cosf(p1) * sinf(p2) - sinf(p1) * cos_p2 * cosf(l2 - l1)) / sin_d;
+          const float c2 = 2.0f * cs1 * cs1 - 1.0f, s2 = 2.0f * cs1 * cs2;
+          const float e1 = e1B[j], e2 = e2B[j], m = mB ? mB[j] : 0.0f;
+          lgt[bi] -= (e1 * c2 + e2 * s2) * w * vf * wf;
+          lgx[bi] -= (-e1 * s2 + e2 * c2) * w * vf * wf;
+          lK[bi] += w * (1.0f + m) * wf;
+        } else {
+          lgt[bi] += e1B[j] * w * vf * wf;
+          lgx[bi] += e2B[j] * w * vf * wf;
+          lK[bi] += w * wf;
+        }
+        lw[bi] += w * wf;
+        lnp[bi] += 1;
+      }
+    }
+#pragma omp critical
+    for (int q = 0; q < n_bin; ++q) {
+      gt[q] += lgt[q]; gx[q] += lgx[q]; W[q] += lw[q]; K[q] += lK[q]; np[q] += lnp[q];
+    }
+  }
+  for (int q = 0; q < n_bin; ++q) {
+    g_t[q] = K[q] > 0 ? gt[q] / K[q] : 0.0f;
+    g_x[q] = K[q] > 0 ? gx[q] / K[q] : 0.0f;
+    weights[q] = W[q];
+    n_pairs[q] = np[q];
+  }
+  return 0;
+}
+
+// Canonical unit vectors on the sphere: sin/cos in FP64 by one fixed
+// sequence of rounded operations (Cody-Waite reduction by pi/2 in three
+// parts, Taylor series through r^17 / r^18), u = (cos phi cos lambda,
+// cos phi sin lambda, sin phi), hi = fl32(u), lo = fl32(u - hi).  This file
+// is built with -ffp-contract=off, so every operation rounds as written.
+namespace sph {
+static void sincos_fixed(double x, double& s, double& c) {
+  const double two_over_pi = 0.6366197723675814;
+  const double p1 = 1.5707963267341256, p2 = 6.077100506303966e-11, p3 = 2.0222662487959506e-21;
+  const double k = std::rint(x * two_over_pi);
+  double r = x - k * p1;
+  r = r - k * p2;
+  r = r - k * p3;
+  const double z = r * r;
+  // 1/n! for odd n = 17, 15, ..., 3 and even n = 18, 16, ..., 4
+  const double so[8] = {2.8114572543455206e-15, 7.647163731819816e-13, 1.6059043836821613e-10,
+                        2.505210838544172e-08, 2.7557319223985893e-06, 0.0001984126984126984,
+                        0.008333333333333333, 0.16666666666666666};
+  const double ce[8] = {4.779477332387385e-14, 1.1470745597729725e-11, 2.08767569878681e-09,
+                        2.755731922398589e-07, 2.48015873015873e-05, 0.001388888888888889,
+                        0.041666666666666664};
+  double ps = so[0];
+  for (int i = 1; i < 8; ++i) ps = (i % 2) ? ps * z - so[i] : ps * z + so[i];
+  const double sr = r + (r * z) * ps;
+  double pc = -1.5619206968586225e-16;
+  for (int i = 0; i < 7; ++i) pc = (i % 2) ? pc * z - ce[i] : pc * z + ce[i];
+  const double cr = 1.0 + (-0.5 * z + (z * z) * pc);
+  switch ((int)((long long)k & 3)) {
+    case 0: s = sr; c = cr; break;
+    case 1: s = cr; c = -sr; break;
+    case 2: s = -sr; c = -cr; break;
+    default: s = -cr; c = sr; break;
+  }
+}
+static void unit_hilo(float lam, float phi, float hi[3], float lo[3]) {
+  double sl, cl, sp, cp;
+  sincos_fixed((double)lam, sl, cl);
+  sincos_fixed((double)phi, sp, cp);
+  const double u[3] = {cp * cl, cp * sl, sp};
+  for (int k = 0; k < 3; ++k) {
+    hi[k] = (float)u[k];
+    lo[k] = (float)(u[k] - (double)hi[k]);
+  }
+}
+}  // namespace sph
+
+int orc_unit_vectors(long n, const float* lam, const float* phi, float* hi, float* lo) {
+  for (long i = 0; i < n; ++i) sph::unit_hilo(lam[i], phi[i], hi + 3 * i, lo + 3 * i);
+  return 0;
+}
+
+// Canonical FP64 spherical sums, [8][n_bin] as orc_canon_pairs (the dw row
+// is theta * w_B * w_A with theta = 2 asin(chord/2)).  e2 are the squared
+// canonical chords (orc_sphere_edges_sq).  Chord^2 from u = hi + lo in FP64:
+// (dx*dx + dy*dy) + dz*dz with d = u_B - u_A.  Position angle at the lens
+// from A = d.east, B = d.north with the lens frame from libm sin/cos (an
+// independent evaluation of angles_sphere, src/utils.f90:618-639).
+int orc_canon_sphere(int mode, long nA, const float* xA, const float* yA, const float* zA, const float* valA,
+                     const float* wA, long nB, const float* xB, const float* yB, const float* zB,
+                     const float* e1B, const float* e2B, const float* wB, const float* mB, const double* e2,
+                     int nb, int num_threads, double* sums) {
+  const int NQ = canon::NQ;
+  std::vector<double> ub(3 * (size_t)nB);
+  for (long j = 0; j < nB; ++j) {
+    float h[3], l[3];
+    sph::unit_hilo(xB[j], yB[j], h, l);
+    for (int k = 0; k < 3; ++k) ub[3 * j + k] = (double)h[k] + (double)l[k];
+  }
+  const long CH = 64;
+  const long nch = (nA + CH - 1) / CH;
+  std::vector<double> part((size_t)nch * NQ * nb, 0.0);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(num_threads)
+  for (long c = 0; c < nch; ++c) {
+    double* acc = part.data() + (size_t)c * NQ * nb;
+    for (long i = c * CH; i < std::min(nA, (c + 1) * CH); ++i) {
+      if (wA[i] == 0.0f || (mode == 0 && zA[i] < 0.0f)) continue;
+      float h[3], l[3];
+      sph::unit_hilo(xA[i], yA[i], h, l);
+      const double ua[3] = {(double)h[0] + (double)l[0], (double)h[1] + (double)l[1], (double)h[2] + (double)l[2]};
+      const double lam = xA[i], ph = yA[i];
+      const double east[3] = {-sin(lam), cos(lam), 0.0};
+      const double north[3] = {-sin(ph) * cos(lam), -sin(ph) * sin(lam), cos(ph)};
+      const double vw = (double)valA[i] * (double)wA[i];
+      for (long j = 0; j < nB; ++j) {
+        if (mode == 0 && (zB[j] < 0.0f || zA[i] > zB[j])) continue;
+        const double d0 = ub[3 * j] - ua[0], d1 = ub[3 * j + 1] - ua[1], d2c = ub[3 * j + 2] - ua[2];
+        const double ch2 = (d0 * d0 + d1 * d1) + d2c * d2c;
+        const int b = canon::bin_of(ch2, e2, nb);
+        if (b < 0) continue;
+        const double w = wB[j];
+        const double ang = 2.0 * asin(sqrt(ch2) / 2.0);
+        double tt, tx, kk;
+        if (mode == 0) {
+          const double A = d0 * east[0] + d1 * east[1] + d2c * east[2];
+          const double B = d0 * north[0] + d1 * north[1] + d2c * north[2];
+          const double s = A * A + B * B;
+          const double c2 = (A * A - B * B) / s, s2 = 2.0 * A * B / s;
+          const double e1 = e1B[j], ee2 = e2B[j];
+          tt = -(e1 * c2 + ee2 * s2) * w * vw;
+          tx = -(-e1 * s2 + ee2 * c2) * w * vw;
+          kk = w * (1.0 + (mB ? (double)mB[j] : 0.0)) * (double)wA[i];
+        } else {
+          tt = (double)e1B[j] * w * vw;
+          tx = (double)e2B[j] * w * vw;
+          kk = w * (double)wA[i];
+        }
+        acc[canon::Q_DW * nb + b] += ang * w * (double)wA[i];
+        acc[canon::Q_GT * nb + b] += tt;
+        acc[canon::Q_GX * nb + b] += tx;
+        acc[canon::Q_W * nb + b] += w * (double)wA[i];
+        acc[canon::Q_K * nb + b] += kk;
+        acc[canon::Q_N * nb + b] += 1.0;
+        acc[canon::Q_AGT * nb + b] += fabs(tt);
+        acc[canon::Q_AGX * nb + b] += fabs(tx);
+      }
+    }
+  }
+  std::fill(sums, sums + (size_t)NQ * nb, 0.0);
+  for (long c = 0; c < nch; ++c)
+    for (int q = 0; q < NQ * nb; ++q) sums[q] += part[(size_t)c * NQ * nb + q];
+  return 0;
+}
+
+// Squared canonical chords of the FP64 angle edges: (2 sin(e/2))^2 with the
+// fixed sine above.
+int orc_sphere_edges_sq(const double* edges, int nb, double* out) {
+  for (int i = 0; i <= nb; ++i) {
+    double s, c;
+    sph::sincos_fixed(edges[i] * 0.5, s, c);
+    const double ch = 2.0 * s;
+    out[i] = ch * ch;
+  }
+  return 0;
+}
+
 // kd-tree radius search (test_kdtree.f90).  Results are 0-based indices.
 int orc_kdtree_search(long n, const float* x, const float* y, float qx, float qy, float r,
                       int leafsize, int brute_force, long* results, long cap, long* n_found) {
