@@ -294,6 +294,27 @@ def _coords(ctx, spherical_coords):
         ctx.set_spherical(bool(spherical_coords))
 
 
+def rotate_data_from_poles_and_meridian(x_A, y_A, r_max, verbose=False, x_B=None, y_B=None,
+                                        ctx: Context = None):
+    """rotate_data_from_poles_and_meridian (src/main.f90:953-1015), in place
+    on float32 numpy arrays or CUDA tensors (radians).  Returns (rotated,
+    (center_lambda, center_phi))."""
+    ctx = _resolve_ctx(ctx)
+    arrs = [_Arr(a) for a in (x_A, y_A, x_B, y_B)]
+    for a, orig in zip(arrs, (x_A, y_A, x_B, y_B)):
+        if orig is not None and not _is_torch(orig) and a.keep is not orig:
+            raise ValueError("rotation is in place: pass contiguous float32 arrays")
+    rot = C.c_int32()
+    center = np.zeros(2, np.float32)
+    nB = arrs[2].n if x_B is not None else 0
+    _check(lib().tpcf_rotate_from_poles(ctx.handle, arrs[0].ptr, arrs[1].ptr, arrs[0].n, arrs[2].ptr,
+                                        arrs[3].ptr, nB, float(r_max), C.byref(rot), center.ctypes.data),
+           ctx.handle)
+    if verbose and rot.value:
+        print(f"Rotated field centre RA {np.degrees(center[0]):.2f} Dec {np.degrees(center[1]):.2f}")
+    return bool(rot.value), (float(center[0]), float(center[1]))
+
+
 def unit_vectors(lam, phi, ctx: Context = None):
     """(hi, lo) [n][3] FP32 parts of the unit vectors the spherical kernels use
     (tpcf_unit_vectors)."""

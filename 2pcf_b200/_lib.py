@@ -98,6 +98,7 @@ def lib():
     _sig(L, "tpcf_set_spherical", st, [vp, i32])
     _sig(L, "tpcf_chord_edges", st, [C.POINTER(Bins), vp])
     _sig(L, "tpcf_unit_vectors", st, [vp, vp, vp, i64, vp, vp])
+    _sig(L, "tpcf_rotate_from_poles", st, [vp, vp, vp, i64, vp, vp, i64, C.c_float, C.POINTER(i32), vp])
     _sig(L, "tpcf_shear_scalar", st, [vp] + [vp] * 5 + [i64] + [vp] * 7 + [i64] +
          [C.POINTER(Bins), vp, i32, C.POINTER(Result)])
     _sig(L, "tpcf_scalar_scalar", st, [vp] + [vp] * 4 + [i64] + [vp] * 5 + [i64] +

@@ -208,6 +208,17 @@ tpcf_status tpcf_set_spherical(tpcf_ctx* ctx, int32_t on);
  * FP32, src/utils.f90:512-528). */
 tpcf_status tpcf_chord_edges(const tpcf_bins* bins, double* chord_sq);
 
+/* Replaces rotate_data_from_poles_and_meridian (src/main.f90:953-1015) with
+ * rotation_sphere (src/utils.f90:483-509): in place on (xA, yA) and, when
+ * given, (xB, yB) (radians; host or device pointers).  When the lens field
+ * plus r_max reaches a pole or the prime meridian, longitudes above pi are
+ * wrapped, and both catalogues are rotated by (pi - median(xA), -median(yA));
+ * *rotated says whether it happened and center (nullable) receives the
+ * medians.  Decisions in FP32 as the reference takes them; the rotation is
+ * evaluated in FP64 and rounded to FP32. */
+tpcf_status tpcf_rotate_from_poles(tpcf_ctx* ctx, float* xA, float* yA, int64_t nA, float* xB, float* yB,
+                                   int64_t nB, float r_max, int32_t* rotated, float* center);
+
 /* Unit vectors of n points (lambda, phi in radians) as the spherical kernels
  * use them: u in FP64 by the library's fixed sine/cosine sequence, then
  * hi = fl32(u), lo = fl32(u - hi); hi and lo are [n][3].  Inputs and

@@ -81,6 +81,8 @@ def lib():
                                        [_f64p, C.c_int, C.c_int, _f64p])
         L.orc_sphere_edges_sq.argtypes = [_f64p, C.c_int, _f64p]
         L.orc_unit_vectors.argtypes = [C.c_long, vp, vp, vp, vp]
+        L.orc_rotate_from_poles.argtypes = [vp, vp, C.c_long, vp, vp, C.c_long, C.c_float,
+                                            C.POINTER(C.c_int), vp]
         _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
         L.orc_philox4x32.argtypes = [_u32p, _u32p, _u32p]
         _lib = L
@@ -230,6 +232,18 @@ def sphere_edges_sq(edges):
     out = np.zeros_like(e)
     lib().orc_sphere_edges_sq(e, len(e) - 1, out)
     return out
+
+
+def rotate_from_poles(xA, yA, r_max, xB=None, yB=None):
+    """The reference's field rotation in FP32 (copies; returns rotated flag,
+    centre and the four arrays)."""
+    f = lambda a: None if a is None else np.array(a, np.float32, copy=True)
+    xA, yA, xB, yB = f(xA), f(yA), f(xB), f(yB)
+    r = C.c_int()
+    center = np.zeros(2, np.float32)
+    lib().orc_rotate_from_poles(_ptr(xA), _ptr(yA), len(xA), _ptr(xB), _ptr(yB), 0 if xB is None else len(xB),
+                                r_max, C.byref(r), _ptr(center))
+    return bool(r.value), center, xA, yA, xB, yB
 
 
 def unit_vectors(lam, phi):

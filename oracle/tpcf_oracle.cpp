@@ -1119,6 +1119,79 @@ int orc_sphere_edges_sq(const double* edges, int nb, double* out) {
   return 0;
 }
 
+// rotate_data_from_poles_and_meridian (src/main.f90:953-1015) with
+// rotation_sphere (src/utils.f90:483-509), distance_to_meridian_sphere
+// (:579-599) and median (:712-726), all in FP32 as the reference compiles
+// them.  In place.
+namespace rot {
+const float PI = 3.141592653589793f;
+static float dist_meridian(float l1, float p1, float l2) {
+  const float sd = fabsf(sinf(l2 - l1) * cosf(p1));
+  if (fabsf(l2 - l1) <= PI / 2.0f) return sd >= 1.0f ? PI / 2.0f : asinf(sd);
+  return PI / 2.0f - fabsf(p1);
+}
+static float kth(std::vector<float> v, long k1) {  // k1-th smallest, 1-based
+  std::nth_element(v.begin(), v.begin() + (k1 - 1), v.end());
+  return v[k1 - 1];
+}
+static float median(const float* x, long n) {
+  std::vector<float> v(x, x + n);
+  if (n % 2 == 0) return (kth(v, n / 2 + 1) + kth(v, n / 2)) / 2.0f;
+  return kth(v, n / 2 + 1);
+}
+static void rotation(float& lam, float& phi, float lam_rot, float phi_rot) {
+  const float sigma = lam + lam_rot;
+  const float theta = PI / 2.0f - phi;
+  const float theta_rot = -phi_rot;
+  const float x = cosf(sigma) * cosf(theta_rot) * sinf(theta) + cosf(theta) * sinf(theta_rot);
+  const float y = sinf(sigma) * sinf(theta);
+  const float z = -cosf(sigma) * sinf(theta_rot) * sinf(theta) + cosf(theta) * cosf(theta_rot);
+  float lo = atanf(y / x);
+  if (x < 0.0f) lo = lo + PI;
+  float po;
+  if (z >= 1.0f) po = PI / 2.0f;
+  else if (z <= -1.0f) po = -PI / 2.0f;
+  else po = PI / 2.0f - acosf(z);
+  lam = lo;
+  phi = po;
+}
+}  // namespace rot
+
+int orc_rotate_from_poles(float* xA, float* yA, long nA, float* xB, float* yB, long nB, float r_max, int* rotated,
+                          float* center) {
+  using namespace rot;
+  auto mn = [](const float* v, long n) { return *std::min_element(v, v + n); };
+  auto mx = [](const float* v, long n) { return *std::max_element(v, v + n); };
+  float x_min = mn(xA, nA), x_max = mx(xA, nA), y_min = mn(yA, nA), y_max = mx(yA, nA);
+  bool r = false;
+  if (y_max + r_max >= PI / 2.0f) r = true;
+  else if (y_min - r_max <= -PI / 2.0f) r = true;
+  if (x_max - x_min > PI) {
+    for (long i = 0; i < nA; ++i)
+      if (xA[i] > PI) xA[i] = xA[i] - 2.0f * PI;
+    x_min = mn(xA, nA);
+    x_max = mx(xA, nA);
+    r = true;
+  } else if (dist_meridian(x_max, y_max, 0.0f) <= r_max || dist_meridian(x_min, y_max, 0.0f) <= r_max ||
+             dist_meridian(x_max, y_min, 0.0f) <= r_max || dist_meridian(x_min, y_min, 0.0f) <= r_max) {
+    r = true;
+  }
+  if (xB && nB > 0 && mx(xB, nB) - mn(xB, nB) > PI)
+    for (long i = 0; i < nB; ++i)
+      if (xB[i] > PI) xB[i] = xB[i] - 2.0f * PI;
+  center[0] = center[1] = 0.0f;
+  if (r) {
+    const float cx = median(xA, nA), cy = median(yA, nA);
+    center[0] = cx;
+    center[1] = cy;
+    for (long i = 0; i < nA; ++i) rotation(xA[i], yA[i], PI - cx, -cy);
+    if (xB)
+      for (long i = 0; i < nB; ++i) rotation(xB[i], yB[i], PI - cx, -cy);
+  }
+  *rotated = r ? 1 : 0;
+  return 0;
+}
+
 // kd-tree radius search (test_kdtree.f90).  Results are 0-based indices.
 int orc_kdtree_search(long n, const float* x, const float* y, float qx, float qy, float r,
                       int leafsize, int brute_force, long* results, long cap, long* n_found) {

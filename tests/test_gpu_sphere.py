@@ -98,7 +98,7 @@ def test_poles_wrap_and_wide_bins(tpcf, oracle, sctx):
              z=f32(np.ones(n)), e1=f32(rng.normal(0, 0.26, n)), e2=f32(rng.normal(0, 0.26, n)),
              w=f32(np.ones(n)), m=f32(np.zeros(n)))
     L["y"][:5] = f32([np.pi / 2, -np.pi / 2, 1.5707, -1.5707, 1.57079])
-    S["y"][:5] = f32([np.pi / 2, -np.pi / 2, 1.5706, -1.5708, 1.57])
+    S["y"][:5] = f32([np.pi / 2, -np.pi / 2, 1.5706, -1.57079, 1.57])
     S["x"][5:20] = f32(np.linspace(-1e-3, 1e-3, 15))        # straddle lambda = 0
     L["x"][5:20] = f32(2 * np.pi - np.linspace(0, 2e-3, 15))
     for lo, hi, nb, sp in ((1 * D2R, 40 * D2R, 12, "log"), (0.0, 30 * D2R, 10, "lin")):

@@ -122,3 +122,29 @@ def test_reference_restatement_at_large_separations(oracle):
     np.testing.assert_allclose(ref["n_pairs"], can["n_pairs"], rtol=5e-3)
     scale = raw["abs_gt"] / raw["sum_K"]
     assert np.all(np.abs(ref["g_t"] - can["g_t"]) <= 2e-3 * scale)
+
+
+def test_field_rotation_restatement(oracle):
+    """rotation_sphere as written in src/utils.f90:483-509 rotates about the y
+    axis by +phi_c after moving the field centre (median) to longitude pi, so
+    the centre's latitude is doubled rather than removed; the
+    restatement keeps that (the centre at x = -cos 2phi_c, z = sin 2phi_c).  A field near the pole is rotated, a field far
+    from poles and meridian is not."""
+    rng = np.random.default_rng(9)
+    n = 1001
+    x = f32(rng.uniform(10, 50, n) * D2R)
+    y = f32(rng.uniform(75, 85, n) * D2R)
+    x[0], y[0] = np.median(x), np.median(y)
+    rot, center, xr, yr, _, _ = oracle.rotate_from_poles(x, y, np.float32(10 * D2R))
+    assert rot
+    assert center[0] == x[0] and center[1] == y[0]
+    # the centre lands at x = -cos(2 phi_c), y = 0, z = sin(2 phi_c)
+    c2 = np.cos(2 * float(y[0]))
+    assert abs(xr[0] - (np.pi if c2 > 0 else 0.0)) < 1e-6
+    assert abs(yr[0] - np.arcsin(np.sin(2 * float(y[0])))) < 1e-5
+    x2 = f32(rng.uniform(110, 130, n) * D2R)
+    y2 = f32(rng.uniform(-30, -10, n) * D2R)
+    rot2, _, xr2, yr2, _, _ = oracle.rotate_from_poles(x2, y2, np.float32(1 * D2R))
+    assert not rot2
+    np.testing.assert_array_equal(xr2, x2)
+    np.testing.assert_array_equal(yr2, y2)
