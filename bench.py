@@ -269,6 +269,8 @@ def main():
     ap.add_argument("--region", type=float, default=0.0,
                     help="profiling: keep only objects with x, y < REGION arcmin (density unchanged)")
     ap.add_argument("--task", type=int, default=-1, help="profiling: run only this task of the 25")
+    ap.add_argument("--cell-divisor", type=int, default=0,
+                    help="grid cell side theta_max/D without autotuning (0: autotune)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -303,11 +305,16 @@ def main():
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     # cell side picked by the autotuner (trial calls on a density-preserving corner)
-    at = importlib.import_module("2pcf_b200.autotune")
-    tune = at.autotune_cell_size(
-        [tpcf.LensCatalog(**{k: l[k] for k in ("x", "y", "val", "w", "z")}) for l in w["lens_bins"]],
-        [tpcf.ShapeCatalog(**{k: s_[k] for k in ("x", "y", "e1", "e2", "w", "z", "m")}) for s_ in w["shape_bins"]],
-        w["tasks"], bins, ctx)
+    if args.cell_divisor > 0:
+        ctx.set_cell_size(bins.x_max / args.cell_divisor)
+        tune = {}
+    else:
+        at = importlib.import_module("2pcf_b200.autotune")
+        tune = at.autotune_cell_size(
+            [tpcf.LensCatalog(**{k: l[k] for k in ("x", "y", "val", "w", "z")}) for l in w["lens_bins"]],
+            [tpcf.ShapeCatalog(**{k: s_[k] for k in ("x", "y", "e1", "e2", "w", "z", "m")})
+             for s_ in w["shape_bins"]],
+            w["tasks"], bins, ctx)
     if world > 1:
         ctx.set_shard(rank, world)
     n_boot = w["n_boot"]
