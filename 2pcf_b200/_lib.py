@@ -55,6 +55,11 @@ class Stats(C.Structure):
                 ("h2d_bytes", C.c_int64), ("kernel_launches", C.c_int64)]
 
 
+class MarksFieldC(C.Structure):
+    _fields_ = [("n", C.c_int64), ("n_bin", C.c_int64)] + [
+        (n, C.c_void_p) for n in ("x", "y", "w", "xi_E", "xi_B", "K")]
+
+
 class TPCFError(RuntimeError):
     def __init__(self, status, msg=""):
         self.status = status
@@ -99,6 +104,12 @@ def lib():
     _sig(L, "tpcf_chord_edges", st, [C.POINTER(Bins), vp])
     _sig(L, "tpcf_unit_vectors", st, [vp, vp, vp, i64, vp, vp])
     _sig(L, "tpcf_rotate_from_poles", st, [vp, vp, vp, i64, vp, vp, i64, C.c_float, C.POINTER(i32), vp])
+    _sig(L, "tpcf_read_table", st, [C.c_char_p, i32, i32, i32, i32, vp, i64, C.POINTER(i64)])
+    _sig(L, "tpcf_write_result_table", st, [C.c_char_p, i32, vp, vp, vp, vp, vp, vp, i32])
+    _sig(L, "tpcf_marks_save", st, [C.c_char_p, i32, C.POINTER(MarksFieldC)])
+    _sig(L, "tpcf_marks_info", st, [C.c_char_p, i32, C.POINTER(i32), vp, vp])
+    _sig(L, "tpcf_marks_load", st, [C.c_char_p, i32, C.POINTER(MarksFieldC)])
+    _sig(L, "tpcf_xi_from_marks", st, [vp, i32, C.POINTER(MarksFieldC), i32, vp, vp, vp, vp] + [vp] * 6)
     _sig(L, "tpcf_shear_scalar", st, [vp] + [vp] * 5 + [i64] + [vp] * 7 + [i64] +
          [C.POINTER(Bins), vp, i32, C.POINTER(Result)])
     _sig(L, "tpcf_scalar_scalar", st, [vp] + [vp] * 4 + [i64] + [vp] * 5 + [i64] +

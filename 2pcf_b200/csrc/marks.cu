@@ -1,0 +1,240 @@
+// marks.cu -- xi from precomputed per-lens marks (calculate_tpcf_from_marks,
+// src/main.f90:1017-1139): for each foreground map m and field i,
+//   g_t[b] = sum_j xi_E[j][b] val_mj w_mj / sum_j K[j][b] w_mj,
+//   g_x[b] = sum_j xi_B[j][b] val_mj w_mj / sum_j K[j][b] w_mj,
+//   weights = sum_j mw_j w_mj,
+// over the lenses j with mw_j w_mj > 0 (the reference packs the others away,
+// :1089-1104), and the fields stacked by summing numerators and K
+// (:1127-1135).  The marks were computed once with val = w = 1; each new map
+// only re-weights them, so this is a streaming pass over the marks (HBM-bound:
+// 12 bytes per lens and bin, plus 8 bytes per lens and map).
+//
+// One block = 256 lenses of one field and up to kMapGroup maps; lane = bin,
+// warp = a slice of the lenses; FP64 accumulation, per-block partial sums in
+// scratch, then a fixed-order reduction over blocks (deterministic).
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "tpcf_b200.h"
+#include "tpcf_ctx.h"
+#include "tpcf_internal.cuh"
+
+namespace tpcf {
+
+constexpr int kMarksChunk = 256;  // lenses per block
+constexpr int kMapGroup = 4;      // maps per pass over the marks
+
+struct MarksField {
+  long long n;
+  int n_bin;
+  int chunk0;               // first block of this field
+  const float* mw;          // marks weight [n]
+  const float* xiE;         // [n][n_bin]
+  const float* xiB;
+  const float* K;
+  const float* val;         // [n_map][n]
+  const float* w;           // [n_map][n]
+};
+
+// partial[(blk * n_map_g + g) * R + r], R = 3 n_bin + 1 (E, B, K rows, weight)
+__global__ void __launch_bounds__(256) k_marks_partials(const MarksField* __restrict__ fields, int n_field,
+                                                         int map0, int n_map_g, int n_map, int n_bin,
+                                                         double* __restrict__ partial) {
+  __shared__ double red[8][kMapGroup][3 * 32 + 1];
+  const int blk = blockIdx.x;
+  int fi = 0;
+  while (fi + 1 < n_field && fields[fi + 1].chunk0 <= blk) ++fi;
+  const MarksField F = fields[fi];
+  const long long j0 = (long long)(blk - F.chunk0) * kMarksChunk;
+  const long long j1 = min(F.n, j0 + kMarksChunk);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int R = 3 * n_bin + 1;
+  for (int b0 = 0; b0 < n_bin; b0 += 32) {
+    const int b = b0 + lane;
+    double aE[kMapGroup], aB[kMapGroup], aK[kMapGroup], aw[kMapGroup];
+#pragma unroll
+    for (int g = 0; g < kMapGroup; ++g) aE[g] = aB[g] = aK[g] = aw[g] = 0.0;
+    for (long long j = j0 + warp; j < j1; j += 8) {
+      const float mw = F.mw[j];
+      const float e = b < n_bin ? F.xiE[j * n_bin + b] : 0.f;
+      const float x = b < n_bin ? F.xiB[j * n_bin + b] : 0.f;
+      const float k = b < n_bin ? F.K[j * n_bin + b] : 0.f;
+#pragma unroll
+      for (int g = 0; g < kMapGroup; ++g) {
+        if (g < n_map_g) {
+          const size_t o = (size_t)(map0 + g) * (size_t)F.n + (size_t)j;
+          const double wm = (double)F.w[o];
+          const double ww = (double)mw * wm;
+          if (ww > 0.0) {  // lenses with marks weight x weight <= 0 are removed
+            const double vw = (double)F.val[o] * wm;
+            aE[g] = fma((double)e, vw, aE[g]);
+            aB[g] = fma((double)x, vw, aB[g]);
+            aK[g] = fma((double)k, wm, aK[g]);
+            aw[g] += ww;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < kMapGroup; ++g) {
+      red[warp][g][lane] = aE[g];
+      red[warp][g][32 + lane] = aB[g];
+      red[warp][g][64 + lane] = aK[g];
+      if (lane == 0) red[warp][g][96] = aw[g];
+    }
+    __syncthreads();
+    // fixed-order sum over the 8 warps
+    for (int t = threadIdx.x; t < kMapGroup * 97; t += blockDim.x) {
+      const int g = t / 97, r = t % 97;
+      if (g >= n_map_g) continue;
+      const int bb = b0 + (r % 32);
+      const int q = r / 32;  // 0 E, 1 B, 2 K, 3 weight
+      if (q < 3 && bb >= n_bin) continue;
+      if (q == 3 && b0 != 0) continue;
+      double s = 0.0;
+      for (int wp = 0; wp < 8; ++wp) s += red[wp][g][r];
+      const int row = q < 3 ? q * n_bin + bb : 3 * n_bin;
+      partial[((size_t)blk * n_map_g + g) * R + row] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// Field sums: out[(g * n_field + fi) * R + r] = sum over the field's blocks.
+__global__ void k_marks_reduce(const double* __restrict__ partial, const MarksField* __restrict__ fields,
+                               int n_field, int n_blocks, int n_map_g, int R, double* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_map_g * n_field * R) return;
+  const int r = t % R, fi = (t / R) % n_field, g = t / (R * n_field);
+  const int c0 = fields[fi].chunk0;
+  const int c1 = fi + 1 < n_field ? fields[fi + 1].chunk0 : n_blocks;
+  double s = 0.0;
+  for (int c = c0; c < c1; ++c) s += partial[((size_t)c * n_map_g + g) * R + r];
+  out[t] = s;
+}
+
+// max |a - b| over n entries, as order-preserving bits of a non-negative float.
+__global__ void k_max_absdiff(const float* __restrict__ a, const float* __restrict__ b, long long n, int* out) {
+  float m = 0.f;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float d = fabsf(a[i] - b[i]);
+    m = fmaxf(m, d != d ? INFINITY : d);
+  }
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_int(m));
+}
+
+}  // namespace tpcf
+
+using namespace tpcf;
+
+extern "C" tpcf_status tpcf_xi_from_marks(tpcf_ctx* c, int32_t n_field, const tpcf_marks_field* marks,
+                                          int32_t n_map, const float* const* val, const float* const* w,
+                                          const float* const* lens_x, const float* const* lens_y, double* g_t,
+                                          double* g_x, double* weights, double* g_t_stacked,
+                                          double* g_x_stacked, double* weights_stacked) {
+  if (!c || n_field < 1 || !marks || n_map < 1 || !val || !w) return TPCF_ERR_INVALID_ARG;
+  const int nb = (int)marks[0].n_bin;
+  if (nb < 1 || nb > kMaxBins) return TPCF_ERR_INVALID_ARG;
+  for (int i = 0; i < n_field; ++i) {
+    const tpcf_marks_field& m = marks[i];
+    if (m.n_bin != nb || m.n < 0 || m.n > (1ll << 31) - 2 || !val[i] || !w[i]) return TPCF_ERR_INVALID_ARG;
+    if (m.n > 0 && (!m.w || !m.xi_E || !m.xi_B || !m.K)) return TPCF_ERR_INVALID_ARG;
+  }
+  try {
+    begin_call(c);
+    cudaStream_t st = c->stream;
+    std::vector<MarksField> hf(n_field);
+    int nblk = 0;
+    for (int i = 0; i < n_field; ++i) {
+      const tpcf_marks_field& m = marks[i];
+      const int64_t n = m.n;
+      MarksField& F = hf[i];
+      F.n = n;
+      F.n_bin = nb;
+      F.chunk0 = nblk;
+      nblk += (int)((n + kMarksChunk - 1) / kMarksChunk);
+      F.mw = stage(c, m.w, n);
+      F.xiE = stage(c, m.xi_E, n * nb);
+      F.xiB = stage(c, m.xi_B, n * nb);
+      F.K = stage(c, m.K, n * nb);
+      F.val = stage(c, val[i], n * n_map);
+      F.w = stage(c, w[i], n * n_map);
+      // the lenses must be the ones the marks were computed for (main.f90:1036-1049)
+      if (lens_x && lens_y && lens_x[i] && lens_y[i] && n > 0) {
+        if (!m.x || !m.y) throw Failure(TPCF_ERR_INVALID_ARG, "marks positions missing for the check");
+        const float* a[2] = {stage(c, m.x, n), stage(c, m.y, n)};
+        const float* b[2] = {stage(c, lens_x[i], n), stage(c, lens_y[i], n)};
+        int* dm = (int*)ws_alloc(c, sizeof(int) * 2);
+        check(cudaMemsetAsync(dm, 0, sizeof(int) * 2, st), "memset");
+        for (int k = 0; k < 2; ++k) {
+          k_max_absdiff<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 8), 256, 0, st>>>(a[k], b[k], n, dm + k);
+          counted(c, cudaGetLastError(), "position check");
+        }
+        int hm[2];
+        check(cudaMemcpyAsync(hm, dm, sizeof(hm), cudaMemcpyDeviceToHost, st), "D2H check");
+        check(cudaStreamSynchronize(st), "sync check");
+        for (int k = 0; k < 2; ++k) {
+          float d;
+          std::memcpy(&d, &hm[k], 4);
+          if (!(d <= 1.0e-5f))
+            throw Failure(TPCF_ERR_INVALID_ARG, std::string(k ? "Y" : "X") + "-coordinates of lenses do not match in field " +
+                                                    std::to_string(i));
+        }
+      }
+    }
+    MarksField* df = (MarksField*)ws_alloc(c, sizeof(MarksField) * n_field);
+    check(cudaMemcpyAsync(df, hf.data(), sizeof(MarksField) * n_field, cudaMemcpyHostToDevice, st), "H2D fields");
+    const int R = 3 * nb + 1;
+    std::vector<double> sums((size_t)n_map * n_field * R, 0.0);
+    double* part = (double*)ws_alloc(c, sizeof(double) * (size_t)std::max(nblk, 1) * kMapGroup * R);
+    double* dout = (double*)ws_alloc(c, sizeof(double) * (size_t)kMapGroup * n_field * R);
+    for (int m0 = 0; m0 < n_map; m0 += kMapGroup) {
+      const int g = std::min(kMapGroup, n_map - m0);
+      if (nblk > 0) {
+        k_marks_partials<<<nblk, 256, 0, st>>>(df, n_field, m0, g, n_map, nb, part);
+        counted(c, cudaGetLastError(), "marks partials");
+      }
+      const int tot = g * n_field * R;
+      if (nblk > 0) {
+        k_marks_reduce<<<(tot + 255) / 256, 256, 0, st>>>(part, df, n_field, nblk, g, R, dout);
+        counted(c, cudaGetLastError(), "marks reduce");
+      } else {
+        check(cudaMemsetAsync(dout, 0, sizeof(double) * tot, st), "memset");
+      }
+      check(cudaMemcpyAsync(sums.data() + (size_t)m0 * n_field * R, dout, sizeof(double) * tot,
+                            cudaMemcpyDeviceToHost, st), "D2H sums");
+    }
+    check(cudaStreamSynchronize(st), "sync marks");
+    // normalisation (main.f90:1118-1133): plain quotients, as the reference
+    for (int m = 0; m < n_map; ++m) {
+      std::vector<double> sE(nb, 0.0), sB(nb, 0.0), sK(nb, 0.0);
+      double sw = 0.0;
+      for (int i = 0; i < n_field; ++i) {
+        const double* s = sums.data() + ((size_t)m * n_field + i) * R;
+        for (int b = 0; b < nb; ++b) {
+          if (g_t) g_t[((size_t)m * n_field + i) * nb + b] = s[b] / s[2 * nb + b];
+          if (g_x) g_x[((size_t)m * n_field + i) * nb + b] = s[nb + b] / s[2 * nb + b];
+          sE[b] += s[b];
+          sB[b] += s[nb + b];
+          sK[b] += s[2 * nb + b];
+        }
+        if (weights) weights[(size_t)m * n_field + i] = s[3 * nb];
+        sw += s[3 * nb];
+      }
+      for (int b = 0; b < nb; ++b) {
+        if (g_t_stacked) g_t_stacked[(size_t)m * nb + b] = sE[b] / sK[b];
+        if (g_x_stacked) g_x_stacked[(size_t)m * nb + b] = sB[b] / sK[b];
+      }
+      if (weights_stacked) weights_stacked[m] = sw;
+    }
+    return TPCF_OK;
+  } catch (const Failure& f) {
+    c->err = f.msg;
+    return f.status;
+  }
+}

@@ -219,6 +219,70 @@ tpcf_status tpcf_chord_edges(const tpcf_bins* bins, double* chord_sq);
 tpcf_status tpcf_rotate_from_poles(tpcf_ctx* ctx, float* xA, float* yA, int64_t nA, float* xB, float* yB,
                                    int64_t nB, float r_max, int32_t* rotated, float* center);
 
+/* ---------------------------------------------------- files and marks -- */
+/* Replaces the text loaders load_standard_shape_catalog (7 columns x y z e1
+ * e2 w m), load_standard_kappa_map (5: x y kappa_E kappa_B w) and
+ * load_standard_lens_catalog (5: x y z val w) of src/input_formats.f90:227-333:
+ * a table of ncols numbers per line separated by blanks or commas.  Lines
+ * whose first non-blank character is '#' and blank lines are skipped (the
+ * reference stops on them).  With cols == NULL, *n_rows receives an upper
+ * bound on the rows (the data lines).  Otherwise cols is column-major
+ * [ncols][capacity]; rows with column keep_pos_col <= 0 (the weight) and, if
+ * keep_nonneg_col >= 0, with that column < 0 (the lens redshift) are dropped
+ * as the loaders' masks do (:250-256, :316-328), and *n_rows receives the rows
+ * kept.  All host threads parse (n_threads <= 0).  A malformed line gives
+ * TPCF_ERR_INVALID_ARG.  Host only. */
+tpcf_status tpcf_read_table(const char* path, int32_t ncols, int32_t keep_pos_col, int32_t keep_nonneg_col,
+                            int32_t n_threads, float* cols, int64_t capacity, int64_t* n_rows);
+
+/* The driver's result table (src/main.f90:699-702): one line per bin with
+ * theta, g_t, g_x, weights, n_pairs, mean_theta, in that order; theta and
+ * mean_theta converted from radians to degrees when to_degrees != 0 (the
+ * spherical case, :690-694).  Reals as %16.7E, n_pairs as %21lld.  Host only. */
+tpcf_status tpcf_write_result_table(const char* path, int32_t n_bin, const float* theta, const float* g_t,
+                                    const float* g_x, const float* weights, const int64_t* n_pairs,
+                                    const float* mean_theta, int32_t to_degrees);
+
+/* Per-lens marks of one field, as save_marks / load_survey_marks hold them
+ * (src/input_formats.f90:528-603): positions, marks weight and
+ * [n][n_bin] marks (the Fortran (n_bin, n) arrays). */
+typedef struct tpcf_marks_field {
+  int64_t n;
+  int64_t n_bin;
+  float* x;
+  float* y;
+  float* w;     /* marks_weight */
+  float* xi_E;  /* [n][n_bin] */
+  float* xi_B;
+  float* K;
+} tpcf_marks_field;
+
+/* Binary marks stream of save_marks (src/input_formats.f90:528-560): 1024-byte
+ * header (int64 1024, int64 n_field, ..., int64 1024 at byte 1016), then per
+ * field int64 n, n_bin, float32 x, y, w, xi_E, xi_B, K.  n_field <= 20. */
+tpcf_status tpcf_marks_save(const char* path, int32_t n_field, const tpcf_marks_field* fields);
+/* Sizes of a marks file: *n_field, and n[i], n_bin[i] for i < max_fields
+ * (load_survey_marks' checks: n_field <= 20, n <= 5e7). */
+tpcf_status tpcf_marks_info(const char* path, int32_t max_fields, int32_t* n_field, int64_t* n, int64_t* n_bin);
+/* Reads a marks file into caller-allocated fields whose n and n_bin match
+ * tpcf_marks_info. */
+tpcf_status tpcf_marks_load(const char* path, int32_t n_field, const tpcf_marks_field* fields);
+
+/* Replaces calculate_tpcf_from_marks (src/main.f90:1017-1139) for n_map
+ * foreground maps at once: val[i] and w[i] are [n_map][n_i] for field i.
+ * Lenses with marks.w * w <= 0 are left out.  Outputs (nullable):
+ * g_t, g_x [n_map][n_field][n_bin] = sum xi_E val w / sum K w (plain
+ * quotients, as the reference); weights [n_map][n_field] = sum marks.w w;
+ * the stacked g_t_stacked, g_x_stacked [n_map][n_bin] and weights_stacked
+ * [n_map] sum numerators and K over fields.  lens_x, lens_y (nullable) are
+ * checked against the marks positions to 1e-5 as the reference does.  FP64
+ * accumulation in a fixed order (deterministic).  Inputs may be host or
+ * device pointers. */
+tpcf_status tpcf_xi_from_marks(tpcf_ctx* ctx, int32_t n_field, const tpcf_marks_field* marks, int32_t n_map,
+                               const float* const* val, const float* const* w, const float* const* lens_x,
+                               const float* const* lens_y, double* g_t, double* g_x, double* weights,
+                               double* g_t_stacked, double* g_x_stacked, double* weights_stacked);
+
 /* Unit vectors of n points (lambda, phi in radians) as the spherical kernels
  * use them: u in FP64 by the library's fixed sine/cosine sequence, then
  * hi = fl32(u), lo = fl32(u - hi); hi and lo are [n][3].  Inputs and

@@ -397,3 +397,59 @@ def covariance(x):
     cov = np.zeros((x.shape[1], x.shape[1]))
     lib().orc_covariance(x.shape[0], x.shape[1], x, cov)
     return cov
+
+
+# ------------------------------------------------------------ files, marks --
+def marks_write(path, fields):
+    """The binary marks stream of save_marks (src/input_formats.f90:528-560),
+    restated with numpy: fields are dicts x, y, w, xi_E, xi_B, K ([n][n_bin])."""
+    head = np.zeros(128, np.int64)
+    head[0], head[1], head[127] = 1024, len(fields), 1024
+    with open(path, "wb") as f:
+        f.write(head.tobytes())
+        for m in fields:
+            n, nb = np.asarray(m["xi_E"]).shape
+            f.write(np.array([n, nb], np.int64).tobytes())
+            for k in ("x", "y", "w", "xi_E", "xi_B", "K"):
+                f.write(np.ascontiguousarray(m[k], np.float32).tobytes())
+
+
+def marks_read(path):
+    """load_survey_marks (src/input_formats.f90:562-603) restated with numpy."""
+    raw = open(path, "rb").read()
+    h = np.frombuffer(raw[:1024], np.int64)
+    assert h[0] == 1024 and h[127] == 1024
+    off, out = 1024, []
+    for _ in range(int(h[1])):
+        n, nb = (int(v) for v in np.frombuffer(raw[off:off + 16], np.int64))
+        off += 16
+        m = {}
+        for k in ("x", "y", "w"):
+            m[k] = np.frombuffer(raw[off:off + 4 * n], np.float32).copy()
+            off += 4 * n
+        for k in ("xi_E", "xi_B", "K"):
+            m[k] = np.frombuffer(raw[off:off + 4 * n * nb], np.float32).reshape(n, nb).copy()
+            off += 4 * n * nb
+        out.append(m)
+    return out
+
+
+def xi_from_marks(fields, vals, ws):
+    """calculate_tpcf_from_marks (src/main.f90:1017-1139) in FP64 for one map:
+    fields[i] dicts with w (marks weight), xi_E, xi_B, K; vals[i], ws[i] the
+    lens values and weights.  Lenses with marks_w * w <= 0 (FP32 product, as
+    the reference forms it) are removed."""
+    res, E, B, K, W = [], 0.0, 0.0, 0.0, 0.0
+    for m, v, w in zip(fields, vals, ws):
+        mw = np.asarray(m["w"], np.float32) * np.asarray(w, np.float32)
+        keep = mw > 0
+        vw = (np.asarray(v, np.float64) * np.asarray(w, np.float64))[keep]
+        e = (np.asarray(m["xi_E"], np.float64)[keep] * vw[:, None]).sum(0)
+        b = (np.asarray(m["xi_B"], np.float64)[keep] * vw[:, None]).sum(0)
+        k = (np.asarray(m["K"], np.float64)[keep] * np.asarray(w, np.float64)[keep][:, None]).sum(0)
+        wsum = (np.asarray(m["w"], np.float64) * np.asarray(w, np.float64))[keep].sum()
+        with np.errstate(invalid="ignore", divide="ignore"):
+            res.append({"g_t": e / k, "g_x": b / k, "weights": wsum})
+        E, B, K, W = E + e, B + b, K + k, W + wsum
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return res, {"g_t": E / K, "g_x": B / K, "weights": W}
