@@ -512,4 +512,4 @@ def tangential_shear_adjoint(x_A, y_A, z_A, val_A, weight_A, x_B, y_B, z_B, e1_B
 
 from .files import (calculate_tpcf_from_marks, load_standard_kappa_map, load_standard_lens_catalog,  # noqa: E402
                     load_standard_shape_catalog, load_survey_marks, read_table, save_marks, write_result_table,
-                    MarksField)
+                    MarksField, marks_bootstrap)

@@ -109,6 +109,8 @@ def lib():
     _sig(L, "tpcf_marks_save", st, [C.c_char_p, i32, C.POINTER(MarksFieldC)])
     _sig(L, "tpcf_marks_info", st, [C.c_char_p, i32, C.POINTER(i32), vp, vp])
     _sig(L, "tpcf_marks_load", st, [C.c_char_p, i32, C.POINTER(MarksFieldC)])
+    _sig(L, "tpcf_marks_bootstrap", st, [vp, i32, C.POINTER(MarksFieldC), vp, i64, vp, C.c_uint64, i32,
+                                         C.c_double, i32] + [vp] * 5)
     _sig(L, "tpcf_xi_from_marks", st, [vp, i32, C.POINTER(MarksFieldC), i32, vp, vp, vp, vp] + [vp] * 6)
     _sig(L, "tpcf_shear_scalar", st, [vp] + [vp] * 5 + [i64] + [vp] * 7 + [i64] +
          [C.POINTER(Bins), vp, i32, C.POINTER(Result)])

@@ -30,6 +30,7 @@
 
 #include "tpcf_b200.h"
 #include "tpcf_ctx.h"
+#include "philox.cuh"
 #include "tpcf_internal.cuh"
 #include "tpcf_kernels.h"
 
@@ -110,18 +111,6 @@ int fixed_scale(long long n, double vmax) {
 }
 
 // ---------------------------------------------------------------- bootstrap --
-__device__ __forceinline__ void philox4x32(uint32_t c[4], uint32_t k0, uint32_t k1) {
-#pragma unroll
-  for (int r = 0; r < 10; ++r) {
-    const uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
-    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
-    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
-    c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
-    k0 += 0x9E3779B9u;
-    k1 += 0xBB67AE85u;
-  }
-}
-
 // One block per resample: n_draw Philox draws of a patch index in [0, n_patch)
 // (counter (d/4, s, 0x2BCF, 0), word d%4, multiply-shift), counted.
 __global__ void k_boot_mult(unsigned long long seed, int n_patch, int n_draw, int* mult) {
@@ -205,6 +194,16 @@ tpcf_status fail(tpcf_ctx* c, const Failure& f) {
 }
 
 }  // namespace
+
+namespace tpcf {
+// Unbiased sample covariance [D][D] of n_s samples x [n_s][D] (covariance_matrix,
+// src/utils.f90:745-764), FP64.
+cudaError_t launch_cov(const double* x, int n_s, int D, double* cov, cudaStream_t st) {
+  dim3 grid((unsigned)((D + 127) / 128), (unsigned)D);
+  k_cov<<<grid, 128, 0, st>>>(x, n_s, D, cov);
+  return cudaGetLastError();
+}
+}  // namespace tpcf
 
 extern "C" {
 

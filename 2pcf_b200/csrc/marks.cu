@@ -19,9 +19,11 @@
 #include <string>
 #include <vector>
 
+#include "philox.cuh"
 #include "tpcf_b200.h"
 #include "tpcf_ctx.h"
 #include "tpcf_internal.cuh"
+#include "tpcf_kernels.h"
 
 namespace tpcf {
 
@@ -32,17 +34,45 @@ struct MarksField {
   long long n;
   int n_bin;
   int chunk0;               // first block of this field
+  long long lens0;          // index of the field's first lens among all fields
   const float* mw;          // marks weight [n]
   const float* xiE;         // [n][n_bin]
   const float* xiB;
   const float* K;
-  const float* val;         // [n_map][n]
-  const float* w;           // [n_map][n]
+  const float* val;         // maps: [n_map][n]
+  const float* w;           // maps: [n_map][n]
 };
 
-// partial[(blk * n_map_g + g) * R + r], R = 3 n_bin + 1 (E, B, K rows, weight)
+// Lens factors of resample/map g for lens j of field F: numerator factor vw,
+// K factor wm, and whether the lens takes part.
+struct MapFactors {  // foreground maps: vw = val w, wm = w
+  int map0;
+  __device__ __forceinline__ void get(const MarksField& F, int g, long long j, double& vw, double& wm) const {
+    const size_t o = (size_t)(map0 + g) * (size_t)F.n + (size_t)j;
+    wm = (double)F.w[o];
+    vw = (double)F.val[o] * wm;
+  }
+  // calculate_tpcf_from_marks drops lenses with marks weight x weight <= 0
+  __device__ __forceinline__ bool keep(float mw, double wm) const { return (double)mw * wm > 0.0; }
+};
+struct MultFactors {  // resamples: vw = wm = multiplicity of the lens's unit
+  const int* mult;    // [G][n_units]
+  const int* unit;    // unit of each lens (all fields concatenated), or nullptr: the lens itself
+  long long n_units;
+  __device__ __forceinline__ void get(const MarksField& F, int g, long long j, double& vw, double& wm) const {
+    const long long gl = F.lens0 + j;
+    const long long u = unit ? (long long)unit[gl] : gl;
+    wm = (double)mult[(size_t)g * (size_t)n_units + (size_t)u];
+    vw = wm;
+  }
+  // the bootstraps take every drawn lens (src/tpcf.f90:601, :917, :1248)
+  __device__ __forceinline__ bool keep(float, double wm) const { return wm > 0.0; }
+};
+
+// partial[(blk * n_g + g) * R + r], R = 3 n_bin + 1 (E, B, K rows, weight)
+template <class Fac>
 __global__ void __launch_bounds__(256) k_marks_partials(const MarksField* __restrict__ fields, int n_field,
-                                                         int map0, int n_map_g, int n_map, int n_bin,
+                                                         const Fac fac, int n_g, int n_bin,
                                                          double* __restrict__ partial) {
   __shared__ double red[8][kMapGroup][3 * 32 + 1];
   const int blk = blockIdx.x;
@@ -65,16 +95,14 @@ __global__ void __launch_bounds__(256) k_marks_partials(const MarksField* __rest
       const float k = b < n_bin ? F.K[j * n_bin + b] : 0.f;
 #pragma unroll
       for (int g = 0; g < kMapGroup; ++g) {
-        if (g < n_map_g) {
-          const size_t o = (size_t)(map0 + g) * (size_t)F.n + (size_t)j;
-          const double wm = (double)F.w[o];
-          const double ww = (double)mw * wm;
-          if (ww > 0.0) {  // lenses with marks weight x weight <= 0 are removed
-            const double vw = (double)F.val[o] * wm;
+        if (g < n_g) {
+          double vw, wm;
+          fac.get(F, g, j, vw, wm);
+          if (fac.keep(mw, wm)) {
             aE[g] = fma((double)e, vw, aE[g]);
             aB[g] = fma((double)x, vw, aB[g]);
             aK[g] = fma((double)k, wm, aK[g]);
-            aw[g] += ww;
+            aw[g] = fma((double)mw, wm, aw[g]);
           }
         }
       }
@@ -90,7 +118,7 @@ __global__ void __launch_bounds__(256) k_marks_partials(const MarksField* __rest
     // fixed-order sum over the 8 warps
     for (int t = threadIdx.x; t < kMapGroup * 97; t += blockDim.x) {
       const int g = t / 97, r = t % 97;
-      if (g >= n_map_g) continue;
+      if (g >= n_g) continue;
       const int bb = b0 + (r % 32);
       const int q = r / 32;  // 0 E, 1 B, 2 K, 3 weight
       if (q < 3 && bb >= n_bin) continue;
@@ -98,9 +126,31 @@ __global__ void __launch_bounds__(256) k_marks_partials(const MarksField* __rest
       double s = 0.0;
       for (int wp = 0; wp < 8; ++wp) s += red[wp][g][r];
       const int row = q < 3 ? q * n_bin + bb : 3 * n_bin;
-      partial[((size_t)blk * n_map_g + g) * R + row] = s;
+      partial[((size_t)blk * n_g + g) * R + row] = s;
     }
     __syncthreads();
+  }
+}
+
+// Multiplicities of G resamples s0.. over n_units units: n_draw draws each,
+// counter (d/4, s, 0x2BCF, 0), word d%4, index by multiply-shift (the stream
+// of the patch bootstrap).  mult must be zeroed.
+__global__ void k_unit_mult(unsigned long long seed, long long n_units, long long n_draw, int s0, int G,
+                            int* mult) {
+  const long long nq = (n_draw + 3) / 4;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nq * G;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int g = (int)(t / nq);
+    const long long q = t % nq;
+    uint32_t c[4] = {(uint32_t)q, (uint32_t)(s0 + g), 0x2BCFu, 0u};
+    philox4x32(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    for (int u = 0; u < 4; ++u) {
+      const long long d = 4 * q + u;
+      if (d < n_draw) {
+        const long long idx = (long long)(((unsigned long long)c[u] * (unsigned long long)n_units) >> 32);
+        atomicAdd(&mult[(size_t)g * (size_t)n_units + (size_t)idx], 1);
+      }
+    }
   }
 }
 
@@ -115,6 +165,12 @@ __global__ void k_marks_reduce(const double* __restrict__ partial, const MarksFi
   double s = 0.0;
   for (int c = c0; c < c1; ++c) s += partial[((size_t)c * n_map_g + g) * R + r];
   out[t] = s;
+}
+
+// Flags a unit label outside [0, n_units).
+__global__ void k_check_units(const int* __restrict__ unit, long long n, long long n_units, int* bad) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    if (unit[i] < 0 || (long long)unit[i] >= n_units) atomicOr(bad, 1);
 }
 
 // max |a - b| over n entries, as order-preserving bits of a non-negative float.
@@ -157,6 +213,7 @@ extern "C" tpcf_status tpcf_xi_from_marks(tpcf_ctx* c, int32_t n_field, const tp
       F.n = n;
       F.n_bin = nb;
       F.chunk0 = nblk;
+      F.lens0 = 0;
       nblk += (int)((n + kMarksChunk - 1) / kMarksChunk);
       F.mw = stage(c, m.w, n);
       F.xiE = stage(c, m.xi_E, n * nb);
@@ -196,7 +253,7 @@ extern "C" tpcf_status tpcf_xi_from_marks(tpcf_ctx* c, int32_t n_field, const tp
     for (int m0 = 0; m0 < n_map; m0 += kMapGroup) {
       const int g = std::min(kMapGroup, n_map - m0);
       if (nblk > 0) {
-        k_marks_partials<<<nblk, 256, 0, st>>>(df, n_field, m0, g, n_map, nb, part);
+        k_marks_partials<MapFactors><<<nblk, 256, 0, st>>>(df, n_field, MapFactors{m0}, g, nb, part);
         counted(c, cudaGetLastError(), "marks partials");
       }
       const int tot = g * n_field * R;
@@ -231,6 +288,134 @@ extern "C" tpcf_status tpcf_xi_from_marks(tpcf_ctx* c, int32_t n_field, const tp
         if (g_x_stacked) g_x_stacked[(size_t)m * nb + b] = sB[b] / sK[b];
       }
       if (weights_stacked) weights_stacked[m] = sw;
+    }
+    return TPCF_OK;
+  } catch (const Failure& f) {
+    c->err = f.msg;
+    return f.status;
+  }
+}
+
+extern "C" tpcf_status tpcf_marks_bootstrap(tpcf_ctx* c, int32_t n_field, const tpcf_marks_field* marks,
+                                            const int32_t* unit, int64_t n_units, const int32_t* multiplicity,
+                                            uint64_t seed, int32_t n_boot, double supersampling, int32_t k_guard,
+                                            double* g_t, double* g_x, double* weights, double* cov_gt,
+                                            double* cov_gx) {
+  if (!c || n_field < 1 || !marks || n_boot < 1 || !(supersampling > 0)) return TPCF_ERR_INVALID_ARG;
+  const int nb = (int)marks[0].n_bin;
+  if (nb < 1 || nb > kMaxBins) return TPCF_ERR_INVALID_ARG;
+  int64_t n_lens = 0;
+  for (int i = 0; i < n_field; ++i) {
+    const tpcf_marks_field& m = marks[i];
+    if (m.n_bin != nb || m.n < 0 || (m.n > 0 && (!m.w || !m.xi_E || !m.xi_B || !m.K))) return TPCF_ERR_INVALID_ARG;
+    n_lens += m.n;
+  }
+  if (n_lens > (1ll << 31) - 2) return TPCF_ERR_INVALID_ARG;
+  if (!unit) n_units = n_lens;
+  if (n_units < 1) return TPCF_ERR_INVALID_ARG;
+  try {
+    begin_call(c);
+    cudaStream_t st = c->stream;
+    std::vector<MarksField> hf(n_field);
+    int nblk = 0;
+    int64_t off = 0;
+    for (int i = 0; i < n_field; ++i) {
+      const tpcf_marks_field& m = marks[i];
+      MarksField& F = hf[i];
+      F.n = m.n;
+      F.n_bin = nb;
+      F.chunk0 = nblk;
+      F.lens0 = off;
+      off += m.n;
+      nblk += (int)((m.n + kMarksChunk - 1) / kMarksChunk);
+      F.mw = stage(c, m.w, m.n);
+      F.xiE = stage(c, m.xi_E, m.n * nb);
+      F.xiB = stage(c, m.xi_B, m.n * nb);
+      F.K = stage(c, m.K, m.n * nb);
+      F.val = F.w = nullptr;
+    }
+    const int* dunit = unit ? stage(c, (const int*)unit, n_lens) : nullptr;
+    if (dunit) {  // labels must lie in [0, n_units): checked on the device before use
+      int* bad = (int*)ws_alloc(c, sizeof(int));
+      check(cudaMemsetAsync(bad, 0, sizeof(int), st), "memset");
+      k_check_units<<<(unsigned)std::min<int64_t>((n_lens + 255) / 256, 148 * 8), 256, 0, st>>>(dunit, n_lens, n_units,
+                                                                                                   bad);
+      counted(c, cudaGetLastError(), "unit check");
+      int hb = 0;
+      check(cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H check");
+      check(cudaStreamSynchronize(st), "sync check");
+      if (hb) throw Failure(TPCF_ERR_INVALID_ARG, "unit label outside [0, n_units)");
+    }
+    const int* dmult_all = multiplicity ? stage(c, (const int*)multiplicity, (int64_t)n_boot * n_units) : nullptr;
+    // n_samples = int(n_objects * supersampling_factor) (src/tpcf.f90:1234, :894)
+    const long long n_draw = (long long)((double)n_units * supersampling);
+    if (!multiplicity && n_draw < 1) throw Failure(TPCF_ERR_INVALID_ARG, "no draws per resample");
+    MarksField* df = (MarksField*)ws_alloc(c, sizeof(MarksField) * n_field);
+    check(cudaMemcpyAsync(df, hf.data(), sizeof(MarksField) * n_field, cudaMemcpyHostToDevice, st), "H2D fields");
+    const int R = 3 * nb + 1;
+    int* mbuf = multiplicity ? nullptr : (int*)ws_alloc(c, sizeof(int) * (size_t)kMapGroup * n_units);
+    double* part = (double*)ws_alloc(c, sizeof(double) * (size_t)std::max(nblk, 1) * kMapGroup * R);
+    double* dout = (double*)ws_alloc(c, sizeof(double) * (size_t)kMapGroup * n_field * R);
+    std::vector<double> sums((size_t)n_boot * n_field * R, 0.0);
+    for (int s0 = 0; s0 < n_boot; s0 += kMapGroup) {
+      const int G = std::min(kMapGroup, n_boot - s0);
+      const int* mult;
+      if (multiplicity) {
+        mult = dmult_all + (size_t)s0 * n_units;
+      } else {
+        check(cudaMemsetAsync(mbuf, 0, sizeof(int) * (size_t)G * n_units, st), "memset mult");
+        const long long work = (n_draw + 3) / 4 * G;
+        k_unit_mult<<<(unsigned)std::min<long long>((work + 255) / 256, 148 * 16), 256, 0, st>>>(seed, n_units, n_draw,
+                                                                                                 s0, G, mbuf);
+        counted(c, cudaGetLastError(), "bootstrap draws");
+        mult = mbuf;
+      }
+      if (nblk > 0) {
+        k_marks_partials<MultFactors><<<nblk, 256, 0, st>>>(df, n_field, MultFactors{mult, dunit, n_units}, G, nb,
+                                                            part);
+        counted(c, cudaGetLastError(), "bootstrap partials");
+        const int tot = G * n_field * R;
+        k_marks_reduce<<<(tot + 255) / 256, 256, 0, st>>>(part, df, n_field, nblk, G, R, dout);
+        counted(c, cudaGetLastError(), "bootstrap reduce");
+        check(cudaMemcpyAsync(sums.data() + (size_t)s0 * n_field * R, dout, sizeof(double) * tot,
+                              cudaMemcpyDeviceToHost, st), "D2H sums");
+      }
+    }
+    check(cudaStreamSynchronize(st), "sync bootstrap");
+    // all fields together (src/tpcf.f90:1245-1262); K > 0 guard of the point
+    // bootstraps, plain quotients for the pair-weighted block bootstrap (:929-930)
+    std::vector<double> gt((size_t)n_boot * nb), gx((size_t)n_boot * nb);
+    for (int s = 0; s < n_boot; ++s) {
+      double W = 0.0;
+      for (int b = 0; b < nb; ++b) {
+        double E = 0.0, B = 0.0, K = 0.0;
+        for (int i = 0; i < n_field; ++i) {
+          const double* r = sums.data() + ((size_t)s * n_field + i) * R;
+          E += r[b];
+          B += r[nb + b];
+          K += r[2 * nb + b];
+        }
+        const bool zero = k_guard && !(K > 0.0);
+        gt[(size_t)s * nb + b] = zero ? 0.0 : E / K;
+        gx[(size_t)s * nb + b] = zero ? 0.0 : B / K;
+      }
+      for (int i = 0; i < n_field; ++i) W += sums[((size_t)s * n_field + i) * R + 3 * nb];
+      if (weights) weights[s] = W;
+    }
+    if (g_t) std::memcpy(g_t, gt.data(), sizeof(double) * gt.size());
+    if (g_x) std::memcpy(g_x, gx.data(), sizeof(double) * gx.size());
+    if ((cov_gt || cov_gx) && n_boot >= 2) {
+      double* dg = (double*)ws_alloc(c, sizeof(double) * gt.size());
+      double* dc = (double*)ws_alloc(c, sizeof(double) * (size_t)nb * nb);
+      for (int q = 0; q < 2; ++q) {
+        double* user = q == 0 ? cov_gt : cov_gx;
+        if (!user) continue;
+        check(cudaMemcpyAsync(dg, (q == 0 ? gt : gx).data(), sizeof(double) * gt.size(), cudaMemcpyHostToDevice, st),
+              "H2D g");
+        counted(c, launch_cov(dg, n_boot, nb, dc, st), "covariance");
+        check(cudaMemcpyAsync(user, dc, sizeof(double) * nb * nb, cudaMemcpyDefault, st), "D2H cov");
+        check(cudaStreamSynchronize(st), "sync cov");
+      }
     }
     return TPCF_OK;
   } catch (const Failure& f) {

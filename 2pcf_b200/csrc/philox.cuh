@@ -1,0 +1,24 @@
+// philox.cuh -- Philox4x32-10 counter-based generator (Salmon et al., SC'11,
+// "Parallel random numbers: as easy as 1, 2, 3"): ten rounds of the published
+// multipliers and Weyl key increments.  Shared by the patch and the per-lens
+// bootstrap draws, which use the same counter layout (d/4, s, 0x2BCF, 0), so
+// the two resamplings draw the same stream for the same seed.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tpcf {
+
+__device__ __forceinline__ void philox4x32(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c[0]), lo0 = 0xD2511F53u * c[0];
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]), lo1 = 0xCD9E8D57u * c[2];
+    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+}  // namespace tpcf

@@ -64,6 +64,8 @@ cudaError_t launch_lens_outputs(const double* acc, const float4* rec, const int*
                                 float* xi_E, float* xi_B, float* K_m, float* w_m, float* marks_weight,
                                 double* lens_sums, double* lens_raw, cudaStream_t st);
 
+cudaError_t launch_cov(const double* x, int n_s, int D, double* cov, cudaStream_t st);
+
 cudaError_t sort_pairs_u32(void* tmp, size_t& tmp_bytes, const unsigned* kin, unsigned* kout, const int* vin,
                            int* vout, int n, int end_bit, cudaStream_t st);
 cudaError_t sort_pairs_u64(void* tmp, size_t& tmp_bytes, const unsigned long long* kin, unsigned long long* kout,

@@ -21,7 +21,8 @@ from . import Context, KappaMap, LensCatalog, ShapeCatalog, _Arr, _check, _resol
 from ._lib import MarksFieldC, lib
 
 __all__ = ["read_table", "load_standard_shape_catalog", "load_standard_kappa_map", "load_standard_lens_catalog",
-           "write_result_table", "MarksField", "save_marks", "load_survey_marks", "calculate_tpcf_from_marks"]
+           "write_result_table", "MarksField", "save_marks", "load_survey_marks", "calculate_tpcf_from_marks",
+           "marks_bootstrap"]
 
 
 def read_table(filename, ncols: int, keep_positive_col: int = -1, keep_nonnegative_col: int = -1,
@@ -175,4 +176,33 @@ def calculate_tpcf_from_marks(marks: Sequence[MarksField], val, w, lens_x=None, 
                ctx.handle)
     if one:
         out = {k: v[0] for k, v in out.items()}
+    return out
+
+
+def marks_bootstrap(marks: Sequence[MarksField], n_boot: int, seed: int = 0, supersampling_factor: float = 1.0,
+                    units=None, n_units: int = 0, multiplicity=None, k_guard: bool = True, covariance: bool = True,
+                    ctx: Context = None):
+    """Point or block bootstrap from per-lens marks (tpcf_marks_bootstrap).
+
+    ``units=None``: every lens of ``marks`` (all fields in order) is a unit --
+    simple_bootstrap_foreground / survey_marked_point_bootstrap
+    (src/tpcf.f90:547-634, :1194-1265).  ``units``: an int label per lens in
+    [0, n_units) -- the resampling of pair_weighted_block_bootstrap (:844-939,
+    with k_guard=False for its plain quotients).  Returns g_t, g_x
+    [n_boot][n_bin], weights [n_boot] and the covariances."""
+    ctx = _resolve_ctx(ctx)
+    arr, keep = _cfields(marks)
+    U = _Arr(units, np.int32)
+    M = _Arr(multiplicity, np.int32)
+    nb = marks[0].n_bin
+    out = {"g_t": np.zeros((n_boot, nb)), "g_x": np.zeros((n_boot, nb)), "weights": np.zeros(n_boot)}
+    if covariance:
+        out["cov_g_t"] = np.zeros((nb, nb))
+        out["cov_g_x"] = np.zeros((nb, nb))
+    p = lambda k: out[k].ctypes.data if k in out else None
+    with np.errstate(invalid="ignore", divide="ignore"):
+        _check(lib().tpcf_marks_bootstrap(ctx.handle, len(marks), arr, U.ptr, int(n_units), M.ptr,
+                                          int(seed) & 0xFFFFFFFFFFFFFFFF, int(n_boot), float(supersampling_factor),
+                                          int(bool(k_guard)), p("g_t"), p("g_x"), p("weights"), p("cov_g_t"),
+                                          p("cov_g_x")), ctx.handle)
     return out

@@ -283,6 +283,24 @@ tpcf_status tpcf_xi_from_marks(tpcf_ctx* ctx, int32_t n_field, const tpcf_marks_
                                const float* const* lens_y, double* g_t, double* g_x, double* weights,
                                double* g_t_stacked, double* g_x_stacked, double* weights_stacked);
 
+/* Resampling of per-lens marks: simple_bootstrap_foreground with marks
+ * (src/tpcf.f90:547-634), survey_marked_point_bootstrap (:1194-1265) and the
+ * resampling step of pair_weighted_block_bootstrap (:844-939).  The units are
+ * the lenses of all fields in order (unit == NULL, n_units ignored) or the
+ * labels unit[j] in [0, n_units) of the lenses (blocks, e.g. from
+ * tpcf_kmeans).  Each resample draws int(n_units * supersampling) units with
+ * replacement -- Philox4x32-10 with the counter layout of tpcf_bootstrap --
+ * unless multiplicity [n_boot][n_units] is given.  Outputs (nullable):
+ * g_t, g_x [n_boot][n_bin] = sum_j mult_j xi_E_j / sum_j mult_j K_j over all
+ * fields (k_guard != 0: 0 where that K <= 0, as the point bootstraps; 0:
+ * plain quotients, as the block one), weights [n_boot] = sum_j mult_j w_j,
+ * and the [n_bin][n_bin] covariances of g_t and g_x over the resamples.
+ * Marks may be host or device pointers. */
+tpcf_status tpcf_marks_bootstrap(tpcf_ctx* ctx, int32_t n_field, const tpcf_marks_field* marks,
+                                 const int32_t* unit, int64_t n_units, const int32_t* multiplicity,
+                                 uint64_t seed, int32_t n_boot, double supersampling, int32_t k_guard,
+                                 double* g_t, double* g_x, double* weights, double* cov_gt, double* cov_gx);
+
 /* Unit vectors of n points (lambda, phi in radians) as the spherical kernels
  * use them: u in FP64 by the library's fixed sine/cosine sequence, then
  * hi = fl32(u), lo = fl32(u - hi); hi and lo are [n][3].  Inputs and

@@ -453,3 +453,23 @@ def xi_from_marks(fields, vals, ws):
         E, B, K, W = E + e, B + b, K + k, W + wsum
     with np.errstate(invalid="ignore", divide="ignore"):
         return res, {"g_t": E / K, "g_x": B / K, "weights": W}
+
+
+def marks_bootstrap(fields, mult, units=None, k_guard=True):
+    """Resampled xi from per-lens marks (src/tpcf.f90:547-634, :844-939,
+    :1194-1265) for given multiplicities [n_boot][n_units], FP64: the lens
+    multiplicity is mult[unit(lens)] (the lens itself when units is None)."""
+    E = np.concatenate([np.asarray(m["xi_E"], np.float64) for m in fields])
+    B = np.concatenate([np.asarray(m["xi_B"], np.float64) for m in fields])
+    K = np.concatenate([np.asarray(m["K"], np.float64) for m in fields])
+    W = np.concatenate([np.asarray(m["w"], np.float64) for m in fields])
+    mult = np.asarray(mult, np.float64)
+    m = mult if units is None else mult[:, np.asarray(units)]
+    e, b, k = m @ E, m @ B, m @ K
+    with np.errstate(invalid="ignore", divide="ignore"):
+        if k_guard:
+            gt = np.where(k > 0, e / np.where(k > 0, k, 1), 0.0)
+            gx = np.where(k > 0, b / np.where(k > 0, k, 1), 0.0)
+        else:
+            gt, gx = e / k, b / k
+    return gt, gx, m @ W

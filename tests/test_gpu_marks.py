@@ -75,3 +75,34 @@ def test_device_tensors(tpcf, oracle, ctx):
     out = tpcf.calculate_tpcf_from_marks(marks, [torch.from_numpy(v).cuda()], [torch.from_numpy(w).cuda()], ctx=ctx)
     per, _ = oracle.xi_from_marks(raw, [v[1]], [w[1]])
     np.testing.assert_allclose(out["g_t"][1, 0], per[0]["g_t"], rtol=1e-9)
+
+
+def test_point_bootstrap_matches_oracle(tpcf, oracle, ctx):
+    """Per-lens resampling over two fields: the drawn multiplicities are those
+    of the patch bootstrap's Philox stream with the lenses as units."""
+    rng = np.random.default_rng(11)
+    raw = [rand_marks(rng, n, 9) for n in (3000, 1234)]
+    marks = [tpcf.MarksField(**m) for m in raw]
+    n_boot, n_units = 37, 4234
+    out = tpcf.marks_bootstrap(marks, n_boot, seed=77, supersampling_factor=1.3, ctx=ctx)
+    mult = oracle.bootstrap_multiplicity(77, n_boot, n_units, int(n_units * 1.3))
+    gt, gx, W = oracle.marks_bootstrap(raw, mult)
+    np.testing.assert_allclose(out["g_t"], gt, rtol=1e-10)
+    np.testing.assert_allclose(out["g_x"], gx, rtol=1e-10)
+    np.testing.assert_allclose(out["weights"], W, rtol=1e-12)
+    np.testing.assert_allclose(out["cov_g_t"], np.cov(gt.T), rtol=1e-8, atol=1e-300)
+
+
+def test_block_bootstrap_from_labels(tpcf, oracle, ctx):
+    rng = np.random.default_rng(12)
+    raw = [rand_marks(rng, 5000, 12)]
+    marks = [tpcf.MarksField(**m) for m in raw]
+    labels = rng.integers(0, 50, 5000).astype(np.int32)
+    mult = rng.integers(0, 3, (20, 50)).astype(np.int32)
+    out = tpcf.marks_bootstrap(marks, 20, units=labels, n_units=50, multiplicity=mult, k_guard=False,
+                               covariance=False, ctx=ctx)
+    gt, gx, W = oracle.marks_bootstrap(raw, mult, units=labels, k_guard=False)
+    np.testing.assert_allclose(out["g_t"], gt, rtol=1e-10)
+    np.testing.assert_allclose(out["weights"], W, rtol=1e-12)
+    with pytest.raises(tpcf.TPCFError):
+        tpcf.marks_bootstrap(marks, 2, units=labels, n_units=40, ctx=ctx)
