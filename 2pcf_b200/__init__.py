@@ -30,7 +30,10 @@ __all__ = [
     "Binning", "create_bins", "Context", "ShapeCatalog", "LensCatalog", "KappaMap",
     "LensingSurveyField", "Shear2pcfResults", "shear_2pcf", "kappa_2pcf",
     "tangential_shear_tpcf", "scalar_kappa_tpcf", "batch_shear_2pcf", "partition_data",
-    "block_bootstrap", "TPCFError",
+    "partition_data_equal", "block_bootstrap", "TPCFError", "rotate_data_from_poles_and_meridian",
+    "unit_vectors", "read_table", "load_standard_shape_catalog", "load_standard_kappa_map",
+    "load_standard_lens_catalog", "write_result_table", "MarksField", "save_marks", "load_survey_marks",
+    "calculate_tpcf_from_marks", "marks_bootstrap",
 ]
 
 
@@ -444,6 +447,27 @@ def partition_data(x, y, weights, k, iterations=1000, reassignment_tol=0.0, ctx:
                              float(reassignment_tol), lab.ctypes.data, cen.ctypes.data, C.byref(it)),
            ctx.handle)
     return lab, cen, it.value
+
+
+def partition_data_equal(x, y, weights, k, weight_equalizer_scaling=3.0, weight_tol=0.05, iterations=1000,
+                         reassignment_tol=0.01, random_init=True, seed=0, ctx: Context = None):
+    """partition_data with equal_size (src/kmeans.f90:12-262) on the GPU: the
+    weight-penalised assignment and the post-processing rebalance that move
+    boundary points out of overweight clusters.  Defaults are those of
+    pair_weighted_block_bootstrap (src/tpcf.f90:892-895).  Returns (labels,
+    centroids, iterations, max weight deviation (max W - min W) / mean W)."""
+    ctx = _resolve_ctx(ctx)
+    X, Y, W = _Arr(x), _Arr(y), _Arr(weights)
+    n = X.n
+    lab = np.zeros(n, np.int32)
+    cen = np.zeros((k, 2), np.float32)
+    it = C.c_int32()
+    dev = C.c_float()
+    _check(lib().tpcf_kmeans_equal(ctx.handle, X.ptr, Y.ptr, W.ptr, n, int(k), int(iterations),
+                                   float(reassignment_tol), float(weight_equalizer_scaling), float(weight_tol),
+                                   int(bool(random_init)), int(seed) & 0xFFFFFFFFFFFFFFFF, lab.ctypes.data,
+                                   cen.ctypes.data, C.byref(it), C.byref(dev)), ctx.handle)
+    return lab, cen, it.value, dev.value
 
 
 def block_bootstrap(patch_sums, n_boot, seed=0, supersampling_factor=1.0, multiplicity=None,

@@ -123,6 +123,8 @@ def lib():
     _sig(L, "tpcf_shear_scalar_adjoint", st, [vp] + [vp] * 5 + [i64] + [vp] * 7 + [i64] +
          [C.POINTER(Bins)] + [vp] * 4 + [vp] * 2 + [vp] * 6)
     _sig(L, "tpcf_kmeans", st, [vp, vp, vp, vp, i64, i32, i32, C.c_float, vp, vp, C.POINTER(i32)])
+    _sig(L, "tpcf_kmeans_equal", st, [vp, vp, vp, vp, i64, i32, i32, C.c_float, C.c_float, C.c_float, i32,
+                                      C.c_uint64, vp, vp, C.POINTER(i32), C.POINTER(C.c_float)])
     _sig(L, "tpcf_bootstrap", st, [vp, vp, i32, i32, i32, vp, C.c_uint64, i32, C.c_double,
                                    vp, vp, vp, vp, vp, vp])
     _declare_extra(L)

@@ -387,6 +387,27 @@ tpcf_status tpcf_kmeans(tpcf_ctx* ctx, const float* x, const float* y, const flo
                         int32_t k, int32_t max_iter, float reassign_tol,
                         int32_t* labels_out, float* centroids_out, int32_t* n_iter_out);
 
+/* Replaces partition_data with equal_size = .true. (src/kmeans.f90:12-262),
+ * as pair_weighted_block_bootstrap calls it (src/tpcf.f90:892-895): from
+ * pass 2 on, the distance to cluster j is scaled by
+ * 1 + (W_j / W_mean - 1) * weight_scaling, W_j the cluster weights after the
+ * previous pass (the reference updates them during the pass, in thread
+ * order); each point keeps its second-nearest cluster and the distance ratio;
+ * after the Lloyd passes, if (max W - min W) / W_mean > weight_tol, clusters
+ * are visited heaviest first and their members, smallest ratio first, move to
+ * their second cluster (if not yet visited) until the cluster is at most
+ * W_mean (1 + weight_tol) -- the greedy rebalance of :221-262.  Weights are
+ * summed in 64-bit fixed point (exact, deterministic).  random_init != 0:
+ * k distinct random points as centroids and random labels (Philox4x32-10
+ * from seed) as kmeans_compute_random_initial_centroids; 0: the fixed grid of
+ * tpcf_kmeans.  centroids_out are those of the last pass (before the
+ * rebalance, as the reference); *max_dev_out (nullable) the final
+ * (max W - min W) / W_mean. */
+tpcf_status tpcf_kmeans_equal(tpcf_ctx* ctx, const float* x, const float* y, const float* w, int64_t n,
+                              int32_t k, int32_t max_iter, float reassign_tol, float weight_scaling,
+                              float weight_tol, int32_t random_init, uint64_t seed, int32_t* labels_out,
+                              float* centroids_out, int32_t* n_iter_out, float* max_dev_out);
+
 /* Replaces the resampling loop of survey_marked_point_block_bootstrap
  * (src/tpcf.f90:1166-1191) and covariance_matrix (src/utils.f90:745-764) for
  * n_task tasks at once.  patch_sums is [n_task][n_patch][6][n_bin] as the pair

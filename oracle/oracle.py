@@ -81,6 +81,9 @@ def lib():
                                        [_f64p, C.c_int, C.c_int, _f64p])
         L.orc_sphere_edges_sq.argtypes = [_f64p, C.c_int, _f64p]
         L.orc_unit_vectors.argtypes = [C.c_long, vp, vp, vp, vp]
+        L.orc_kmeans_equal_det.argtypes = [C.c_long, vp, vp, vp, C.c_int, C.c_int, C.c_float, C.c_float,
+                                           C.c_float, C.c_int, C.c_uint64, vp, vp, vp, C.POINTER(C.c_int),
+                                           C.POINTER(C.c_float)]
         L.orc_rotate_from_poles.argtypes = [vp, vp, C.c_long, vp, vp, C.c_long, C.c_float,
                                             C.POINTER(C.c_int), vp]
         _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
@@ -473,3 +476,19 @@ def marks_bootstrap(fields, mult, units=None, k_guard=True):
         else:
             gt, gx = e / k, b / k
     return gt, gx, m @ W
+
+
+def kmeans_equal(x, y, w, k, scaling=3.0, weight_tol=0.05, max_iter=1000, reassign_tol=0.01, random_init=True,
+                 seed=0):
+    """Equal-weight k-means restated serially (labels, centroids, iterations, max deviation)."""
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+    x, y, w = f(x), f(y), f(w)
+    n = len(x)
+    lab = np.zeros(n, np.int32)
+    cx = np.zeros(k, np.float32)
+    cy = np.zeros(k, np.float32)
+    it = C.c_int()
+    dev = C.c_float()
+    lib().orc_kmeans_equal_det(n, _ptr(x), _ptr(y), _ptr(w), k, max_iter, reassign_tol, scaling, weight_tol,
+                               int(random_init), seed, _ptr(lab), _ptr(cx), _ptr(cy), C.byref(it), C.byref(dev))
+    return lab, np.stack([cx, cy], 1), it.value, dev.value

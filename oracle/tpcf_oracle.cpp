@@ -1288,6 +1288,156 @@ int orc_kmeans_det(long n, const float* x, const float* y, const float* w, int k
   return 0;
 }
 
+// Equal-weight k-means (partition_data with equal_size, src/kmeans.f90:12-262)
+// restated serially with the library's deterministic choices: the points are
+// swept in order in chunks (32..1024 points, n/2048) and the points of a chunk
+// see the cluster weights the previous chunks left (the reference moves the
+// weight of each reassigned point at once, in OpenMP thread order);
+// fixed-point weights and sums; Philox draws for the random start.  The rebalance follows
+// postprocess_weights (:221-262) point by point.
+int orc_kmeans_equal_det(long n, const float* x, const float* y, const float* w, int k, int max_iter,
+                         float reassign_tol, float scaling, float weight_tol, int random_init, uint64_t seed,
+                         int* labels, float* cx, float* cy, int* n_iter_out, float* max_dev_out) {
+  if (k <= 1 || n < 1) return 1;
+  float xmn = x[0], xmx = x[0], ymn = y[0], ymx = y[0];
+  double wmax = 0;
+  for (long i = 0; i < n; ++i) {
+    xmn = std::min(xmn, x[i]); xmx = std::max(xmx, x[i]);
+    ymn = std::min(ymn, y[i]); ymx = std::max(ymx, y[i]);
+    wmax = std::max(wmax, fabs((double)w[i]));
+  }
+  const double amax = std::max(std::max(fabs((double)xmn), fabs((double)xmx)), std::max(fabs((double)ymn), fabs((double)ymx)));
+  const float diam = sqrtf((xmx - xmn) * (xmx - xmn) + (ymx - ymn) * (ymx - ymn));
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  if (random_init) {
+    std::vector<long> chosen;
+    for (uint32_t t = 0; (int)chosen.size() < k; ++t) {
+      uint32_t c[4] = {t / 4, 0xC3u, 0x4B4Du, 0u};
+      det::philox4x32(c, k0, k1);
+      const long idx = (long)(((uint64_t)c[t % 4] * (uint64_t)n) >> 32);
+      if (std::find(chosen.begin(), chosen.end(), idx) == chosen.end()) chosen.push_back(idx);
+    }
+    for (int j = 0; j < k; ++j) { cx[j] = x[chosen[j]]; cy[j] = y[chosen[j]]; }
+    for (long q = 0; q < (n + 3) / 4; ++q) {
+      uint32_t c[4] = {(uint32_t)q, 0xC4u, 0x4B4Du, 0u};
+      det::philox4x32(c, k0, k1);
+      for (int u = 0; u < 4; ++u)
+        if (4 * q + u < n) labels[4 * q + u] = (int)(((uint64_t)c[u] * (uint32_t)k) >> 32);
+    }
+  } else {
+    int n_side = (int)sqrtf((float)k);
+    if (xmx - xmn > ymx - ymn) {
+      float dy = (ymx - ymn) / (float)n_side;
+      float dx = (xmx - xmn) * (float)n_side / (float)k;
+      for (int j = 1; j <= k; ++j) {
+        int row = (int)((dx / 2.0f + dx * (float)(j - 1)) / (xmx - xmn));
+        cx[j - 1] = xmn + fmodf(dx / 2.0f + dx * (float)(j - 1), xmx - xmn);
+        cy[j - 1] = ymn + dy / 2.0f + dy * (float)row;
+      }
+    } else {
+      float dx = (xmx - xmn) / (float)n_side;
+      float dy = (ymx - ymn) * (float)n_side / (float)k;
+      for (int j = 1; j <= k; ++j) {
+        int row = (int)((dy / 2.0f + dy * (float)(j - 1)) / (ymx - ymn));
+        cy[j - 1] = ymn + fmodf(dy / 2.0f + dy * (float)(j - 1), ymx - ymn);
+        cx[j - 1] = xmn + dx / 2.0f + dx * (float)row;
+      }
+    }
+    for (long i = 0; i < n; ++i) labels[i] = (int)((float)i / (float)n * (float)k + 1.0f) - 1;
+  }
+  const int sp = det::fixed_scale(n, amax * wmax);
+  const int sw = det::fixed_scale(n, wmax);
+  std::vector<long long> W(k, 0);
+  for (long i = 0; i < n; ++i)
+    if (labels[i] >= 0) W[labels[i]] += llrint(ldexp((double)w[i], sw));
+  long long tot = 0;
+  for (int j = 0; j < k; ++j) tot += W[j];
+  const float wmean = (float)(ldexp((double)tot, -sw) / k);
+  const long chunk = std::max(32L, std::min(1024L, n / 2048));
+  std::vector<int> cand(n, -1);
+  std::vector<float> memb(n, 0.0f), f(k, 1.0f);
+  int it = 0;
+  while (it <= max_iter) {
+    ++it;
+    const bool pen = it > 1 && scaling > 0.0f, cands = it > 1;
+    long n_re = 0;
+    for (long base = 0; base < n; base += chunk) {
+      // the points of one chunk see the weights the previous chunks left
+      for (int j = 0; j < k; ++j)
+        f[j] = pen ? 1.0f + (((float)ldexp((double)W[j], -sw) / wmean) - 1.0f) * scaling : 1.0f;
+      for (long i = base; i < std::min(n, base + chunk); ++i) {
+        float best = diam * 10.0f, cm = 0.0f;
+        int bi = -1, ci = -1;
+        for (int j = 0; j < k; ++j) {
+          const float ddx = x[i] - cx[j], ddy = y[i] - cy[j];
+          const float d = f[j] * sqrtf(ddx * ddx + ddy * ddy);
+          if (cands && d > 0.0f) {
+            if (d < best) { cm = best / d; ci = bi; best = d; bi = j; }
+            else if (d < cm * best) { cm = d / best; ci = j; }
+          } else if (d < best) { best = d; bi = j; }
+        }
+        if (cands) { cand[i] = ci; memb[i] = cm; }
+        const int old = labels[i];
+        if (bi != old) {
+          labels[i] = bi;
+          ++n_re;
+          const long long wf = llrint(ldexp((double)w[i], sw));
+          if (old >= 0) W[old] -= wf;
+          if (bi >= 0) W[bi] += wf;
+        }
+      }
+    }
+    std::vector<long long> ax(k, 0), ay(k, 0), aw(k, 0);
+    for (long i = 0; i < n; ++i) {
+      const int c = labels[i];
+      if (c < 0) continue;
+      ax[c] += llrint(ldexp((double)x[i] * (double)w[i], sp));
+      ay[c] += llrint(ldexp((double)y[i] * (double)w[i], sp));
+      aw[c] += llrint(ldexp((double)w[i], sw));
+    }
+    for (int j = 0; j < k; ++j) {
+      const double Wd = ldexp((double)aw[j], -sw);
+      cx[j] = (float)(ldexp((double)ax[j], -sp) / Wd);
+      cy[j] = (float)(ldexp((double)ay[j], -sp) / Wd);
+    }
+    if (n_re == 0) break;
+    if ((float)n_re / (float)n < reassign_tol) break;
+  }
+  auto max_dev = [&]() {
+    const long long mx = *std::max_element(W.begin(), W.end()), mn = *std::min_element(W.begin(), W.end());
+    return (float)(ldexp((double)(mx - mn), -sw) / (double)wmean);
+  };
+  float dev = max_dev();
+  if (dev > weight_tol && it > 1) {
+    std::vector<int> corder(k);
+    for (int j = 0; j < k; ++j) corder[j] = j;
+    std::stable_sort(corder.begin(), corder.end(), [&](int a, int b) { return W[a] > W[b]; });
+    std::vector<long> order(n);
+    for (long i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](long a, long b) { return memb[a] < memb[b]; });
+    const long long thr = llrint(ldexp((double)(wmean * (1.0f + weight_tol)), sw));
+    std::vector<char> done(k, 0);
+    for (int j = 0; j < k; ++j) {
+      const int cj = corder[j];
+      done[cj] = 1;
+      for (long r = 0; r < n; ++r) {
+        const long p = order[r];
+        const int d = cand[p];
+        if (labels[p] != cj || d < 0 || done[d]) continue;
+        const long long wf = llrint(ldexp((double)w[p], sw));
+        labels[p] = d;
+        W[cj] -= wf;
+        W[d] += wf;
+        if (W[cj] <= thr) break;
+      }
+    }
+    dev = max_dev();
+  }
+  if (n_iter_out) *n_iter_out = it;
+  if (max_dev_out) *max_dev_out = dev;
+  return 0;
+}
+
 int orc_fixed_scale(long n, double vmax) { return det::fixed_scale(n, vmax); }
 
 // Raw Philox4x32-10 block, for known-answer tests.

@@ -77,3 +77,27 @@ def test_pairs_kmeans_bootstrap_chain(tpcf, oracle, ctx):
     assert np.all(np.abs(boot["g_t"][:, 0] - gt) <= 1e-6 * scale)
     cov = oracle.covariance(gt)
     assert np.all(np.abs(boot["cov_g_t"] - cov) <= 1e-5 * np.abs(cov).max())
+
+
+@pytest.mark.parametrize("random_init", [True, False])
+def test_equal_weight_kmeans_bit_exact(tpcf, oracle, ctx, random_init):
+    """partition_data with equal_size (src/kmeans.f90:12-262): labels and
+    centroids bit-exact with the oracle's serial restatement (chunked sweep,
+    fixed-point weights, rebalance), and far more even cluster weights than
+    plain k-means."""
+    rng = np.random.default_rng(31)
+    n = 60000
+    x = np.concatenate([rng.normal(200, 20, n // 2), rng.uniform(0, 1000, n - n // 2)]).astype(np.float32)
+    y = np.concatenate([rng.normal(300, 20, n // 2), rng.uniform(0, 800, n - n // 2)]).astype(np.float32)
+    w = rng.uniform(0.01, 1.01, n).astype(np.float32)
+    lab, cen, it, dev = tpcf.partition_data_equal(x, y, w, 40, random_init=random_init, seed=9, ctx=ctx)
+    olab, ocen, oit, odev = oracle.kmeans_equal(x, y, w, 40, random_init=random_init, seed=9)
+    assert it == oit
+    np.testing.assert_array_equal(lab, olab)
+    np.testing.assert_array_equal(cen, ocen)
+    assert dev == odev
+    W = np.bincount(lab, weights=w.astype(np.float64), minlength=40)
+    assert abs((W.max() - W.min()) / W.mean() - dev) < 1e-5
+    plab, _, _ = tpcf.partition_data(x, y, w, 40, ctx=ctx)
+    Wp = np.bincount(plab, weights=w.astype(np.float64), minlength=40)
+    assert dev < 0.5 * (Wp.max() - Wp.min()) / Wp.mean()

@@ -181,3 +181,19 @@ def test_kmeans_deterministic_vs_reference_fraction(oracle):
     agree = np.mean(g["det_labels"] == g["ref_labels"])
     assert agree > 0.99
     assert len(np.unique(g["det_labels"])) == int(g["k"])
+
+
+def test_equal_weight_kmeans_restatement_balances(oracle):
+    """The equal-weight restatement gives valid labels, cluster weights that
+    match its reported deviation, and a much smaller spread than plain k-means."""
+    rng = np.random.default_rng(7)
+    n = 20000
+    x = np.concatenate([rng.normal(0, 5, n // 2), rng.uniform(0, 100, n // 2)]).astype(np.float32)
+    y = np.concatenate([rng.normal(0, 5, n // 2), rng.uniform(0, 100, n // 2)]).astype(np.float32)
+    w = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    lab, cen, it, dev = oracle.kmeans_equal(x, y, w, 20, random_init=False)
+    assert lab.min() >= 0 and lab.max() < 20
+    W = np.bincount(lab, weights=w.astype(np.float64), minlength=20)
+    assert abs((W.max() - W.min()) / W.mean() - dev) < 1e-5
+    _, _, _, dev0 = oracle.kmeans_equal(x, y, w, 20, scaling=0.0, weight_tol=1e9, random_init=False)
+    assert dev < 0.3 * dev0
