@@ -194,24 +194,23 @@ __device__ __forceinline__ void chunk_dual(const SrcRec* __restrict__ S, int cnt
     const float4 b = S[j].b;
     float d2, d, r, X, Y;
     pair_terms<MODE, LOGB>(lx, ly, a, d2, d, r, X, Y);
-    const float t1 = r * X, t2 = r * Y;
     bool up = d2 >= E;
     if (fabsf(d2 - E) <= gE) {
       // canonical bin is blo or blo+1, or -1 on a side outside [x_min, x_max]
       const int cb = slow_bin(lx, ly, a.x, a.y, C.e2s, C.nb);
       up = (cb == blo + 1) || (cb < 0 && blo + 1 == C.nb);
     }
-    const float dw = d * b.x;
-    tot[QGT] += t1;
-    tot[QGX] += t2;
+    // products folded into the sums: one FFMA per quantity and side
+    tot[QGT] = fmaf(r, X, tot[QGT]);
+    tot[QGX] = fmaf(r, Y, tot[QGX]);
     tot[QW] += b.x;
-    tot[QDW] += dw;
+    tot[QDW] = fmaf(d, b.x, tot[QDW]);
     if (MODE == 0 && HAS_M) tot[QK] += b.y;
     if (up) {
-      hi[QGT] += t1;
-      hi[QGX] += t2;
+      hi[QGT] = fmaf(r, X, hi[QGT]);
+      hi[QGX] = fmaf(r, Y, hi[QGX]);
       hi[QW] += b.x;
-      hi[QDW] += dw;
+      hi[QDW] = fmaf(d, b.x, hi[QDW]);
       hi[QN] += 1.f;
       if (MODE == 0 && HAS_M) hi[QK] += b.y;
     }

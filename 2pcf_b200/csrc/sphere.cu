@@ -235,23 +235,21 @@ __device__ __forceinline__ void chunk_dual_s(const SrcRecS* __restrict__ S, int 
     const float4 a = S[j].a, b = S[j].b, cc = S[j].c;
     float d2, th, r, X, Y;
     sph_terms<MODE, SMALL>(L, a, b, d2, th, r, X, Y);
-    const float t1 = r * X, t2 = r * Y;
     bool up = d2 >= E;
     if (fabsf(d2 - E) <= gE) {
       const int cb = slow_bin_s(L.h, L.l, a, b, C.e2s, C.nb);
       up = (cb == blo + 1) || (cb < 0 && blo + 1 == C.nb);
     }
-    const float dw = th * cc.x;
-    tot[QGT] += t1;
-    tot[QGX] += t2;
+    tot[QGT] = fmaf(r, X, tot[QGT]);
+    tot[QGX] = fmaf(r, Y, tot[QGX]);
     tot[QW] += cc.x;
-    tot[QDW] += dw;
+    tot[QDW] = fmaf(th, cc.x, tot[QDW]);
     if (MODE == 0 && HAS_M) tot[QK] += cc.y;
     if (up) {
-      hi[QGT] += t1;
-      hi[QGX] += t2;
+      hi[QGT] = fmaf(r, X, hi[QGT]);
+      hi[QGX] = fmaf(r, Y, hi[QGX]);
       hi[QW] += cc.x;
-      hi[QDW] += dw;
+      hi[QDW] = fmaf(th, cc.x, hi[QDW]);
       hi[QN] += 1.f;
       if (MODE == 0 && HAS_M) hi[QK] += cc.y;
     }

@@ -170,28 +170,31 @@ def adjoint_timing(w, ctx, bins, step_ms, pair_ms, stream):
     import torch
     ag = importlib.import_module("2pcf_b200.autograd")
     d = lambda a: torch.from_numpy(a).cuda()
-    rng = np.random.default_rng(1004)
     t_fwd = t_all = 0.0
     pairs = 0
-    for (i, j) in w["tasks"]:
-        L, S = w["lens_bins"][i], w["shape_bins"][j]
-        geo = dict(x_A=d(L["x"]), y_A=d(L["y"]), z_A=d(L["z"]), x_B=d(S["x"]), y_B=d(S["y"]),
-                   z_B=d(S["z"]), m_B=d(S["m"]))
-        leaves = [d(a).requires_grad_(True) for a in (L["val"], L["w"], S["e1"], S["e2"], S["w"])]
-        target = torch.from_numpy(rng.normal(0, 1e-4, bins.n_bin)).cuda()
-        torch.cuda.synchronize()
-        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-        e0.record(stream)
-        xi_t, _ = ag.xi_shear(*leaves, geo, bins, ctx)
-        e1.record(stream)
-        loss = (((xi_t - target) / 1e-3) ** 2).sum()
-        loss.backward()
-        e2.record(stream)
-        torch.cuda.synchronize()
-        t_fwd += e0.elapsed_time(e1)
-        t_all += e0.elapsed_time(e2)
-        pairs += int(ctx.stats()["n_pairs"])
-        del geo, leaves, xi_t, loss
+    for rep in range(2):  # one untimed pass (workspace sizing, first launches), one timed
+        rng = np.random.default_rng(1004)
+        t_fwd = t_all = 0.0
+        pairs = 0
+        for (i, j) in w["tasks"]:
+            L, S = w["lens_bins"][i], w["shape_bins"][j]
+            geo = dict(x_A=d(L["x"]), y_A=d(L["y"]), z_A=d(L["z"]), x_B=d(S["x"]), y_B=d(S["y"]),
+                       z_B=d(S["z"]), m_B=d(S["m"]))
+            leaves = [d(a).requires_grad_(True) for a in (L["val"], L["w"], S["e1"], S["e2"], S["w"])]
+            target = torch.from_numpy(rng.normal(0, 1e-4, bins.n_bin)).cuda()
+            torch.cuda.synchronize()
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            xi_t, _ = ag.xi_shear(*leaves, geo, bins, ctx)
+            e1.record(stream)
+            loss = (((xi_t - target) / 1e-3) ** 2).sum()
+            loss.backward()
+            e2.record(stream)
+            torch.cuda.synchronize()
+            t_fwd += e0.elapsed_time(e1)
+            t_all += e0.elapsed_time(e2)
+            pairs += int(ctx.stats()["n_pairs"])
+            del geo, leaves, xi_t, loss
     return {"value": pairs / (t_all * 1e-3) / 1e9, "unit": UNIT,
             "forward_ms": t_fwd, "forward_plus_adjoint_ms": t_all,
             "fwd_adj_over_plain_fwd": t_all / pair_ms,
