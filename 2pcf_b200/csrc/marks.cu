@@ -9,8 +9,8 @@
 // only re-weights them, so this is a streaming pass over the marks (HBM-bound:
 // 12 bytes per lens and bin, plus 8 bytes per lens and map).
 //
-// One block = 256 lenses of one field and up to kMapGroup maps; lane = bin,
-// warp = a slice of the lenses; FP64 accumulation, per-block partial sums in
+// One block = 256 lenses of one field and up to kMapGroup maps, staged 32 lenses
+// at a time in shared memory; FP64 accumulation, per-block partial sums in
 // scratch, then a fixed-order reduction over blocks (deterministic).
 
 #include <algorithm>
@@ -28,7 +28,7 @@
 namespace tpcf {
 
 constexpr int kMarksChunk = 256;  // lenses per block
-constexpr int kMapGroup = 4;      // maps per pass over the marks
+constexpr int kMapGroup = 16;     // maps or resamples per pass over the marks
 
 struct MarksField {
   long long n;
@@ -69,67 +69,83 @@ struct MultFactors {  // resamples: vw = wm = multiplicity of the lens's unit
   __device__ __forceinline__ bool keep(float, double wm) const { return wm > 0.0; }
 };
 
-// partial[(blk * n_g + g) * R + r], R = 3 n_bin + 1 (E, B, K rows, weight)
+// partial[(blk * n_g + g) * R + r], R = 3 n_bin + 1 (E, B, K rows, weight).
+// The block's 256 lenses are taken 32 at a time: the tile's marks
+// (3 x 32 x n_bin floats, contiguous in HBM) and its lens factors for the n_g
+// maps are staged in shared memory with coalesced loads; then each sum
+// (map, quantity, bin) is owned by one thread and accumulated over the 32
+// lenses in lens order, in FP64 in shared memory (no atomics: deterministic).
+constexpr int kTileL = 32;
 template <class Fac>
 __global__ void __launch_bounds__(256) k_marks_partials(const MarksField* __restrict__ fields, int n_field,
                                                          const Fac fac, int n_g, int n_bin,
                                                          double* __restrict__ partial) {
-  __shared__ double red[8][kMapGroup][3 * 32 + 1];
+  extern __shared__ __align__(16) unsigned char sm[];
+  const int R = 3 * n_bin + 1;
+  double* acc = reinterpret_cast<double*>(sm);                       // [n_g][R]
+  double* fvw = acc + (size_t)n_g * R;                               // [n_g][kTileL]
+  double* fwm = fvw + (size_t)n_g * kTileL;                          // [n_g][kTileL]
+  float* mk = reinterpret_cast<float*>(fwm + (size_t)n_g * kTileL);  // [3][kTileL * n_bin]
+  float* mw = mk + 3 * kTileL * n_bin;                               // [kTileL]
   const int blk = blockIdx.x;
   int fi = 0;
   while (fi + 1 < n_field && fields[fi + 1].chunk0 <= blk) ++fi;
   const MarksField F = fields[fi];
   const long long j0 = (long long)(blk - F.chunk0) * kMarksChunk;
   const long long j1 = min(F.n, j0 + kMarksChunk);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int R = 3 * n_bin + 1;
-  for (int b0 = 0; b0 < n_bin; b0 += 32) {
-    const int b = b0 + lane;
-    double aE[kMapGroup], aB[kMapGroup], aK[kMapGroup], aw[kMapGroup];
-#pragma unroll
-    for (int g = 0; g < kMapGroup; ++g) aE[g] = aB[g] = aK[g] = aw[g] = 0.0;
-    for (long long j = j0 + warp; j < j1; j += 8) {
-      const float mw = F.mw[j];
-      const float e = b < n_bin ? F.xiE[j * n_bin + b] : 0.f;
-      const float x = b < n_bin ? F.xiB[j * n_bin + b] : 0.f;
-      const float k = b < n_bin ? F.K[j * n_bin + b] : 0.f;
-#pragma unroll
-      for (int g = 0; g < kMapGroup; ++g) {
-        if (g < n_g) {
-          double vw, wm;
-          fac.get(F, g, j, vw, wm);
-          if (fac.keep(mw, wm)) {
-            aE[g] = fma((double)e, vw, aE[g]);
-            aB[g] = fma((double)x, vw, aB[g]);
-            aK[g] = fma((double)k, wm, aK[g]);
-            aw[g] = fma((double)mw, wm, aw[g]);
-          }
-        }
+  const int tid = threadIdx.x;
+  for (int c = tid; c < n_g * R; c += blockDim.x) acc[c] = 0.0;
+  for (long long t0 = j0; t0 < j1; t0 += kTileL) {
+    const int nt = (int)min((long long)kTileL, j1 - t0);
+    __syncthreads();
+    const size_t off = (size_t)t0 * n_bin;
+    for (int e = tid; e < nt * n_bin; e += blockDim.x) {
+      mk[e] = F.xiE[off + e];
+      mk[kTileL * n_bin + e] = F.xiB[off + e];
+      mk[2 * kTileL * n_bin + e] = F.K[off + e];
+    }
+    for (int e = tid; e < n_g * kTileL; e += blockDim.x) {
+      const int g = e / kTileL, jj = e % kTileL;
+      double vw = 0.0, wm = 0.0;
+      if (jj < nt) {
+        const long long j = t0 + jj;
+        fac.get(F, g, j, vw, wm);
+        if (!fac.keep(F.mw[j], wm)) vw = wm = 0.0;  // left out: contributes nothing
       }
+      fvw[e] = vw;
+      fwm[e] = wm;
     }
-#pragma unroll
-    for (int g = 0; g < kMapGroup; ++g) {
-      red[warp][g][lane] = aE[g];
-      red[warp][g][32 + lane] = aB[g];
-      red[warp][g][64 + lane] = aK[g];
-      if (lane == 0) red[warp][g][96] = aw[g];
-    }
+    for (int jj = tid; jj < kTileL; jj += blockDim.x) mw[jj] = jj < nt ? F.mw[t0 + jj] : 0.f;
     __syncthreads();
-    // fixed-order sum over the 8 warps
-    for (int t = threadIdx.x; t < kMapGroup * 97; t += blockDim.x) {
-      const int g = t / 97, r = t % 97;
-      if (g >= n_g) continue;
-      const int bb = b0 + (r % 32);
-      const int q = r / 32;  // 0 E, 1 B, 2 K, 3 weight
-      if (q < 3 && bb >= n_bin) continue;
-      if (q == 3 && b0 != 0) continue;
-      double s = 0.0;
-      for (int wp = 0; wp < 8; ++wp) s += red[wp][g][r];
-      const int row = q < 3 ? q * n_bin + bb : 3 * n_bin;
-      partial[((size_t)blk * n_g + g) * R + row] = s;
+    for (int c = tid; c < n_g * R; c += blockDim.x) {
+      const int g = c / R, r = c % R;
+      const double* fv = fvw + g * kTileL;
+      const double* fw = fwm + g * kTileL;
+      double a = acc[c];
+      if (r < 3 * n_bin) {
+        const int q = r / n_bin, bb = r % n_bin;
+        const float* m = mk + q * kTileL * n_bin + bb;
+        const double* f = q < 2 ? fv : fw;
+        for (int jj = 0; jj < nt; ++jj) a = fma((double)m[jj * n_bin], f[jj], a);
+      } else {
+        for (int jj = 0; jj < nt; ++jj) a = fma((double)mw[jj], fw[jj], a);
+      }
+      acc[c] = a;
     }
-    __syncthreads();
   }
+  __syncthreads();
+  for (int c = tid; c < n_g * R; c += blockDim.x) partial[(size_t)blk * n_g * R + c] = acc[c];
+}
+
+size_t marks_smem(int n_g, int n_bin) {
+  const int R = 3 * n_bin + 1;
+  return sizeof(double) * ((size_t)n_g * R + 2 * (size_t)n_g * kTileL) + sizeof(float) * (3 * kTileL * n_bin + kTileL);
+}
+// maps or resamples per pass: at most kMapGroup, and the shared memory within 96 KB
+int marks_group(int n_bin) {
+  int g = kMapGroup;
+  while (g > 1 && marks_smem(g, n_bin) > 96 * 1024) --g;
+  return g;
 }
 
 // Multiplicities of G resamples s0.. over n_units units: n_draw draws each,
@@ -250,10 +266,14 @@ extern "C" tpcf_status tpcf_xi_from_marks(tpcf_ctx* c, int32_t n_field, const tp
     std::vector<double> sums((size_t)n_map * n_field * R, 0.0);
     double* part = (double*)ws_alloc(c, sizeof(double) * (size_t)std::max(nblk, 1) * kMapGroup * R);
     double* dout = (double*)ws_alloc(c, sizeof(double) * (size_t)kMapGroup * n_field * R);
-    for (int m0 = 0; m0 < n_map; m0 += kMapGroup) {
-      const int g = std::min(kMapGroup, n_map - m0);
+    const int MG = marks_group(nb);
+    const size_t msm = marks_smem(MG, nb);
+    check(cudaFuncSetAttribute(k_marks_partials<MapFactors>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm),
+          "smem attr");
+    for (int m0 = 0; m0 < n_map; m0 += MG) {
+      const int g = std::min(MG, n_map - m0);
       if (nblk > 0) {
-        k_marks_partials<MapFactors><<<nblk, 256, 0, st>>>(df, n_field, MapFactors{m0}, g, nb, part);
+        k_marks_partials<MapFactors><<<nblk, 256, marks_smem(g, nb), st>>>(df, n_field, MapFactors{m0}, g, nb, part);
         counted(c, cudaGetLastError(), "marks partials");
       }
       const int tot = g * n_field * R;
@@ -357,8 +377,11 @@ extern "C" tpcf_status tpcf_marks_bootstrap(tpcf_ctx* c, int32_t n_field, const 
     double* part = (double*)ws_alloc(c, sizeof(double) * (size_t)std::max(nblk, 1) * kMapGroup * R);
     double* dout = (double*)ws_alloc(c, sizeof(double) * (size_t)kMapGroup * n_field * R);
     std::vector<double> sums((size_t)n_boot * n_field * R, 0.0);
-    for (int s0 = 0; s0 < n_boot; s0 += kMapGroup) {
-      const int G = std::min(kMapGroup, n_boot - s0);
+    const int MG = marks_group(nb);
+    check(cudaFuncSetAttribute(k_marks_partials<MultFactors>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)marks_smem(MG, nb)), "smem attr");
+    for (int s0 = 0; s0 < n_boot; s0 += MG) {
+      const int G = std::min(MG, n_boot - s0);
       const int* mult;
       if (multiplicity) {
         mult = dmult_all + (size_t)s0 * n_units;
@@ -371,8 +394,9 @@ extern "C" tpcf_status tpcf_marks_bootstrap(tpcf_ctx* c, int32_t n_field, const 
         mult = mbuf;
       }
       if (nblk > 0) {
-        k_marks_partials<MultFactors><<<nblk, 256, 0, st>>>(df, n_field, MultFactors{mult, dunit, n_units}, G, nb,
-                                                            part);
+        k_marks_partials<MultFactors><<<nblk, 256, marks_smem(G, nb), st>>>(df, n_field,
+                                                                            MultFactors{mult, dunit, n_units}, G,
+                                                                            nb, part);
         counted(c, cudaGetLastError(), "bootstrap partials");
         const int tot = G * n_field * R;
         k_marks_reduce<<<(tot + 255) / 256, 256, 0, st>>>(part, df, n_field, nblk, G, R, dout);

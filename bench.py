@@ -38,6 +38,8 @@ sys.path.insert(0, ROOT)
 METRIC = "Gpairs/s for xi_t at 10M objects, plain vs batched+adjoint form at 1e-6 rel. error"
 UNIT = "Gpairs/s"
 FLOP_PER_PAIR = 26  # shear-scalar, FMA = 2, MUFU = 1 (per binned pair)
+K_PAIRS_DRAM_BYTES = 64.49e9 + 197.6e6  # read + written by one launch of the default workload
+SPH_FLOP_PER_PAIR = 52  # spherical shear-scalar: hi/lo unit-vector differences, east/north projection, angle series
 WORKLOAD_DESC = ("tomography: 5 shear bins (0.2,0.5,1.0,1.9,4.0 M) x 5 scalar bins "
                  "(0.1,0.2,0.4,0.7,1.0 M) = 10.0 M objects, 25 cross-pairs in one launch, "
                  "20 log bins 1-300 arcmin, 1000 deg^2 clustered, 100 lens patches")
@@ -204,6 +206,126 @@ def adjoint_timing(w, ctx, bins, step_ms, pair_ms, stream):
                     "of the batched step"}
 
 
+def widened_timing(tpcf, w, peak_fp32, stream, cpu_threads, with_cpu=True):
+    """Measurements of the rows around the pair sum: the spherical pair sum on
+    the tomography catalogues projected onto a sky patch, xi from precomputed
+    marks for 16 maps, a 1000-resample bootstrap of marks, the equal-weight
+    k-means, and the text catalogue reader.  CUDA events on the launch stream;
+    each timed call follows an untimed one."""
+    import tempfile
+    import torch
+    out = {}
+    d2r = np.pi / 180.0
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, e0.elapsed_time(e1)
+
+    # spherical pair sum: the 25 tomography tasks on a 31.6 x 31.6 deg patch at
+    # Dec -30 (flat arcmin coordinates mapped to longitude / latitude)
+    phi0, lam0, box = -30.0 * d2r, 40.0 * d2r, w["box"]
+
+    def sph(c):
+        phi = phi0 + (c["y"].astype(np.float64) - box / 2) / 60.0 * d2r
+        lam = lam0 + (c["x"].astype(np.float64) - box / 2) / 60.0 * d2r / np.cos(phi)
+        return lam.astype(np.float32), phi.astype(np.float32)
+
+    Ls, Ss = [], []
+    for l in w["lens_bins"]:
+        lam, phi = sph(l)
+        Ls.append(tpcf.LensCatalog(x=dev(lam), y=dev(phi), val=dev(l["val"]), w=dev(l["w"]), z=dev(l["z"])))
+    for s_ in w["shape_bins"]:
+        lam, phi = sph(s_)
+        Ss.append(tpcf.ShapeCatalog(x=dev(lam), y=dev(phi), e1=dev(s_["e1"]), e2=dev(s_["e2"]), w=dev(s_["w"]),
+                                    z=dev(s_["z"]), m=dev(s_["m"])))
+    lo, hi, nb = w["bins"]
+    sbins = tpcf.create_bins(lo / 60 * d2r, hi / 60 * d2r, nb)
+    sctx = tpcf.Context(0)
+    sctx.set_timing(True)
+    sctx.set_stream(stream.cuda_stream)
+    sctx.set_cell_size(sbins.x_max / 64)
+    outs, ms = timed(lambda: tpcf.batch_shear_2pcf(Ls, Ss, w["tasks"], sbins, spherical_coords=True, ctx=sctx))
+    pairs = sum(int(o.n_pairs.sum()) for o in outs)
+    kms = sctx.stats()["pair_kernel_ms"]
+    ach = pairs * SPH_FLOP_PER_PAIR / (kms * 1e-3) / 1e12
+    out["sphere"] = {"value": pairs / (ms * 1e-3) / 1e9, "unit": UNIT, "binned_pairs": pairs, "call_ms": ms,
+                     "roofline": {"bound": "fp32", "achieved": ach, "peak": peak_fp32, "unit": "TFLOP/s",
+                                  "frac": ach / peak_fp32, "kernel": "k_pairs_sph",
+                                  "flop_per_pair": SPH_FLOP_PER_PAIR, "kernel_ms": kms}}
+    if with_cpu:
+        from oracle import oracle as O
+        Lh = {k: np.ascontiguousarray(v.cpu().numpy()[::2000]) for k, v in vars(Ls[4]).items()}
+        Sh = {k: np.ascontiguousarray(v.cpu().numpy()) for k, v in vars(Ss[2]).items()}
+        t0 = time.time()
+        r = O.ref_sphere_f32(O.SHEAR, Lh, Sh, sbins.x_min, sbins.x_max, nb, num_threads=cpu_threads)
+        dt = time.time() - t0
+        out["sphere"]["cpu_baseline"] = {
+            "value": int(r["n_pairs"].sum()) / dt / 1e9, "unit": UNIT, "cores": cpu_threads, "kind": "port",
+            "sample": f"every 2000-th lens of scalar bin 5 ({len(Lh['x'])}) against shear bin 3 "
+                      f"({len(Sh['x'])}), the reference's spherical loop (acos, all pairs) in FP32"}
+    sctx.close()
+    del Ls, Ss
+
+    # xi from marks: 1.0 M lenses x 20 bins, 16 maps
+    rng = np.random.default_rng(77)
+    n, nbm, n_map = 1_000_000, nb, 16
+    mk = tpcf.MarksField(x=dev(rng.normal(size=n).astype(np.float32)), y=dev(rng.normal(size=n).astype(np.float32)),
+                         w=dev(rng.uniform(0.5, 1.5, n).astype(np.float32)),
+                         xi_E=dev(rng.normal(size=(n, nbm)).astype(np.float32)),
+                         xi_B=dev(rng.normal(size=(n, nbm)).astype(np.float32)),
+                         K=dev(rng.uniform(0.5, 1.5, (n, nbm)).astype(np.float32)))
+    val = dev(rng.normal(size=(n_map, n)).astype(np.float32))
+    wm = dev(rng.uniform(0.5, 1.5, (n_map, n)).astype(np.float32))
+    mctx = tpcf.Context(0)
+    mctx.set_stream(stream.cuda_stream)
+    _, ms = timed(lambda: tpcf.calculate_tpcf_from_marks([mk], [val], [wm], ctx=mctx))
+    byt = (n_map + 3) // 4 * (3 * 4 * n * nbm + 4 * n) + n_map * 8 * n
+    hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"] \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    out["marks_reweight"] = {"maps": n_map, "lenses": n, "n_bin": nbm, "call_ms": ms,
+                             "roofline": {"bound": "hbm", "achieved": byt / (ms * 1e-3) / 1e9, "peak": hbm,
+                                          "unit": "GB/s", "frac": byt / (ms * 1e-3) / 1e9 / hbm,
+                                          "bytes": byt}}
+    _, ms = timed(lambda: tpcf.marks_bootstrap([mk], 1000, seed=5, covariance=True, ctx=mctx))
+    byt = 250 * (3 * 4 * n * nbm + 4 * n)
+    out["marks_bootstrap"] = {"resamples": 1000, "lenses": n, "call_ms": ms,
+                              "roofline": {"bound": "hbm", "achieved": byt / (ms * 1e-3) / 1e9, "peak": hbm,
+                                           "unit": "GB/s", "frac": byt / (ms * 1e-3) / 1e9 / hbm, "bytes": byt}}
+    del mk, val, wm
+
+    # equal-weight k-means on all lens positions, 100 blocks
+    ux = np.concatenate([l["x"] for l in w["lens_bins"]])
+    uy = np.concatenate([l["y"] for l in w["lens_bins"]])
+    uw = np.concatenate([l["w"] for l in w["lens_bins"]])
+    uw = (0.01 + uw / uw.max()).astype(np.float32)
+    U = [dev(a) for a in (ux, uy, uw)]
+    (lab, _, it, devw), ms = timed(lambda: tpcf.partition_data_equal(U[0], U[1], U[2], 100, seed=3, ctx=mctx))
+    out["kmeans_equal"] = {"points": int(len(ux)), "k": 100, "iterations": it, "max_weight_deviation": devw,
+                           "call_ms": ms}
+    mctx.close()
+
+    # text catalogue: 0.5 M shape rows
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "shapes.txt")
+        S0 = w["shape_bins"][3]
+        m = 500_000
+        np.savetxt(path, np.stack([S0[k][:m] for k in ("x", "y", "z", "e1", "e2", "w", "m")], 1), fmt="%.8g")
+        size = os.path.getsize(path)
+        t0 = time.time()
+        tpcf.load_standard_shape_catalog(path)
+        dt = time.time() - t0
+        out["text_reader"] = {"rows": m, "bytes": size, "seconds": dt, "MB_per_s": size / dt / 1e6,
+                              "threads": host_threads()}
+    return out
+
+
 def path_stats(tpcf, args):
     """One batched call on the diagnostic build; prints the share of warp
     sub-chunks and lane-pairs per path of k_pairs."""
@@ -272,6 +394,8 @@ def main():
     ap.add_argument("--region", type=float, default=0.0,
                     help="profiling: keep only objects with x, y < REGION arcmin (density unchanged)")
     ap.add_argument("--task", type=int, default=-1, help="profiling: run only this task of the 25")
+    ap.add_argument("--no-widened", action="store_true",
+                    help="skip the spherical, marks, bootstrap, k-means and reader measurements")
     ap.add_argument("--cell-divisor", type=int, default=0,
                     help="grid cell side theta_max/D without autotuning (0: autotune)")
     args = ap.parse_args()
@@ -402,14 +526,12 @@ def main():
         adjoint = adjoint_timing(w, ctx, bins, ms, pair_ms, stream)
     peak = ctx.measure_fp32_peak()
     achieved = pairs * FLOP_PER_PAIR / (pair_ms * 1e-3) / 1e12
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "pairs_traffic.json")
-    if os.path.exists(tfile):
-        try:
-            t = json.load(open(tfile))
-            traffic = t["dram_bytes_per_pair"] * pairs
-        except Exception:
-            traffic = None
+    # DRAM bytes of one pair-kernel launch of this exact workload, from one ncu
+    # capture (profiles/k_pairs_tomography_10M_dram.md); other configurations
+    # were not captured
+    default_cfg = args.scale == 1.0 and args.region <= 0 and args.task < 0 and \
+        abs(ctx.cell_size - bins.x_max / 64) < 1e-6
+    traffic = K_PAIRS_DRAM_BYTES if default_cfg else None
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -439,6 +561,8 @@ def main():
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         cb = cpu_baseline(w, args.cpu_seconds, host_threads())
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if world == 1 and not args.no_widened and args.region <= 0 and args.task < 0:
+        line["widened"] = widened_timing(tpcf, w, peak, stream, host_threads(), with_cpu=not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
