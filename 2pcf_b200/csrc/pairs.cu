@@ -188,18 +188,15 @@ __device__ __forceinline__ void chunk_dual(const SrcRec* __restrict__ S, int cnt
   // lanes of class 1 (or 0) keep an edge no pair reaches
   const float E = (cls == 2) ? C.e2f[blo + 1] : 3.0e38f;
   const float gE = (cls == 2) ? E * C.eps_rel : 0.f;
+  bool near = false;  // some pair lies within the guard band of E
 #pragma unroll 2
   for (int j = 0; j < cnt; ++j) {
     const float4 a = S[j].a;
     const float4 b = S[j].b;
     float d2, d, r, X, Y;
     pair_terms<MODE, LOGB>(lx, ly, a, d2, d, r, X, Y);
-    bool up = d2 >= E;
-    if (fabsf(d2 - E) <= gE) {
-      // canonical bin is blo or blo+1, or -1 on a side outside [x_min, x_max]
-      const int cb = slow_bin(lx, ly, a.x, a.y, C.e2s, C.nb);
-      up = (cb == blo + 1) || (cb < 0 && blo + 1 == C.nb);
-    }
+    const bool up = d2 >= E;
+    near |= fabsf(d2 - E) <= gE;
     // products folded into the sums: one FFMA per quantity and side
     tot[QGT] = fmaf(r, X, tot[QGT]);
     tot[QGX] = fmaf(r, Y, tot[QGX]);
@@ -217,6 +214,13 @@ __device__ __forceinline__ void chunk_dual(const SrcRec* __restrict__ S, int cnt
   }
   tot[QN] = (float)cnt;
   if (cls == 0) return;
+  if (near) {
+    // rare (a pair within a relative 4e-6 of the edge): this lane's register
+    // sums are dropped and the sub-chunk is binned pair by pair, each pair by
+    // the canonical rule
+    for (int j = 0; j < cnt; ++j) do_pair<MODE, HAS_M, false, LOGB, NC, QA>(lx, ly, 0.f, S[j].a, S[j].b, hcol, C);
+    return;
+  }
   float lo[QA];
 #pragma unroll
   for (int q = 0; q < QA; ++q) lo[q] = tot[q] - hi[q];

@@ -230,16 +230,14 @@ __device__ __forceinline__ void chunk_dual_s(const SrcRecS* __restrict__ S, int 
   for (int q = 0; q < QA; ++q) tot[q] = hi[q] = 0.f;
   const float E = (cls == 2) ? C.e2f[blo + 1] : 3.0e38f;
   const float gE = (cls == 2) ? E * C.eps_rel : 0.f;
+  bool near = false;  // some pair lies within the guard band of E
 #pragma unroll 2
   for (int j = 0; j < cnt; ++j) {
     const float4 a = S[j].a, b = S[j].b, cc = S[j].c;
     float d2, th, r, X, Y;
     sph_terms<MODE, SMALL>(L, a, b, d2, th, r, X, Y);
-    bool up = d2 >= E;
-    if (fabsf(d2 - E) <= gE) {
-      const int cb = slow_bin_s(L.h, L.l, a, b, C.e2s, C.nb);
-      up = (cb == blo + 1) || (cb < 0 && blo + 1 == C.nb);
-    }
+    const bool up = d2 >= E;
+    near |= fabsf(d2 - E) <= gE;
     tot[QGT] = fmaf(r, X, tot[QGT]);
     tot[QGX] = fmaf(r, Y, tot[QGX]);
     tot[QW] += cc.x;
@@ -256,6 +254,10 @@ __device__ __forceinline__ void chunk_dual_s(const SrcRecS* __restrict__ S, int 
   }
   tot[QN] = (float)cnt;
   if (cls == 0) return;
+  if (near) {  // rare: the sub-chunk is binned pair by pair by the canonical rule
+    for (int j = 0; j < cnt; ++j) do_pair_s<MODE, HAS_M, false, SMALL, SMALL, NC, QA>(L, 0.f, S[j], hcol, C);
+    return;
+  }
   float lo[QA];
 #pragma unroll
   for (int q = 0; q < QA; ++q) lo[q] = tot[q] - hi[q];
