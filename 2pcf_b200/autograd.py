@@ -79,4 +79,99 @@ def xi_shear(val_A, w_A, e1_B, e2_B, w_B, geometry: dict, bins: Binning, ctx: Co
     """Differentiable (xi_t, xi_x) of the shear-scalar estimator.  ``geometry``
     holds x_A, y_A, x_B, y_B and optionally z_A, z_B, m_B as CUDA tensors."""
     ctx = ctx if ctx is not None else default_context(val_A.device.index or 0)
+    if ctx.spherical:
+        ctx.set_spherical(False)
     return ShearXi.apply(val_A, w_A, e1_B, e2_B, w_B, geometry, bins, ctx)
+
+
+class ShearXiBatch(torch.autograd.Function):
+    """All tasks of a tomography in one forward launch (tpcf_batch_shear_scalar
+    keeping every task's raw per-lens sums on the device), one adjoint call per
+    task in backward; gradients of a catalogue sum over the tasks that use it."""
+
+    @staticmethod
+    def forward(actx, tasks, geo_L, geo_S, bins, tctx, *leaves):
+        from . import _lib as L_
+        n_L, n_S = len(geo_L), len(geo_S)
+        vals, wAs = leaves[:n_L], leaves[n_L:2 * n_L]
+        e1s, e2s, wBs = leaves[2 * n_L:2 * n_L + n_S], leaves[2 * n_L + n_S:2 * n_L + 2 * n_S], \
+            leaves[2 * n_L + 2 * n_S:]
+        dev = vals[0].device
+        nb = bins.n_bin
+        f64 = dict(dtype=torch.float64, device=dev)
+        opt = lambda t: None if t is None else _f32(t)
+        lv = [(_f32(g["x"]), _f32(g["y"]), opt(g.get("z")), _f32(v), _f32(w)) for g, v, w in zip(geo_L, vals, wAs)]
+        sv = [(_f32(g["x"]), _f32(g["y"]), opt(g.get("z")), _f32(a), _f32(b), _f32(w), opt(g.get("m")))
+              for g, a, b, w in zip(geo_S, e1s, e2s, wBs)]
+        lc = (L_.LensCat * n_L)(*[L_.LensCat(t[0].numel(), *[_p(a) for a in t], None) for t in lv])
+        sc = (L_.ShearCat * n_S)(*[L_.ShearCat(t[0].numel(), *[_p(a) for a in t]) for t in sv])
+        nT = len(tasks)
+        sums = [torch.zeros(5, nb, **f64) for _ in range(nT)]
+        npairs = [torch.zeros(nb, dtype=torch.int64, device=dev) for _ in range(nT)]
+        raws = [torch.zeros(lv[li][0].numel(), 6, nb, **f64) for li, _ in tasks]
+        outs = (Result * nT)()
+        for t in range(nT):
+            s = sums[t]
+            outs[t] = Result(sum_dw=_p(s[0]), sum_gt=_p(s[1]), sum_gx=_p(s[2]), sum_w=_p(s[3]), sum_K=_p(s[4]),
+                             n_pairs=_p(npairs[t]), lens_raw=_p(raws[t]))
+        import numpy as np
+        tl = np.ascontiguousarray([a for a, _ in tasks], np.int32)
+        ts = np.ascontiguousarray([b for _, b in tasks], np.int32)
+        cb = bins.c_struct()
+        tctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        _check(lib().tpcf_batch_shear_scalar(tctx.handle, n_L, lc, n_S, sc, nT, tl.ctypes.data, ts.ctypes.data,
+                                             C.byref(cb), 0, outs), tctx.handle)
+        S = torch.stack(sums)                       # [n_task][5][nb]
+        K = S[:, 4]
+        pos = K > 0
+        xi_t = torch.where(pos, S[:, 1] / torch.where(pos, K, 1.0), torch.zeros_like(K))
+        xi_x = torch.where(pos, S[:, 2] / torch.where(pos, K, 1.0), torch.zeros_like(K))
+        actx.save_for_backward(S, *raws)
+        actx.lv, actx.sv, actx.tasks, actx.bins, actx.tctx = lv, sv, tasks, bins, tctx
+        actx.n_L, actx.n_S = n_L, n_S
+        return xi_t, xi_x
+
+    @staticmethod
+    def backward(actx, d_xi_t, d_xi_x):
+        S, *raws = actx.saved_tensors
+        lv, sv, tasks, bins, tctx = actx.lv, actx.sv, actx.tasks, actx.bins, actx.tctx
+        dev = S.device
+        g_val = [torch.zeros_like(t[3]) for t in lv]
+        g_wA = [torch.zeros_like(t[4]) for t in lv]
+        g_e1 = [torch.zeros_like(t[3]) for t in sv]
+        g_e2 = [torch.zeros_like(t[4]) for t in sv]
+        g_wB = [torch.zeros_like(t[5]) for t in sv]
+        cb = bins.c_struct()
+        tctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+        for t, (li, si) in enumerate(tasks):
+            lt = (d_xi_t[t] if d_xi_t is not None else torch.zeros(bins.n_bin, device=dev)).to(torch.float64)
+            lt = lt.contiguous()
+            lx = None if d_xi_x is None else d_xi_x[t].to(torch.float64).contiguous()
+            A, B = lv[li], sv[si]
+            o = [torch.zeros(A[0].numel(), dtype=torch.float32, device=dev) for _ in range(2)] + \
+                [torch.zeros(B[0].numel(), dtype=torch.float32, device=dev) for _ in range(3)]
+            _check(lib().tpcf_shear_scalar_adjoint(
+                tctx.handle, _p(A[0]), _p(A[1]), _p(A[2]), _p(A[3]), _p(A[4]), A[0].numel(), _p(B[0]), _p(B[1]),
+                _p(B[2]), _p(B[3]), _p(B[4]), _p(B[5]), _p(B[6]), B[0].numel(), C.byref(cb), _p(S[t, 1]),
+                _p(S[t, 2]), _p(S[t, 4]), _p(raws[t]), _p(lt), _p(lx), *[_p(x) for x in o], None), tctx.handle)
+            g_val[li] += o[0]
+            g_wA[li] += o[1]
+            g_e1[si] += o[2]
+            g_e2[si] += o[3]
+            g_wB[si] += o[4]
+        return (None, None, None, None, None, *g_val, *g_wA, *g_e1, *g_e2, *g_wB)
+
+
+def xi_shear_batch(tasks, lens_geometry, shape_geometry, val_A, w_A, e1_B, e2_B, w_B, bins: Binning,
+                   ctx: Context = None):
+    """Differentiable (xi_t, xi_x) [n_task][n_bin] of every (lens catalogue,
+    shape catalogue) task in one forward launch.  ``lens_geometry[i]`` holds
+    x, y, z of lens catalogue i and ``shape_geometry[j]`` x, y, z, m of shape
+    catalogue j (CUDA tensors); ``val_A``, ``w_A`` (per lens catalogue) and
+    ``e1_B``, ``e2_B``, ``w_B`` (per shape catalogue) are lists of CUDA
+    tensors that may require gradients."""
+    ctx = ctx if ctx is not None else default_context(val_A[0].device.index or 0)
+    if ctx.spherical:
+        ctx.set_spherical(False)
+    return ShearXiBatch.apply(list(tasks), lens_geometry, shape_geometry, bins, ctx, *val_A, *w_A, *e1_B, *e2_B,
+                              *w_B)

@@ -29,7 +29,17 @@
 #include "tpcf_internal.cuh"
 #include "tpcf_kernels.h"
 
+#ifndef TPCF_DUAL_UNROLL
+#define TPCF_DUAL_UNROLL 2
+#endif
+#ifndef TPCF_SINGLE_UNROLL
+#define TPCF_SINGLE_UNROLL 4
+#endif
+
 namespace tpcf {
+
+constexpr int kDualUnroll = TPCF_DUAL_UNROLL;      // source-loop unrolling of the one-edge path
+constexpr int kSingleUnroll = TPCF_SINGLE_UNROLL;  // and of the single-bin path
 
 // ------------------------------------------------------- shared-memory map --
 struct PairSmem {
@@ -161,7 +171,7 @@ __device__ __forceinline__ void chunk_single(const SrcRec* __restrict__ S, int c
   float acc[QA];
 #pragma unroll
   for (int q = 0; q < QA; ++q) acc[q] = 0.f;
-#pragma unroll 4
+#pragma unroll kSingleUnroll
   for (int j = 0; j < cnt; ++j) {
     const float4 a = S[j].a;
     const float4 b = S[j].b;
@@ -189,7 +199,7 @@ __device__ __forceinline__ void chunk_dual(const SrcRec* __restrict__ S, int cnt
   const float E = (cls == 2) ? C.e2f[blo + 1] : 3.0e38f;
   const float gE = (cls == 2) ? E * C.eps_rel : 0.f;
   bool near = false;  // some pair lies within the guard band of E
-#pragma unroll 2
+#pragma unroll kDualUnroll
   for (int j = 0; j < cnt; ++j) {
     const float4 a = S[j].a;
     const float4 b = S[j].b;

@@ -119,3 +119,37 @@ def test_autograd_chi2_loss(tpcf, oracle):
         close(leaf.grad.cpu().numpy(), ref[k], name=k)
     can = oracle.normalise(oracle.canon_pairs(oracle.SHEAR, L, S, bins.bin_edges_sq))
     np.testing.assert_allclose(xi_t.detach().cpu().numpy(), can["g_t"], rtol=1e-5, atol=1e-9)
+
+
+def test_batched_autograd_equals_per_task(tpcf, oracle):
+    """xi_shear_batch (one forward launch for all tasks) gives the values and
+    gradients of per-task xi_shear calls; a catalogue used by two tasks gets
+    the sum of its gradients."""
+    import torch
+    ag = importlib.import_module("2pcf_b200.autograd")
+    cats = [catalogue(1500, 2000, 200.0, 70 + k) for k in range(2)]
+    bins = tpcf.create_bins(1.0, 60.0, 8)
+    d = lambda a: torch.from_numpy(a).cuda()
+    geo_L = [dict(x=d(L["x"]), y=d(L["y"]), z=d(L["z"])) for L, _ in cats]
+    geo_S = [dict(x=d(S["x"]), y=d(S["y"]), z=d(S["z"]), m=d(S["m"])) for _, S in cats]
+    tasks = [(0, 0), (0, 1), (1, 1)]
+    leaves = lambda: ([d(L["val"]).requires_grad_(True) for L, _ in cats], [d(L["w"]).requires_grad_(True) for L, _ in cats],
+                      [d(S["e1"]).requires_grad_(True) for _, S in cats], [d(S["e2"]).requires_grad_(True) for _, S in cats],
+                      [d(S["w"]).requires_grad_(True) for _, S in cats])
+    v, wa, e1, e2, wb = leaves()
+    xt, xx = ag.xi_shear_batch(tasks, geo_L, geo_S, v, wa, e1, e2, wb, bins)
+    rng = np.random.default_rng(71)
+    ct = torch.from_numpy(rng.normal(size=(3, 8))).cuda()
+    cx = torch.from_numpy(rng.normal(size=(3, 8))).cuda()
+    ((xt * ct).sum() + (xx * cx).sum()).backward()
+    v2, wa2, e12, e22, wb2 = leaves()
+    loss = 0
+    for t, (li, si) in enumerate(tasks):
+        geo = dict(x_A=geo_L[li]["x"], y_A=geo_L[li]["y"], z_A=geo_L[li]["z"], x_B=geo_S[si]["x"],
+                   y_B=geo_S[si]["y"], z_B=geo_S[si]["z"], m_B=geo_S[si]["m"])
+        a, b = ag.xi_shear(v2[li], wa2[li], e12[si], e22[si], wb2[si], geo, bins)
+        np.testing.assert_array_equal(a.detach().cpu().numpy(), xt[t].detach().cpu().numpy())
+        loss = loss + (a * ct[t]).sum() + (b * cx[t]).sum()
+    loss.backward()
+    for p1, p2 in zip(v + wa + e1 + e2 + wb, v2 + wa2 + e12 + e22 + wb2):
+        close(p1.grad.cpu().numpy(), p2.grad.cpu().numpy(), rtol=1e-6, name="batched grad")
