@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(BT) k_adj(const AdjParams P) {
             const int base = sc * 32;
             const int cnt = min(32, n - base);
             int blo = 0;
-            const int cls = act ? classify<LOGB, HAS_Z>(sx, sy, subbox[sc], C, blo) : 0;
+            const int cls = act ? classify<LOGB, HAS_Z, true>(sx, sy, subbox[sc], C, blo) : 0;
             const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)cls);
             if (m == 0) continue;
             const SrcRec* __restrict__ Sc = S + base;
@@ -257,7 +257,8 @@ __global__ void __launch_bounds__(BT) k_adj(const AdjParams P) {
               // every pair of this lane is in bin blo (or the lane has none)
               const float4 kc = cls == 1 ? coef[blo] : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll 4
-              for (int j = 0; j < cnt; ++j) adj_pair<LOGB, WX>(sx, sy, Sc[j].a, kc, Ac);
+              for (int j = 0; j < cnt; ++j)  // a lens behind the source adds nothing (src/tpcf.f90:322)
+                if (!HAS_Z || Sc[j].b.x <= sz) adj_pair<LOGB, WX>(sx, sy, Sc[j].a, kc, Ac);
             } else if (m == 2) {
               const float4 kl = (cls >= 1 && blo >= 0) ? coef[blo] : make_float4(0.f, 0.f, 0.f, 0.f);
               // a side outside [x_min, x_max] contributes nothing
@@ -265,17 +266,27 @@ __global__ void __launch_bounds__(BT) k_adj(const AdjParams P) {
               const float4 kh = cls == 2 ? (blo + 1 < nb ? coef[blo + 1] : kz) : kl;
               const float E = cls == 2 ? e2f[blo + 1] : 3.0e38f;
               const float gE = cls == 2 ? E * C.eps_rel : 0.f;
+              bool near = false;  // some pair lies within the guard band of E
 #pragma unroll 2
               for (int j = 0; j < cnt; ++j) {
                 const float4 l = Sc[j].a;
                 const float dx = l.x - sx, dy = l.y - sy;
                 const float d2 = fmaf(dy, dy, dx * dx);
-                bool up = d2 >= E;
-                if (fabsf(d2 - E) <= gE) {
-                  const int cb = slow_bin(l.x, l.y, sx, sy, e2s, nb);
-                  up = (cb == blo + 1) || (cb < 0 && blo + 1 == nb);
+                if (HAS_Z && Sc[j].b.x > sz) continue;
+                near |= fabsf(d2 - E) <= gE;
+                adj_pair<LOGB, WX>(sx, sy, l, d2 >= E ? kh : kl, Ac);
+              }
+              if (near) {  // rare: this lane's sub-chunk again, pair by pair, by the canonical rule
+                Ac = Acc{0.f, 0.f, 0.f, 0.f, 0.f};
+                for (int j = 0; j < cnt; ++j) {
+                  const float4 l = Sc[j].a;
+                  if (HAS_Z && Sc[j].b.x > sz) continue;
+                  const float dx = l.x - sx, dy = l.y - sy;
+                  const float d2 = fmaf(dy, dy, dx * dx);
+                  const int b = pair_bin<LOGB>(d2, l.x, l.y, sx, sy, C);
+                  if ((unsigned)b >= (unsigned)nb) continue;
+                  adj_pair<LOGB, WX>(sx, sy, l, coef[b], Ac);
                 }
-                adj_pair<LOGB, WX>(sx, sy, l, up ? kh : kl, Ac);
               }
             } else if (act) {
               for (int j = 0; j < cnt; ++j) {

@@ -126,7 +126,8 @@ __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const floa
 //   2  pairs fall in bins blo and blo+1 only    -> register sums split at the
 //                                                  one edge, FP64 re-binning
 //                                                  inside its guard band
-//   3  anything else (or a z cut)               -> per-pair binning (do_pair)
+//   3  anything else                           -> per-pair binning (do_pair)
+// A z cut (z_A > z_B skips the pair) is a per-pair mask inside all paths.
 // The path is chosen per warp (the largest class of its lanes), so lanes never
 // diverge inside a source loop.  Every pair still lands in its canonical bin:
 // in classes 1 and 2 the box bounds prove which bins are possible.
@@ -164,10 +165,11 @@ __device__ __forceinline__ void pair_terms(float lx, float ly, const float4 a, f
   }
 }
 
-// Class 1: every pair of the chunk is in bin `blo`.
-template <int MODE, bool HAS_M, bool LOGB, int NC, int QA>
-__device__ __forceinline__ void chunk_single(const SrcRec* __restrict__ S, int cnt, float lx, float ly, int cls,
-                                             int blo, float* __restrict__ hcol) {
+// Class 1: every pair of the chunk is in bin `blo`.  With a z cut, a pair
+// with z_A > z_B (src/tpcf.f90:322) adds nothing.
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int NC, int QA>
+__device__ __forceinline__ void chunk_single(const SrcRec* __restrict__ S, int cnt, float lx, float ly, float lz,
+                                             int cls, int blo, float* __restrict__ hcol) {
   float acc[QA];
 #pragma unroll
   for (int q = 0; q < QA; ++q) acc[q] = 0.f;
@@ -177,21 +179,24 @@ __device__ __forceinline__ void chunk_single(const SrcRec* __restrict__ S, int c
     const float4 b = S[j].b;
     float d2, d, r, X, Y;
     pair_terms<MODE, LOGB>(lx, ly, a, d2, d, r, X, Y);
-    acc[QGT] = fmaf(r, X, acc[QGT]);
-    acc[QGX] = fmaf(r, Y, acc[QGX]);
-    acc[QW] += b.x;
-    acc[QDW] = fmaf(d, b.x, acc[QDW]);
-    if (MODE == 0 && HAS_M) acc[QK] += b.y;
+    if (!HAS_Z || lz <= b.z) {
+      acc[QGT] = fmaf(r, X, acc[QGT]);
+      acc[QGX] = fmaf(r, Y, acc[QGX]);
+      acc[QW] += b.x;
+      acc[QDW] = fmaf(d, b.x, acc[QDW]);
+      if (MODE == 0 && HAS_M) acc[QK] += b.y;
+      if (HAS_Z) acc[QN] += 1.f;
+    }
   }
-  acc[QN] = (float)cnt;
+  if (!HAS_Z) acc[QN] = (float)cnt;
   if (cls == 1) hist_add<QA, NC>(hcol, blo, acc);
 }
 
 // Class 2: pairs in bins blo and blo+1 (either may be out of range, then it is
 // dropped); the edge between them is e2f[blo+1].
-template <int MODE, bool HAS_M, bool LOGB, int NC, int QA>
-__device__ __forceinline__ void chunk_dual(const SrcRec* __restrict__ S, int cnt, float lx, float ly, int cls,
-                                           int blo, float* __restrict__ hcol, const BinCtx& C) {
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int NC, int QA>
+__device__ __forceinline__ void chunk_dual(const SrcRec* __restrict__ S, int cnt, float lx, float ly, float lz,
+                                           int cls, int blo, float* __restrict__ hcol, const BinCtx& C) {
   float tot[QA], hi[QA];
 #pragma unroll
   for (int q = 0; q < QA; ++q) tot[q] = hi[q] = 0.f;
@@ -205,6 +210,7 @@ __device__ __forceinline__ void chunk_dual(const SrcRec* __restrict__ S, int cnt
     const float4 b = S[j].b;
     float d2, d, r, X, Y;
     pair_terms<MODE, LOGB>(lx, ly, a, d2, d, r, X, Y);
+    if (HAS_Z && lz > b.z) continue;  // src/tpcf.f90:322
     const bool up = d2 >= E;
     near |= fabsf(d2 - E) <= gE;
     // products folded into the sums: one FFMA per quantity and side
@@ -213,6 +219,7 @@ __device__ __forceinline__ void chunk_dual(const SrcRec* __restrict__ S, int cnt
     tot[QW] += b.x;
     tot[QDW] = fmaf(d, b.x, tot[QDW]);
     if (MODE == 0 && HAS_M) tot[QK] += b.y;
+    if (HAS_Z) tot[QN] += 1.f;
     if (up) {
       hi[QGT] = fmaf(r, X, hi[QGT]);
       hi[QGX] = fmaf(r, Y, hi[QGX]);
@@ -222,13 +229,13 @@ __device__ __forceinline__ void chunk_dual(const SrcRec* __restrict__ S, int cnt
       if (MODE == 0 && HAS_M) hi[QK] += b.y;
     }
   }
-  tot[QN] = (float)cnt;
+  if (!HAS_Z) tot[QN] = (float)cnt;
   if (cls == 0) return;
   if (near) {
     // rare (a pair within a relative 4e-6 of the edge): this lane's register
     // sums are dropped and the sub-chunk is binned pair by pair, each pair by
     // the canonical rule
-    for (int j = 0; j < cnt; ++j) do_pair<MODE, HAS_M, false, LOGB, NC, QA>(lx, ly, 0.f, S[j].a, S[j].b, hcol, C);
+    for (int j = 0; j < cnt; ++j) do_pair<MODE, HAS_M, HAS_Z, LOGB, NC, QA>(lx, ly, lz, S[j].a, S[j].b, hcol, C);
     return;
   }
   float lo[QA];
@@ -409,7 +416,7 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
               const int base = sc * 32;
               const int cnt = min(32, n - base);
               int blo = 0;
-              const int cls = act ? classify<LOGB, HAS_Z>(lx, ly, subbox[sc], C, blo) : 0;
+              const int cls = act ? classify<LOGB, HAS_Z, true>(lx, ly, subbox[sc], C, blo) : 0;
               const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)cls);
 #ifdef TPCF_MODE_STATS
               {
@@ -423,9 +430,9 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
               if (m == 0) continue;
               const SrcRec* __restrict__ Sc = S + base;
               if (m == 1) {
-                chunk_single<MODE, HAS_M, LOGB, BT, QA>(Sc, cnt, lx, ly, cls, blo, hcol);
+                chunk_single<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(Sc, cnt, lx, ly, lz, cls, blo, hcol);
               } else if (m == 2) {
-                chunk_dual<MODE, HAS_M, LOGB, BT, QA>(Sc, cnt, lx, ly, cls, blo, hcol, C);
+                chunk_dual<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(Sc, cnt, lx, ly, lz, cls, blo, hcol, C);
               } else if (act) {
                 int j = 0;
                 for (; j + 4 <= cnt; j += 4) {

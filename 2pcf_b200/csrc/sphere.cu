@@ -176,8 +176,7 @@ __device__ __forceinline__ int classify_s(const LensS& L, const float4 mn, const
   }
   if (b1 < 0 || b0 >= C.nb) return 0;
   blo = b0;
-  if (HAS_Z) return 3;
-  if (b0 == b1) return 1;
+  if (b0 == b1) return 1;  // a z cut is applied inside the register paths
   if (b1 == b0 + 1) return 2;
   return 3;
 }
@@ -201,9 +200,9 @@ __device__ __forceinline__ void do_pair_s(const LensS& L, float lz, const SrcRec
   if (MODE == 0 && HAS_M) h[QK * NC] += s.c.y;
 }
 
-template <int MODE, bool HAS_M, bool SMALL, int NC, int QA>
-__device__ __forceinline__ void chunk_single_s(const SrcRecS* __restrict__ S, int cnt, const LensS& L, int cls,
-                                               int blo, float* __restrict__ hcol) {
+template <int MODE, bool HAS_M, bool HAS_Z, bool SMALL, int NC, int QA>
+__device__ __forceinline__ void chunk_single_s(const SrcRecS* __restrict__ S, int cnt, const LensS& L, float lz,
+                                               int cls, int blo, float* __restrict__ hcol) {
   float acc[QA];
 #pragma unroll
   for (int q = 0; q < QA; ++q) acc[q] = 0.f;
@@ -212,19 +211,22 @@ __device__ __forceinline__ void chunk_single_s(const SrcRecS* __restrict__ S, in
     const float4 a = S[j].a, b = S[j].b, cc = S[j].c;
     float d2, th, r, X, Y;
     sph_terms<MODE, SMALL>(L, a, b, d2, th, r, X, Y);
-    acc[QGT] = fmaf(r, X, acc[QGT]);
-    acc[QGX] = fmaf(r, Y, acc[QGX]);
-    acc[QW] += cc.x;
-    acc[QDW] = fmaf(th, cc.x, acc[QDW]);
-    if (MODE == 0 && HAS_M) acc[QK] += cc.y;
+    if (!HAS_Z || lz <= cc.z) {  // src/tpcf.f90:322
+      acc[QGT] = fmaf(r, X, acc[QGT]);
+      acc[QGX] = fmaf(r, Y, acc[QGX]);
+      acc[QW] += cc.x;
+      acc[QDW] = fmaf(th, cc.x, acc[QDW]);
+      if (MODE == 0 && HAS_M) acc[QK] += cc.y;
+      if (HAS_Z) acc[QN] += 1.f;
+    }
   }
-  acc[QN] = (float)cnt;
+  if (!HAS_Z) acc[QN] = (float)cnt;
   if (cls == 1) hist_add<QA, NC>(hcol, blo, acc);
 }
 
-template <int MODE, bool HAS_M, bool SMALL, int NC, int QA>
-__device__ __forceinline__ void chunk_dual_s(const SrcRecS* __restrict__ S, int cnt, const LensS& L, int cls,
-                                             int blo, float* __restrict__ hcol, const BinCtx& C) {
+template <int MODE, bool HAS_M, bool HAS_Z, bool SMALL, int NC, int QA>
+__device__ __forceinline__ void chunk_dual_s(const SrcRecS* __restrict__ S, int cnt, const LensS& L, float lz,
+                                             int cls, int blo, float* __restrict__ hcol, const BinCtx& C) {
   float tot[QA], hi[QA];
 #pragma unroll
   for (int q = 0; q < QA; ++q) tot[q] = hi[q] = 0.f;
@@ -236,6 +238,7 @@ __device__ __forceinline__ void chunk_dual_s(const SrcRecS* __restrict__ S, int 
     const float4 a = S[j].a, b = S[j].b, cc = S[j].c;
     float d2, th, r, X, Y;
     sph_terms<MODE, SMALL>(L, a, b, d2, th, r, X, Y);
+    if (HAS_Z && lz > cc.z) continue;  // src/tpcf.f90:322
     const bool up = d2 >= E;
     near |= fabsf(d2 - E) <= gE;
     tot[QGT] = fmaf(r, X, tot[QGT]);
@@ -243,6 +246,7 @@ __device__ __forceinline__ void chunk_dual_s(const SrcRecS* __restrict__ S, int 
     tot[QW] += cc.x;
     tot[QDW] = fmaf(th, cc.x, tot[QDW]);
     if (MODE == 0 && HAS_M) tot[QK] += cc.y;
+    if (HAS_Z) tot[QN] += 1.f;
     if (up) {
       hi[QGT] = fmaf(r, X, hi[QGT]);
       hi[QGX] = fmaf(r, Y, hi[QGX]);
@@ -252,10 +256,10 @@ __device__ __forceinline__ void chunk_dual_s(const SrcRecS* __restrict__ S, int 
       if (MODE == 0 && HAS_M) hi[QK] += cc.y;
     }
   }
-  tot[QN] = (float)cnt;
+  if (!HAS_Z) tot[QN] = (float)cnt;
   if (cls == 0) return;
   if (near) {  // rare: the sub-chunk is binned pair by pair by the canonical rule
-    for (int j = 0; j < cnt; ++j) do_pair_s<MODE, HAS_M, false, SMALL, SMALL, NC, QA>(L, 0.f, S[j], hcol, C);
+    for (int j = 0; j < cnt; ++j) do_pair_s<MODE, HAS_M, HAS_Z, SMALL, SMALL, NC, QA>(L, lz, S[j], hcol, C);
     return;
   }
   float lo[QA];
@@ -523,9 +527,9 @@ __global__ void __launch_bounds__(BT) k_pairs_sph(const PairParams P) {
             if (m == 0) continue;
             const SrcRecS* __restrict__ Sc = S + base;
             if (m == 1) {
-              chunk_single_s<MODE, HAS_M, SMALL, BT, QA>(Sc, cnt, Lf, cls, blo, hcol);
+              chunk_single_s<MODE, HAS_M, HAS_Z, SMALL, BT, QA>(Sc, cnt, Lf, lz, cls, blo, hcol);
             } else if (m == 2) {
-              chunk_dual_s<MODE, HAS_M, SMALL, BT, QA>(Sc, cnt, Lf, cls, blo, hcol, C);
+              chunk_dual_s<MODE, HAS_M, HAS_Z, SMALL, BT, QA>(Sc, cnt, Lf, lz, cls, blo, hcol, C);
             } else if (act) {
               for (int j = 0; j < cnt; ++j) do_pair_s<MODE, HAS_M, HAS_Z, LOGB, SMALL, BT, QA>(Lf, lz, Sc[j], hcol, C);
             }

@@ -135,7 +135,7 @@ __device__ __forceinline__ int edge_index_f32(float v, const float* e2f, int nb)
   return lo;
 }
 
-template <bool LOGB, bool HAS_Z>
+template <bool LOGB, bool HAS_Z, bool ZREG = false>
 __device__ __forceinline__ int classify(float lx, float ly, const float4 box, const BinCtx& C, int& blo) {
   const float dxl = fmaxf(fmaxf(box.x - lx, lx - box.z), 0.f);
   const float dyl = fmaxf(fmaxf(box.y - ly, ly - box.w), 0.f);
@@ -153,7 +153,7 @@ __device__ __forceinline__ int classify(float lx, float ly, const float4 box, co
   }
   if (b1 < 0 || b0 >= C.nb) return 0;
   blo = b0;
-  if (HAS_Z) return 3;
+  if (HAS_Z && !ZREG) return 3;  // z cut: per-pair path unless the register paths apply it
   if (b0 == b1) return 1;
   if (b1 == b0 + 1) return 2;
   return 3;
