@@ -28,7 +28,8 @@ def _corner(cats, x_cut, y_cut):
     return out
 
 
-def autotune_cell_size(lenses, shapes, tasks, bins, ctx: Context, divisors=DIVISORS, corner=0.6, reps=2):
+def autotune_cell_size(lenses, shapes, tasks, bins, ctx: Context, divisors=DIVISORS, corner=0.6, reps=2,
+                       spherical_coords=False):
     """Pick the cell side theta_max/d (d in ``divisors``) with the shortest pair
     kernel on the lower-left ``corner`` fraction of the field, set it on ``ctx``
     and return {d: ms per 1e9 binned pairs}.  Host (numpy) catalogues."""
@@ -43,7 +44,7 @@ def autotune_cell_size(lenses, shapes, tasks, bins, ctx: Context, divisors=DIVIS
         ctx.set_cell_size(bins.x_max / d)
         best = None
         for _ in range(reps):
-            outs = batch_shear_2pcf(L, S, tasks, bins, ctx=ctx)
+            outs = batch_shear_2pcf(L, S, tasks, bins, spherical_coords=spherical_coords, ctx=ctx)
             st = ctx.stats()
             pairs = sum(int(o.n_pairs.sum()) for o in outs)
             cost = st["pair_kernel_ms"] / max(pairs, 1) * 1e9

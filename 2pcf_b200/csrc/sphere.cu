@@ -276,6 +276,13 @@ __device__ __forceinline__ void chunk_dual_s(const SrcRecS* __restrict__ S, int 
 // ------------------------------------------------------------ cell runs -----
 constexpr float kTwoPiF = 6.28318548f;      // 2 pi rounded up to FP32
 constexpr int kRowsS = kMaxRows / 4;        // rows per chunk: 3 runs each fit kMaxRows
+#ifndef TPCF_SPH_TILE
+#define TPCF_SPH_TILE 160
+#endif
+// Sources per shared-memory tile (48-byte records): the tile size sets how
+// many blocks share an SM next to the FP32 histogram.
+constexpr int kTileS = TPCF_SPH_TILE;
+constexpr int kFlushSrcS = 1024;  // FP32 histogram -> FP64 after about this many sources
 
 // Lambda reach of a work item: full = every cell of a row, else the interval
 // [box.x - dl, box.z + dl] modulo 2 pi.
@@ -326,7 +333,7 @@ __host__ __device__ inline size_t align_up_s(size_t v, size_t a) { return (v + a
 __host__ __device__ inline SphSmem sph_smem_layout(int nb, int qa, int bt) {
   SphSmem s;
   size_t o = 0;
-  s.tiles = o; o += 2 * kTile * sizeof(SrcRecS);
+  s.tiles = o; o += 2 * kTileS * sizeof(SrcRecS);
   s.hist = o;  o += (size_t)nb * qa * bt * sizeof(float);
   o = align_up_s(o, 16);
   s.bsum = o;  o += (size_t)kQ * nb * sizeof(double);
@@ -339,7 +346,7 @@ __host__ __device__ inline SphSmem sph_smem_layout(int nb, int qa, int bt) {
   s.span1 = o; o += kMaxRows * sizeof(int);
   s.tpref = o; o += (kMaxRows + 1) * sizeof(int);
   o = align_up_s(o, 16);
-  s.subbox = o; o += 2 * (kTile / 32) * sizeof(float4);
+  s.subbox = o; o += 2 * (kTileS / 32) * sizeof(float4);
   s.mbar = o;  o += 2 * sizeof(uint64_t);
   s.misc = o;  o += 16;
   s.total = align_up_s(o, 128);
@@ -455,7 +462,7 @@ __global__ void __launch_bounds__(BT) k_pairs_sph(const PairParams P) {
         int acc = 0;
         for (int r = 0; r < ns; ++r) {
           tpref[r] = acc;
-          acc += (span1[r] - span0[r] + kTile - 1) / kTile;
+          acc += (span1[r] - span0[r] + kTileS - 1) / kTileS;
         }
         tpref[ns] = acc;
       }
@@ -465,27 +472,27 @@ __global__ void __launch_bounds__(BT) k_pairs_sph(const PairParams P) {
       if (tid == 0 && ntiles > 0) {
         while (tpref[ri + 1] <= 0) ++ri;
         const int s0 = span0[ri];
-        const int n0 = min(kTile, span1[ri] - s0);
+        const int n0 = min(kTileS, span1[ri] - s0);
         const int bb = tcount & 1u;
         mbar_arrive_tx(&mbar[bb], (uint32_t)(n0 * sizeof(SrcRecS)));
-        bulk_g2s(tiles + bb * kTile, G.recs + s0, (uint32_t)(n0 * sizeof(SrcRecS)), &mbar[bb]);
+        bulk_g2s(tiles + bb * kTileS, G.recs + s0, (uint32_t)(n0 * sizeof(SrcRecS)), &mbar[bb]);
       }
       for (int k = 0; k < ntiles; ++k) {
         if (tid == 0 && k + 1 < ntiles) {
           while (tpref[ri + 1] <= k + 1) ++ri;
-          const int s1 = span0[ri] + (k + 1 - tpref[ri]) * kTile;
-          const int n1 = min(kTile, span1[ri] - s1);
+          const int s1 = span0[ri] + (k + 1 - tpref[ri]) * kTileS;
+          const int n1 = min(kTileS, span1[ri] - s1);
           const int bb = (tcount + k + 1) & 1u;
           mbar_arrive_tx(&mbar[bb], (uint32_t)(n1 * sizeof(SrcRecS)));
-          bulk_g2s(tiles + bb * kTile, G.recs + s1, (uint32_t)(n1 * sizeof(SrcRecS)), &mbar[bb]);
+          bulk_g2s(tiles + bb * kTileS, G.recs + s1, (uint32_t)(n1 * sizeof(SrcRecS)), &mbar[bb]);
         }
         while (tpref[rc + 1] <= k) ++rc;
-        const int s = span0[rc] + (k - tpref[rc]) * kTile;
-        const int n = min(kTile, span1[rc] - s);
+        const int s = span0[rc] + (k - tpref[rc]) * kTileS;
+        const int n = min(kTileS, span1[rc] - s);
         const int bb = (tcount + k) & 1u;
         const bool ok = mbar_wait_bounded(&mbar[bb], (phase >> bb) & 1u);
         phase ^= (1u << bb);
-        const SrcRecS* __restrict__ S = tiles + bb * kTile;
+        const SrcRecS* __restrict__ S = tiles + bb * kTileS;
         const int nsub = (n + 31) >> 5;
         if (ok) {
           // 3-D box of each 32-source sub-chunk, widened by 2^-23 per side:
@@ -536,7 +543,7 @@ __global__ void __launch_bounds__(BT) k_pairs_sph(const PairParams P) {
           }
         }
         since_flush += n;
-        if (since_flush >= 4 * kTile) {
+        if (since_flush >= kFlushSrcS) {
           flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
           first_flush = false;
           since_flush = 0;

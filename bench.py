@@ -203,6 +203,16 @@ def adjoint_timing(w, ctx, bins, pairs, pair_ms, stream):
                     "the batched step"}
 
 
+def sky_patch(x, y, box, lam0_deg=40.0, phi0_deg=-30.0):
+    """Flat arcmin coordinates of a box of side ``box`` mapped onto a sky
+    patch centred at (lam0, phi0): latitude offset = y, longitude offset =
+    x / cos(latitude) (radians, FP32)."""
+    d2r = np.pi / 180.0
+    phi = phi0_deg * d2r + (np.asarray(y, np.float64) - box / 2) / 60.0 * d2r
+    lam = lam0_deg * d2r + (np.asarray(x, np.float64) - box / 2) / 60.0 * d2r / np.cos(phi)
+    return lam.astype(np.float32), phi.astype(np.float32)
+
+
 def widened_timing(tpcf, w, peak_fp32, stream, cpu_threads, with_cpu=True):
     """Measurements of the rows around the pair sum: the spherical pair sum on
     the tomography catalogues projected onto a sky patch, xi from precomputed
@@ -247,12 +257,8 @@ def widened_timing(tpcf, w, peak_fp32, stream, cpu_threads, with_cpu=True):
 
     # spherical pair sum: the 25 tomography tasks on a 31.6 x 31.6 deg patch at
     # Dec -30 (flat arcmin coordinates mapped to longitude / latitude)
-    phi0, lam0, box = -30.0 * d2r, 40.0 * d2r, w["box"]
-
     def sph(c):
-        phi = phi0 + (c["y"].astype(np.float64) - box / 2) / 60.0 * d2r
-        lam = lam0 + (c["x"].astype(np.float64) - box / 2) / 60.0 * d2r / np.cos(phi)
-        return lam.astype(np.float32), phi.astype(np.float32)
+        return sky_patch(c["x"], c["y"], w["box"])
 
     Ls, Ss = [], []
     for l in w["lens_bins"]:
@@ -411,6 +417,9 @@ def main():
     ap.add_argument("--region", type=float, default=0.0,
                     help="profiling: keep only objects with x, y < REGION arcmin (density unchanged)")
     ap.add_argument("--task", type=int, default=-1, help="profiling: run only this task of the 25")
+    ap.add_argument("--geometry", default="plane", choices=["plane", "sphere"],
+                    help="profiling: 'sphere' projects the catalogues onto a sky patch and times the spherical "
+                         "pair kernel instead")
     ap.add_argument("--no-widened", action="store_true",
                     help="skip the spherical, marks, bootstrap, k-means and reader measurements")
     ap.add_argument("--cell-divisor", type=int, default=0,
@@ -442,6 +451,12 @@ def main():
                 cat[k] = np.ascontiguousarray(cat[k][keep])
     if args.task >= 0:
         w["tasks"] = [w["tasks"][args.task]]
+    sphere = args.geometry == "sphere"
+    if sphere:
+        for cat in w["lens_bins"] + w["shape_bins"]:
+            cat["x"], cat["y"] = sky_patch(cat["x"], cat["y"], w["box"])
+        lo, hi, nb_ = w["bins"]
+        w["bins"] = (lo / 60.0 * np.pi / 180.0, hi / 60.0 * np.pi / 180.0, nb_)
     bins = tpcf.create_bins(*w["bins"])
     n_patch = w["n_patch"]
     ctx = tpcf.Context(local)
@@ -458,7 +473,7 @@ def main():
             [tpcf.LensCatalog(**{k: l[k] for k in ("x", "y", "val", "w", "z")}) for l in w["lens_bins"]],
             [tpcf.ShapeCatalog(**{k: s_[k] for k in ("x", "y", "e1", "e2", "w", "z", "m")})
              for s_ in w["shape_bins"]],
-            w["tasks"], bins, ctx)
+            w["tasks"], bins, ctx, spherical_coords=sphere)
     if world > 1:
         ctx.set_shard(rank, world)
     n_boot = w["n_boot"]
@@ -489,7 +504,8 @@ def main():
     def step(L, S, U):
         lab, _, _ = tpcf.partition_data(U[0], U[1], U[2], n_patch, ctx=ctx)
         P = [lab[offs[i]:offs[i + 1]] for i in range(len(L))]
-        outs = tpcf.batch_shear_2pcf(L, S, w["tasks"], bins, lens_patches=P, n_patch=n_patch, ctx=ctx)
+        outs = tpcf.batch_shear_2pcf(L, S, w["tasks"], bins, lens_patches=P, n_patch=n_patch,
+                                     spherical_coords=sphere, ctx=ctx)
         ctx_pair_ms[0] = ctx.stats()["pair_kernel_ms"]  # the pair kernel's own CUDA-event time
         ps = np.stack([o.patch_sums for o in outs])
         if world > 1:
@@ -539,14 +555,15 @@ def main():
            + 2 * n_boot * len(w["tasks"]) * bins.n_bin * 8 + 2 * (len(w["tasks"]) * bins.n_bin) ** 2 * 8)
 
     adjoint = None
-    if world == 1 and not args.no_adjoint:
+    if world == 1 and not args.no_adjoint and not sphere:
         adjoint = adjoint_timing(w, ctx, bins, pairs, pair_ms, stream)
     peak = ctx.measure_fp32_peak()
-    achieved = pairs * FLOP_PER_PAIR / (pair_ms * 1e-3) / 1e12
+    fpp = SPH_FLOP_PER_PAIR if sphere else FLOP_PER_PAIR
+    achieved = pairs * fpp / (pair_ms * 1e-3) / 1e12
     # DRAM bytes of one pair-kernel launch of this exact workload, from one ncu
     # capture (profiles/k_pairs_tomography_10M_dram.md); other configurations
     # were not captured
-    default_cfg = args.scale == 1.0 and args.region <= 0 and args.task < 0 and \
+    default_cfg = not sphere and args.scale == 1.0 and args.region <= 0 and args.task < 0 and \
         abs(ctx.cell_size - bins.x_max / 64) < 1e-6
     traffic = K_PAIRS_DRAM_BYTES if default_cfg else None
 
@@ -567,18 +584,18 @@ def main():
         "e2e": {"value": pairs_e2e / (ms_e2e * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": traffic, "kernel": "k_pairs",
-                     "flop_per_pair": FLOP_PER_PAIR, "kernel_ms": pair_ms,
+                     "frac": achieved / peak, "traffic": traffic, "kernel": "k_pairs_sph" if sphere else "k_pairs",
+                     "flop_per_pair": fpp, "kernel_ms": pair_ms,
                      "peak_source": "measured in this run: FFMA loop (tpcf_measure_fp32_peak); "
                                     "MEASURED_PEAKS.json has no FP32 figure"},
         "gpu_launches": int(launches),
         "batched_adjoint": adjoint,
         "clocks": clocks,
     }
-    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+    if world == 1 and rank == 0 and not args.no_cpu_baseline and not sphere:
         cb = cpu_baseline(w, args.cpu_seconds, host_threads())
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
-    if world == 1 and not args.no_widened and args.region <= 0 and args.task < 0:
+    if world == 1 and not args.no_widened and args.region <= 0 and args.task < 0 and not sphere:
         line["widened"] = widened_timing(tpcf, w, peak, stream, host_threads(), with_cpu=not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
