@@ -340,6 +340,7 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
     for (int e = tid; e < kQ * nb; e += BT) bsum[e] = 0.0;
     bool first_flush = true;
     int since_flush = 0;
+    const int flush_src = P.flush_src > 0 ? P.flush_src : 4096;
     const float4 box = LD.group_box[g];
     int cy0, cy1;
     row_range(G, box, P.R, P.margin, cy0, cy1);
@@ -465,7 +466,7 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
           }
         }
         since_flush += n;
-        if (since_flush >= 4 * kTile) {
+        if (since_flush >= flush_src) {
           flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
           first_flush = false;
           since_flush = 0;

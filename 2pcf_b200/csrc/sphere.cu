@@ -282,7 +282,7 @@ constexpr int kRowsS = kMaxRows / 4;        // rows per chunk: 3 runs each fit k
 // Sources per shared-memory tile (48-byte records): the tile size sets how
 // many blocks share an SM next to the FP32 histogram.
 constexpr int kTileS = TPCF_SPH_TILE;
-constexpr int kFlushSrcS = 1024;  // FP32 histogram -> FP64 after about this many sources
+constexpr int kFlushSrcS = 4096;  // FP32 histogram -> FP64 after about this many sources
 
 // Lambda reach of a work item: full = every cell of a row, else the interval
 // [box.x - dl, box.z + dl] modulo 2 pi.
@@ -543,7 +543,7 @@ __global__ void __launch_bounds__(BT) k_pairs_sph(const PairParams P) {
           }
         }
         since_flush += n;
-        if (since_flush >= kFlushSrcS) {
+        if (since_flush >= (P.flush_src > 0 ? P.flush_src : kFlushSrcS)) {
           flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
           first_flush = false;
           since_flush = 0;

@@ -20,7 +20,6 @@ namespace tpcf {
 constexpr int kMaxBins = 128;
 constexpr int kMaxRows = 256;   // cell rows scanned per chunk of one work item
 constexpr int kTile = 256;      // sources per shared-memory tile
-constexpr int kFlushTiles = 4;  // FP32 histogram -> FP64 every 4 tiles (<= 1024 sources)
 constexpr int kQ = 6;           // quantities per bin in item/patch/lens sums
 
 // Quantity rows of every FP64 sum array (item, patch, lens and result sums).
@@ -98,7 +97,7 @@ struct PairParams {
   float margin;             // absolute margin for cell-boundary rounding
   float binA, binB;         // log spacing: t = lg2(d2)*binA + binB
   float eps;                // guard band half-width in t units (log) or relative (generic)
-  int pad;
+  int flush_src;            // FP32 histogram -> FP64 after this many sources (0: 4096)
 };
 
 }  // namespace tpcf
