@@ -1,7 +1,7 @@
 // pair_hist.cuh -- the per-thread FP32 pair histogram shared by the planar
 // and spherical pair kernels: layout [bin][quantity][thread] in shared
 // memory (a warp's read-modify-writes hit 32 distinct banks), folded into FP64
-// every ~1024 sources.
+// every ~4096 sources.
 #pragma once
 #include <cuda_runtime.h>
 

@@ -10,7 +10,7 @@
 // and bins the pair into its own FP32 histogram column in shared memory.  The
 // histogram is laid out [bin][quantity][thread], so a warp's 32 read-modify-
 // writes fall in 32 distinct banks whatever bins the lanes pick, and no
-// atomics are needed.  Every ~1024 sources the FP32 columns are folded into
+// atomics are needed.  Every ~4096 sources the FP32 columns are folded into
 // FP64: per block (times the lens factors val*w or w) and, when per-lens output
 // is requested, per lens.
 //
