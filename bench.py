@@ -422,8 +422,10 @@ def main():
                          "pair kernel instead")
     ap.add_argument("--no-widened", action="store_true",
                     help="skip the spherical, marks, bootstrap, k-means and reader measurements")
-    ap.add_argument("--cell-divisor", type=int, default=0,
-                    help="grid cell side theta_max/D without autotuning (0: autotune)")
+    ap.add_argument("--cell-divisor", type=int, default=64,
+                    help="grid cell side theta_max/D (64: the autotuner's usual choice on this workload)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick the cell side with 2pcf_b200.autotune on a corner of the field instead")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -464,7 +466,7 @@ def main():
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     # cell side picked by the autotuner (trial calls on a density-preserving corner)
-    if args.cell_divisor > 0:
+    if not args.autotune:
         ctx.set_cell_size(bins.x_max / args.cell_divisor)
         tune = {}
     else:
