@@ -92,6 +92,41 @@ struct Acc {
 };
 
 // One pair (source j owns the thread, lens i from the tile) with coefficients k.
+// The bin-independent part of a pair's adjoint terms: with F = val_A w_A / d^2
+// (l.z = val_A w_A), S1 += F (dx^2 - dy^2), S2 += F dx dy, SN += w_A.  Within
+// a run of pairs of one bin the bin's coefficients multiply these sums once:
+// a1 = k.x S1, a2 = 2 k.x S2, b1 = k.y S1, b2 = 2 k.y S2, n = k.z SN.
+template <bool LOGB>
+__device__ __forceinline__ void adj_factors(float sx, float sy, const float4 l, float& S1, float& S2, float& SN,
+                                            float& d2) {
+  const float dx = l.x - sx;  // lens minus source, as in the forward pass
+  const float dy = l.y - sy;
+  const float dx2 = dx * dx;
+  d2 = fmaf(dy, dy, dx2);
+  float r;
+  if (LOGB) {
+    const float rs = rsqrtf(d2);
+    r = rs * rs;
+  } else {
+    r = __frcp_rn(d2);
+  }
+  const float F = l.z * r;
+  S1 = fmaf(F, fmaf(-dy, dy, dx2), S1);
+  S2 = fmaf(F, dx * dy, S2);
+  SN += l.w;
+}
+
+template <bool WX>
+__device__ __forceinline__ void adj_apply(const float4 k, float S1, float S2, float SN, Acc& A) {
+  A.a1 = fmaf(k.x, S1, A.a1);
+  A.a2 = fmaf(2.f * k.x, S2, A.a2);
+  if (WX) {
+    A.b1 = fmaf(k.y, S1, A.b1);
+    A.b2 = fmaf(2.f * k.y, S2, A.b2);
+  }
+  A.n = fmaf(k.z, SN, A.n);
+}
+
 template <bool LOGB, bool WX>
 __device__ __forceinline__ void adj_pair(float sx, float sy, const float4 l, const float4 k, Acc& A) {
   const float dx = l.x - sx;  // lens minus source, as in the forward pass
@@ -256,9 +291,11 @@ __global__ void __launch_bounds__(BT) k_adj(const AdjParams P) {
             if (m == 1) {
               // every pair of this lane is in bin blo (or the lane has none)
               const float4 kc = cls == 1 ? coef[blo] : make_float4(0.f, 0.f, 0.f, 0.f);
+              float S1 = 0.f, S2 = 0.f, SN = 0.f, d2;
 #pragma unroll 4
               for (int j = 0; j < cnt; ++j)  // a lens behind the source adds nothing (src/tpcf.f90:322)
-                if (!HAS_Z || Sc[j].b.x <= sz) adj_pair<LOGB, WX>(sx, sy, Sc[j].a, kc, Ac);
+                if (!HAS_Z || Sc[j].b.x <= sz) adj_factors<LOGB>(sx, sy, Sc[j].a, S1, S2, SN, d2);
+              adj_apply<WX>(kc, S1, S2, SN, Ac);
             } else if (m == 2) {
               const float4 kl = (cls >= 1 && blo >= 0) ? coef[blo] : make_float4(0.f, 0.f, 0.f, 0.f);
               // a side outside [x_min, x_max] contributes nothing
@@ -267,15 +304,29 @@ __global__ void __launch_bounds__(BT) k_adj(const AdjParams P) {
               const float E = cls == 2 ? e2f[blo + 1] : 3.0e38f;
               const float gE = cls == 2 ? E * C.eps_rel : 0.f;
               bool near = false;  // some pair lies within the guard band of E
+              float T1 = 0.f, T2 = 0.f, TN = 0.f, H1 = 0.f, H2 = 0.f, HN = 0.f;
 #pragma unroll 2
               for (int j = 0; j < cnt; ++j) {
+                if (HAS_Z && Sc[j].b.x > sz) continue;
                 const float4 l = Sc[j].a;
                 const float dx = l.x - sx, dy = l.y - sy;
-                const float d2 = fmaf(dy, dy, dx * dx);
-                if (HAS_Z && Sc[j].b.x > sz) continue;
+                const float dx2 = dx * dx;
+                const float d2 = fmaf(dy, dy, dx2);
                 near |= fabsf(d2 - E) <= gE;
-                adj_pair<LOGB, WX>(sx, sy, l, d2 >= E ? kh : kl, Ac);
+                float r;
+                if (LOGB) {
+                  const float rs = rsqrtf(d2);
+                  r = rs * rs;
+                } else {
+                  r = __frcp_rn(d2);
+                }
+                const float F = l.z * r;
+                const float p1 = F * fmaf(-dy, dy, dx2), p2 = F * (dx * dy);
+                T1 += p1; T2 += p2; TN += l.w;
+                if (d2 >= E) { H1 += p1; H2 += p2; HN += l.w; }
               }
+              adj_apply<WX>(kl, T1 - H1, T2 - H2, TN - HN, Ac);
+              adj_apply<WX>(kh, H1, H2, HN, Ac);
               if (near) {  // rare: this lane's sub-chunk again, pair by pair, by the canonical rule
                 Ac = Acc{0.f, 0.f, 0.f, 0.f, 0.f};
                 for (int j = 0; j < cnt; ++j) {
