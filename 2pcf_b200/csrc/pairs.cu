@@ -40,6 +40,9 @@ namespace tpcf {
 
 constexpr int kDualUnroll = TPCF_DUAL_UNROLL;      // source-loop unrolling of the one-edge path
 constexpr int kSingleUnroll = TPCF_SINGLE_UNROLL;  // and of the single-bin path
+// Coordinate of the null source that pads an odd sub-chunk in SrcPair form:
+// its d2 (~2e36) stays finite in FP32 and its weight and values are zero.
+constexpr float kNullPos = 1.0e18f;
 
 // ------------------------------------------------------- shared-memory map --
 struct PairSmem {
@@ -132,119 +135,174 @@ __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const floa
 // diverge inside a source loop.  Every pair still lands in its canonical bin:
 // in classes 1 and 2 the box bounds prove which bins are possible.
 
-// Per-pair quantities shared by the register paths.  Shear: with
-// P = dx^2 - dy^2, u = 2 dx dy and r = 1/d^2, cos 2phi = P r, sin 2phi = u r
-// (src/tpcf.f90:343-344), so the g_t, g_x terms are r*X and r*Y with
-// X = p P + q u, Y = q P - p u  (p = -e1 w, q = -e2 w).  Scalar-scalar:
-// X = kE w, Y = kB w, r = 1.
+// Per-pair quantities shared by the register paths, for the two sources of
+// one SrcPair at once (packed FP32: one instruction per operation for both
+// pairs).  Shear: with P = dx^2 - dy^2, u = 2 dx dy and r = 1/d^2,
+// cos 2phi = P r, sin 2phi = u r (src/tpcf.f90:343-344), so the g_t, g_x
+// terms are r*X and r*Y with X = p P + q u, Y = q P - p u (p = -e1 w,
+// q = -e2 w).  Scalar-scalar: X = kE w, Y = kB w, r = 1.  Both signs of dy
+// come from adds (y - ly and ny + ly), so no operand needs a negation; every
+// term equals the scalar computation lx - x, ly - y, ... bit for bit.
+struct LensP {
+  float2 nlx, nly, ly;  // (-lx, -lx), (-ly, -ly), (ly, ly)
+};
+
 template <int MODE, bool LOGB>
-__device__ __forceinline__ void pair_terms(float lx, float ly, const float4 a, float& d2, float& d, float& r,
-                                           float& X, float& Y) {
-  const float dx = lx - a.x;
-  const float dy = ly - a.y;
-  const float dx2 = dx * dx;
-  d2 = fmaf(dy, dy, dx2);
+__device__ __forceinline__ void pair_terms2(const LensP& L, const float4 xy, const float4 pq, const float2 ny,
+                                            float2& d2, float2& d, float2& r, float2& X, float2& Y) {
+  const float2 dxp = add2(lo2(xy), L.nlx);  // x - lx
+  const float2 dyp = add2(hi2(xy), L.nly);  // y - ly
+  const float2 dx2 = mul2(dxp, dxp);
+  d2 = fma2(dyp, dyp, dx2);
   if (LOGB) {
-    const float rs = rsqrtf(d2);
-    d = d2 * rs;
-    r = rs * rs;
+    const float2 rs = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+    d = mul2(d2, rs);
+    r = mul2(rs, rs);
   } else {
-    d = sqrtf(d2);
-    r = __frcp_rn(d2);
+    d = make_float2(sqrtf(d2.x), sqrtf(d2.y));
+    r = make_float2(__frcp_rn(d2.x), __frcp_rn(d2.y));
   }
   if (MODE == 0) {
-    const float P = fmaf(-dy, dy, dx2);
-    const float qq = dx * dy;
-    const float u = qq + qq;
-    X = fmaf(a.z, P, a.w * u);
-    Y = fmaf(a.w, P, -(a.z * u));
+    const float2 dym = add2(ny, L.ly);         // ly - y
+    const float2 P = fma2(dym, dyp, dx2);      // dx^2 - dy^2
+    const float2 dxx = add2(dxp, dxp);
+    const float2 u = mul2(dxx, dyp);           //  2 dx dy
+    const float2 un = mul2(dxx, dym);          // -2 dx dy
+    X = fma2(lo2(pq), P, mul2(hi2(pq), u));
+    Y = fma2(hi2(pq), P, mul2(lo2(pq), un));
   } else {
-    r = 1.f;
-    X = a.z;
-    Y = a.w;
+    r = dup2(1.f);
+    X = lo2(pq);
+    Y = hi2(pq);
   }
+}
+
+// Source j of a sub-chunk in SrcPair form, as the (a, b) records of do_pair.
+__device__ __forceinline__ void src_of(const SrcPair* __restrict__ S, int j, float4& a, float4& b) {
+  const float* f = reinterpret_cast<const float*>(S + (j >> 1)) + (j & 1);
+  a = make_float4(f[0], f[2], f[4], f[6]);
+  b = make_float4(f[8], f[10], f[12], 0.f);
 }
 
 // Class 1: every pair of the chunk is in bin `blo`.  With a z cut, a pair
-// with z_A > z_B (src/tpcf.f90:322) adds nothing.
+// with z_A > z_B (src/tpcf.f90:322) adds nothing.  An odd count is padded by
+// a null source (zero weight and values, far away, NaN z): it adds zero to
+// every sum, and the pair count is cnt (or the z-mask sum, which excludes it).
 template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int NC, int QA>
-__device__ __forceinline__ void chunk_single(const SrcRec* __restrict__ S, int cnt, float lx, float ly, float lz,
+__device__ __forceinline__ void chunk_single(const SrcPair* __restrict__ S, int cnt, const LensP& L, float lz,
                                              int cls, int blo, float* __restrict__ hcol) {
-  float acc[QA];
-#pragma unroll
-  for (int q = 0; q < QA; ++q) acc[q] = 0.f;
+  float2 sgt = dup2(0.f), sgx = dup2(0.f), sw = dup2(0.f), sdw = dup2(0.f), sk = dup2(0.f), sn = dup2(0.f);
+  const int np = (cnt + 1) >> 1;
 #pragma unroll kSingleUnroll
-  for (int j = 0; j < cnt; ++j) {
-    const float4 a = S[j].a;
-    const float4 b = S[j].b;
-    float d2, d, r, X, Y;
-    pair_terms<MODE, LOGB>(lx, ly, a, d2, d, r, X, Y);
-    if (!HAS_Z || lz <= b.z) {
-      acc[QGT] = fmaf(r, X, acc[QGT]);
-      acc[QGX] = fmaf(r, Y, acc[QGX]);
-      acc[QW] += b.x;
-      acc[QDW] = fmaf(d, b.x, acc[QDW]);
-      if (MODE == 0 && HAS_M) acc[QK] += b.y;
-      if (HAS_Z) acc[QN] += 1.f;
+  for (int k = 0; k < np; ++k) {
+    const float4 xy = S[k].xy, pq = S[k].pq, wk = S[k].wk, zn = S[k].zn;
+    float2 d2, d, r, X, Y;
+    pair_terms2<MODE, LOGB>(L, xy, pq, hi2(zn), d2, d, r, X, Y);
+    float2 w = lo2(wk), K = hi2(wk);
+    if (HAS_Z) {
+      const float2 zm = make_float2(lz <= zn.x ? 1.f : 0.f, lz <= zn.y ? 1.f : 0.f);
+      r = mul2(r, zm);
+      w = mul2(w, zm);
+      if (MODE == 0 && HAS_M) K = mul2(K, zm);
+      sn = add2(sn, zm);
     }
+    sgt = fma2(r, X, sgt);
+    sgx = fma2(r, Y, sgx);
+    sw = add2(sw, w);
+    sdw = fma2(d, w, sdw);
+    if (MODE == 0 && HAS_M) sk = add2(sk, K);
   }
-  if (!HAS_Z) acc[QN] = (float)cnt;
-  if (cls == 1) hist_add<QA, NC>(hcol, blo, acc);
+  if (cls != 1) return;
+  float acc[QA];
+  acc[QGT] = sum2(sgt);
+  acc[QGX] = sum2(sgx);
+  acc[QW] = sum2(sw);
+  acc[QDW] = sum2(sdw);
+  acc[QN] = HAS_Z ? sum2(sn) : (float)cnt;
+  if (MODE == 0 && HAS_M) acc[QK] = sum2(sk);
+  hist_add<QA, NC>(hcol, blo, acc);
 }
 
 // Class 2: pairs in bins blo and blo+1 (either may be out of range, then it is
-// dropped); the edge between them is e2f[blo+1].
+// dropped); the edge between them is e2f[blo+1].  Sums over all pairs (s*)
+// and over the upper side (h*, masked by d2 >= E as 1/0); the lower side is
+// their difference.
 template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int NC, int QA>
-__device__ __forceinline__ void chunk_dual(const SrcRec* __restrict__ S, int cnt, float lx, float ly, float lz,
-                                           int cls, int blo, float* __restrict__ hcol, const BinCtx& C) {
-  float tot[QA], hi[QA];
-#pragma unroll
-  for (int q = 0; q < QA; ++q) tot[q] = hi[q] = 0.f;
+__device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int cnt, const LensP& L, float lx, float ly,
+                                           float lz, int cls, int blo, float* __restrict__ hcol, const BinCtx& C) {
+  float2 sgt = dup2(0.f), sgx = dup2(0.f), sw = dup2(0.f), sdw = dup2(0.f), sk = dup2(0.f), sn = dup2(0.f);
+  float2 hgt = dup2(0.f), hgx = dup2(0.f), hw = dup2(0.f), hdw = dup2(0.f), hk = dup2(0.f), hn = dup2(0.f);
   // lanes of class 1 (or 0) keep an edge no pair reaches
   const float E = (cls == 2) ? C.e2f[blo + 1] : 3.0e38f;
   const float gE = (cls == 2) ? E * C.eps_rel : 0.f;
+  const float2 nE = dup2(-E);
   bool near = false;  // some pair lies within the guard band of E
+  const int np = (cnt + 1) >> 1;
 #pragma unroll kDualUnroll
-  for (int j = 0; j < cnt; ++j) {
-    const float4 a = S[j].a;
-    const float4 b = S[j].b;
-    float d2, d, r, X, Y;
-    pair_terms<MODE, LOGB>(lx, ly, a, d2, d, r, X, Y);
-    if (HAS_Z && lz > b.z) continue;  // src/tpcf.f90:322
-    const bool up = d2 >= E;
-    near |= fabsf(d2 - E) <= gE;
-    // products folded into the sums: one FFMA per quantity and side
-    tot[QGT] = fmaf(r, X, tot[QGT]);
-    tot[QGX] = fmaf(r, Y, tot[QGX]);
-    tot[QW] += b.x;
-    tot[QDW] = fmaf(d, b.x, tot[QDW]);
-    if (MODE == 0 && HAS_M) tot[QK] += b.y;
-    if (HAS_Z) tot[QN] += 1.f;
-    if (up) {
-      hi[QGT] = fmaf(r, X, hi[QGT]);
-      hi[QGX] = fmaf(r, Y, hi[QGX]);
-      hi[QW] += b.x;
-      hi[QDW] = fmaf(d, b.x, hi[QDW]);
-      hi[QN] += 1.f;
-      if (MODE == 0 && HAS_M) hi[QK] += b.y;
+  for (int k = 0; k < np; ++k) {
+    const float4 xy = S[k].xy, pq = S[k].pq, wk = S[k].wk, zn = S[k].zn;
+    float2 d2, d, r, X, Y;
+    pair_terms2<MODE, LOGB>(L, xy, pq, hi2(zn), d2, d, r, X, Y);
+    const float2 dE = add2(d2, nE);
+    near |= fabsf(dE.x) <= gE;
+    near |= fabsf(dE.y) <= gE;
+    float2 mk = make_float2(d2.x >= E ? 1.f : 0.f, d2.y >= E ? 1.f : 0.f);
+    float2 w = lo2(wk), K = hi2(wk);
+    if (HAS_Z) {
+      const float2 zm = make_float2(lz <= zn.x ? 1.f : 0.f, lz <= zn.y ? 1.f : 0.f);
+      r = mul2(r, zm);
+      w = mul2(w, zm);
+      if (MODE == 0 && HAS_M) K = mul2(K, zm);
+      sn = add2(sn, zm);
+      mk = mul2(mk, zm);
     }
+    // products folded into the sums: one packed FFMA per quantity and side
+    sgt = fma2(r, X, sgt);
+    sgx = fma2(r, Y, sgx);
+    sw = add2(sw, w);
+    sdw = fma2(d, w, sdw);
+    if (MODE == 0 && HAS_M) sk = add2(sk, K);
+    const float2 rm = mul2(r, mk), wm = mul2(w, mk);
+    hgt = fma2(rm, X, hgt);
+    hgx = fma2(rm, Y, hgx);
+    hw = add2(hw, wm);
+    hdw = fma2(d, wm, hdw);
+    hn = add2(hn, mk);
+    if (MODE == 0 && HAS_M) hk = fma2(K, mk, hk);
   }
-  if (!HAS_Z) tot[QN] = (float)cnt;
   if (cls == 0) return;
   if (near) {
     // rare (a pair within a relative 4e-6 of the edge): this lane's register
     // sums are dropped and the sub-chunk is binned pair by pair, each pair by
     // the canonical rule
-    for (int j = 0; j < cnt; ++j) do_pair<MODE, HAS_M, HAS_Z, LOGB, NC, QA>(lx, ly, lz, S[j].a, S[j].b, hcol, C);
+    for (int j = 0; j < cnt; ++j) {
+      float4 a, b;
+      src_of(S, j, a, b);
+      do_pair<MODE, HAS_M, HAS_Z, LOGB, NC, QA>(lx, ly, lz, a, b, hcol, C);
+    }
+    return;
+  }
+  float tot[QA], hi[QA];
+  tot[QGT] = sum2(sgt); hi[QGT] = sum2(hgt);
+  tot[QGX] = sum2(sgx); hi[QGX] = sum2(hgx);
+  tot[QW] = sum2(sw);   hi[QW] = sum2(hw);
+  tot[QDW] = sum2(sdw); hi[QDW] = sum2(hdw);
+  tot[QN] = HAS_Z ? sum2(sn) : (float)cnt;
+  hi[QN] = sum2(hn);
+  if (MODE == 0 && HAS_M) { tot[QK] = sum2(sk); hi[QK] = sum2(hk); }
+  if (!HAS_Z && (cnt & 1)) {
+    // the null source that pads an odd count counts on the upper side when
+    // its (huge) distance reaches E; it adds zero to every other sum
+    const float dxn = kNullPos - lx, dyn = kNullPos - ly;
+    if (fmaf(dyn, dyn, dxn * dxn) >= E) hi[QN] -= 1.f;
+  }
+  if (cls == 1) {
+    hist_add<QA, NC>(hcol, blo, tot);
     return;
   }
   float lo[QA];
 #pragma unroll
   for (int q = 0; q < QA; ++q) lo[q] = tot[q] - hi[q];
-  if (cls == 1) {
-    hist_add<QA, NC>(hcol, blo, tot);
-    return;
-  }
   if (blo >= 0) hist_add<QA, NC>(hcol, blo, lo);
   if (blo + 1 < C.nb) hist_add<QA, NC>(hcol, blo + 1, hi);
 }
@@ -334,6 +392,10 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
       if (HAS_Z) lz = LD.z[gs + tid];
       if (P.lens_acc && T.lens_acc_off >= 0) lens_col = P.lens_acc + T.lens_acc_off + gs + tid;
     }
+    LensP LP;
+    LP.nlx = dup2(-lx);
+    LP.nly = dup2(-ly);
+    LP.ly = dup2(ly);
     fvw[tid] = vw;
     fw[tid] = w;
     const size_t lens_stride = (size_t)LD.n_valid;
@@ -391,15 +453,37 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
         const SrcRec* __restrict__ S = tiles + bb * kTile;
         const int nsub = (n + 31) >> 5;
         if (PATH == 0 && ok) {
-          // bounding box of each 32-source sub-chunk (one warp per sub-chunk)
+          // One warp per 32-source sub-chunk: its bounding box, and the
+          // rewrite of its records into SrcPair form (lanes 2k, 2k+1 trade
+          // halves with one shuffle round; each lane stores only the 32 bytes
+          // of its own record, so the rewrite in place needs no ordering
+          // between lanes).  Slots past the tile's end get the null source.
           for (int sc = warp; sc < nsub; sc += NW) {
             const int j = sc * 32 + lane;
+            float4 a = make_float4(kNullPos, kNullPos, 0.f, 0.f);
+            float4 b = make_float4(0.f, 0.f, __int_as_float(0x7fc00000), 0.f);
             float mnx = INFINITY, mny = INFINITY, mxx = -INFINITY, mxy = -INFINITY;
             if (j < n) {
-              const float4 a = S[j].a;
+              a = S[j].a;
+              b = S[j].b;
               mnx = mxx = a.x;
               mny = mxy = a.y;
             }
+            const bool odd = lane & 1;
+            // even lane keeps {x, y, p, q} of both, odd lane {w, K, z, ny}
+            const float r0 = __shfl_xor_sync(0xffffffffu, odd ? a.x : b.x, 1);
+            const float r1 = __shfl_xor_sync(0xffffffffu, odd ? a.y : b.y, 1);
+            const float r2 = __shfl_xor_sync(0xffffffffu, odd ? a.z : b.z, 1);
+            const float r3 = __shfl_xor_sync(0xffffffffu, odd ? a.w : a.y, 1);
+            float4* dst = reinterpret_cast<float4*>(tiles + bb * kTile + j);
+            if (!odd) {
+              dst[0] = make_float4(a.x, r0, a.y, r1);
+              dst[1] = make_float4(a.z, r2, a.w, r3);
+            } else {
+              dst[0] = make_float4(r0, b.x, r1, b.y);
+              dst[1] = make_float4(r2, b.z, -r3, -a.y);
+            }
+            fence_proxy_async_smem();  // before the bulk copy that later refills this buffer
 #pragma unroll
             for (int o = 16; o; o >>= 1) {
               mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
@@ -429,25 +513,26 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
               }
 #endif
               if (m == 0) continue;
-              const SrcRec* __restrict__ Sc = S + base;
+              const SrcPair* __restrict__ Sc = reinterpret_cast<const SrcPair*>(S + base);
               if (m == 1) {
-                chunk_single<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(Sc, cnt, lx, ly, lz, cls, blo, hcol);
+                chunk_single<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(Sc, cnt, LP, lz, cls, blo, hcol);
               } else if (m == 2) {
-                chunk_dual<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(Sc, cnt, lx, ly, lz, cls, blo, hcol, C);
+                chunk_dual<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(Sc, cnt, LP, lx, ly, lz, cls, blo, hcol, C);
               } else if (act) {
-                int j = 0;
-                for (; j + 4 <= cnt; j += 4) {
-                  float4 a[4], b[4];
-#pragma unroll
-                  for (int u = 0; u < 4; ++u) {
-                    a[u] = Sc[j + u].a;
-                    b[u] = Sc[j + u].b;
-                  }
-#pragma unroll
-                  for (int u = 0; u < 4; ++u)
-                    do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, a[u], b[u], hcol, C);
+                for (int k = 0; k < (cnt >> 1); ++k) {
+                  const SrcPair sp = Sc[k];
+                  do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(
+                      lx, ly, lz, make_float4(sp.xy.x, sp.xy.z, sp.pq.x, sp.pq.z),
+                      make_float4(sp.wk.x, sp.wk.z, sp.zn.x, 0.f), hcol, C);
+                  do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(
+                      lx, ly, lz, make_float4(sp.xy.y, sp.xy.w, sp.pq.y, sp.pq.w),
+                      make_float4(sp.wk.y, sp.wk.w, sp.zn.y, 0.f), hcol, C);
                 }
-                for (; j < cnt; ++j) do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, Sc[j].a, Sc[j].b, hcol, C);
+                if (cnt & 1) {
+                  float4 a, b;
+                  src_of(Sc, cnt - 1, a, b);
+                  do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, a, b, hcol, C);
+                }
               }
             }
           } else if (act) {

@@ -39,6 +39,19 @@ struct __align__(16) SrcRec {
   float4 b;
 };
 
+// Two consecutive sources (2k, 2k+1) of a 32-source sub-chunk in shared
+// memory with their fields interleaved, so that one 64-bit register pair holds
+// a field of both sources: the operand form of the sm_100 packed FP32
+// instructions (add/mul/fma .f32x2).  The planar pair kernel rewrites each
+// tile in place into this form (the same 64 bytes as the two SrcRec), after
+// the bulk copy.  p, q, w, K, z are a.z, a.w, b.x, b.y, b.z of SrcRec; ny = -y.
+struct __align__(16) SrcPair {
+  float4 xy;  // x0 x1 y0 y1
+  float4 pq;  // p0 p1 q0 q1
+  float4 wk;  // w0 w1 K0 K1
+  float4 zn;  // z0 z1 ny0 ny1
+};
+
 // A source on the sphere: the unit vector u of (lambda, phi) split into FP32
 // hi + lo parts (u = hi + lo to ~2^-48), so that u_B - u_A keeps full FP32
 // relative precision at small separations.  Shear: a = {hi, -e1*w},
