@@ -40,13 +40,18 @@ namespace tpcf {
 
 constexpr int kDualUnroll = TPCF_DUAL_UNROLL;      // source-loop unrolling of the one-edge path
 constexpr int kSingleUnroll = TPCF_SINGLE_UNROLL;  // and of the single-bin path
+// Blocks per SM that the pair kernel is compiled for: the shared-memory
+// occupancy of 128 threads at 20 bins (51 KB histogram + tiles).  Declaring it
+// gives the compiler a register budget (up to 170 per thread) that it spends
+// on overlapping the packed FP32 chains of the register paths.
+constexpr int kPairMinBlocks = 3;
 // Coordinate of the null source that pads an odd sub-chunk in SrcPair form:
 // its d2 (~2e36) stays finite in FP32 and its weight and values are zero.
 constexpr float kNullPos = 1.0e18f;
 
 // ------------------------------------------------------- shared-memory map --
 struct PairSmem {
-  size_t tiles, hist, bsum, e2s, fvw, fw, e2f, span0, span1, tpref, subbox, mbar, misc, total;
+  size_t tiles, hist, bsum, e2s, fvw, fw, e2f, span0, span1, tpref, subbox, subsum, mbar, misc, total;
 };
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // bt here is the number of histogram columns (threads x lenses per thread).
@@ -67,6 +72,7 @@ __host__ __device__ inline PairSmem pair_smem_layout(int nb, int qa, int bt) {
   s.tpref = o; o += (kMaxRows + 1) * sizeof(int);
   o = align_up(o, 16);
   s.subbox = o; o += (kTile / 32) * sizeof(float4);
+  s.subsum = o; o += (kTile / 32) * sizeof(float4);
   s.mbar = o;  o += 2 * sizeof(uint64_t);
   s.misc = o;  o += 16;
   s.total = align_up(o, 128);
@@ -140,16 +146,16 @@ __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const floa
 // pairs).  Shear: with P = dx^2 - dy^2, u = 2 dx dy and r = 1/d^2,
 // cos 2phi = P r, sin 2phi = u r (src/tpcf.f90:343-344), so the g_t, g_x
 // terms are r*X and r*Y with X = p P + q u, Y = q P - p u (p = -e1 w,
-// q = -e2 w).  Scalar-scalar: X = kE w, Y = kB w, r = 1.  Both signs of dy
-// come from adds (y - ly and ny + ly), so no operand needs a negation; every
-// term equals the scalar computation lx - x, ly - y, ... bit for bit.
+// q = -e2 w).  Scalar-scalar: X = kE w, Y = kB w, r = 1.  Each term equals
+// the scalar computation from dx = lx - x, dy = ly - y bit for bit (the
+// packed halves round like the scalar operations; x - lx = -(lx - x)).
 struct LensP {
-  float2 nlx, nly, ly;  // (-lx, -lx), (-ly, -ly), (ly, ly)
+  float2 nlx, nly;  // (-lx, -lx), (-ly, -ly)
 };
 
 template <int MODE, bool LOGB>
-__device__ __forceinline__ void pair_terms2(const LensP& L, const float4 xy, const float4 pq, const float2 ny,
-                                            float2& d2, float2& d, float2& r, float2& X, float2& Y) {
+__device__ __forceinline__ void pair_terms2(const LensP& L, const float4 xy, const float4 pq, float2& d2, float2& d,
+                                            float2& r, float2& X, float2& Y) {
   const float2 dxp = add2(lo2(xy), L.nlx);  // x - lx
   const float2 dyp = add2(hi2(xy), L.nly);  // y - ly
   const float2 dx2 = mul2(dxp, dxp);
@@ -163,13 +169,12 @@ __device__ __forceinline__ void pair_terms2(const LensP& L, const float4 xy, con
     r = make_float2(__frcp_rn(d2.x), __frcp_rn(d2.y));
   }
   if (MODE == 0) {
-    const float2 dym = add2(ny, L.ly);         // ly - y
-    const float2 P = fma2(dym, dyp, dx2);      // dx^2 - dy^2
-    const float2 dxx = add2(dxp, dxp);
-    const float2 u = mul2(dxx, dyp);           //  2 dx dy
-    const float2 un = mul2(dxx, dym);          // -2 dx dy
+    const float2 P = fma2(make_float2(-dyp.x, -dyp.y), dyp, dx2);  // dx^2 - dy^2
+    const float2 qq = mul2(dxp, dyp);
+    const float2 u = add2(qq, qq);                                 // 2 dx dy
     X = fma2(lo2(pq), P, mul2(hi2(pq), u));
-    Y = fma2(hi2(pq), P, mul2(lo2(pq), un));
+    const float2 pu = mul2(lo2(pq), u);
+    Y = fma2(hi2(pq), P, make_float2(-pu.x, -pu.y));
   } else {
     r = dup2(1.f);
     X = lo2(pq);
@@ -184,54 +189,66 @@ __device__ __forceinline__ void src_of(const SrcPair* __restrict__ S, int j, flo
   b = make_float4(f[8], f[10], f[12], 0.f);
 }
 
+// The register paths share the sub-chunk sums ss = {sum p, sum q, sum w,
+// sum K} over its sources: without a z cut, the w and K sums of every lens
+// are these (and, for scalar-scalar, so are the g_t and g_x sums, r = 1), so
+// they are not accumulated per pair.
+//
 // Class 1: every pair of the chunk is in bin `blo`.  With a z cut, a pair
 // with z_A > z_B (src/tpcf.f90:322) adds nothing.  An odd count is padded by
 // a null source (zero weight and values, far away, NaN z): it adds zero to
 // every sum, and the pair count is cnt (or the z-mask sum, which excludes it).
 template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int NC, int QA>
 __device__ __forceinline__ void chunk_single(const SrcPair* __restrict__ S, int cnt, const LensP& L, float lz,
-                                             int cls, int blo, float* __restrict__ hcol) {
+                                             int cls, int blo, float* __restrict__ hcol, const float4 ss) {
+  constexpr bool LI = !HAS_Z;  // lens-independent sums come from ss
   float2 sgt = dup2(0.f), sgx = dup2(0.f), sw = dup2(0.f), sdw = dup2(0.f), sk = dup2(0.f), sn = dup2(0.f);
   const int np = (cnt + 1) >> 1;
 #pragma unroll kSingleUnroll
   for (int k = 0; k < np; ++k) {
-    const float4 xy = S[k].xy, pq = S[k].pq, wk = S[k].wk, zn = S[k].zn;
+    const float4 xy = S[k].xy, pq = S[k].pq, wk = S[k].wk;
     float2 d2, d, r, X, Y;
-    pair_terms2<MODE, LOGB>(L, xy, pq, hi2(zn), d2, d, r, X, Y);
+    pair_terms2<MODE, LOGB>(L, xy, pq, d2, d, r, X, Y);
     float2 w = lo2(wk), K = hi2(wk);
     if (HAS_Z) {
+      const float4 zn = S[k].zn;
       const float2 zm = make_float2(lz <= zn.x ? 1.f : 0.f, lz <= zn.y ? 1.f : 0.f);
       r = mul2(r, zm);
       w = mul2(w, zm);
       if (MODE == 0 && HAS_M) K = mul2(K, zm);
       sn = add2(sn, zm);
     }
-    sgt = fma2(r, X, sgt);
-    sgx = fma2(r, Y, sgx);
-    sw = add2(sw, w);
+    if (!(LI && MODE == 1)) {
+      sgt = fma2(r, X, sgt);
+      sgx = fma2(r, Y, sgx);
+    }
+    if (!LI) sw = add2(sw, w);
     sdw = fma2(d, w, sdw);
-    if (MODE == 0 && HAS_M) sk = add2(sk, K);
+    if (MODE == 0 && HAS_M && !LI) sk = add2(sk, K);
   }
   if (cls != 1) return;
   float acc[QA];
-  acc[QGT] = sum2(sgt);
-  acc[QGX] = sum2(sgx);
-  acc[QW] = sum2(sw);
+  acc[QGT] = (LI && MODE == 1) ? ss.x : sum2(sgt);
+  acc[QGX] = (LI && MODE == 1) ? ss.y : sum2(sgx);
+  acc[QW] = LI ? ss.z : sum2(sw);
   acc[QDW] = sum2(sdw);
   acc[QN] = HAS_Z ? sum2(sn) : (float)cnt;
-  if (MODE == 0 && HAS_M) acc[QK] = sum2(sk);
+  if (MODE == 0 && HAS_M) acc[QK] = LI ? ss.w : sum2(sk);
   hist_add<QA, NC>(hcol, blo, acc);
 }
 
 // Class 2: pairs in bins blo and blo+1 (either may be out of range, then it is
 // dropped); the edge between them is e2f[blo+1].  Sums over all pairs (s*)
-// and over the upper side (h*, masked by d2 >= E as 1/0); the lower side is
-// their difference.
+// and over the upper side (h*: the pair's r, w, K selected by d2 >= E, the
+// count as an integer); the lower side is their difference.
 template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int NC, int QA>
 __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int cnt, const LensP& L, float lx, float ly,
-                                           float lz, int cls, int blo, float* __restrict__ hcol, const BinCtx& C) {
+                                           float lz, int cls, int blo, float* __restrict__ hcol, const BinCtx& C,
+                                           const float4 ss) {
+  constexpr bool LI = !HAS_Z;
   float2 sgt = dup2(0.f), sgx = dup2(0.f), sw = dup2(0.f), sdw = dup2(0.f), sk = dup2(0.f), sn = dup2(0.f);
-  float2 hgt = dup2(0.f), hgx = dup2(0.f), hw = dup2(0.f), hdw = dup2(0.f), hk = dup2(0.f), hn = dup2(0.f);
+  float2 hgt = dup2(0.f), hgx = dup2(0.f), hw = dup2(0.f), hdw = dup2(0.f), hk = dup2(0.f);
+  int hn = 0;
   // lanes of class 1 (or 0) keep an edge no pair reaches
   const float E = (cls == 2) ? C.e2f[blo + 1] : 3.0e38f;
   const float gE = (cls == 2) ? E * C.eps_rel : 0.f;
@@ -240,35 +257,41 @@ __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int cn
   const int np = (cnt + 1) >> 1;
 #pragma unroll kDualUnroll
   for (int k = 0; k < np; ++k) {
-    const float4 xy = S[k].xy, pq = S[k].pq, wk = S[k].wk, zn = S[k].zn;
+    const float4 xy = S[k].xy, pq = S[k].pq, wk = S[k].wk;
     float2 d2, d, r, X, Y;
-    pair_terms2<MODE, LOGB>(L, xy, pq, hi2(zn), d2, d, r, X, Y);
+    pair_terms2<MODE, LOGB>(L, xy, pq, d2, d, r, X, Y);
     const float2 dE = add2(d2, nE);
     near |= fabsf(dE.x) <= gE;
     near |= fabsf(dE.y) <= gE;
-    float2 mk = make_float2(d2.x >= E ? 1.f : 0.f, d2.y >= E ? 1.f : 0.f);
     float2 w = lo2(wk), K = hi2(wk);
+    bool u0 = d2.x >= E, u1 = d2.y >= E;
     if (HAS_Z) {
-      const float2 zm = make_float2(lz <= zn.x ? 1.f : 0.f, lz <= zn.y ? 1.f : 0.f);
+      const float4 zn = S[k].zn;
+      const bool z0 = lz <= zn.x, z1 = lz <= zn.y;
+      const float2 zm = make_float2(z0 ? 1.f : 0.f, z1 ? 1.f : 0.f);
       r = mul2(r, zm);
       w = mul2(w, zm);
       if (MODE == 0 && HAS_M) K = mul2(K, zm);
       sn = add2(sn, zm);
-      mk = mul2(mk, zm);
+      u0 = u0 && z0;
+      u1 = u1 && z1;
     }
     // products folded into the sums: one packed FFMA per quantity and side
-    sgt = fma2(r, X, sgt);
-    sgx = fma2(r, Y, sgx);
-    sw = add2(sw, w);
+    if (!(LI && MODE == 1)) {
+      sgt = fma2(r, X, sgt);
+      sgx = fma2(r, Y, sgx);
+    }
+    if (!LI) sw = add2(sw, w);
     sdw = fma2(d, w, sdw);
-    if (MODE == 0 && HAS_M) sk = add2(sk, K);
-    const float2 rm = mul2(r, mk), wm = mul2(w, mk);
+    if (MODE == 0 && HAS_M && !LI) sk = add2(sk, K);
+    const float2 rm = make_float2(u0 ? r.x : 0.f, u1 ? r.y : 0.f);
+    const float2 wm = make_float2(u0 ? w.x : 0.f, u1 ? w.y : 0.f);
     hgt = fma2(rm, X, hgt);
     hgx = fma2(rm, Y, hgx);
     hw = add2(hw, wm);
     hdw = fma2(d, wm, hdw);
-    hn = add2(hn, mk);
-    if (MODE == 0 && HAS_M) hk = fma2(K, mk, hk);
+    hn += (int)u0 + (int)u1;
+    if (MODE == 0 && HAS_M) hk = add2(hk, make_float2(u0 ? K.x : 0.f, u1 ? K.y : 0.f));
   }
   if (cls == 0) return;
   if (near) {
@@ -283,13 +306,20 @@ __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int cn
     return;
   }
   float tot[QA], hi[QA];
-  tot[QGT] = sum2(sgt); hi[QGT] = sum2(hgt);
-  tot[QGX] = sum2(sgx); hi[QGX] = sum2(hgx);
-  tot[QW] = sum2(sw);   hi[QW] = sum2(hw);
-  tot[QDW] = sum2(sdw); hi[QDW] = sum2(hdw);
+  tot[QGT] = (LI && MODE == 1) ? ss.x : sum2(sgt);
+  tot[QGX] = (LI && MODE == 1) ? ss.y : sum2(sgx);
+  tot[QW] = LI ? ss.z : sum2(sw);
+  tot[QDW] = sum2(sdw);
   tot[QN] = HAS_Z ? sum2(sn) : (float)cnt;
-  hi[QN] = sum2(hn);
-  if (MODE == 0 && HAS_M) { tot[QK] = sum2(sk); hi[QK] = sum2(hk); }
+  hi[QGT] = sum2(hgt);
+  hi[QGX] = sum2(hgx);
+  hi[QW] = sum2(hw);
+  hi[QDW] = sum2(hdw);
+  hi[QN] = (float)hn;
+  if (MODE == 0 && HAS_M) {
+    tot[QK] = LI ? ss.w : sum2(sk);
+    hi[QK] = sum2(hk);
+  }
   if (!HAS_Z && (cnt & 1)) {
     // the null source that pads an odd count counts on the upper side when
     // its (huge) distance reaches E; it adds zero to every other sum
@@ -318,7 +348,7 @@ extern "C" int tpcf_debug_mode_stats(unsigned long long* out) {
 // PATH 0: sub-chunk classification with the register paths (default);
 // PATH 1: per-pair binning for every pair (kept for A/B measurement).
 template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int PATH>
-__global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
+__global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P) {
   constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
   constexpr int NW = BT / 32;
   const int nb = P.nb;
@@ -337,6 +367,7 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
   int* span1 = reinterpret_cast<int*>(smem + L.span1);
   int* tpref = reinterpret_cast<int*>(smem + L.tpref);
   float4* subbox = reinterpret_cast<float4*>(smem + L.subbox);
+  float4* subsum = reinterpret_cast<float4*>(smem + L.subsum);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + L.mbar);
   int* sh_item = reinterpret_cast<int*>(smem + L.misc);
 
@@ -395,7 +426,6 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
     LensP LP;
     LP.nlx = dup2(-lx);
     LP.nly = dup2(-ly);
-    LP.ly = dup2(ly);
     fvw[tid] = vw;
     fw[tid] = w;
     const size_t lens_stride = (size_t)LD.n_valid;
@@ -453,7 +483,7 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
         const SrcRec* __restrict__ S = tiles + bb * kTile;
         const int nsub = (n + 31) >> 5;
         if (PATH == 0 && ok) {
-          // One warp per 32-source sub-chunk: its bounding box, and the
+          // One warp per 32-source sub-chunk: its bounding box and sums, and the
           // rewrite of its records into SrcPair form (lanes 2k, 2k+1 trade
           // halves with one shuffle round; each lane stores only the 32 bytes
           // of its own record, so the rewrite in place needs no ordering
@@ -470,18 +500,18 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
               mny = mxy = a.y;
             }
             const bool odd = lane & 1;
-            // even lane keeps {x, y, p, q} of both, odd lane {w, K, z, ny}
+            // even lane keeps {x, y, p, q} of both, odd lane {w, K, z}
             const float r0 = __shfl_xor_sync(0xffffffffu, odd ? a.x : b.x, 1);
             const float r1 = __shfl_xor_sync(0xffffffffu, odd ? a.y : b.y, 1);
             const float r2 = __shfl_xor_sync(0xffffffffu, odd ? a.z : b.z, 1);
-            const float r3 = __shfl_xor_sync(0xffffffffu, odd ? a.w : a.y, 1);
+            const float r3 = __shfl_xor_sync(0xffffffffu, a.w, 1);
             float4* dst = reinterpret_cast<float4*>(tiles + bb * kTile + j);
             if (!odd) {
               dst[0] = make_float4(a.x, r0, a.y, r1);
               dst[1] = make_float4(a.z, r2, a.w, r3);
             } else {
               dst[0] = make_float4(r0, b.x, r1, b.y);
-              dst[1] = make_float4(r2, b.z, -r3, -a.y);
+              dst[1] = make_float4(r2, b.z, 0.f, 0.f);
             }
             fence_proxy_async_smem();  // before the bulk copy that later refills this buffer
 #pragma unroll
@@ -491,7 +521,19 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
               mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
               mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
             }
-            if (lane == 0) subbox[sc] = make_float4(mnx, mny, mxx, mxy);
+            // sums of p, q, w, K over the sub-chunk (lens-independent)
+            float s0 = a.z, s1 = a.w, s2 = b.x, s3 = b.y;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+              s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+              s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+              s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+              s3 += __shfl_xor_sync(0xffffffffu, s3, o);
+            }
+            if (lane == 0) {
+              subbox[sc] = make_float4(mnx, mny, mxx, mxy);
+              subsum[sc] = make_float4(s0, s1, s2, s3);
+            }
           }
         }
         if (__syncthreads_or(!ok)) timed_out = true;
@@ -515,9 +557,9 @@ __global__ void __launch_bounds__(BT) k_pairs(const PairParams P) {
               if (m == 0) continue;
               const SrcPair* __restrict__ Sc = reinterpret_cast<const SrcPair*>(S + base);
               if (m == 1) {
-                chunk_single<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(Sc, cnt, LP, lz, cls, blo, hcol);
+                chunk_single<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(Sc, cnt, LP, lz, cls, blo, hcol, subsum[sc]);
               } else if (m == 2) {
-                chunk_dual<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(Sc, cnt, LP, lx, ly, lz, cls, blo, hcol, C);
+                chunk_dual<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(Sc, cnt, LP, lx, ly, lz, cls, blo, hcol, C, subsum[sc]);
               } else if (act) {
                 for (int k = 0; k < (cnt >> 1); ++k) {
                   const SrcPair sp = Sc[k];

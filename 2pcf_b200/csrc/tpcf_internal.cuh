@@ -44,12 +44,12 @@ struct __align__(16) SrcRec {
 // a field of both sources: the operand form of the sm_100 packed FP32
 // instructions (add/mul/fma .f32x2).  The planar pair kernel rewrites each
 // tile in place into this form (the same 64 bytes as the two SrcRec), after
-// the bulk copy.  p, q, w, K, z are a.z, a.w, b.x, b.y, b.z of SrcRec; ny = -y.
+// the bulk copy.  p, q, w, K, z are a.z, a.w, b.x, b.y, b.z of SrcRec.
 struct __align__(16) SrcPair {
   float4 xy;  // x0 x1 y0 y1
   float4 pq;  // p0 p1 q0 q1
   float4 wk;  // w0 w1 K0 K1
-  float4 zn;  // z0 z1 ny0 ny1
+  float4 zn;  // z0 z1 0 0
 };
 
 // A source on the sphere: the unit vector u of (lambda, phi) split into FP32
