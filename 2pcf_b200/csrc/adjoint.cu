@@ -40,6 +40,10 @@ namespace {
 using namespace tpcf;
 
 constexpr int BT = 128;
+// Blocks per SM the adjoint kernel is compiled for.  Declaring it gives the
+// compiler a register budget (up to 85 per thread) in place of a spilling
+// 56-register schedule; 6 blocks of 128 threads still fit every SM.
+constexpr int kAdjMinBlocks = 6;
 
 struct AdjParams {
   const SrcRec* lens;       // lens grid records: a = {x, y, val*w, w}, b = {z, 0, 0, 0}
@@ -65,7 +69,7 @@ struct AdjParams {
 };
 
 struct AdjSmem {
-  size_t tiles, e2s, e2f, coef, span0, span1, tpref, subbox, mbar, misc, total;
+  size_t tiles, e2s, e2f, coef, span0, span1, tpref, subbox, subw, mbar, misc, total;
 };
 __host__ __device__ inline size_t au(size_t v, size_t a) { return (v + a - 1) / a * a; }
 __host__ __device__ inline AdjSmem adj_smem(int nb) {
@@ -81,6 +85,8 @@ __host__ __device__ inline AdjSmem adj_smem(int nb) {
   s.tpref = o; o += (kMaxRows + 1) * sizeof(int);
   o = au(o, 16);
   s.subbox = o; o += (kTile / 32) * sizeof(float4);
+  s.subw = o; o += (kTile / 32) * sizeof(float);
+  o = au(o, 8);
   s.mbar = o; o += 2 * sizeof(uint64_t);
   s.misc = o; o += 16;
   s.total = au(o, 128);
@@ -91,31 +97,10 @@ struct Acc {
   float a1, a2, b1, b2, n;
 };
 
-// One pair (source j owns the thread, lens i from the tile) with coefficients k.
 // The bin-independent part of a pair's adjoint terms: with F = val_A w_A / d^2
-// (l.z = val_A w_A), S1 += F (dx^2 - dy^2), S2 += F dx dy, SN += w_A.  Within
+// (vw = val_A w_A), S1 += F (dx^2 - dy^2), S2 += F dx dy, SN += w_A.  Within
 // a run of pairs of one bin the bin's coefficients multiply these sums once:
 // a1 = k.x S1, a2 = 2 k.x S2, b1 = k.y S1, b2 = 2 k.y S2, n = k.z SN.
-template <bool LOGB>
-__device__ __forceinline__ void adj_factors(float sx, float sy, const float4 l, float& S1, float& S2, float& SN,
-                                            float& d2) {
-  const float dx = l.x - sx;  // lens minus source, as in the forward pass
-  const float dy = l.y - sy;
-  const float dx2 = dx * dx;
-  d2 = fmaf(dy, dy, dx2);
-  float r;
-  if (LOGB) {
-    const float rs = rsqrtf(d2);
-    r = rs * rs;
-  } else {
-    r = __frcp_rn(d2);
-  }
-  const float F = l.z * r;
-  S1 = fmaf(F, fmaf(-dy, dy, dx2), S1);
-  S2 = fmaf(F, dx * dy, S2);
-  SN += l.w;
-}
-
 template <bool WX>
 __device__ __forceinline__ void adj_apply(const float4 k, float S1, float S2, float SN, Acc& A) {
   A.a1 = fmaf(k.x, S1, A.a1);
@@ -127,6 +112,8 @@ __device__ __forceinline__ void adj_apply(const float4 k, float S1, float S2, fl
   A.n = fmaf(k.z, SN, A.n);
 }
 
+// One pair (the source owns the thread, the lens comes from the tile) with
+// its bin's coefficients k: the per-pair form, where bins vary pair to pair.
 template <bool LOGB, bool WX>
 __device__ __forceinline__ void adj_pair(float sx, float sy, const float4 l, const float4 k, Acc& A) {
   const float dx = l.x - sx;  // lens minus source, as in the forward pass
@@ -154,8 +141,62 @@ __device__ __forceinline__ void adj_pair(float sx, float sy, const float4 l, con
   A.n = fmaf(k.z, l.w, A.n);
 }
 
+// Two consecutive lenses (2k, 2k+1) of a 32-lens sub-chunk in shared memory
+// with their fields interleaved, so that a 64-bit register pair holds one
+// field of both (the operand form of the sm_100 packed FP32 instructions).
+// The kernel rewrites each lens tile in place into this form (the same 64
+// bytes as the two SrcRec).  vw = val_A w_A, w = w_A.
+struct __align__(16) LensPair {
+  float4 xy;  // x0 x1 y0 y1
+  float4 fw;  // vw0 vw1 w0 w1
+  float4 zz;  // z0 z1 0 0
+  float4 pad;
+};
+// Coordinate of the null lens that pads an odd sub-chunk: finite d^2, zero
+// weight and value, NaN z (never in front of a source).
+constexpr float kNullLens = 1.0e18f;
+
+// Lens j of a sub-chunk in LensPair form: {x, y, vw, w} and z.
+__device__ __forceinline__ float4 lens_of(const LensPair* __restrict__ S, int j, float& z) {
+  const float* f = reinterpret_cast<const float*>(S + (j >> 1)) + (j & 1);
+  z = f[8];
+  return make_float4(f[0], f[2], f[4], f[6]);
+}
+
+// The terms of the bin-independent sums (S1: F P, S2: F Q, SN: w) for the two
+// lenses of one LensPair (packed FP32): F = vw r (times the z mask),
+// P = dx^2 - dy^2, Q = dx dy, each half equal to the scalar computation.  w
+// gets the z mask too.
+template <bool HAS_Z, bool LOGB>
+__device__ __forceinline__ void adj_terms2(float2 nsx, float2 nsy, float sz, const LensPair& lp, float2& d2,
+                                           float2& F, float2& Pq, float2& Q, float2& w, bool& z0, bool& z1) {
+  const float2 dx = add2(lo2(lp.xy), nsx);  // lens minus source, as in the forward pass
+  const float2 dy = add2(hi2(lp.xy), nsy);
+  const float2 dx2 = mul2(dx, dx);
+  d2 = fma2(dy, dy, dx2);
+  float2 r;
+  if (LOGB) {
+    const float2 rs = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+    r = mul2(rs, rs);
+  } else {
+    r = make_float2(__frcp_rn(d2.x), __frcp_rn(d2.y));
+  }
+  F = mul2(lo2(lp.fw), r);
+  w = hi2(lp.fw);
+  z0 = z1 = true;
+  if (HAS_Z) {  // a lens behind the source adds nothing (src/tpcf.f90:322)
+    z0 = lp.zz.x <= sz;
+    z1 = lp.zz.y <= sz;
+    const float2 zm = make_float2(z0 ? 1.f : 0.f, z1 ? 1.f : 0.f);
+    F = mul2(F, zm);
+    w = mul2(w, zm);
+  }
+  Pq = fma2(make_float2(-dy.x, -dy.y), dy, dx2);
+  Q = mul2(dx, dy);
+}
+
 template <bool HAS_Z, bool LOGB, bool WX>
-__global__ void __launch_bounds__(BT) k_adj(const AdjParams P) {
+__global__ void __launch_bounds__(BT, kAdjMinBlocks) k_adj(const AdjParams P) {
   constexpr int NW = BT / 32;
   const int nb = P.nb;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -169,6 +210,7 @@ __global__ void __launch_bounds__(BT) k_adj(const AdjParams P) {
   int* span1 = reinterpret_cast<int*>(smem + L.span1);
   int* tpref = reinterpret_cast<int*>(smem + L.tpref);
   float4* subbox = reinterpret_cast<float4*>(smem + L.subbox);
+  float* subw = reinterpret_cast<float*>(smem + L.subw);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + L.mbar);
   int* sh_item = reinterpret_cast<int*>(smem + L.misc);
   if (tid == 0) {
@@ -206,6 +248,7 @@ __global__ void __launch_bounds__(BT) k_adj(const AdjParams P) {
       r1 = P.s1[si];
     }
     const float sx = r0.x, sy = r0.y, sz = r1.z;
+    const float2 nsx = dup2(-sx), nsy = dup2(-sy);
     double D1 = 0, D2 = 0, D3 = 0, D4 = 0, DN = 0;
     const float4 box = P.gbox[g];
     int cy0, cy1;
@@ -256,22 +299,50 @@ __global__ void __launch_bounds__(BT) k_adj(const AdjParams P) {
         const SrcRec* __restrict__ S = tiles + bb * kTile;
         const int nsub = (n + 31) >> 5;
         if (ok) {
+          // One warp per 32-lens sub-chunk: its bounding box and weight sum,
+          // and the rewrite of its records into LensPair form (lanes 2k, 2k+1
+          // trade halves with one shuffle round; each lane stores only the 32
+          // bytes of its own record).  Slots past the tile's end get the null
+          // lens.
           for (int sc = warp; sc < nsub; sc += NW) {
             const int j = sc * 32 + lane;
+            float4 a = make_float4(kNullLens, kNullLens, 0.f, 0.f);
+            float bz = __int_as_float(0x7fc00000);
             float mnx = INFINITY, mny = INFINITY, mxx = -INFINITY, mxy = -INFINITY;
             if (j < n) {
-              const float4 a = S[j].a;
+              a = S[j].a;
+              bz = S[j].b.x;
               mnx = mxx = a.x;
               mny = mxy = a.y;
             }
+            const bool odd = lane & 1;
+            // the even lane takes {x, y, vw, w} of its partner, the odd lane z
+            const float r0 = __shfl_xor_sync(0xffffffffu, odd ? a.x : bz, 1);
+            const float r1 = __shfl_xor_sync(0xffffffffu, a.y, 1);
+            const float r2 = __shfl_xor_sync(0xffffffffu, a.z, 1);
+            const float r3 = __shfl_xor_sync(0xffffffffu, a.w, 1);
+            float4* dst = reinterpret_cast<float4*>(tiles + bb * kTile + j);
+            if (!odd) {
+              dst[0] = make_float4(a.x, r0, a.y, r1);
+              dst[1] = make_float4(a.z, r2, a.w, r3);
+            } else {
+              dst[0] = make_float4(r0, bz, 0.f, 0.f);
+              dst[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            fence_proxy_async_smem();  // before the bulk copy that later refills this buffer
+            float sw = a.w;
 #pragma unroll
             for (int o = 16; o; o >>= 1) {
               mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
               mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
               mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
               mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+              sw += __shfl_xor_sync(0xffffffffu, sw, o);
             }
-            if (lane == 0) subbox[sc] = make_float4(mnx, mny, mxx, mxy);
+            if (lane == 0) {
+              subbox[sc] = make_float4(mnx, mny, mxx, mxy);
+              subw[sc] = sw;
+            }
           }
         }
         if (__syncthreads_or(!ok)) timed_out = true;
@@ -284,18 +355,26 @@ __global__ void __launch_bounds__(BT) k_adj(const AdjParams P) {
             const int cls = act ? classify<LOGB, HAS_Z, true>(sx, sy, subbox[sc], C, blo) : 0;
             const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)cls);
             if (m == 0) continue;
-            const SrcRec* __restrict__ Sc = S + base;
+            const LensPair* __restrict__ Sc = reinterpret_cast<const LensPair*>(S + base);
+            const int np = (cnt + 1) >> 1;
+            constexpr bool LI = !HAS_Z;  // the w sum of every source is the sub-chunk's
             // chunk-local sums: a lane with no pair in range discards its
             // (possibly non-finite) arithmetic instead of adding it to A
             Acc Ac{0.f, 0.f, 0.f, 0.f, 0.f};
             if (m == 1) {
               // every pair of this lane is in bin blo (or the lane has none)
               const float4 kc = cls == 1 ? coef[blo] : make_float4(0.f, 0.f, 0.f, 0.f);
-              float S1 = 0.f, S2 = 0.f, SN = 0.f, d2;
+              float2 S1 = dup2(0.f), S2 = dup2(0.f), SN = dup2(0.f);
 #pragma unroll 4
-              for (int j = 0; j < cnt; ++j)  // a lens behind the source adds nothing (src/tpcf.f90:322)
-                if (!HAS_Z || Sc[j].b.x <= sz) adj_factors<LOGB>(sx, sy, Sc[j].a, S1, S2, SN, d2);
-              adj_apply<WX>(kc, S1, S2, SN, Ac);
+              for (int q = 0; q < np; ++q) {
+                float2 d2, F, Pq, Q, w;
+                bool z0, z1;
+                adj_terms2<HAS_Z, LOGB>(nsx, nsy, sz, Sc[q], d2, F, Pq, Q, w, z0, z1);
+                S1 = fma2(F, Pq, S1);
+                S2 = fma2(F, Q, S2);
+                if (!LI) SN = add2(SN, w);
+              }
+              adj_apply<WX>(kc, sum2(S1), sum2(S2), LI ? subw[sc] : sum2(SN), Ac);
             } else if (m == 2) {
               const float4 kl = (cls >= 1 && blo >= 0) ? coef[blo] : make_float4(0.f, 0.f, 0.f, 0.f);
               // a side outside [x_min, x_max] contributes nothing
@@ -303,35 +382,36 @@ __global__ void __launch_bounds__(BT) k_adj(const AdjParams P) {
               const float4 kh = cls == 2 ? (blo + 1 < nb ? coef[blo + 1] : kz) : kl;
               const float E = cls == 2 ? e2f[blo + 1] : 3.0e38f;
               const float gE = cls == 2 ? E * C.eps_rel : 0.f;
+              const float2 nE = dup2(-E);
               bool near = false;  // some pair lies within the guard band of E
-              float T1 = 0.f, T2 = 0.f, TN = 0.f, H1 = 0.f, H2 = 0.f, HN = 0.f;
+              float2 T1 = dup2(0.f), T2 = dup2(0.f), TN = dup2(0.f), H1 = dup2(0.f), H2 = dup2(0.f), HN = dup2(0.f);
 #pragma unroll 2
-              for (int j = 0; j < cnt; ++j) {
-                if (HAS_Z && Sc[j].b.x > sz) continue;
-                const float4 l = Sc[j].a;
-                const float dx = l.x - sx, dy = l.y - sy;
-                const float dx2 = dx * dx;
-                const float d2 = fmaf(dy, dy, dx2);
-                near |= fabsf(d2 - E) <= gE;
-                float r;
-                if (LOGB) {
-                  const float rs = rsqrtf(d2);
-                  r = rs * rs;
-                } else {
-                  r = __frcp_rn(d2);
-                }
-                const float F = l.z * r;
-                const float p1 = F * fmaf(-dy, dy, dx2), p2 = F * (dx * dy);
-                T1 += p1; T2 += p2; TN += l.w;
-                if (d2 >= E) { H1 += p1; H2 += p2; HN += l.w; }
+              for (int q = 0; q < np; ++q) {
+                float2 d2, F, Pq, Q, w;
+                bool z0, z1;
+                adj_terms2<HAS_Z, LOGB>(nsx, nsy, sz, Sc[q], d2, F, Pq, Q, w, z0, z1);
+                const float2 dE = add2(d2, nE);
+                near |= fabsf(dE.x) <= gE;
+                near |= fabsf(dE.y) <= gE;
+                const bool u0 = z0 && d2.x >= E, u1 = z1 && d2.y >= E;
+                T1 = fma2(F, Pq, T1);
+                T2 = fma2(F, Q, T2);
+                if (!LI) TN = add2(TN, w);
+                const float2 Fm = make_float2(u0 ? F.x : 0.f, u1 ? F.y : 0.f);
+                H1 = fma2(Fm, Pq, H1);
+                H2 = fma2(Fm, Q, H2);
+                HN = add2(HN, make_float2(u0 ? w.x : 0.f, u1 ? w.y : 0.f));
               }
-              adj_apply<WX>(kl, T1 - H1, T2 - H2, TN - HN, Ac);
-              adj_apply<WX>(kh, H1, H2, HN, Ac);
+              const float h1 = sum2(H1), h2 = sum2(H2), hn = sum2(HN);
+              const float tn = LI ? subw[sc] : sum2(TN);
+              adj_apply<WX>(kl, sum2(T1) - h1, sum2(T2) - h2, tn - hn, Ac);
+              adj_apply<WX>(kh, h1, h2, hn, Ac);
               if (near) {  // rare: this lane's sub-chunk again, pair by pair, by the canonical rule
                 Ac = Acc{0.f, 0.f, 0.f, 0.f, 0.f};
                 for (int j = 0; j < cnt; ++j) {
-                  const float4 l = Sc[j].a;
-                  if (HAS_Z && Sc[j].b.x > sz) continue;
+                  float lz;
+                  const float4 l = lens_of(Sc, j, lz);
+                  if (HAS_Z && lz > sz) continue;
                   const float dx = l.x - sx, dy = l.y - sy;
                   const float d2 = fmaf(dy, dy, dx * dx);
                   const int b = pair_bin<LOGB>(d2, l.x, l.y, sx, sy, C);
@@ -341,8 +421,9 @@ __global__ void __launch_bounds__(BT) k_adj(const AdjParams P) {
               }
             } else if (act) {
               for (int j = 0; j < cnt; ++j) {
-                const float4 l = Sc[j].a;
-                if (HAS_Z && Sc[j].b.x > sz) continue;  // lens behind source (src/tpcf.f90:322)
+                float lz;
+                const float4 l = lens_of(Sc, j, lz);
+                if (HAS_Z && lz > sz) continue;  // lens behind source (src/tpcf.f90:322)
                 const float dx = l.x - sx, dy = l.y - sy;
                 const float d2 = fmaf(dy, dy, dx * dx);
                 const int b = pair_bin<LOGB>(d2, l.x, l.y, sx, sy, C);

@@ -357,7 +357,9 @@ __host__ __device__ inline SphSmem sph_smem_layout(int nb, int qa, int bt) {
 // streams the item's source runs through shared memory (bulk copies,
 // double-buffered, bounded waits), as the planar kernel does.
 template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT>
-__global__ void __launch_bounds__(BT) k_pairs_sph(const PairParams P) {
+// Compiled for 3 blocks per SM (the shared-memory occupancy at 20 bins),
+// which gives the compiler a register budget of up to 170 per thread.
+__global__ void __launch_bounds__(BT, 3) k_pairs_sph(const PairParams P) {
   constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
   constexpr int NW = BT / 32;
   constexpr bool SMALL = LOGB;  // log spacing on the sphere is only chosen with chord(x_max) <= 0.25
