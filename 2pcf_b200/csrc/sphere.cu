@@ -200,75 +200,221 @@ __device__ __forceinline__ void do_pair_s(const LensS& L, float lz, const SrcRec
   if (MODE == 0 && HAS_M) h[QK * NC] += s.c.y;
 }
 
-template <int MODE, bool HAS_M, bool HAS_Z, bool SMALL, int NC, int QA>
-__device__ __forceinline__ void chunk_single_s(const SrcRecS* __restrict__ S, int cnt, const LensS& L, float lz,
-                                               int cls, int blo, float* __restrict__ hcol) {
-  float acc[QA];
-#pragma unroll
-  for (int q = 0; q < QA; ++q) acc[q] = 0.f;
-#pragma unroll 2
-  for (int j = 0; j < cnt; ++j) {
-    const float4 a = S[j].a, b = S[j].b, cc = S[j].c;
-    float d2, th, r, X, Y;
-    sph_terms<MODE, SMALL>(L, a, b, d2, th, r, X, Y);
-    if (!HAS_Z || lz <= cc.z) {  // src/tpcf.f90:322
-      acc[QGT] = fmaf(r, X, acc[QGT]);
-      acc[QGX] = fmaf(r, Y, acc[QGX]);
-      acc[QW] += cc.x;
-      acc[QDW] = fmaf(th, cc.x, acc[QDW]);
-      if (MODE == 0 && HAS_M) acc[QK] += cc.y;
-      if (HAS_Z) acc[QN] += 1.f;
-    }
-  }
-  if (!HAS_Z) acc[QN] = (float)cnt;
-  if (cls == 1) hist_add<QA, NC>(hcol, blo, acc);
+// Two consecutive sources (2k, 2k+1) of a 32-source sub-chunk in shared
+// memory with their fields interleaved, so that a 64-bit register pair holds
+// one field of both (the operand form of the sm_100 packed FP32
+// instructions).  The kernel rewrites each tile in place into this form (the
+// same 96 bytes as the two SrcRecS).  p, q = a.w, b.w of SrcRecS; w, K, z =
+// c.x, c.y, c.z.
+struct __align__(16) SrcPairS {
+  float4 hxy;  // hi.x0 hi.x1 hi.y0 hi.y1
+  float4 hzp;  // hi.z0 hi.z1 p0 p1
+  float4 lxy;  // lo.x0 lo.x1 lo.y0 lo.y1
+  float4 lzq;  // lo.z0 lo.z1 q0 q1
+  float4 wk;   // w0 w1 K0 K1
+  float4 zz;   // z0 z1 0 0
+};
+
+// Source j of a sub-chunk in SrcPairS form, as a SrcRecS.
+__device__ __forceinline__ SrcRecS src_of_s(const SrcPairS* __restrict__ S, int j) {
+  const float* f = reinterpret_cast<const float*>(S + (j >> 1)) + (j & 1);
+  SrcRecS r;
+  r.a = make_float4(f[0], f[2], f[4], f[6]);
+  r.b = make_float4(f[8], f[10], f[12], f[14]);
+  r.c = make_float4(f[16], f[18], f[20], 0.f);
+  return r;
 }
 
+// One source in both halves of a SrcPairS (the odd last source of a sub-chunk;
+// the second half is masked out by the step that takes it).
+__device__ __forceinline__ SrcPairS dup_pair_s(const SrcRecS& r) {
+  SrcPairS p;
+  p.hxy = make_float4(r.a.x, r.a.x, r.a.y, r.a.y);
+  p.hzp = make_float4(r.a.z, r.a.z, r.a.w, r.a.w);
+  p.lxy = make_float4(r.b.x, r.b.x, r.b.y, r.b.y);
+  p.lzq = make_float4(r.b.z, r.b.z, r.b.w, r.b.w);
+  p.wk = make_float4(r.c.x, r.c.x, r.c.y, r.c.y);
+  p.zz = make_float4(r.c.z, r.c.z, 0.f, 0.f);
+  return p;
+}
+
+// A lens's constants in packed form: -hi, -lo and the east/north basis.
+struct LensS2 {
+  float2 nhx, nhy, nhz, nlx, nly, nlz, ex, ey, nx, ny, nz;
+};
+__device__ __forceinline__ LensS2 lens_pack(const LensS& L) {
+  LensS2 P;
+  P.nhx = dup2(-L.h.x); P.nhy = dup2(-L.h.y); P.nhz = dup2(-L.h.z);
+  P.nlx = dup2(-L.l.x); P.nly = dup2(-L.l.y); P.nlz = dup2(-L.l.z);
+  P.ex = dup2(L.ex); P.ey = dup2(L.ey);
+  P.nx = dup2(L.nx); P.ny = dup2(L.ny); P.nz = dup2(L.nz);
+  return P;
+}
+
+// sph_terms for the two sources of one SrcPairS (packed FP32; each half
+// equals the scalar computation: a.x - h.x = a.x + (-h.x)).
+template <int MODE, bool SMALL>
+__device__ __forceinline__ void sph_terms2(const LensS2& L, const SrcPairS& s, float2& d2, float2& th, float2& r,
+                                           float2& X, float2& Y) {
+  const float2 dx = add2(add2(lo2(s.hxy), L.nhx), add2(lo2(s.lxy), L.nlx));
+  const float2 dy = add2(add2(hi2(s.hxy), L.nhy), add2(hi2(s.lxy), L.nly));
+  const float2 dz = add2(add2(lo2(s.hzp), L.nhz), add2(lo2(s.lzq), L.nlz));
+  d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+  if (SMALL) {
+    const float2 c = mul2(d2, make_float2(rsqrtf(d2.x), rsqrtf(d2.y)));
+    th = mul2(c, fma2(d2, fma2(d2, fma2(d2, dup2(6.9754464e-4f), dup2(4.6875e-3f)), dup2(4.16666679e-2f)),
+                      dup2(1.f)));
+  } else {
+    th = make_float2(chord_theta<false>(d2.x, sqrtf(d2.x)), chord_theta<false>(d2.y, sqrtf(d2.y)));
+  }
+  if (MODE == 0) {
+    const float2 A = fma2(dy, L.ey, mul2(dx, L.ex));
+    const float2 B = fma2(dz, L.nz, fma2(dy, L.ny, mul2(dx, L.nx)));
+    const float2 A2 = mul2(A, A);
+    const float2 P = fma2(make_float2(-B.x, -B.y), B, A2);
+    const float2 sq = fma2(B, B, A2);
+    const float2 ab = mul2(A, B);
+    const float2 U = add2(ab, ab);
+    r = make_float2(__fdividef(1.f, sq.x), __fdividef(1.f, sq.y));
+    X = fma2(hi2(s.hzp), P, mul2(hi2(s.lzq), U));
+    const float2 pU = mul2(hi2(s.hzp), U);
+    Y = fma2(hi2(s.lzq), P, make_float2(-pU.x, -pU.y));
+  } else {
+    r = dup2(1.f);
+    X = hi2(s.hzp);
+    Y = hi2(s.lzq);
+  }
+}
+
+// Register sums of one lens over a sub-chunk: all pairs (s*) and, in the
+// one-edge path, the upper side (h*).
+struct SphAcc {
+  float2 sgt, sgx, sw, sdw, sk, sn, hgt, hgx, hw, hdw, hk;
+  int hn;
+};
+__device__ __forceinline__ void sph_acc_zero(SphAcc& A) {
+  A.sgt = A.sgx = A.sw = A.sdw = A.sk = A.sn = dup2(0.f);
+  A.hgt = A.hgx = A.hw = A.hdw = A.hk = dup2(0.f);
+  A.hn = 0;
+}
+
+// The two pairs of one SrcPairS against a lens (TAIL: only the first; the
+// second half is a copy, masked out).  With a z cut a pair with z_A > z_B
+// (src/tpcf.f90:322) adds nothing.  DUAL also forms the upper-side sums
+// (d2 >= E, selected) and the guard-band flag.  Without a z cut the w and K
+// sums of all pairs (and, scalar-scalar, the g sums) are the sub-chunk's
+// totals, so they are not accumulated here.
+template <int MODE, bool HAS_M, bool HAS_Z, bool SMALL, bool DUAL, bool TAIL>
+__device__ __forceinline__ void sph_step(const LensS2& L, float lz, const SrcPairS& s, float E, float2 nE, float gE,
+                                         SphAcc& A, bool& near) {
+  constexpr bool LI = !HAS_Z;
+  float2 d2, th, r, X, Y;
+  sph_terms2<MODE, SMALL>(L, s, d2, th, r, X, Y);
+  float2 w = lo2(s.wk), K = hi2(s.wk);
+  bool v0 = true, v1 = !TAIL;
+  if (HAS_Z) {
+    v0 = lz <= s.zz.x;
+    v1 = v1 && lz <= s.zz.y;
+  }
+  if (HAS_Z || TAIL) {
+    const float2 vm = make_float2(v0 ? 1.f : 0.f, v1 ? 1.f : 0.f);
+    r = mul2(r, vm);
+    w = mul2(w, vm);
+    if (MODE == 0 && HAS_M) K = mul2(K, vm);
+    if (HAS_Z) A.sn = add2(A.sn, vm);
+  }
+  if (!(LI && MODE == 1)) {
+    A.sgt = fma2(r, X, A.sgt);
+    A.sgx = fma2(r, Y, A.sgx);
+  }
+  if (!LI) A.sw = add2(A.sw, w);
+  A.sdw = fma2(th, w, A.sdw);
+  if (MODE == 0 && HAS_M && !LI) A.sk = add2(A.sk, K);
+  if (DUAL) {
+    const float2 dE = add2(d2, nE);
+    near |= fabsf(dE.x) <= gE;
+    near |= fabsf(dE.y) <= gE;
+    const bool u0 = v0 && d2.x >= E, u1 = v1 && d2.y >= E;
+    const float2 rm = make_float2(u0 ? r.x : 0.f, u1 ? r.y : 0.f);
+    const float2 wm = make_float2(u0 ? w.x : 0.f, u1 ? w.y : 0.f);
+    A.hgt = fma2(rm, X, A.hgt);
+    A.hgx = fma2(rm, Y, A.hgx);
+    A.hw = add2(A.hw, wm);
+    A.hdw = fma2(th, wm, A.hdw);
+    A.hn += (int)u0 + (int)u1;
+    if (MODE == 0 && HAS_M) A.hk = add2(A.hk, make_float2(u0 ? K.x : 0.f, u1 ? K.y : 0.f));
+  }
+}
+
+// Sums over all pairs of a sub-chunk; ss = {sum p, sum q, sum w, sum K}.
+template <int MODE, bool HAS_M, bool HAS_Z, int QA>
+__device__ __forceinline__ void sph_totals(const SphAcc& A, int cnt, const float4 ss, float* tot) {
+  constexpr bool LI = !HAS_Z;
+  tot[QGT] = (LI && MODE == 1) ? ss.x : sum2(A.sgt);
+  tot[QGX] = (LI && MODE == 1) ? ss.y : sum2(A.sgx);
+  tot[QW] = LI ? ss.z : sum2(A.sw);
+  tot[QDW] = sum2(A.sdw);
+  tot[QN] = HAS_Z ? sum2(A.sn) : (float)cnt;
+  if (MODE == 0 && HAS_M) tot[QK] = LI ? ss.w : sum2(A.sk);
+}
+
+// Class 1: every pair of the chunk is in bin `blo`.
 template <int MODE, bool HAS_M, bool HAS_Z, bool SMALL, int NC, int QA>
-__device__ __forceinline__ void chunk_dual_s(const SrcRecS* __restrict__ S, int cnt, const LensS& L, float lz,
-                                             int cls, int blo, float* __restrict__ hcol, const BinCtx& C) {
-  float tot[QA], hi[QA];
-#pragma unroll
-  for (int q = 0; q < QA; ++q) tot[q] = hi[q] = 0.f;
+__device__ __forceinline__ void chunk_single_s(const SrcPairS* __restrict__ S, int cnt, const LensS2& L, float lz,
+                                               int cls, int blo, float* __restrict__ hcol, const float4 ss) {
+  SphAcc A;
+  sph_acc_zero(A);
+  bool near = false;
+  const int np = cnt >> 1;
+#pragma unroll 2
+  for (int k = 0; k < np; ++k)
+    sph_step<MODE, HAS_M, HAS_Z, SMALL, false, false>(L, lz, S[k], 0.f, dup2(0.f), 0.f, A, near);
+  if (cnt & 1)
+    sph_step<MODE, HAS_M, HAS_Z, SMALL, false, true>(L, lz, dup_pair_s(src_of_s(S, cnt - 1)), 0.f, dup2(0.f), 0.f,
+                                                     A, near);
+  if (cls != 1) return;
+  float acc[QA];
+  sph_totals<MODE, HAS_M, HAS_Z, QA>(A, cnt, ss, acc);
+  hist_add<QA, NC>(hcol, blo, acc);
+}
+
+// Class 2: pairs in bins blo and blo+1 (either may be out of range, then it is
+// dropped); the edge between them is e2f[blo+1].
+template <int MODE, bool HAS_M, bool HAS_Z, bool SMALL, int NC, int QA>
+__device__ __forceinline__ void chunk_dual_s(const SrcPairS* __restrict__ S, int cnt, const LensS& Lf,
+                                             const LensS2& L, float lz, int cls, int blo, float* __restrict__ hcol,
+                                             const BinCtx& C, const float4 ss) {
   const float E = (cls == 2) ? C.e2f[blo + 1] : 3.0e38f;
   const float gE = (cls == 2) ? E * C.eps_rel : 0.f;
+  const float2 nE = dup2(-E);
+  SphAcc A;
+  sph_acc_zero(A);
   bool near = false;  // some pair lies within the guard band of E
+  const int np = cnt >> 1;
 #pragma unroll 2
-  for (int j = 0; j < cnt; ++j) {
-    const float4 a = S[j].a, b = S[j].b, cc = S[j].c;
-    float d2, th, r, X, Y;
-    sph_terms<MODE, SMALL>(L, a, b, d2, th, r, X, Y);
-    if (HAS_Z && lz > cc.z) continue;  // src/tpcf.f90:322
-    const bool up = d2 >= E;
-    near |= fabsf(d2 - E) <= gE;
-    tot[QGT] = fmaf(r, X, tot[QGT]);
-    tot[QGX] = fmaf(r, Y, tot[QGX]);
-    tot[QW] += cc.x;
-    tot[QDW] = fmaf(th, cc.x, tot[QDW]);
-    if (MODE == 0 && HAS_M) tot[QK] += cc.y;
-    if (HAS_Z) tot[QN] += 1.f;
-    if (up) {
-      hi[QGT] = fmaf(r, X, hi[QGT]);
-      hi[QGX] = fmaf(r, Y, hi[QGX]);
-      hi[QW] += cc.x;
-      hi[QDW] = fmaf(th, cc.x, hi[QDW]);
-      hi[QN] += 1.f;
-      if (MODE == 0 && HAS_M) hi[QK] += cc.y;
-    }
-  }
-  if (!HAS_Z) tot[QN] = (float)cnt;
+  for (int k = 0; k < np; ++k) sph_step<MODE, HAS_M, HAS_Z, SMALL, true, false>(L, lz, S[k], E, nE, gE, A, near);
+  if (cnt & 1)
+    sph_step<MODE, HAS_M, HAS_Z, SMALL, true, true>(L, lz, dup_pair_s(src_of_s(S, cnt - 1)), E, nE, gE, A, near);
   if (cls == 0) return;
   if (near) {  // rare: the sub-chunk is binned pair by pair by the canonical rule
-    for (int j = 0; j < cnt; ++j) do_pair_s<MODE, HAS_M, HAS_Z, SMALL, SMALL, NC, QA>(L, lz, S[j], hcol, C);
+    for (int j = 0; j < cnt; ++j) do_pair_s<MODE, HAS_M, HAS_Z, SMALL, SMALL, NC, QA>(Lf, lz, src_of_s(S, j), hcol, C);
+    return;
+  }
+  float tot[QA], hi[QA];
+  sph_totals<MODE, HAS_M, HAS_Z, QA>(A, cnt, ss, tot);
+  hi[QGT] = sum2(A.hgt);
+  hi[QGX] = sum2(A.hgx);
+  hi[QW] = sum2(A.hw);
+  hi[QDW] = sum2(A.hdw);
+  hi[QN] = (float)A.hn;
+  if (MODE == 0 && HAS_M) hi[QK] = sum2(A.hk);
+  if (cls == 1) {
+    hist_add<QA, NC>(hcol, blo, tot);
     return;
   }
   float lo[QA];
 #pragma unroll
   for (int q = 0; q < QA; ++q) lo[q] = tot[q] - hi[q];
-  if (cls == 1) {
-    hist_add<QA, NC>(hcol, blo, tot);
-    return;
-  }
   if (blo >= 0) hist_add<QA, NC>(hcol, blo, lo);
   if (blo + 1 < C.nb) hist_add<QA, NC>(hcol, blo + 1, hi);
 }
@@ -327,7 +473,7 @@ __device__ __forceinline__ int sph_row_spans(const GridDesc& G, float4 box, floa
 
 // ------------------------------------------------------------ the kernel ----
 struct SphSmem {
-  size_t tiles, hist, bsum, e2s, fvw, fw, e2f, span0, span1, tpref, subbox, mbar, misc, total;
+  size_t tiles, hist, bsum, e2s, fvw, fw, e2f, span0, span1, tpref, subbox, subsum, mbar, misc, total;
 };
 __host__ __device__ inline size_t align_up_s(size_t v, size_t a) { return (v + a - 1) / a * a; }
 __host__ __device__ inline SphSmem sph_smem_layout(int nb, int qa, int bt) {
@@ -347,6 +493,7 @@ __host__ __device__ inline SphSmem sph_smem_layout(int nb, int qa, int bt) {
   s.tpref = o; o += (kMaxRows + 1) * sizeof(int);
   o = align_up_s(o, 16);
   s.subbox = o; o += 2 * (kTileS / 32) * sizeof(float4);
+  s.subsum = o; o += (kTileS / 32) * sizeof(float4);
   s.mbar = o;  o += 2 * sizeof(uint64_t);
   s.misc = o;  o += 16;
   s.total = align_up_s(o, 128);
@@ -379,6 +526,7 @@ __global__ void __launch_bounds__(BT, 3) k_pairs_sph(const PairParams P) {
   int* span1 = reinterpret_cast<int*>(smem + Ls.span1);
   int* tpref = reinterpret_cast<int*>(smem + Ls.tpref);
   float4* subbox = reinterpret_cast<float4*>(smem + Ls.subbox);
+  float4* subsum = reinterpret_cast<float4*>(smem + Ls.subsum);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + Ls.mbar);
   int* sh_item = reinterpret_cast<int*>(smem + Ls.misc);
 
@@ -432,6 +580,7 @@ __global__ void __launch_bounds__(BT, 3) k_pairs_sph(const PairParams P) {
     } else {
       Lf = lens_frame(make_float4(1.f, 0.f, 0.f, 0.f), make_float4(0.f, 0.f, 0.f, 0.f));
     }
+    const LensS2 LP = lens_pack(Lf);
     fvw[tid] = vw;
     fw[tid] = w;
     const size_t lens_stride = (size_t)LD.n_valid;
@@ -497,18 +646,53 @@ __global__ void __launch_bounds__(BT, 3) k_pairs_sph(const PairParams P) {
         const SrcRecS* __restrict__ S = tiles + bb * kTileS;
         const int nsub = (n + 31) >> 5;
         if (ok) {
-          // 3-D box of each 32-source sub-chunk, widened by 2^-23 per side:
-          // the hi/lo split of both ends moves u_B - u_A by at most 2^-24.
+          // One warp per 32-source sub-chunk: its 3-D box, widened by 2^-23
+          // per side (the hi/lo split of both ends moves u_B - u_A by at most
+          // 2^-24), its sums of p, q, w, K, and the rewrite of its records
+          // into SrcPairS form (lanes 2k, 2k+1 trade halves with one shuffle
+          // round; each lane stores only the 48 bytes of its own record).
           for (int sc = warp; sc < nsub; sc += NW) {
             const int j = sc * 32 + lane;
             float mnx = INFINITY, mny = INFINITY, mnz = INFINITY, mxx = -INFINITY, mxy = -INFINITY,
                   mxz = -INFINITY;
+            const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+            float4 a = z4, b = z4, c = z4;
             if (j < n) {
-              const float4 a = S[j].a;
+              a = S[j].a;
+              b = S[j].b;
+              c = S[j].c;
               mnx = mxx = a.x;
               mny = mxy = a.y;
               mnz = mxz = a.z;
             }
+            const bool odd = lane & 1;
+            // even lane keeps {hi.x, hi.y, hi.z, p, lo.x, lo.y} of both, odd lane {lo.z, q, w, K, z}
+            const float r0 = __shfl_xor_sync(0xffffffffu, odd ? a.x : b.z, 1);
+            const float r1 = __shfl_xor_sync(0xffffffffu, odd ? a.y : b.w, 1);
+            const float r2 = __shfl_xor_sync(0xffffffffu, odd ? a.z : c.x, 1);
+            const float r3 = __shfl_xor_sync(0xffffffffu, odd ? a.w : c.y, 1);
+            const float r4 = __shfl_xor_sync(0xffffffffu, odd ? b.x : c.z, 1);
+            const float r5 = __shfl_xor_sync(0xffffffffu, b.y, 1);
+            float4* dst = reinterpret_cast<float4*>(tiles + bb * kTileS + j);
+            if (!odd) {
+              dst[0] = make_float4(a.x, r0, a.y, r1);
+              dst[1] = make_float4(a.z, r2, a.w, r3);
+              dst[2] = make_float4(b.x, r4, b.y, r5);
+            } else {
+              dst[0] = make_float4(r0, b.z, r1, b.w);
+              dst[1] = make_float4(r2, c.x, r3, c.y);
+              dst[2] = make_float4(r4, c.z, 0.f, 0.f);
+            }
+            fence_proxy_async_smem();  // before the bulk copy that later refills this buffer
+            float s0 = a.w, s1 = b.w, s2 = c.x, s3 = c.y;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+              s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+              s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+              s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+              s3 += __shfl_xor_sync(0xffffffffu, s3, o);
+            }
+            if (lane == 0) subsum[sc] = make_float4(s0, s1, s2, s3);
 #pragma unroll
             for (int o = 16; o; o >>= 1) {
               mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
@@ -534,13 +718,14 @@ __global__ void __launch_bounds__(BT, 3) k_pairs_sph(const PairParams P) {
             const int cls = act ? classify_s<LOGB, HAS_Z>(Lf, subbox[2 * sc], subbox[2 * sc + 1], C, blo) : 0;
             const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)cls);
             if (m == 0) continue;
-            const SrcRecS* __restrict__ Sc = S + base;
+            const SrcPairS* __restrict__ Sc = reinterpret_cast<const SrcPairS*>(S + base);
             if (m == 1) {
-              chunk_single_s<MODE, HAS_M, HAS_Z, SMALL, BT, QA>(Sc, cnt, Lf, lz, cls, blo, hcol);
+              chunk_single_s<MODE, HAS_M, HAS_Z, SMALL, BT, QA>(Sc, cnt, LP, lz, cls, blo, hcol, subsum[sc]);
             } else if (m == 2) {
-              chunk_dual_s<MODE, HAS_M, HAS_Z, SMALL, BT, QA>(Sc, cnt, Lf, lz, cls, blo, hcol, C);
+              chunk_dual_s<MODE, HAS_M, HAS_Z, SMALL, BT, QA>(Sc, cnt, Lf, LP, lz, cls, blo, hcol, C, subsum[sc]);
             } else if (act) {
-              for (int j = 0; j < cnt; ++j) do_pair_s<MODE, HAS_M, HAS_Z, LOGB, SMALL, BT, QA>(Lf, lz, Sc[j], hcol, C);
+              for (int j = 0; j < cnt; ++j)
+                do_pair_s<MODE, HAS_M, HAS_Z, LOGB, SMALL, BT, QA>(Lf, lz, src_of_s(Sc, j), hcol, C);
             }
           }
         }
