@@ -30,7 +30,7 @@
 #include "tpcf_kernels.h"
 
 #ifndef TPCF_DUAL_UNROLL
-#define TPCF_DUAL_UNROLL 2
+#define TPCF_DUAL_UNROLL 4
 #endif
 #ifndef TPCF_SINGLE_UNROLL
 #define TPCF_SINGLE_UNROLL 4

@@ -38,7 +38,7 @@ sys.path.insert(0, ROOT)
 METRIC = "Gpairs/s for xi_t at 10M objects, plain vs batched+adjoint form at 1e-6 rel. error"
 UNIT = "Gpairs/s"
 FLOP_PER_PAIR = 26  # shear-scalar, FMA = 2, MUFU = 1 (per binned pair)
-K_PAIRS_DRAM_BYTES = 64.49e9 + 197.6e6  # read + written by one launch of the default workload
+K_PAIRS_DRAM_BYTES = 63.414e9 + 135.05e6  # read + written by one launch of the default workload (ncu, one pass)
 SPH_FLOP_PER_PAIR = 52  # spherical shear-scalar: hi/lo unit-vector differences, east/north projection, angle series
 WORKLOAD_DESC = ("tomography: 5 shear bins (0.2,0.5,1.0,1.9,4.0 M) x 5 scalar bins "
                  "(0.1,0.2,0.4,0.7,1.0 M) = 10.0 M objects, 25 cross-pairs in one launch, "
