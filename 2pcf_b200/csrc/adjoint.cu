@@ -19,7 +19,9 @@
 // the binned estimator.  The pass mirrors k_pairs with the roles swapped:
 // lenses are sorted into the cell grid and streamed through shared memory,
 // each thread owns one source and accumulates five sums in registers (FP32
-// per tile, FP64 across tiles); there is no histogram.
+// per tile, FP64 across tiles); there is no histogram.  As in k_pairs, the
+// one-bin and one-edge sub-chunk paths run on packed FP32 instructions over
+// lens tiles rewritten in place into pair-interleaved LensPair blocks.
 
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>

@@ -14,6 +14,12 @@
 // FP64: per block (times the lens factors val*w or w) and, when per-lens output
 // is requested, per lens.
 //
+// Most pairs never touch the histogram: per 32-source sub-chunk a lens whose
+// bin range (from the sub-chunk's box) is one bin or two adjacent bins sums in
+// registers and adds once per sub-chunk.  Those register paths run on sm_100's
+// packed FP32 instructions (two pairs per instruction), for which each copied
+// tile is rewritten in place into pair-interleaved SrcPair blocks.
+//
 // Binning.  The pair arithmetic is FP32.  For log spacing the bin comes from
 // t = log2(d2)*A + B (one MUFU.LG2 and one FFMA): bin = floor(t).  When t is
 // within `eps` of an integer the pair is re-binned in FP64 by the canonical

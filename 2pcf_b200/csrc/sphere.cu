@@ -15,6 +15,8 @@
 // The pair arithmetic is FP32 on hi + lo differences (relative error ~1e-7
 // at any separation).  The FP64 guard band re-bins a pair by the canonical
 // rule: u = hi + lo in FP64, c^2 = (dx^2 + dy^2) + dz^2 rounded as written.
+// The one-bin and one-edge sub-chunk paths run on packed FP32 instructions
+// (two pairs per instruction) over tiles rewritten in place into SrcPairS.
 //
 // Pruning: a cell grid over (lambda reduced to [0, 2 pi), phi).  The rows of a
 // work item are the phi rows within R of the lens box (angular distance
