@@ -145,9 +145,10 @@ def cpu_baseline(w, seconds, nthreads, steps=1, warmup=0):
             loop += O.last_timing()[1]
         return pairs, loop, len(Ls["x"])
 
-    p0, t0, _ = run(20000)                       # calibration (~120 lenses)
+    cal = 20000 if nthreads >= 4 else 200000     # calibration (~120 / ~12 lenses)
+    p0, t0, _ = run(cal)
     rate = p0 / max(t0, 1e-6)
-    pairs_per_lens = p0 / len(sample(20000)["x"])
+    pairs_per_lens = p0 / len(sample(cal)["x"])
     n_tot = sum(len(L["x"]) for L in lenses)
     want = max(1.0, seconds * rate / pairs_per_lens)
     stride = max(1, int(n_tot / want))
@@ -597,6 +598,9 @@ def main():
     if world == 1 and rank == 0 and not args.no_cpu_baseline and not sphere:
         cb = cpu_baseline(w, args.cpu_seconds, host_threads())
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        # the same restatement on one host thread (a shorter bounded sample)
+        c1 = cpu_baseline(w, min(args.cpu_seconds, 5.0), 1)
+        line["cpu_baseline"]["single_thread"] = {k: c1[k] for k in ("value", "unit", "cores", "sample")}
     if world == 1 and not args.no_widened and args.region <= 0 and args.task < 0 and not sphere:
         line["widened"] = widened_timing(tpcf, w, peak, stream, host_threads(), with_cpu=not args.no_cpu_baseline)
     if rank == 0:
