@@ -154,6 +154,7 @@ struct __align__(16) LensPair {
   float4 zz;  // z0 z1 0 0
   float4 pad;
 };
+static_assert(sizeof(LensPair) == 2 * sizeof(SrcRec), "a LensPair rewrites two SrcRec in place");
 // Coordinate of the null lens that pads an odd sub-chunk: finite d^2, zero
 // weight and value, NaN z (never in front of a source).
 constexpr float kNullLens = 1.0e18f;

@@ -216,6 +216,7 @@ struct __align__(16) SrcPairS {
   float4 wk;   // w0 w1 K0 K1
   float4 zz;   // z0 z1 0 0
 };
+static_assert(sizeof(SrcPairS) == 2 * sizeof(SrcRecS), "a SrcPairS rewrites two SrcRecS in place");
 
 // Source j of a sub-chunk in SrcPairS form, as a SrcRecS.
 __device__ __forceinline__ SrcRecS src_of_s(const SrcPairS* __restrict__ S, int j) {
@@ -430,6 +431,7 @@ constexpr int kRowsS = kMaxRows / 4;        // rows per chunk: 3 runs each fit k
 // Sources per shared-memory tile (48-byte records): the tile size sets how
 // many blocks share an SM next to the FP32 histogram.
 constexpr int kTileS = TPCF_SPH_TILE;
+static_assert(kTileS % 32 == 0, "tiles hold whole 32-source sub-chunks");
 constexpr int kFlushSrcS = 4096;  // FP32 histogram -> FP64 after about this many sources
 
 // Lambda reach of a work item: full = every cell of a row, else the interval

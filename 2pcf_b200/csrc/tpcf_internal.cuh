@@ -51,6 +51,8 @@ struct __align__(16) SrcPair {
   float4 wk;  // w0 w1 K0 K1
   float4 zn;  // z0 z1 0 0
 };
+static_assert(sizeof(SrcPair) == 2 * sizeof(SrcRec), "a SrcPair rewrites two SrcRec in place");
+static_assert(kTile % 32 == 0, "tiles hold whole 32-source sub-chunks");
 
 // A source on the sphere: the unit vector u of (lambda, phi) split into FP32
 // hi + lo parts (u = hi + lo to ~2^-48), so that u_B - u_A keeps full FP32
