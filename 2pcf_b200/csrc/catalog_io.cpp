@@ -1,8 +1,9 @@
 // catalog_io.cpp -- host file I/O of the driver around the pair sums:
 //   * text catalogues (load_standard_shape_catalog, load_standard_kappa_map,
-//     load_standard_lens_catalog, src/input_formats.f90:227-333), parsed by
-//     all host threads with std::from_chars (correctly rounded to FP32, as a
-//     list-directed read into `real` is);
+//     load_standard_lens_catalog, src/input_formats.f90:227-333), memory-
+//     mapped and parsed by all host threads with std::from_chars (correctly
+//     rounded to FP32, as a list-directed read into `real` is), the masks
+//     applied while parsing and the rows scattered into columns in parallel;
 //   * the per-bin result table the driver writes (src/main.f90:699-702);
 //   * the binary marks stream (save_marks / load_survey_marks,
 //     src/input_formats.f90:528-603).
@@ -17,7 +18,13 @@
 #include <cstring>
 #include <string>
 #include <thread>
+#include <utility>
 #include <vector>
+
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include "tpcf_b200.h"
 
@@ -36,6 +43,67 @@ bool read_file(const char* path, std::string& buf) {
   return got == (size_t)sz;
 }
 
+// A read-only view of a whole file: memory-mapped (no copy; the parser
+// threads fault the pages in in parallel), or read into a buffer where
+// mapping is not possible.
+struct FileView {
+  const char* b = "";
+  size_t n = 0;
+  void* map = nullptr;
+  std::string buf;
+  bool open(const char* path) {
+    const int fd = ::open(path, O_RDONLY);
+    if (fd < 0) return false;
+    struct stat st;
+    if (::fstat(fd, &st) == 0 && S_ISREG(st.st_mode) && st.st_size > 0) {
+      void* p = ::mmap(nullptr, (size_t)st.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
+      if (p != MAP_FAILED) {
+        ::close(fd);
+        map = p;
+        n = (size_t)st.st_size;
+        b = static_cast<const char*>(p);
+        ::madvise(p, n, MADV_WILLNEED);
+        return true;
+      }
+    }
+    ::close(fd);
+    if (!read_file(path, buf)) return false;
+    b = buf.data();
+    n = buf.size();
+    return true;
+  }
+  ~FileView() {
+    if (map) ::munmap(map, n);
+  }
+};
+
+// [b, e) cut into nt pieces at line boundaries.
+std::vector<std::pair<const char*, const char*>> split_lines(const char* b, const char* e, int nt) {
+  std::vector<std::pair<const char*, const char*>> out(nt);
+  const size_t n = (size_t)(e - b);
+  const char* s = b;
+  for (int t = 0; t < nt; ++t) {
+    const char* cut = (t == nt - 1) ? e : b + (size_t)((double)n * (t + 1) / nt);
+    if (cut < s) cut = s;
+    if (cut < e && cut > b && cut[-1] != '\n') {
+      const char* nl = static_cast<const char*>(std::memchr(cut, '\n', (size_t)(e - cut)));
+      cut = nl ? nl + 1 : e;
+    }
+    out[t] = {s, cut};
+    s = cut;
+  }
+  return out;
+}
+
+// Runs fn(t) on nt threads (the caller's thread takes t = 0).
+template <class F>
+void run_threads(int nt, F fn) {
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; ++t) th.emplace_back(fn, t);
+  fn(0);
+  for (auto& x : th) x.join();
+}
+
 inline bool is_sep(char c) { return c == ' ' || c == '\t' || c == ',' || c == '\r' || c == '\f' || c == '\v'; }
 
 // A line holds data when its first non-blank character exists and is not '#'.
@@ -44,19 +112,34 @@ inline bool data_line(const char* p, const char* e) {
   return p < e && *p != '#';
 }
 
+int64_t count_data_lines(const char* p, const char* e) {
+  int64_t n = 0;
+  while (p < e) {
+    const char* le = static_cast<const char*>(std::memchr(p, '\n', (size_t)(e - p)));
+    if (!le) le = e;
+    if (data_line(p, le)) ++n;
+    p = le + 1;
+  }
+  return n;
+}
+
 struct Chunk {
   const char* b;
   const char* e;
-  std::vector<float> vals;  // row-major values of this chunk
-  int64_t rows = 0;
+  std::vector<float> vals;  // row-major values of the kept rows of this chunk
+  int64_t rows = 0;         // kept rows
   bool bad = false;
   int64_t bad_line = 0;     // 1-based line within the chunk
 };
 
-// Parses the data lines of [b, e) into row-major floats, ncols per line.
-void parse_chunk(Chunk& c, int ncols) {
+// Parses the data lines of [b, e), ncols values per line, and keeps the rows
+// that pass the masks (keep_pos: value > 0, keep_nonneg: value >= 0; -1 = no
+// mask) as row-major floats.
+void parse_chunk(Chunk& c, int ncols, int keep_pos, int keep_nonneg) {
   const char* p = c.b;
   int64_t line = 0;
+  float row[64];
+  c.vals.reserve((size_t)(c.e - c.b) / 8);
   while (p < c.e) {
     const char* le = static_cast<const char*>(std::memchr(p, '\n', (size_t)(c.e - p)));
     if (!le) le = c.e;
@@ -82,8 +165,7 @@ void parse_chunk(Chunk& c, int ncols) {
         }
         // Fortran exponent letters d/D are not accepted by from_chars
         if (q < le && !is_sep(*q)) break;
-        c.vals.push_back(v);
-        ++got;
+        row[got++] = v;
       }
       while (q < le && is_sep(*q)) ++q;
       if (got != ncols || q < le) {
@@ -91,7 +173,12 @@ void parse_chunk(Chunk& c, int ncols) {
         c.bad_line = line;
         return;
       }
-      ++c.rows;
+      const bool keep = (keep_pos < 0 || row[keep_pos] > 0.0f) &&        // w > 0 (input_formats.f90:250)
+                        (keep_nonneg < 0 || row[keep_nonneg] >= 0.0f);  // z >= 0 (input_formats.f90:320)
+      if (keep) {
+        c.vals.insert(c.vals.end(), row, row + ncols);
+        ++c.rows;
+      }
     }
     p = le + 1;
   }
@@ -104,55 +191,43 @@ extern "C" tpcf_status tpcf_read_table(const char* path, int32_t ncols, int32_t 
                                        int64_t* n_rows) {
   if (!path || ncols < 1 || ncols > 64 || !n_rows || keep_pos_col >= ncols || keep_nonneg_col >= ncols)
     return TPCF_ERR_INVALID_ARG;
-  std::string buf;
-  if (!read_file(path, buf)) return TPCF_ERR_INVALID_ARG;
-  const char* b = buf.data();
-  const char* e = b + buf.size();
+  FileView f;
+  if (!f.open(path)) return TPCF_ERR_INVALID_ARG;
+  const char* b = f.b;
+  const char* e = b + f.n;
+  int nt = n_threads > 0 ? n_threads : (int)std::max(1u, std::thread::hardware_concurrency());
+  nt = (int)std::min<int64_t>(nt, std::max<int64_t>(1, (int64_t)f.n / (1 << 16)));
+  const auto parts = split_lines(b, e, nt);
   if (!cols) {  // upper bound: data lines
+    std::vector<int64_t> cnt(nt, 0);
+    run_threads(nt, [&](int t) { cnt[t] = count_data_lines(parts[t].first, parts[t].second); });
     int64_t n = 0;
-    const char* p = b;
-    while (p < e) {
-      const char* le = static_cast<const char*>(std::memchr(p, '\n', (size_t)(e - p)));
-      if (!le) le = e;
-      if (data_line(p, le)) ++n;
-      p = le + 1;
-    }
+    for (int64_t v : cnt) n += v;
     *n_rows = n;
     return TPCF_OK;
   }
-  int nt = n_threads > 0 ? n_threads : (int)std::max(1u, std::thread::hardware_concurrency());
-  nt = (int)std::min<int64_t>(nt, std::max<int64_t>(1, (int64_t)buf.size() / (1 << 16)));
-  // split at line boundaries
   std::vector<Chunk> ch(nt);
-  const char* s = b;
   for (int t = 0; t < nt; ++t) {
-    const char* cut = (t == nt - 1) ? e : b + (size_t)((double)buf.size() * (t + 1) / nt);
-    if (cut < s) cut = s;
-    if (cut < e) {
-      const char* nl = static_cast<const char*>(std::memchr(cut, '\n', (size_t)(e - cut)));
-      cut = nl ? nl + 1 : e;
-    }
-    ch[t].b = s;
-    ch[t].e = cut;
-    s = cut;
+    ch[t].b = parts[t].first;
+    ch[t].e = parts[t].second;
   }
-  std::vector<std::thread> th;
-  for (int t = 1; t < nt; ++t) th.emplace_back(parse_chunk, std::ref(ch[t]), ncols);
-  parse_chunk(ch[0], ncols);
-  for (auto& x : th) x.join();
-  int64_t out = 0;
-  for (auto& c : ch) {
-    if (c.bad) return TPCF_ERR_INVALID_ARG;
-    for (int64_t r = 0; r < c.rows; ++r) {
-      const float* row = c.vals.data() + r * ncols;
-      if (keep_pos_col >= 0 && !(row[keep_pos_col] > 0.0f)) continue;       // w > 0 (input_formats.f90:250)
-      if (keep_nonneg_col >= 0 && !(row[keep_nonneg_col] >= 0.0f)) continue; // z >= 0 (input_formats.f90:320)
-      if (out >= capacity) return TPCF_ERR_OVERFLOW;
-      for (int k = 0; k < ncols; ++k) cols[(size_t)k * (size_t)capacity + (size_t)out] = row[k];
-      ++out;
-    }
+  run_threads(nt, [&](int t) { parse_chunk(ch[t], ncols, keep_pos_col, keep_nonneg_col); });
+  std::vector<int64_t> off(nt + 1, 0);
+  for (int t = 0; t < nt; ++t) {
+    if (ch[t].bad) return TPCF_ERR_INVALID_ARG;
+    off[t + 1] = off[t] + ch[t].rows;
   }
-  *n_rows = out;
+  if (off[nt] > capacity) return TPCF_ERR_OVERFLOW;
+  // rows to columns, each chunk's rows at its offset (in file order)
+  run_threads(nt, [&](int t) {
+    const Chunk& c = ch[t];
+    for (int k = 0; k < ncols; ++k) {
+      float* dst = cols + (size_t)k * (size_t)capacity + (size_t)off[t];
+      const float* src = c.vals.data() + k;
+      for (int64_t r = 0; r < c.rows; ++r) dst[r] = src[(size_t)r * (size_t)ncols];
+    }
+  });
+  *n_rows = off[nt];
   return TPCF_OK;
 }
 
