@@ -53,11 +53,42 @@ def test_decimal_rounding_matches_numpy(tpcf, tmp_path):
     np.testing.assert_array_equal(got.T, txt.astype(np.float32))
 
 
+def test_thread_counts_agree_across_chunk_boundaries(tpcf, tmp_path):
+    # ~1.5 MB, so up to ~20 threads get a piece; pieces start and end among
+    # comment lines, blank lines, CRLF endings and '+' signs, and the last line
+    # has no newline.  Every thread count must give the rows in file order.
+    rng = np.random.default_rng(7)
+    a = rng.normal(size=(30000, 5)).astype(np.float32)
+    lines = []
+    for i, row in enumerate(a):
+        if i % 101 == 0:
+            lines.append("# comment " + str(i))
+        if i % 37 == 0:
+            lines.append("")
+        txt = " ".join(("+" if (i + k) % 11 == 0 and v >= 0 else "") + f"{v:.9g}" for k, v in enumerate(row))
+        lines.append(txt + ("\r" if i % 13 == 0 else ""))
+    p = tmp_path / "mixed.txt"
+    p.write_bytes("\n".join(lines).encode())
+    keep = (a[:, 4] > 0) & (a[:, 2] >= 0)
+    ref = None
+    for nt in (1, 3, 8, 20):
+        got = tpcf.read_table(p, 5, keep_positive_col=4, keep_nonnegative_col=2, n_threads=nt)
+        np.testing.assert_array_equal(got.T, a[keep])
+        if ref is None:
+            ref = got
+        np.testing.assert_array_equal(got, ref)
+
+
 def test_malformed_line_is_an_error(tpcf, tmp_path):
     p = tmp_path / "bad.txt"
     p.write_text("1 2 3\n4 5\n")
     with pytest.raises(tpcf.TPCFError):
         tpcf.read_table(p, 3)
+    # a bad line in the last of several threads' pieces
+    big = tmp_path / "bad_late.txt"
+    big.write_text("1 2 3\n" * 200000 + "4 5\n" + "6 7 8\n" * 10)
+    with pytest.raises(tpcf.TPCFError):
+        tpcf.read_table(big, 3, n_threads=8)
 
 
 def test_result_table(tpcf, tmp_path):
