@@ -486,7 +486,8 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
         const int bb = (tcount + k) & 1u;
         const bool ok = mbar_wait_bounded(&mbar[bb], (phase >> bb) & 1u);
         phase ^= (1u << bb);
-        const SrcRec* __restrict__ S = tiles + bb * kTile;
+        // not __restrict__: the sub-chunk pass rewrites these bytes in place
+        const SrcRec* S = tiles + bb * kTile;
         const int nsub = (n + 31) >> 5;
         if (PATH == 0 && ok) {
           // One warp per 32-source sub-chunk: its bounding box and sums, and the

@@ -647,7 +647,8 @@ __global__ void __launch_bounds__(BT, 3) k_pairs_sph(const PairParams P) {
         const int bb = (tcount + k) & 1u;
         const bool ok = mbar_wait_bounded(&mbar[bb], (phase >> bb) & 1u);
         phase ^= (1u << bb);
-        const SrcRecS* __restrict__ S = tiles + bb * kTileS;
+        // not __restrict__: the sub-chunk pass rewrites these bytes in place
+        const SrcRecS* S = tiles + bb * kTileS;
         const int nsub = (n + 31) >> 5;
         if (ok) {
           // One warp per 32-source sub-chunk: its 3-D box, widened by 2^-23
