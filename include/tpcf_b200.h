@@ -230,8 +230,9 @@ tpcf_status tpcf_rotate_from_poles(tpcf_ctx* ctx, float* xA, float* yA, int64_t 
  * [ncols][capacity]; rows with column keep_pos_col <= 0 (the weight) and, if
  * keep_nonneg_col >= 0, with that column < 0 (the lens redshift) are dropped
  * as the loaders' masks do (:250-256, :316-328), and *n_rows receives the rows
- * kept.  All host threads parse (n_threads <= 0).  A malformed line gives
- * TPCF_ERR_INVALID_ARG.  Host only. */
+ * kept, in file order.  More kept rows than capacity gives
+ * TPCF_ERR_OVERFLOW.  All host threads parse (n_threads <= 0).  A malformed
+ * line gives TPCF_ERR_INVALID_ARG.  Host only. */
 tpcf_status tpcf_read_table(const char* path, int32_t ncols, int32_t keep_pos_col, int32_t keep_nonneg_col,
                             int32_t n_threads, float* cols, int64_t capacity, int64_t* n_rows);
 
