@@ -21,7 +21,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import Bins, LensCat, Opts, Result, ShearCat, Stats, TPCFError, lib
+from ._lib import Bins, KappaCat, LensCat, Opts, Result, ShearCat, Stats, TPCFError, lib
 
 LIN_BINNING, LOG_BINNING, IHS_BINNING, SQRT_BINNING = 0, 1, 2, 3  # src/utils.f90:7
 _SPACING = {"lin": 0, "log": 1, "ihs": 2, "sqrt": 3}
@@ -29,7 +29,7 @@ _SPACING = {"lin": 0, "log": 1, "ihs": 2, "sqrt": 3}
 __all__ = [
     "Binning", "create_bins", "Context", "ShapeCatalog", "LensCatalog", "KappaMap",
     "LensingSurveyField", "Shear2pcfResults", "shear_2pcf", "kappa_2pcf",
-    "tangential_shear_tpcf", "scalar_kappa_tpcf", "batch_shear_2pcf", "partition_data",
+    "tangential_shear_tpcf", "scalar_kappa_tpcf", "batch_shear_2pcf", "batch_kappa_2pcf", "partition_data",
     "partition_data_equal", "block_bootstrap", "TPCFError", "rotate_data_from_poles_and_meridian",
     "unit_vectors", "read_table", "load_standard_shape_catalog", "load_standard_kappa_map",
     "load_standard_lens_catalog", "write_result_table", "MarksField", "save_marks", "load_survey_marks",
@@ -123,10 +123,11 @@ class Context:
     def __init__(self, device: int = 0, use_grid: bool = True, cell_size: float = 0.0,
                  verbose: bool = False):
         self._h = C.c_void_p()
-        o = Opts(int(use_grid), int(verbose), float(cell_size), 0, 0, 0, (C.c_int32 * 5)())
+        o = Opts(int(use_grid), int(verbose), float(cell_size), 0, 0, 0, 0, 0, (C.c_int32 * 3)())
         _check(lib().tpcf_create(C.byref(self._h), int(device), C.byref(o)))
         self.device = device
         self.cell_size = float(cell_size)
+        self.tile_shape = (0, 0)
         self.spherical = False
 
     @property
@@ -154,6 +155,13 @@ class Context:
         """Grid cell side for later calls (0 = theta_max/16)."""
         _check(lib().tpcf_set_cell_size(self._h, float(cell_size)), self._h)
         self.cell_size = float(cell_size)
+
+    def set_tile_shape(self, group_size: int = 0, tile_chunks: int = 0):
+        """Planar pair kernel tile shape for later calls: lenses per group
+        (32, 64, 128) and 32-source sub-chunks per source tile (2, 4); 0 keeps
+        the default.  Changes speed only, never results."""
+        _check(lib().tpcf_set_tile_shape(self._h, int(group_size), int(tile_chunks)), self._h)
+        self.tile_shape = (int(group_size), int(tile_chunks))
 
     def set_spherical(self, on: bool):
         """Positions (longitude, latitude) and bins in radians for later calls."""
@@ -272,13 +280,17 @@ def _alloc_result(nb, nA, marks, lens_sums, n_patch, lens_raw=False):
         for k in ("xi_E_marks", "xi_B_marks", "K_marks", "w_marks"):
             r[k] = np.zeros((nA, nb), np.float32)
         r["marks_weight"] = np.zeros(nA, np.float32)
-    if lens_sums:
+    if lens_sums == "device":   # stays in device memory (a torch tensor on the current device)
+        import torch
+        r["lens_sums"] = torch.zeros((nA, 6, nb), dtype=torch.float64, device="cuda")
+    elif lens_sums:
         r["lens_sums"] = np.zeros((nA, 6, nb))
     if n_patch and n_patch > 0:
         r["patch_sums"] = np.zeros((n_patch, 6, nb))
     if lens_raw:
         r["lens_raw"] = np.zeros((nA, 6, nb))
-    cres = Result(**{k: (v.ctypes.data if v is not None else None) for k, v in r.items()})
+    ptr = lambda v: None if v is None else (v.data_ptr() if hasattr(v, "data_ptr") else v.ctypes.data)
+    cres = Result(**{k: ptr(v) for k, v in r.items()})
     return r, cres
 
 
@@ -398,7 +410,9 @@ def batch_shear_2pcf(lenses: Sequence[LensCatalog], shapes: Sequence[ShapeCatalo
                      tasks: Sequence[tuple], bins: Binning, lens_patches=None, n_patch=0,
                      marks=False, lens_sums=False, spherical_coords=False, ctx: Context = None):
     """All (lens catalogue, shape catalogue) tasks in one persistent launch
-    (tpcf_batch_shear_scalar).  ``lens_patches[i]`` labels lens catalogue i."""
+    (tpcf_batch_shear_scalar).  ``lens_patches[i]`` labels lens catalogue i.
+    ``lens_sums`` = True gives per-lens FP64 rows [nA][6][n_bin] as numpy
+    arrays, "device" as torch tensors left in device memory."""
     ctx = _resolve_ctx(ctx)
     _coords(ctx, spherical_coords)
     keep = []
@@ -428,6 +442,42 @@ def batch_shear_2pcf(lenses: Sequence[LensCatalog], shapes: Sequence[ShapeCatalo
                                        tl.ctypes.data, ts.ctypes.data, C.byref(cb),
                                        int(n_patch) if lens_patches is not None else 0, outs)
     _check(st, ctx.handle)
+    return [_finish(r, nb) for r in pyouts]
+
+
+def batch_kappa_2pcf(lenses: Sequence[LensCatalog], kappas: Sequence[KappaMap], tasks: Sequence[tuple],
+                     bins: Binning, lens_patches=None, n_patch=0, marks=False, lens_sums=False,
+                     spherical_coords=False, ctx: Context = None):
+    """All (scalar catalogue, kappa map) tasks of the scalar-scalar estimator
+    in one persistent launch (tpcf_batch_scalar_scalar)."""
+    ctx = _resolve_ctx(ctx)
+    _coords(ctx, spherical_coords)
+    keep = []
+    lc = (LensCat * len(lenses))()
+    for i, L in enumerate(lenses):
+        arrs = [_Arr(a) for a in (L.x, L.y, None, L.val, L.w)]
+        p = _Arr(None if lens_patches is None else lens_patches[i], np.int32)
+        keep += arrs + [p]
+        lc[i] = LensCat(arrs[0].n, *[a.ptr for a in arrs], p.ptr)
+    kc = (KappaCat * len(kappas))()
+    for i, K in enumerate(kappas):
+        arrs = [_Arr(a) for a in (K.x, K.y, K.kappa_E, K.kappa_B, K.w)]
+        keep += arrs
+        kc[i] = KappaCat(arrs[0].n, *[a.ptr for a in arrs])
+    tl = np.ascontiguousarray([t[0] for t in tasks], np.int32)
+    tk = np.ascontiguousarray([t[1] for t in tasks], np.int32)
+    nb = bins.n_bin
+    outs = (Result * len(tasks))()
+    pyouts = []
+    for t in range(len(tasks)):
+        r, cres = _alloc_result(nb, lenses[tasks[t][0]].n, marks, lens_sums,
+                                n_patch if lens_patches is not None else 0)
+        outs[t] = cres
+        pyouts.append(r)
+    cb = bins.c_struct()
+    _check(lib().tpcf_batch_scalar_scalar(ctx.handle, len(lenses), lc, len(kappas), kc, len(tasks), tl.ctypes.data,
+                                          tk.ctypes.data, C.byref(cb),
+                                          int(n_patch) if lens_patches is not None else 0, outs), ctx.handle)
     return [_finish(r, nb) for r in pyouts]
 
 

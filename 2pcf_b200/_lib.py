@@ -18,6 +18,7 @@ STATUS_NAMES = {
     0: "TPCF_OK", 1: "TPCF_ERR_INVALID_ARG", 2: "TPCF_ERR_OOM", 3: "TPCF_ERR_OVERFLOW",
     4: "TPCF_ERR_TIMEOUT", 5: "TPCF_ERR_CUDA", 6: "TPCF_ERR_NOT_SUPPORTED", 7: "TPCF_ERR_NO_DEVICE",
 }
+globals().update({name: code for code, name in STATUS_NAMES.items()})
 
 # Every symbol declared in include/tpcf_b200.h (checked by tests/test_abi.py).
 EXPORTED = []
@@ -31,7 +32,7 @@ class Bins(C.Structure):
 class Opts(C.Structure):
     _fields_ = [("use_grid", C.c_int32), ("verbose", C.c_int32), ("cell_size", C.c_double),
                 ("spherical", C.c_int32), ("shard_index", C.c_int32), ("shard_count", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("group_size", C.c_int32), ("tile_chunks", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class Result(C.Structure):
@@ -50,9 +51,25 @@ class ShearCat(C.Structure):
     _fields_ = [("n", C.c_int64)] + [(n, C.c_void_p) for n in ("x", "y", "z", "e1", "e2", "w", "m")]
 
 
+class KappaCat(C.Structure):
+    _fields_ = [("n", C.c_int64)] + [(n, C.c_void_p) for n in ("x", "y", "kE", "kB", "w")]
+
+
 class Stats(C.Structure):
     _fields_ = [("pair_kernel_ms", C.c_double), ("call_ms", C.c_double), ("n_pairs", C.c_int64),
                 ("h2d_bytes", C.c_int64), ("kernel_launches", C.c_int64)]
+
+
+class LensGrad(C.Structure):
+    _fields_ = [("val", C.c_void_p), ("w", C.c_void_p)]
+
+
+class ShearGrad(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("e1", "e2", "w", "m")]
+
+
+class AdjointTask(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("sum_gt", "sum_gx", "sum_K", "lens_raw", "dL_dgt", "dL_dgx")]
 
 
 class MarksFieldC(C.Structure):
@@ -97,6 +114,8 @@ def lib():
     _sig(L, "tpcf_last_stats", st, [vp, C.POINTER(Stats)])
     _sig(L, "tpcf_set_shard", st, [vp, i32, i32])
     _sig(L, "tpcf_set_cell_size", st, [vp, C.c_double])
+    _sig(L, "tpcf_set_tile_shape", st, [vp, i32, i32])
+    _sig(L, "tpcf_debug_inject", st, [vp, i64, i32, C.c_uint32])
     _sig(L, "tpcf_measure_fp32_peak", st, [vp, C.POINTER(C.c_double)])
     _sig(L, "tpcf_canonical_edges", st, [C.POINTER(Bins), vp, vp])
     _sig(L, "tpcf_bin_centers", st, [C.POINTER(Bins), vp])
@@ -122,6 +141,11 @@ def lib():
          [C.POINTER(Bins), C.POINTER(Result)])
     _sig(L, "tpcf_shear_scalar_adjoint", st, [vp] + [vp] * 5 + [i64] + [vp] * 7 + [i64] +
          [C.POINTER(Bins)] + [vp] * 4 + [vp] * 2 + [vp] * 6)
+    _sig(L, "tpcf_batch_scalar_scalar", st, [vp, i32, C.POINTER(LensCat), i32, C.POINTER(KappaCat),
+                                             i32, vp, vp, C.POINTER(Bins), i32, C.POINTER(Result)])
+    _sig(L, "tpcf_batch_shear_scalar_adjoint", st, [vp, i32, C.POINTER(LensCat), C.POINTER(LensGrad), i32,
+                                                    C.POINTER(ShearCat), C.POINTER(ShearGrad), i32, vp, vp,
+                                                    C.POINTER(Bins), C.POINTER(AdjointTask)])
     _sig(L, "tpcf_kmeans", st, [vp, vp, vp, vp, i64, i32, i32, C.c_float, vp, vp, C.POINTER(i32)])
     _sig(L, "tpcf_kmeans_equal", st, [vp, vp, vp, vp, i64, i32, i32, C.c_float, C.c_float, C.c_float, i32,
                                       C.c_uint64, vp, vp, C.POINTER(i32), C.POINTER(C.c_float)])

@@ -86,8 +86,9 @@ def xi_shear(val_A, w_A, e1_B, e2_B, w_B, geometry: dict, bins: Binning, ctx: Co
 
 class ShearXiBatch(torch.autograd.Function):
     """All tasks of a tomography in one forward launch (tpcf_batch_shear_scalar
-    keeping every task's raw per-lens sums on the device), one adjoint call per
-    task in backward; gradients of a catalogue sum over the tasks that use it."""
+    keeping every task's raw per-lens sums on the device) and one backward
+    launch (tpcf_batch_shear_scalar_adjoint); gradients of a catalogue sum over
+    the tasks that use it."""
 
     @staticmethod
     def forward(actx, tasks, geo_L, geo_S, bins, tctx, *leaves):
@@ -143,22 +144,23 @@ class ShearXiBatch(torch.autograd.Function):
         g_wB = [torch.zeros_like(t[5]) for t in sv]
         cb = bins.c_struct()
         tctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
-        for t, (li, si) in enumerate(tasks):
-            lt = (d_xi_t[t] if d_xi_t is not None else torch.zeros(bins.n_bin, device=dev)).to(torch.float64)
-            lt = lt.contiguous()
-            lx = None if d_xi_x is None else d_xi_x[t].to(torch.float64).contiguous()
-            A, B = lv[li], sv[si]
-            o = [torch.zeros(A[0].numel(), dtype=torch.float32, device=dev) for _ in range(2)] + \
-                [torch.zeros(B[0].numel(), dtype=torch.float32, device=dev) for _ in range(3)]
-            _check(lib().tpcf_shear_scalar_adjoint(
-                tctx.handle, _p(A[0]), _p(A[1]), _p(A[2]), _p(A[3]), _p(A[4]), A[0].numel(), _p(B[0]), _p(B[1]),
-                _p(B[2]), _p(B[3]), _p(B[4]), _p(B[5]), _p(B[6]), B[0].numel(), C.byref(cb), _p(S[t, 1]),
-                _p(S[t, 2]), _p(S[t, 4]), _p(raws[t]), _p(lt), _p(lx), *[_p(x) for x in o], None), tctx.handle)
-            g_val[li] += o[0]
-            g_wA[li] += o[1]
-            g_e1[si] += o[2]
-            g_e2[si] += o[3]
-            g_wB[si] += o[4]
+        from . import _lib as L_
+        nT = len(tasks)
+        lts = [(d_xi_t[t] if d_xi_t is not None else torch.zeros(bins.n_bin, device=dev)).to(torch.float64)
+               .contiguous() for t in range(nT)]
+        lxs = [None if d_xi_x is None else d_xi_x[t].to(torch.float64).contiguous() for t in range(nT)]
+        ta = (L_.AdjointTask * nT)(*[L_.AdjointTask(_p(S[t, 1]), _p(S[t, 2]), _p(S[t, 4]), _p(raws[t]), _p(lts[t]),
+                                                    _p(lxs[t])) for t in range(nT)])
+        lc = (L_.LensCat * len(lv))(*[L_.LensCat(t[0].numel(), *[_p(a) for a in t], None) for t in lv])
+        sc = (L_.ShearCat * len(sv))(*[L_.ShearCat(t[0].numel(), *[_p(a) for a in t]) for t in sv])
+        lg = (L_.LensGrad * len(lv))(*[L_.LensGrad(_p(a), _p(b)) for a, b in zip(g_val, g_wA)])
+        sg = (L_.ShearGrad * len(sv))(*[L_.ShearGrad(_p(a), _p(b), _p(c), None) for a, b, c in zip(g_e1, g_e2, g_wB)])
+        import numpy as np
+        tl = np.ascontiguousarray([a for a, _ in tasks], np.int32)
+        ts = np.ascontiguousarray([b for _, b in tasks], np.int32)
+        # every task's gradient in one launch; a catalogue used by several tasks gets their sum
+        _check(lib().tpcf_batch_shear_scalar_adjoint(tctx.handle, len(lv), lc, lg, len(sv), sc, sg, nT,
+                                                     tl.ctypes.data, ts.ctypes.data, C.byref(cb), ta), tctx.handle)
         return (None, None, None, None, None, *g_val, *g_wA, *g_e1, *g_e2, *g_wB)
 
 

@@ -47,27 +47,29 @@ constexpr int BT = 128;
 // 56-register schedule; 6 blocks of 128 threads still fit every SM.
 constexpr int kAdjMinBlocks = 6;
 
-struct AdjParams {
+// One (lens catalogue, source catalogue) task of a batched backward pass.
+struct AdjTask {
+  GridDesc grid;            // grid over the task's lenses
   const SrcRec* lens;       // lens grid records: a = {x, y, val*w, w}, b = {z, 0, 0, 0}
-  GridDesc grid;            // grid over the lenses
-  const float4* s0;         // sources sorted: {x, y, e1, e2}
+  const float4* s0;         // the task's sources, sorted: {x, y, e1, e2}
   const float4* s1;         // {w, 1+m, z, 0}
-  const int* perm;          // sorted source -> input index
   const float4* gbox;       // source group boxes
-  const int2* items;        // (0, group) in processing order
-  int n_items;
   int n_src;                // valid sources
+  int pad;
+  double* dsum;             // [5][n_src] FP64 sums D1, D2, D3, D4, DN of this task (sorted order)
+};
+
+struct AdjParams {
+  const AdjTask* tasks;
+  const int2* items;        // (task, source group) in processing order
+  int n_items;
   int nb;
   int* queue_head;
   unsigned* err;
   const double* e2;
   const float* e2f;
-  const float4* coef;       // [nb] {mu, mux, nu, 0}
+  const float4* coef;       // [n_task][nb] {mu, mux, nu, 0}
   float R, margin, binA, binB, eps;
-  float* g_e1;
-  float* g_e2;
-  float* g_w;
-  float* g_m;
 };
 
 struct AdjSmem {
@@ -224,7 +226,6 @@ __global__ void __launch_bounds__(BT, kAdjMinBlocks) k_adj(const AdjParams P) {
   for (int i = tid; i <= nb; i += BT) {
     e2s[i] = P.e2[i];
     e2f[i] = P.e2f[i];
-    coef[i] = i < nb ? P.coef[i] : make_float4(0.f, 0.f, 0.f, 0.f);
   }
   __syncthreads();
   BinCtx C;
@@ -235,25 +236,30 @@ __global__ void __launch_bounds__(BT, kAdjMinBlocks) k_adj(const AdjParams P) {
   C.hi_g = e2f[nb] * (1.f + P.eps);
   uint32_t phase = 0u, tcount = 0u;
   bool timed_out = false;
-  const GridDesc& G = P.grid;
 
   for (;;) {
     if (tid == 0) *sh_item = atomicAdd(P.queue_head, 1);
     __syncthreads();
     const int item = *sh_item;
     if (item >= P.n_items) break;
-    const int g = P.items[item].y;
+    const int2 it = P.items[item];
+    const AdjTask& T = P.tasks[it.x];
+    const GridDesc G = T.grid;
+    // this task's bin coefficients (read after the next barrier)
+    for (int i = tid; i <= nb; i += BT)
+      coef[i] = i < nb ? P.coef[(size_t)it.x * nb + i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int g = it.y;
     const int si = g * BT + tid;
-    const bool act = si < P.n_src;
+    const bool act = si < T.n_src;
     float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0;
     if (act) {
-      r0 = P.s0[si];
-      r1 = P.s1[si];
+      r0 = T.s0[si];
+      r1 = T.s1[si];
     }
     const float sx = r0.x, sy = r0.y, sz = r1.z;
     const float2 nsx = dup2(-sx), nsy = dup2(-sy);
     double D1 = 0, D2 = 0, D3 = 0, D4 = 0, DN = 0;
-    const float4 box = P.gbox[g];
+    const float4 box = T.gbox[g];
     int cy0, cy1;
     row_range(G, box, P.R, P.margin, cy0, cy1);
     for (int c0 = cy0; c0 <= cy1; c0 += kMaxRows) {
@@ -282,7 +288,7 @@ __global__ void __launch_bounds__(BT, kAdjMinBlocks) k_adj(const AdjParams P) {
         const int n0 = min(kTile, span1[ri] - s0);
         const int bb = tcount & 1u;
         mbar_arrive_tx(&mbar[bb], (uint32_t)(n0 * sizeof(SrcRec)));
-        bulk_g2s(tiles + bb * kTile, P.lens + s0, (uint32_t)(n0 * sizeof(SrcRec)), &mbar[bb]);
+        bulk_g2s(tiles + bb * kTile, T.lens + s0, (uint32_t)(n0 * sizeof(SrcRec)), &mbar[bb]);
       }
       for (int k = 0; k < ntiles; ++k) {
         if (tid == 0 && k + 1 < ntiles) {
@@ -291,7 +297,7 @@ __global__ void __launch_bounds__(BT, kAdjMinBlocks) k_adj(const AdjParams P) {
           const int n1 = min(kTile, span1[ri] - s1);
           const int bb = (tcount + k + 1) & 1u;
           mbar_arrive_tx(&mbar[bb], (uint32_t)(n1 * sizeof(SrcRec)));
-          bulk_g2s(tiles + bb * kTile, P.lens + s1, (uint32_t)(n1 * sizeof(SrcRec)), &mbar[bb]);
+          bulk_g2s(tiles + bb * kTile, T.lens + s1, (uint32_t)(n1 * sizeof(SrcRec)), &mbar[bb]);
         }
         while (tpref[rc + 1] <= k) ++rc;
         const int s = span0[rc] + (k - tpref[rc]) * kTile;
@@ -446,13 +452,13 @@ __global__ void __launch_bounds__(BT, kAdjMinBlocks) k_adj(const AdjParams P) {
       tcount += (uint32_t)ntiles;
     }
     if (act) {
-      const int j = P.perm[si];
-      const double w = (double)r1.x;
-      const double e1 = r0.z, e2 = r0.w;
-      if (P.g_e1) P.g_e1[j] = (float)(w * (-D1 + D4));
-      if (P.g_e2) P.g_e2[j] = (float)(w * (-D2 - D3));
-      if (P.g_w) P.g_w[j] = (float)(-e1 * D1 - e2 * D2 + e1 * D4 - e2 * D3 - (double)r1.y * DN);
-      if (P.g_m) P.g_m[j] = (float)(-w * DN);
+      double* d = T.dsum;
+      const size_t n = (size_t)T.n_src;
+      d[si] = D1;
+      d[n + si] = D2;
+      d[2 * n + si] = D3;
+      d[3 * n + si] = D4;
+      d[4 * n + si] = DN;
     }
     __syncthreads();
   }
@@ -534,17 +540,18 @@ __global__ void k_adj_src_gather(const int* __restrict__ idx, int n_valid, const
   perm[s] = i;
 }
 
-__global__ void k_adj_groups(int n_groups, int n_valid, int* gstart, int2* items) {
+__global__ void k_adj_groups(int n_groups, int n_valid, int* gstart) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g <= n_groups) gstart[g] = min(g * BT, n_valid);
-  if (g < n_groups) items[g] = make_int2(0, g);
 }
 
-// Lens-side gradients from the raw per-lens sums [nA][6][nb] (rows dw, gt, gx,
-// w, K, n without lens factors).
-__global__ void k_adj_lens_grads(const double* __restrict__ raw, const float* __restrict__ val,
-                                 const float* __restrict__ w, long long nA, int nb, const double* __restrict__ mu,
-                                 float* g_val, float* g_w) {
+// Lens-side gradient terms of one task from its raw per-lens sums
+// [nA][6][nb] (rows dw, gt, gx, w, K, n without lens factors), added to the
+// lens catalogue's FP64 accumulators: acc_a += sum_b (mu_b Rt + mux_b Rx),
+// acc_k += sum_b nu_b RK.  Tasks are added one launch after another (fixed
+// order).
+__global__ void k_adj_lens_acc(const double* __restrict__ raw, long long nA, int nb, const double* __restrict__ mu,
+                               double* acc_a, double* acc_k) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nA; i += (long long)gridDim.x * blockDim.x) {
     const double* r = raw + (size_t)i * 6 * nb;
     double a = 0, k = 0;
@@ -552,9 +559,40 @@ __global__ void k_adj_lens_grads(const double* __restrict__ raw, const float* __
       a += mu[b] * r[1 * nb + b] + mu[nb + b] * r[2 * nb + b];
       k += mu[2 * nb + b] * r[4 * nb + b];
     }
-    if (g_val) g_val[i] = (float)((double)w[i] * a);
-    if (g_w) g_w[i] = (float)((double)val[i] * a - k);
+    acc_a[i] += a;
+    acc_k[i] += k;
   }
+}
+
+// dL/dval_i = w_i acc_a, dL/dw_i = val_i acc_a - acc_k.
+__global__ void k_adj_lens_finish(const double* __restrict__ acc_a, const double* __restrict__ acc_k,
+                                  const float* __restrict__ val, const float* __restrict__ w, long long nA,
+                                  float* g_val, float* g_w) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nA; i += (long long)gridDim.x * blockDim.x) {
+    if (g_val) g_val[i] = (float)((double)w[i] * acc_a[i]);
+    if (g_w) g_w[i] = (float)((double)val[i] * acc_a[i] - acc_k[i]);
+  }
+}
+
+// Source gradients of one source catalogue from the D sums of the tasks that
+// use it (added in task order), in input order:
+//   dL/de1 = w (-D1 + D4), dL/de2 = w (-D2 - D3),
+//   dL/dw = -e1 D1 - e2 D2 + e1 D4 - e2 D3 - (1 + m) DN, dL/dm = -w DN.
+__global__ void k_adj_src_finish(const double* const* __restrict__ dsums, int n_sum, int ns,
+                                 const float4* __restrict__ s0, const float4* __restrict__ s1,
+                                 const int* __restrict__ perm, float* g_e1, float* g_e2, float* g_w, float* g_m) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  double D[5] = {0, 0, 0, 0, 0};
+  for (int t = 0; t < n_sum; ++t)
+    for (int q = 0; q < 5; ++q) D[q] += dsums[t][(size_t)q * ns + s];
+  const int j = perm[s];
+  const float4 a = s0[s], b = s1[s];
+  const double w = (double)b.x, e1 = a.z, e2 = a.w;
+  if (g_e1) g_e1[j] = (float)(w * (-D[0] + D[3]));
+  if (g_e2) g_e2[j] = (float)(w * (-D[1] - D[2]));
+  if (g_w) g_w[j] = (float)(-e1 * D[0] - e2 * D[1] + e1 * D[3] - e2 * D[2] - (double)b.y * D[4]);
+  if (g_m) g_m[j] = (float)(-w * D[4]);
 }
 
 template <bool HAS_Z, bool LOGB, bool WX>
@@ -588,199 +626,301 @@ std::vector<T> to_host(tpcf_ctx* c, const T* p, size_t n) {
   return h;
 }
 
-tpcf_status run_adjoint(tpcf_ctx* c, const float* xA, const float* yA, const float* zA, const float* valA,
-                        const float* wA, int64_t nA, const float* xB, const float* yB, const float* zB,
-                        const float* e1B, const float* e2B, const float* wB, const float* mB, int64_t nB,
-                        const tpcf_bins* bins, const double* sum_gt, const double* sum_gx, const double* sum_K,
-                        const double* lens_raw, const double* dL_dgt, const double* dL_dgx, float* g_val,
-                        float* g_wA, float* g_e1, float* g_e2, float* g_wB, float* g_m) {
+struct AdjLensIn {
+  int64_t n;
+  const float *x, *y, *z, *val, *w;
+  float *g_val, *g_w;
+};
+struct AdjSrcIn {
+  int64_t n;
+  const float *x, *y, *z, *e1, *e2, *w, *m;
+  float *g_e1, *g_e2, *g_w, *g_m;
+};
+struct AdjTaskIn {
+  int lens, src;
+  const double *sum_gt, *sum_gx, *sum_K, *lens_raw, *dL_dgt, *dL_dgx;
+};
+
+// The backward pass of a batched forward call: every task's source gradients
+// in one persistent launch over all (task, source group) work items, with one
+// lens grid per lens catalogue and one sorted source set per source catalogue;
+// gradients of a catalogue used by several tasks are summed over them in task
+// order (FP64).
+tpcf_status run_adjoint_batch(tpcf_ctx* c, std::vector<AdjLensIn> lens, std::vector<AdjSrcIn> srcs,
+                              const std::vector<AdjTaskIn>& tasks, const tpcf_bins* bins) {
+  Phase ph_nvtx("tpcf: adjoint");
   begin_call(c);
   cudaStream_t st = c->stream;
   const int nb = bins->n_bin;
+  const int nL = (int)lens.size(), nS = (int)srcs.size(), nT = (int)tasks.size();
   std::vector<double> e(nb + 1), e2(nb + 1);
   tpcf_status bs = canonical_edges(bins, e.data(), e2.data());
   if (bs != TPCF_OK) throw Failure(bs, "invalid binning");
   if (c->opts.spherical) throw Failure(TPCF_ERR_NOT_SUPPORTED, "spherical coordinates are not supported");
-  if (!sum_gt || !sum_K || !dL_dgt || ((g_val || g_wA) && !lens_raw))
-    throw Failure(TPCF_ERR_INVALID_ARG, "missing forward sums, lens_raw or dL/dg_t");
-  if (nA < 0 || nB < 0 || nA > (1ll << 31) - 2 || nB > (1ll << 31) - 2)
-    throw Failure(TPCF_ERR_INVALID_ARG, "catalogue size out of range");
+  for (const auto& l : lens)
+    if (l.n < 0 || l.n > (1ll << 31) - 2 || (l.n > 0 && (!l.x || !l.y || !l.val || !l.w)))
+      throw Failure(TPCF_ERR_INVALID_ARG, "lens catalogue size out of range or array missing");
+  for (const auto& s : srcs)
+    if (s.n < 0 || s.n > (1ll << 31) - 2 || (s.n > 0 && (!s.x || !s.y || !s.e1 || !s.e2 || !s.w)))
+      throw Failure(TPCF_ERR_INVALID_ARG, "source catalogue size out of range or array missing");
+  for (const auto& t : tasks) {
+    if (t.lens < 0 || t.lens >= nL || t.src < 0 || t.src >= nS) throw Failure(TPCF_ERR_INVALID_ARG, "task index out of range");
+    const AdjLensIn& l = lens[t.lens];
+    if (!t.sum_gt || !t.sum_K || !t.dL_dgt || ((l.g_val || l.g_w) && !t.lens_raw))
+      throw Failure(TPCF_ERR_INVALID_ARG, "missing forward sums, lens_raw or dL/dg_t");
+  }
 
-  // per-bin coefficients mu, mux, nu (FP64 on the host)
-  const std::vector<double> hgt = to_host(c, sum_gt, nb), hK = to_host(c, sum_K, nb), hl = to_host(c, dL_dgt, nb);
-  std::vector<double> hgx(nb, 0.0), hlx(nb, 0.0);
-  if (sum_gx) hgx = to_host(c, sum_gx, nb);
-  if (dL_dgx) hlx = to_host(c, dL_dgx, nb);
-  const bool wx = dL_dgx != nullptr;
-  std::vector<double> mu(3 * nb, 0.0);
-  std::vector<float4> coef(nb);
-  for (int b = 0; b < nb; ++b) {
-    if (hK[b] > 0) {
-      mu[b] = hl[b] / hK[b];
-      mu[nb + b] = hlx[b] / hK[b];
-      mu[2 * nb + b] = (hl[b] * (hgt[b] / hK[b]) + hlx[b] * (hgx[b] / hK[b])) / hK[b];
+  // per-task bin coefficients mu, mux, nu (FP64 on the host)
+  bool wx = false;
+  std::vector<double> mu((size_t)nT * 3 * nb, 0.0);
+  std::vector<float4> coef((size_t)nT * nb);
+  for (int t = 0; t < nT; ++t) {
+    const AdjTaskIn& T = tasks[t];
+    const std::vector<double> hgt = to_host(c, T.sum_gt, nb), hK = to_host(c, T.sum_K, nb),
+                              hl = to_host(c, T.dL_dgt, nb);
+    std::vector<double> hgx(nb, 0.0), hlx(nb, 0.0);
+    if (T.sum_gx) hgx = to_host(c, T.sum_gx, nb);
+    if (T.dL_dgx) hlx = to_host(c, T.dL_dgx, nb);
+    wx = wx || T.dL_dgx != nullptr;
+    double* m = mu.data() + (size_t)t * 3 * nb;
+    for (int b = 0; b < nb; ++b) {
+      if (hK[b] > 0) {
+        m[b] = hl[b] / hK[b];
+        m[nb + b] = hlx[b] / hK[b];
+        m[2 * nb + b] = (hl[b] * (hgt[b] / hK[b]) + hlx[b] * (hgx[b] / hK[b])) / hK[b];
+      }
+      coef[(size_t)t * nb + b] = make_float4((float)m[b], (float)m[nb + b], (float)m[2 * nb + b], 0.f);
     }
-    coef[b] = make_float4((float)mu[b], (float)mu[nb + b], (float)mu[2 * nb + b], 0.f);
   }
 
-  xA = stage(c, xA, nA); yA = stage(c, yA, nA); zA = stage(c, zA, nA);
-  valA = stage(c, valA, nA); wA = stage(c, wA, nA);
-  xB = stage(c, xB, nB); yB = stage(c, yB, nB); zB = stage(c, zB, nB);
-  e1B = stage(c, e1B, nB); e2B = stage(c, e2B, nB); wB = stage(c, wB, nB); mB = stage(c, mB, nB);
+  for (auto& l : lens) {
+    l.x = stage(c, l.x, l.n); l.y = stage(c, l.y, l.n); l.z = stage(c, l.z, l.n);
+    l.val = stage(c, l.val, l.n); l.w = stage(c, l.w, l.n);
+  }
+  for (auto& s : srcs) {
+    s.x = stage(c, s.x, s.n); s.y = stage(c, s.y, s.n); s.z = stage(c, s.z, s.n);
+    s.e1 = stage(c, s.e1, s.n); s.e2 = stage(c, s.e2, s.n); s.w = stage(c, s.w, s.n); s.m = stage(c, s.m, s.n);
+  }
+  double* dmu = (double*)ws_alloc(c, sizeof(double) * mu.size());
+  check(cudaMemcpyAsync(dmu, mu.data(), sizeof(double) * mu.size(), cudaMemcpyHostToDevice, st), "H2D mu");
+  auto dev_or_ws = [&](float* user, int64_t n) -> float* {
+    if (!user) return nullptr;
+    return is_device_ptr(user) ? user : (float*)ws_alloc(c, sizeof(float) * (size_t)std::max<int64_t>(n, 1));
+  };
 
-  // lens-side gradients
-  double* dmu = (double*)ws_alloc(c, sizeof(double) * 3 * nb);
-  check(cudaMemcpyAsync(dmu, mu.data(), sizeof(double) * 3 * nb, cudaMemcpyHostToDevice, st), "H2D mu");
-  if ((g_val || g_wA) && nA > 0) {
-    const double* raw = stage(c, lens_raw, nA * 6 * nb);
-    float* dv = g_val ? (is_device_ptr(g_val) ? g_val : (float*)ws_alloc(c, sizeof(float) * nA)) : nullptr;
-    float* dw = g_wA ? (is_device_ptr(g_wA) ? g_wA : (float*)ws_alloc(c, sizeof(float) * nA)) : nullptr;
-    k_adj_lens_grads<<<(unsigned)std::min<long long>((nA + 255) / 256, 4096), 256, 0, st>>>(raw, valA, wA, nA, nb,
-                                                                                          dmu, dv, dw);
+  // lens-side gradients: FP64 accumulators per lens catalogue, tasks in order
+  for (int i = 0; i < nL; ++i) {
+    AdjLensIn& l = lens[i];
+    if (!(l.g_val || l.g_w) || l.n == 0) continue;
+    double* acc = (double*)ws_alloc(c, sizeof(double) * 2 * l.n);
+    check(cudaMemsetAsync(acc, 0, sizeof(double) * 2 * l.n, st), "memset lens acc");
+    const unsigned gb = (unsigned)std::min<long long>((l.n + 255) / 256, 4096);
+    for (int t = 0; t < nT; ++t) {
+      if (tasks[t].lens != i) continue;
+      const double* raw = stage(c, tasks[t].lens_raw, l.n * 6 * nb);
+      k_adj_lens_acc<<<gb, 256, 0, st>>>(raw, l.n, nb, dmu + (size_t)t * 3 * nb, acc, acc + l.n);
+      counted(c, cudaGetLastError(), "lens gradient terms");
+    }
+    float* dv = dev_or_ws(l.g_val, l.n);
+    float* dw = dev_or_ws(l.g_w, l.n);
+    k_adj_lens_finish<<<gb, 256, 0, st>>>(acc, acc + l.n, l.val, l.w, l.n, dv, dw);
     counted(c, cudaGetLastError(), "lens gradients");
-    if (dv && dv != g_val) copy_out(c, g_val, dv, sizeof(float) * nA);
-    if (dw && dw != g_wA) copy_out(c, g_wA, dw, sizeof(float) * nA);
+    if (dv && dv != l.g_val) copy_out(c, l.g_val, dv, sizeof(float) * l.n);
+    if (dw && dw != l.g_w) copy_out(c, l.g_w, dw, sizeof(float) * l.n);
   }
-  if (!(g_e1 || g_e2 || g_wB || g_m) || nB == 0) {
+  bool any_src = false;
+  for (const auto& s : srcs) any_src = any_src || ((s.g_e1 || s.g_e2 || s.g_w || s.g_m) && s.n > 0);
+  if (!any_src) {
     check(cudaStreamSynchronize(st), "sync");
     return TPCF_OK;
   }
 
-  // boxes: lens (kind 1) and source (kind 0)
-  int* box_ord = (int*)ws_alloc(c, sizeof(int) * 16);
-  unsigned long long* cnt = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * 2);
-  int* pr = (int*)ws_alloc(c, sizeof(int) * 4);
-  float* boxf = (float*)ws_alloc(c, sizeof(float) * 16);
-  counted(c, launch_bbox_init(box_ord, cnt, pr, 2, st), "bbox init");
-  counted(c, launch_bbox(xA, yA, zA, wA, nullptr, nullptr, nA, 1, box_ord, cnt, pr, st), "bbox lens");
-  counted(c, launch_bbox(xB, yB, zB, nullptr, nullptr, nullptr, nB, 0, box_ord + 8, cnt + 1, pr + 2, st), "bbox src");
-  counted(c, launch_bbox_finish(box_ord, boxf, 16, st), "bbox finish");
-  float hb[16];
-  unsigned long long hc[2];
-  check(cudaMemcpyAsync(hb, boxf, sizeof(hb), cudaMemcpyDeviceToHost, st), "D2H box");
-  check(cudaMemcpyAsync(hc, cnt, sizeof(hc), cudaMemcpyDeviceToHost, st), "D2H count");
+  // boxes and counts: lens catalogues (kind 1), then source catalogues (kind 0)
+  const int ncat = nL + nS;
+  int* box_ord = (int*)ws_alloc(c, sizeof(int) * 8 * ncat);
+  unsigned long long* cnt = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * ncat);
+  int* pr = (int*)ws_alloc(c, sizeof(int) * 2 * ncat);
+  float* boxf = (float*)ws_alloc(c, sizeof(float) * 8 * ncat);
+  counted(c, launch_bbox_init(box_ord, cnt, pr, ncat, st), "bbox init");
+  for (int i = 0; i < nL; ++i)
+    counted(c, launch_bbox(lens[i].x, lens[i].y, lens[i].z, lens[i].w, nullptr, nullptr, lens[i].n, 1,
+                           box_ord + 8 * i, cnt + i, pr + 2 * i, st), "bbox lens");
+  for (int i = 0; i < nS; ++i)
+    counted(c, launch_bbox(srcs[i].x, srcs[i].y, srcs[i].z, nullptr, nullptr, nullptr, srcs[i].n, 0,
+                           box_ord + 8 * (nL + i), cnt + nL + i, pr + 2 * (nL + i), st), "bbox src");
+  counted(c, launch_bbox_finish(box_ord, boxf, 8 * ncat, st), "bbox finish");
+  std::vector<float> hb(8 * ncat);
+  std::vector<unsigned long long> hc(ncat);
+  check(cudaMemcpyAsync(hb.data(), boxf, sizeof(float) * 8 * ncat, cudaMemcpyDeviceToHost, st), "D2H box");
+  check(cudaMemcpyAsync(hc.data(), cnt, sizeof(unsigned long long) * ncat, cudaMemcpyDeviceToHost, st), "D2H count");
   check(cudaStreamSynchronize(st), "sync box");
-  const int nl = (int)hc[0], ns = (int)hc[1];
-  // sources with no pair keep gradient 0
-  auto zero_out = [&](float* p) {
-    if (p) check(cudaMemsetAsync(p, 0, sizeof(float) * nB, st), "memset grad");
-  };
-  float* out_e1 = g_e1 ? (is_device_ptr(g_e1) ? g_e1 : (float*)ws_alloc(c, sizeof(float) * nB)) : nullptr;
-  float* out_e2 = g_e2 ? (is_device_ptr(g_e2) ? g_e2 : (float*)ws_alloc(c, sizeof(float) * nB)) : nullptr;
-  float* out_w = g_wB ? (is_device_ptr(g_wB) ? g_wB : (float*)ws_alloc(c, sizeof(float) * nB)) : nullptr;
-  float* out_m = g_m ? (is_device_ptr(g_m) ? g_m : (float*)ws_alloc(c, sizeof(float) * nB)) : nullptr;
-  zero_out(out_e1); zero_out(out_e2); zero_out(out_w); zero_out(out_m);
-  const bool has_z = nl > 0 && ns > 0 && hb[5] > hb[8 + 4];
+
+  // outputs, zero for sources with no pair
+  std::vector<float*> o_e1(nS), o_e2(nS), o_w(nS), o_m(nS);
+  for (int i = 0; i < nS; ++i) {
+    AdjSrcIn& s = srcs[i];
+    o_e1[i] = dev_or_ws(s.g_e1, s.n); o_e2[i] = dev_or_ws(s.g_e2, s.n);
+    o_w[i] = dev_or_ws(s.g_w, s.n); o_m[i] = dev_or_ws(s.g_m, s.n);
+    for (float* p : {o_e1[i], o_e2[i], o_w[i], o_m[i]})
+      if (p && s.n > 0) check(cudaMemsetAsync(p, 0, sizeof(float) * s.n, st), "memset grad");
+  }
+  bool has_z = false;
+  for (const auto& t : tasks) {
+    const int li = t.lens, si = nL + t.src;
+    if (hc[li] > 0 && hc[si] > 0 && hb[8 * li + 5] > hb[8 * si + 4]) has_z = true;
+  }
   const bool logb = bins->spacing == TPCF_LOG;
   const double Rd = bins->x_max;
   const float R = (float)(Rd * (1.0 + 1e-6));
 
-  if (nl > 0 && ns > 0) {
-    // grid over the lenses
-    GridDesc g{};
-    const float x0 = hb[0], y0 = hb[1], ex = hb[2] - hb[0], ey = hb[3] - hb[1];
+  // one lens grid per lens catalogue
+  std::vector<GridDesc> lgrid(nL);
+  std::vector<SrcRec*> lrec(nL, nullptr);
+  double maxcell = 0.0;
+  for (int i = 0; i < nL; ++i) {
+    const AdjLensIn& l = lens[i];
+    const int nl = (int)hc[i];
+    GridDesc& g = lgrid[i];
+    const float* b = &hb[8 * i];
+    const float x0 = nl ? b[0] : 0.f, y0 = nl ? b[1] : 0.f, ex = nl ? b[2] - b[0] : 0.f, ey = nl ? b[3] - b[1] : 0.f;
     double cell = c->opts.cell_size > 0 ? c->opts.cell_size : Rd / 16.0;
     const double span = std::max((double)ex, (double)ey);
     if (!c->opts.use_grid) cell = span * 2.0 + 1.0;
     while ((span / cell + 2.0) * (span / cell + 2.0) > (double)(1 << 24)) cell *= 1.5;
     if (!(cell > 0)) cell = 1.0;
+    maxcell = std::max(maxcell, cell);
     const int ncx = std::max(1, (int)std::floor(ex / cell) + 1), ncy = std::max(1, (int)std::floor(ey / cell) + 1);
     const unsigned ncells = (unsigned)ncx * (unsigned)ncy;
     g.x0 = x0; g.y0 = y0; g.cell = (float)cell; g.inv_cell = (float)(1.0 / cell);
     g.ncx = ncx; g.ncy = ncy; g.n_valid = nl;
     int* cs = (int*)ws_alloc(c, sizeof(int) * (ncells + 1));
-    SrcRec* lrec = (SrcRec*)ws_alloc(c, sizeof(SrcRec) * nl);
-    {
-      unsigned* k0 = (unsigned*)ws_alloc(c, sizeof(unsigned) * nA);
-      unsigned* k1 = (unsigned*)ws_alloc(c, sizeof(unsigned) * nA);
-      int* i0 = (int*)ws_alloc(c, sizeof(int) * nA);
-      int* i1 = (int*)ws_alloc(c, sizeof(int) * nA);
+    lrec[i] = (SrcRec*)ws_alloc(c, sizeof(SrcRec) * std::max(nl, 1));
+    if (l.n > 0) {
+      unsigned* k0 = (unsigned*)ws_alloc(c, sizeof(unsigned) * l.n);
+      unsigned* k1 = (unsigned*)ws_alloc(c, sizeof(unsigned) * l.n);
+      int* i0 = (int*)ws_alloc(c, sizeof(int) * l.n);
+      int* i1 = (int*)ws_alloc(c, sizeof(int) * l.n);
       int cell_bits = 1;
       while (cell_bits < 32 && (1ull << cell_bits) <= (unsigned long long)ncells) ++cell_bits;
       const int mb = std::min(16, (32 - cell_bits) & ~1);
-      k_adj_lens_keys<<<(unsigned)std::min<long long>((nA + 255) / 256, 4096), 256, 0, st>>>(
-          xA, yA, zA, wA, nA, x0, y0, g.inv_cell, ncx, ncy, mb, k0, i0);
+      k_adj_lens_keys<<<(unsigned)std::min<long long>((l.n + 255) / 256, 4096), 256, 0, st>>>(
+          l.x, l.y, l.z, l.w, l.n, x0, y0, g.inv_cell, ncx, ncy, mb, k0, i0);
       counted(c, cudaGetLastError(), "lens keys");
       size_t tb = 0;
-      check(sort_pairs_u32(nullptr, tb, k0, k1, i0, i1, (int)nA, cell_bits + mb, st), "sort size");
+      check(sort_pairs_u32(nullptr, tb, k0, k1, i0, i1, (int)l.n, cell_bits + mb, st), "sort size");
       void* tmp = ws_alloc(c, tb);
-      check(sort_pairs_u32(tmp, tb, k0, k1, i0, i1, (int)nA, cell_bits + mb, st), "sort lenses");
-      counted(c, launch_cell_start(k1, nA, ncells, mb, cs, st), "cell start");
-      k_adj_lens_gather<<<(nl + 255) / 256, 256, 0, st>>>(i1, nl, xA, yA, zA, valA, wA, lrec);
-      counted(c, cudaGetLastError(), "lens gather");
+      check(sort_pairs_u32(tmp, tb, k0, k1, i0, i1, (int)l.n, cell_bits + mb, st), "sort lenses");
+      counted(c, launch_cell_start(k1, l.n, ncells, mb, cs, st), "cell start");
+      if (nl > 0) {
+        k_adj_lens_gather<<<(nl + 255) / 256, 256, 0, st>>>(i1, nl, l.x, l.y, l.z, l.val, l.w, lrec[i]);
+        counted(c, cudaGetLastError(), "lens gather");
+      }
+    } else {
+      check(cudaMemsetAsync(cs, 0, sizeof(int) * (ncells + 1), st), "memset cells");
     }
     g.cell_start = cs;
-    g.rec = lrec;
-    // source groups
-    float4* s0 = (float4*)ws_alloc(c, sizeof(float4) * ns);
-    float4* s1 = (float4*)ws_alloc(c, sizeof(float4) * ns);
-    int* perm = (int*)ws_alloc(c, sizeof(int) * ns);
-    {
-      unsigned long long* k0 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * nB);
-      unsigned long long* k1 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * nB);
-      int* i0 = (int*)ws_alloc(c, sizeof(int) * nB);
-      int* i1 = (int*)ws_alloc(c, sizeof(int) * nB);
-      k_adj_src_keys<<<(unsigned)std::min<long long>((nB + 255) / 256, 4096), 256, 0, st>>>(
-          xB, yB, zB, nB, make_float4(hb[8], hb[9], hb[10], hb[11]), k0, i0);
-      counted(c, cudaGetLastError(), "source keys");
-      size_t tb = 0;
-      check(sort_pairs_u64(nullptr, tb, k0, k1, i0, i1, (int)nB, st), "sort size");
-      void* tmp = ws_alloc(c, tb);
-      check(sort_pairs_u64(tmp, tb, k0, k1, i0, i1, (int)nB, st), "sort sources");
-      k_adj_src_gather<<<(ns + 255) / 256, 256, 0, st>>>(i1, ns, xB, yB, zB, e1B, e2B, wB, mB, s0, s1, perm);
-      counted(c, cudaGetLastError(), "source gather");
-    }
-    const int n_groups = (ns + BT - 1) / BT;
-    int* gstart = (int*)ws_alloc(c, sizeof(int) * (n_groups + 1));
-    int2* items0 = (int2*)ws_alloc(c, sizeof(int2) * n_groups);
-    int2* items = (int2*)ws_alloc(c, sizeof(int2) * n_groups);
-    float4* gbox = (float4*)ws_alloc(c, sizeof(float4) * n_groups);
-    k_adj_groups<<<(n_groups + 1 + 255) / 256, 256, 0, st>>>(n_groups, ns, gstart, items0);
+    g.rec = lrec[i];
+  }
+  // one sorted source set (with groups of BT) per source catalogue
+  std::vector<float4*> s0(nS), s1(nS), gbox(nS);
+  std::vector<int*> perm(nS), gstart(nS);
+  std::vector<int> ngroups(nS, 0);
+  for (int i = 0; i < nS; ++i) {
+    const AdjSrcIn& s = srcs[i];
+    const int ns = (int)hc[nL + i];
+    s0[i] = (float4*)ws_alloc(c, sizeof(float4) * std::max(ns, 1));
+    s1[i] = (float4*)ws_alloc(c, sizeof(float4) * std::max(ns, 1));
+    perm[i] = (int*)ws_alloc(c, sizeof(int) * std::max(ns, 1));
+    ngroups[i] = (ns + BT - 1) / BT;
+    gstart[i] = (int*)ws_alloc(c, sizeof(int) * (ngroups[i] + 1));
+    gbox[i] = (float4*)ws_alloc(c, sizeof(float4) * std::max(ngroups[i], 1));
+    if (ns == 0) continue;
+    const float* b = &hb[8 * (nL + i)];
+    unsigned long long* k0 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * s.n);
+    unsigned long long* k1 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * s.n);
+    int* i0 = (int*)ws_alloc(c, sizeof(int) * s.n);
+    int* i1 = (int*)ws_alloc(c, sizeof(int) * s.n);
+    k_adj_src_keys<<<(unsigned)std::min<long long>((s.n + 255) / 256, 4096), 256, 0, st>>>(
+        s.x, s.y, s.z, s.n, make_float4(b[0], b[1], b[2], b[3]), k0, i0);
+    counted(c, cudaGetLastError(), "source keys");
+    size_t tb = 0;
+    check(sort_pairs_u64(nullptr, tb, k0, k1, i0, i1, (int)s.n, st), "sort size");
+    void* tmp = ws_alloc(c, tb);
+    check(sort_pairs_u64(tmp, tb, k0, k1, i0, i1, (int)s.n, st), "sort sources");
+    k_adj_src_gather<<<(ns + 255) / 256, 256, 0, st>>>(i1, ns, s.x, s.y, s.z, s.e1, s.e2, s.w, s.m, s0[i], s1[i],
+                                                         perm[i]);
+    counted(c, cudaGetLastError(), "source gather");
+    k_adj_groups<<<(ngroups[i] + 1 + 255) / 256, 256, 0, st>>>(ngroups[i], ns, gstart[i]);
     counted(c, cudaGetLastError(), "groups");
-    counted(c, launch_group_box(s0, gstart, n_groups, gbox, st), "group box");
-    float margin = 0.f;
-    for (int i = 0; i < 2; ++i)
+    counted(c, launch_group_box(s0[i], gstart[i], ngroups[i], gbox[i], st), "group box");
+  }
+  float margin = 0.f;
+  for (int i = 0; i < ncat; ++i)
+    if (hc[i] > 0)
       margin = std::max(margin, std::fabs(hb[8 * i]) + std::fabs(hb[8 * i + 1]) + std::fabs(hb[8 * i + 2]) +
                                     std::fabs(hb[8 * i + 3]));
-    margin = (float)(1e-5 * (margin + Rd) + 1e-4 * g.cell);
-    // longest items first: cost = lenses in the rows of each group
-    {
-      TaskDesc td{};
-      td.lens_cat = 0; td.src_cat = 0; td.item_base = 0; td.lens_acc_off = -1;
-      LensDesc ld{};
-      ld.rec = s0; ld.group_start = gstart; ld.group_box = gbox; ld.n_valid = ns; ld.n_groups = n_groups;
-      TaskDesc* dt = (TaskDesc*)ws_alloc(c, sizeof(TaskDesc));
-      LensDesc* dl = (LensDesc*)ws_alloc(c, sizeof(LensDesc));
-      GridDesc* dg = (GridDesc*)ws_alloc(c, sizeof(GridDesc));
-      check(cudaMemcpyAsync(dt, &td, sizeof(td), cudaMemcpyHostToDevice, st), "H2D");
-      check(cudaMemcpyAsync(dl, &ld, sizeof(ld), cudaMemcpyHostToDevice, st), "H2D");
-      check(cudaMemcpyAsync(dg, &g, sizeof(g), cudaMemcpyHostToDevice, st), "H2D");
-      unsigned long long* ck0 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * n_groups);
-      unsigned long long* ck1 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * n_groups);
-      int* o0 = (int*)ws_alloc(c, sizeof(int) * n_groups);
-      int* o1 = (int*)ws_alloc(c, sizeof(int) * n_groups);
-      counted(c, launch_item_cost(items0, n_groups, dt, dl, dg, R, margin, ck0, o0, st), "item cost");
-      size_t tb = 0;
-      check(sort_pairs_u64_desc(nullptr, tb, ck0, ck1, o0, o1, n_groups, st), "sort size");
-      void* tmp = ws_alloc(c, tb);
-      check(sort_pairs_u64_desc(tmp, tb, ck0, ck1, o0, o1, n_groups, st), "sort items");
-      counted(c, launch_permute_items(items0, o1, n_groups, 0, 1, items, st), "permute items");
-      check(cudaStreamSynchronize(st), "sync items");  // host descriptors above go out of scope
+  margin = (float)(1e-5 * (margin + Rd) + 1e-4 * maxcell);
+
+  // tasks, their D sums and the work items (task, source group)
+  std::vector<AdjTask> at(nT);
+  std::vector<double*> dsum(nT, nullptr);
+  std::vector<int2> items;
+  std::vector<TaskDesc> tdesc(nT);
+  for (int t = 0; t < nT; ++t) {
+    const int li = tasks[t].lens, si = tasks[t].src;
+    const int ns = (int)hc[nL + si];
+    dsum[t] = (double*)ws_alloc(c, sizeof(double) * 5 * std::max(ns, 1));
+    if (ns > 0) check(cudaMemsetAsync(dsum[t], 0, sizeof(double) * 5 * ns, st), "memset D sums");
+    AdjTask& a = at[t];
+    a.grid = lgrid[li]; a.lens = lrec[li]; a.s0 = s0[si]; a.s1 = s1[si]; a.gbox = gbox[si]; a.n_src = ns;
+    a.dsum = dsum[t];
+    // item cost: the source groups play the lens-group role, the lens grid the source grid
+    tdesc[t].lens_cat = si; tdesc[t].src_cat = li; tdesc[t].item_base = 0; tdesc[t].lens_acc_off = -1;
+    if (hc[li] > 0)
+      for (int g = 0; g < ngroups[si]; ++g) items.push_back(make_int2(t, g));
+  }
+  const int n_items = (int)items.size();
+  if (n_items > 0) {
+    std::vector<LensDesc> gdesc(nS);
+    for (int i = 0; i < nS; ++i) {
+      gdesc[i].rec = s0[i]; gdesc[i].group_start = gstart[i]; gdesc[i].group_box = gbox[i];
+      gdesc[i].n_valid = (int)hc[nL + i]; gdesc[i].n_groups = ngroups[i];
     }
+    AdjTask* d_at = (AdjTask*)ws_alloc(c, sizeof(AdjTask) * nT);
+    TaskDesc* d_td = (TaskDesc*)ws_alloc(c, sizeof(TaskDesc) * nT);
+    LensDesc* d_gd = (LensDesc*)ws_alloc(c, sizeof(LensDesc) * nS);
+    GridDesc* d_lg = (GridDesc*)ws_alloc(c, sizeof(GridDesc) * nL);
+    check(cudaMemcpyAsync(d_at, at.data(), sizeof(AdjTask) * nT, cudaMemcpyHostToDevice, st), "H2D tasks");
+    check(cudaMemcpyAsync(d_td, tdesc.data(), sizeof(TaskDesc) * nT, cudaMemcpyHostToDevice, st), "H2D");
+    check(cudaMemcpyAsync(d_gd, gdesc.data(), sizeof(LensDesc) * nS, cudaMemcpyHostToDevice, st), "H2D");
+    check(cudaMemcpyAsync(d_lg, lgrid.data(), sizeof(GridDesc) * nL, cudaMemcpyHostToDevice, st), "H2D");
+    int2* items0 = (int2*)ws_alloc(c, sizeof(int2) * n_items);
+    int2* d_items = (int2*)ws_alloc(c, sizeof(int2) * n_items);
+    check(cudaMemcpyAsync(items0, items.data(), sizeof(int2) * n_items, cudaMemcpyHostToDevice, st), "H2D items");
+    // longest items first: cost = lenses in the rows of each source group
+    unsigned long long* ck0 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * n_items);
+    unsigned long long* ck1 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * n_items);
+    int* o0 = (int*)ws_alloc(c, sizeof(int) * n_items);
+    int* o1 = (int*)ws_alloc(c, sizeof(int) * n_items);
+    counted(c, launch_item_cost(items0, n_items, d_td, d_gd, d_lg, R, margin, ck0, o0, st), "item cost");
+    size_t tb = 0;
+    check(sort_pairs_u64_desc(nullptr, tb, ck0, ck1, o0, o1, n_items, st), "sort size");
+    void* tmp = ws_alloc(c, tb);
+    check(sort_pairs_u64_desc(tmp, tb, ck0, ck1, o0, o1, n_items, st), "sort items");
+    counted(c, launch_permute_items(items0, o1, n_items, 0, 1, d_items, st), "permute items");
     double* de2 = (double*)ws_alloc(c, sizeof(double) * (nb + 1));
     float* de2f = (float*)ws_alloc(c, sizeof(float) * (nb + 1));
-    float4* dcoef = (float4*)ws_alloc(c, sizeof(float4) * nb);
+    float4* dcoef = (float4*)ws_alloc(c, sizeof(float4) * coef.size());
     int* head = (int*)ws_alloc(c, sizeof(int) * 4);
     std::vector<float> e2f(nb + 1);
     for (int i = 0; i <= nb; ++i) e2f[i] = (float)e2[i];
     check(cudaMemcpyAsync(de2, e2.data(), sizeof(double) * (nb + 1), cudaMemcpyHostToDevice, st), "H2D e2");
     check(cudaMemcpyAsync(de2f, e2f.data(), sizeof(float) * (nb + 1), cudaMemcpyHostToDevice, st), "H2D e2f");
-    check(cudaMemcpyAsync(dcoef, coef.data(), sizeof(float4) * nb, cudaMemcpyHostToDevice, st), "H2D coef");
+    check(cudaMemcpyAsync(dcoef, coef.data(), sizeof(float4) * coef.size(), cudaMemcpyHostToDevice, st), "H2D coef");
     check(cudaMemsetAsync(head, 0, sizeof(int) * 4, st), "memset head");
     AdjParams P{};
-    P.lens = lrec; P.grid = g; P.s0 = s0; P.s1 = s1; P.perm = perm; P.gbox = gbox; P.items = items;
-    P.n_items = n_groups; P.n_src = ns; P.nb = nb; P.queue_head = head; P.err = (unsigned*)(head + 1);
-    P.e2 = de2; P.e2f = de2f; P.coef = dcoef; P.R = R; P.margin = margin;
+    P.tasks = d_at; P.items = d_items; P.n_items = n_items; P.nb = nb; P.queue_head = head;
+    P.err = (unsigned*)(head + 1); P.e2 = de2; P.e2f = de2f; P.coef = dcoef; P.R = R; P.margin = margin;
     if (logb) {
       const double l0 = std::log2(e2[0]), l1 = std::log2(e2[nb]);
       const double A = nb / (l1 - l0);
@@ -790,7 +930,6 @@ tpcf_status run_adjoint(tpcf_ctx* c, const float* xA, const float* yA, const flo
     } else {
       P.eps = 4e-6f;
     }
-    P.g_e1 = out_e1; P.g_e2 = out_e2; P.g_w = out_w; P.g_m = out_m;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     if (c->time_pairs) {
       check(cudaEventCreate(&ev0), "event");
@@ -809,13 +948,29 @@ tpcf_status run_adjoint(tpcf_ctx* c, const float* xA, const float* yA, const flo
     }
     unsigned herr = 0;
     check(cudaMemcpyAsync(&herr, head + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "D2H err");
-    check(cudaStreamSynchronize(st), "sync adjoint");
+    check(cudaStreamSynchronize(st), "sync adjoint");  // also keeps the host descriptors alive until here
     if (herr & kErrTimeout) throw Failure(TPCF_ERR_TIMEOUT, "a bounded device wait timed out in the adjoint kernel");
   }
-  if (out_e1 && out_e1 != g_e1) copy_out(c, g_e1, out_e1, sizeof(float) * nB);
-  if (out_e2 && out_e2 != g_e2) copy_out(c, g_e2, out_e2, sizeof(float) * nB);
-  if (out_w && out_w != g_wB) copy_out(c, g_wB, out_w, sizeof(float) * nB);
-  if (out_m && out_m != g_m) copy_out(c, g_m, out_m, sizeof(float) * nB);
+  // per source catalogue: D sums of its tasks in task order -> gradients
+  for (int i = 0; i < nS; ++i) {
+    const int ns = (int)hc[nL + i];
+    std::vector<const double*> ds;
+    for (int t = 0; t < nT; ++t)
+      if (tasks[t].src == i && hc[tasks[t].lens] > 0) ds.push_back(dsum[t]);
+    if (ns > 0 && !ds.empty()) {
+      const double** d_ds = (const double**)ws_alloc(c, sizeof(double*) * ds.size());
+      check(cudaMemcpyAsync(d_ds, ds.data(), sizeof(double*) * ds.size(), cudaMemcpyHostToDevice, st), "H2D sums");
+      k_adj_src_finish<<<(ns + 255) / 256, 256, 0, st>>>(d_ds, (int)ds.size(), ns, s0[i], s1[i], perm[i], o_e1[i],
+                                                         o_e2[i], o_w[i], o_m[i]);
+      counted(c, cudaGetLastError(), "source gradients");
+      check(cudaStreamSynchronize(st), "sync source gradients");  // ds outlives its copy
+    }
+    const AdjSrcIn& s = srcs[i];
+    if (o_e1[i] && o_e1[i] != s.g_e1) copy_out(c, s.g_e1, o_e1[i], sizeof(float) * s.n);
+    if (o_e2[i] && o_e2[i] != s.g_e2) copy_out(c, s.g_e2, o_e2[i], sizeof(float) * s.n);
+    if (o_w[i] && o_w[i] != s.g_w) copy_out(c, s.g_w, o_w[i], sizeof(float) * s.n);
+    if (o_m[i] && o_m[i] != s.g_m) copy_out(c, s.g_m, o_m[i], sizeof(float) * s.n);
+  }
   check(cudaStreamSynchronize(st), "sync outputs");
   return TPCF_OK;
 }
@@ -830,8 +985,43 @@ extern "C" tpcf_status tpcf_shear_scalar_adjoint(
     float* grad_wA, float* grad_e1B, float* grad_e2B, float* grad_wB, float* grad_mB) {
   if (!c || !bins) return TPCF_ERR_INVALID_ARG;
   try {
-    return run_adjoint(c, xA, yA, zA, valA, wA, nA, xB, yB, zB, e1B, e2B, wB, mB, nB, bins, sum_gt, sum_gx, sum_K,
-                       lens_raw, dL_dgt, dL_dgx, grad_valA, grad_wA, grad_e1B, grad_e2B, grad_wB, grad_mB);
+    std::vector<AdjLensIn> L{{nA, xA, yA, zA, valA, wA, grad_valA, grad_wA}};
+    std::vector<AdjSrcIn> S{{nB, xB, yB, zB, e1B, e2B, wB, mB, grad_e1B, grad_e2B, grad_wB, grad_mB}};
+    std::vector<AdjTaskIn> T{{0, 0, sum_gt, sum_gx, sum_K, lens_raw, dL_dgt, dL_dgx}};
+    return run_adjoint_batch(c, L, S, T, bins);
+  } catch (const Failure& f) {
+    c->err = f.msg;
+    return f.status;
+  }
+}
+
+extern "C" tpcf_status tpcf_batch_shear_scalar_adjoint(
+    tpcf_ctx* c, int32_t n_lens_cat, const tpcf_lens_catalog* lenses, tpcf_lens_grad* lens_grads,
+    int32_t n_src_cat, const tpcf_shear_catalog* sources, tpcf_shear_grad* src_grads, int32_t n_task,
+    const int32_t* task_lens, const int32_t* task_src, const tpcf_bins* bins, const tpcf_adjoint_task* task_in) {
+  if (!c || !bins || n_lens_cat < 1 || n_src_cat < 1 || n_task < 1 || !lenses || !sources || !task_lens ||
+      !task_src || !task_in)
+    return TPCF_ERR_INVALID_ARG;
+  try {
+    std::vector<AdjLensIn> L;
+    for (int i = 0; i < n_lens_cat; ++i) {
+      const tpcf_lens_catalog& l = lenses[i];
+      L.push_back({l.n, l.x, l.y, l.z, l.val, l.w, lens_grads ? lens_grads[i].val : nullptr,
+                   lens_grads ? lens_grads[i].w : nullptr});
+    }
+    std::vector<AdjSrcIn> S;
+    for (int i = 0; i < n_src_cat; ++i) {
+      const tpcf_shear_catalog& s = sources[i];
+      const tpcf_shear_grad* g = src_grads ? &src_grads[i] : nullptr;
+      S.push_back({s.n, s.x, s.y, s.z, s.e1, s.e2, s.w, s.m, g ? g->e1 : nullptr, g ? g->e2 : nullptr,
+                   g ? g->w : nullptr, g ? g->m : nullptr});
+    }
+    std::vector<AdjTaskIn> T;
+    for (int t = 0; t < n_task; ++t) {
+      const tpcf_adjoint_task& a = task_in[t];
+      T.push_back({task_lens[t], task_src[t], a.sum_gt, a.sum_gx, a.sum_K, a.lens_raw, a.dL_dgt, a.dL_dgx});
+    }
+    return run_adjoint_batch(c, L, S, T, bins);
   } catch (const Failure& f) {
     c->err = f.msg;
     return f.status;

@@ -30,6 +30,8 @@ namespace tpcf {
 
 void* ws_alloc(tpcf_ctx* c, size_t bytes) {
   if (bytes == 0) bytes = 16;
+  if (c->fail_alloc >= 0 && c->fail_alloc-- == 0)
+    throw Failure(TPCF_ERR_OOM, "device allocation failed (injected by tpcf_debug_inject)");
   if (c->next_slot == c->slots.size()) c->slots.push_back(Slot{nullptr, 0});
   Slot& s = c->slots[c->next_slot++];
   if (s.bytes < bytes) {
@@ -233,6 +235,7 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
   }
 
   // ---- stage inputs
+  Phase ph_stage("tpcf: stage inputs + grid build");
   for (auto& l : lens) {
     l.x = stage(c, l.x, l.n); l.y = stage(c, l.y, l.n); l.z = stage(c, l.z, l.n);
     l.val = stage(c, l.val, l.n); l.w = stage(c, l.w, l.n); l.patch = stage(c, l.patch, l.n);
@@ -308,6 +311,9 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
   const int qa = has_m ? 6 : 5;
   int bt = 128;
   while (bt > 32 && (size_t)nb * qa * bt * 4 > 100 * 1024) bt /= 2;
+  int tch = 4;
+  if (!sph && c->opts.group_size > 0 && c->opts.group_size <= bt) bt = c->opts.group_size;
+  if (!sph && bt == 128 && c->opts.tile_chunks == 2) tch = 2;
 
   const double Rd = bins->x_max;
   float R = (float)(Rd * (1.0 + 1e-6));
@@ -337,7 +343,9 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     g.x0 = x0; g.y0 = y0; g.cell = (float)cell; g.inv_cell = (float)(1.0 / cell);
     g.ncx = ncx; g.ncy = ncy; g.n_valid = n_valid;
     int* cs = (int*)ws_alloc(c, sizeof(int) * (ncells + 1));
-    SrcRec* rec = sph ? nullptr : (SrcRec*)ws_alloc(c, sizeof(SrcRec) * std::max(n_valid, 1));
+    const int n_chunks = std::max((n_valid + kChunk - 1) / kChunk, 1);
+    SrcPair* pairs = sph ? nullptr : (SrcPair*)ws_alloc(c, sizeof(SrcPair) * (kChunk / 2) * n_chunks);
+    ChunkMeta* cmeta = sph ? nullptr : (ChunkMeta*)ws_alloc(c, sizeof(ChunkMeta) * n_chunks);
     SrcRecS* recs = sph ? (SrcRecS*)ws_alloc(c, sizeof(SrcRecS) * std::max(n_valid, 1)) : nullptr;
     if (s.n > 0) {
       unsigned* k0 = (unsigned*)ws_alloc(c, sizeof(unsigned) * s.n);
@@ -358,13 +366,16 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
         counted(c, launch_src_gather_sph(i1, n_valid, mode, lamS[i], s.y, s.z, s.f1, s.f2, s.w, s.m, recs, st),
                 "src gather");
       else
-        counted(c, launch_src_gather(i1, n_valid, mode, s.x, s.y, s.z, s.f1, s.f2, s.w, s.m, rec, st), "src gather");
+        counted(c, launch_src_pairs(i1, n_valid, mode, s.x, s.y, s.z, s.f1, s.f2, s.w, s.m, pairs, cmeta, st),
+                "src gather");
     } else {
       check(cudaMemsetAsync(cs, 0, sizeof(int) * (ncells + 1), st), "memset cells");
     }
     g.cell_start = cs;
-    g.rec = rec;
+    g.rec = nullptr;
     g.recs = recs;
+    g.pairs = pairs;
+    g.meta = cmeta;
   }
   float margin = 0.f;
   for (int i = 0; i < ncat; ++i) {
@@ -439,6 +450,7 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
   }
 
   // ---- tasks and work items
+  Phase ph_items("tpcf: work items + pair kernel");
   std::vector<TaskDesc> tdesc(nT);
   std::vector<int2> items;
   std::vector<char> want_lens(nT, 0);
@@ -522,6 +534,8 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     // faster than 1024, and 18% with per-lens outputs, whose FP64 columns are
     // updated at every fold)
     P.flush_src = 4096;
+    P.debug_skip_tile = c->skip_tile + 1;
+    P.wait_limit = c->wait_limit;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     if (c->time_pairs) {
       check(cudaEventCreate(&ev0), "event");
@@ -533,7 +547,7 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     if (sph)
       counted(c, launch_pairs_sph(P, mode, has_m, has_z, logb, bt, c->num_sms, st, &grid), "pair kernel");
     else
-      counted(c, launch_pairs(P, mode, has_m, has_z, logb, bt, variant, c->num_sms, st, &grid), "pair kernel");
+      counted(c, launch_pairs(P, mode, has_m, has_z, logb, bt, tch, variant, c->num_sms, st, &grid), "pair kernel");
     if (c->time_pairs) {
       check(cudaEventRecord(ev1, st), "event record");
       c->pending_ev0 = ev0;
@@ -544,6 +558,7 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
        (int)has_z);
 
   // ---- per-patch sums and per-lens outputs
+  Phase ph_reduce("tpcf: patch reduction + outputs");
   std::vector<std::vector<double>> hpatch(nT);
   std::vector<double*> dpatch(nT);
   for (int t = 0; t < nT; ++t) {
@@ -733,6 +748,23 @@ tpcf_status tpcf_set_cell_size(tpcf_ctx* c, double cell_size) {
   return TPCF_OK;
 }
 
+tpcf_status tpcf_debug_inject(tpcf_ctx* c, int64_t fail_alloc, int32_t skip_tile, uint32_t wait_polls) {
+  if (!c || fail_alloc < -1 || skip_tile < -1) return TPCF_ERR_INVALID_ARG;
+  c->fail_alloc = fail_alloc;
+  c->skip_tile = skip_tile;
+  c->wait_limit = wait_polls;
+  return TPCF_OK;
+}
+
+tpcf_status tpcf_set_tile_shape(tpcf_ctx* c, int32_t group_size, int32_t tile_chunks) {
+  if (!c || (group_size != 0 && group_size != 32 && group_size != 64 && group_size != 128) ||
+      (tile_chunks != 0 && tile_chunks != 2 && tile_chunks != 4))
+    return TPCF_ERR_INVALID_ARG;
+  c->opts.group_size = group_size;
+  c->opts.tile_chunks = tile_chunks;
+  return TPCF_OK;
+}
+
 tpcf_status tpcf_set_spherical(tpcf_ctx* c, int32_t on) {
   if (!c || (on != 0 && on != 1)) return TPCF_ERR_INVALID_ARG;
   c->opts.spherical = on;
@@ -872,6 +904,31 @@ tpcf_status tpcf_batch_shear_scalar(tpcf_ctx* c, int32_t n_lens_cat, const tpcf_
     }
     std::vector<int> tl(task_lens, task_lens + n_task), ts(task_src, task_src + n_task);
     return run_batch(c, 0, L, S, tl, ts, bins, n_patch, outs);
+  } catch (const Failure& f) {
+    return fail(c, f);
+  }
+}
+
+tpcf_status tpcf_batch_scalar_scalar(tpcf_ctx* c, int32_t n_lens_cat, const tpcf_lens_catalog* lenses,
+                                     int32_t n_kappa_cat, const tpcf_kappa_catalog* kappas, int32_t n_task,
+                                     const int32_t* task_lens, const int32_t* task_kappa, const tpcf_bins* bins,
+                                     int32_t n_patch, tpcf_result* outs) {
+  if (!c || !bins || !outs || n_lens_cat < 1 || n_kappa_cat < 1 || n_task < 1 || !lenses || !kappas ||
+      !task_lens || !task_kappa)
+    return TPCF_ERR_INVALID_ARG;
+  try {
+    std::vector<LensIn> L;
+    for (int i = 0; i < n_lens_cat; ++i) {
+      const tpcf_lens_catalog& l = lenses[i];
+      L.push_back({l.n, l.x, l.y, nullptr, l.val, l.w, l.patch});
+    }
+    std::vector<SrcIn> S;
+    for (int i = 0; i < n_kappa_cat; ++i) {
+      const tpcf_kappa_catalog& k = kappas[i];
+      S.push_back({k.n, k.x, k.y, nullptr, k.kE, k.kB, k.w, nullptr});
+    }
+    std::vector<int> tl(task_lens, task_lens + n_task), ts(task_kappa, task_kappa + n_task);
+    return run_batch(c, 1, L, S, tl, ts, bins, n_patch, outs);
   } catch (const Failure& f) {
     return fail(c, f);
   }

@@ -54,7 +54,9 @@ __global__ void k_km_init_labels(int* labels, long long n, int k) {
 // x*w, y*w and w per cluster and count the reassignments.
 __global__ void k_km_assign(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ w,
                             long long n, const float2* __restrict__ cen, int k, float min_init, double sp_scale,
-                            double sw_scale, int* labels, unsigned long long* acc, unsigned long long* n_re) {
+                            double sw_scale, int* labels, unsigned long long* acc, unsigned long long* n_re,
+                            const int* state) {
+  if (state[0]) return;  // converged in an earlier pass of this batch
   extern __shared__ unsigned char sm[];
   float2* c = reinterpret_cast<float2*>(sm);
   unsigned long long* a = reinterpret_cast<unsigned long long*>(c + k);
@@ -92,14 +94,26 @@ __global__ void k_km_assign(const float* __restrict__ x, const float* __restrict
   if ((threadIdx.x & 31) == 0 && re) atomicAdd(n_re, re);
 }
 
-// Centroids from the fixed-point sums (two's-complement int64), then clear them.
-__global__ void k_km_update(unsigned long long* acc, int k, int sp, int sw, float2* cen) {
+// Centroids from the fixed-point sums (two's-complement int64), then clear
+// them; then the stopping rule of src/kmeans.f90:118-137 on the device:
+// state = {done, passes}; the run stops after a pass with no reassignment, a
+// reassigned fraction below tol, or max_iter + 1 passes.  Without state only
+// the centroids are updated.
+__global__ void k_km_update(unsigned long long* acc, int k, int sp, int sw, float2* cen, unsigned long long* n_re,
+                            long long n, float tol, int max_iter, int* state) {
+  if (state && state[0]) return;
   for (int j = threadIdx.x; j < k; j += blockDim.x) {
     const double W = ldexp((double)(long long)acc[3 * j + 2], -sw);
     const double cx = ldexp((double)(long long)acc[3 * j + 0], -sp) / W;
     const double cy = ldexp((double)(long long)acc[3 * j + 1], -sp) / W;
     cen[j] = make_float2((float)cx, (float)cy);
     acc[3 * j + 0] = acc[3 * j + 1] = acc[3 * j + 2] = 0ull;
+  }
+  if (state && threadIdx.x == 0) {
+    const int it = ++state[1];
+    const unsigned long long re = *n_re;
+    *n_re = 0ull;
+    if (re == 0ull || (float)re / (float)n < tol || it > max_iter) state[0] = 1;
   }
 }
 
@@ -381,6 +395,7 @@ tpcf_status tpcf_kmeans(tpcf_ctx* c, const float* x, const float* y, const float
       n > (1ll << 31) - 2)
     return c ? (c->err = "invalid k-means arguments", TPCF_ERR_INVALID_ARG) : TPCF_ERR_INVALID_ARG;
   try {
+    Phase ph("tpcf: k-means");
     begin_call(c);
     cudaStream_t st = c->stream;
     x = stage(c, x, n);
@@ -428,30 +443,33 @@ tpcf_status tpcf_kmeans(tpcf_ctx* c, const float* x, const float* y, const float
     const int sp = fixed_scale(n, amax * wmax), sw = fixed_scale(n, wmax);
     int* lab = (int*)ws_alloc(c, sizeof(int) * n);
     float2* dcen = (float2*)ws_alloc(c, sizeof(float2) * k);
-    unsigned long long* acc = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * (3 * k + 1));
+    unsigned long long* acc = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * (3 * k + 2));
     unsigned long long* n_re = acc + 3 * k;
+    int* state = reinterpret_cast<int*>(acc + 3 * k + 1);  // {done, passes}
     check(cudaMemcpyAsync(dcen, cen.data(), sizeof(float2) * k, cudaMemcpyHostToDevice, st), "H2D centroids");
-    check(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * (3 * k + 1), st), "memset acc");
+    check(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * (3 * k + 2), st), "memset acc");
     k_km_init_labels<<<std::min<long long>((n + 255) / 256, 4096), 256, 0, st>>>(lab, n, k);
     counted(c, cudaGetLastError(), "init labels");
     const size_t smem = sizeof(float2) * k + sizeof(unsigned long long) * 3 * k;
     check(cudaFuncSetAttribute(k_km_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attr");
     const int blocks = std::max(1, std::min<int>((int)((n + 255) / 256), c->num_sms * 4));
-    int it = 0;
-    unsigned long long hre = 0;
-    while (it <= max_iter) {
-      ++it;
-      check(cudaMemsetAsync(n_re, 0, sizeof(unsigned long long), st), "memset n_re");
-      k_km_assign<<<blocks, 256, smem, st>>>(x, y, w, n, dcen, k, diam * 10.0f, std::ldexp(1.0, sp),
-                                             std::ldexp(1.0, sw), lab, acc, n_re);
-      counted(c, cudaGetLastError(), "k-means assign");
-      k_km_update<<<1, 256, 0, st>>>(acc, k, sp, sw, dcen);
-      counted(c, cudaGetLastError(), "k-means update");
-      check(cudaMemcpyAsync(&hre, n_re, sizeof(hre), cudaMemcpyDeviceToHost, st), "D2H n_re");
+    // Lloyd passes in batches of kPassBatch with the stopping rule evaluated on
+    // the device (k_km_update): one host synchronisation per batch; passes
+    // after convergence return at once.
+    constexpr int kPassBatch = 8;
+    int hstate[2] = {0, 0};
+    for (int done_passes = 0; !hstate[0] && done_passes <= max_iter; done_passes += kPassBatch) {
+      for (int b = 0; b < kPassBatch; ++b) {
+        k_km_assign<<<blocks, 256, smem, st>>>(x, y, w, n, dcen, k, diam * 10.0f, std::ldexp(1.0, sp),
+                                               std::ldexp(1.0, sw), lab, acc, n_re, state);
+        counted(c, cudaGetLastError(), "k-means assign");
+        k_km_update<<<1, 256, 0, st>>>(acc, k, sp, sw, dcen, n_re, n, reassign_tol, max_iter, state);
+        counted(c, cudaGetLastError(), "k-means update");
+      }
+      check(cudaMemcpyAsync(hstate, state, sizeof(hstate), cudaMemcpyDeviceToHost, st), "D2H k-means state");
       check(cudaStreamSynchronize(st), "sync k-means");
-      if (hre == 0) break;
-      if ((float)hre / (float)n < reassign_tol) break;
     }
+    const int it = hstate[1];
     copy_out(c, labels_out, lab, sizeof(int) * n);
     if (centroids_out) copy_out(c, centroids_out, dcen, sizeof(float2) * k);
     check(cudaStreamSynchronize(st), "sync outputs");
@@ -470,6 +488,7 @@ tpcf_status tpcf_bootstrap(tpcf_ctx* c, const double* patch_sums, int32_t n_task
       !g_x || !(supersampling > 0))
     return c ? (c->err = "invalid bootstrap arguments", TPCF_ERR_INVALID_ARG) : TPCF_ERR_INVALID_ARG;
   try {
+    Phase ph_nvtx("tpcf: bootstrap");
     begin_call(c);
     cudaStream_t st = c->stream;
     const double* ps = stage(c, patch_sums, (int64_t)n_task * n_patch * 6 * n_bin);
@@ -521,6 +540,7 @@ tpcf_status tpcf_kmeans_equal(tpcf_ctx* c, const float* x, const float* y, const
       !(weight_scaling >= 0) || !(weight_tol >= 0) || (random_init && n < k))
     return c ? (c->err = "invalid k-means arguments", TPCF_ERR_INVALID_ARG) : TPCF_ERR_INVALID_ARG;
   try {
+    Phase ph_nvtx("tpcf: equal-weight k-means");
     begin_call(c);
     cudaStream_t st = c->stream;
     x = stage(c, x, n);
@@ -626,7 +646,7 @@ tpcf_status tpcf_kmeans_equal(tpcf_ctx* c, const float* x, const float* y, const
       counted(c, cudaGetLastError(), "k-means sweep");
       k_km_sums<<<sblocks, 256, ssm, st>>>(x, y, w, lab, n, k, std::ldexp(1.0, sp), std::ldexp(1.0, sw), acc);
       counted(c, cudaGetLastError(), "k-means sums");
-      k_km_update<<<1, 256, 0, st>>>(acc, k, sp, sw, dcen);
+      k_km_update<<<1, 256, 0, st>>>(acc, k, sp, sw, dcen, nullptr, n, 0.f, 0, nullptr);
       counted(c, cudaGetLastError(), "k-means update");
       check(cudaMemcpyAsync(&hre, n_re, sizeof(hre), cudaMemcpyDeviceToHost, st), "D2H n_re");
       check(cudaMemcpyAsync(hw.data(), wfix, sizeof(long long) * k, cudaMemcpyDeviceToHost, st), "D2H weights");

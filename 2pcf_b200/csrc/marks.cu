@@ -218,6 +218,7 @@ extern "C" tpcf_status tpcf_xi_from_marks(tpcf_ctx* c, int32_t n_field, const tp
     if (m.n > 0 && (!m.w || !m.xi_E || !m.xi_B || !m.K)) return TPCF_ERR_INVALID_ARG;
   }
   try {
+    Phase ph_nvtx("tpcf: marks");
     begin_call(c);
     cudaStream_t st = c->stream;
     std::vector<MarksField> hf(n_field);
@@ -334,6 +335,7 @@ extern "C" tpcf_status tpcf_marks_bootstrap(tpcf_ctx* c, int32_t n_field, const 
   if (!unit) n_units = n_lens;
   if (n_units < 1) return TPCF_ERR_INVALID_ARG;
   try {
+    Phase ph_nvtx("tpcf: marks bootstrap");
     begin_call(c);
     cudaStream_t st = c->stream;
     std::vector<MarksField> hf(n_field);

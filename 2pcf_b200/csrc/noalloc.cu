@@ -158,13 +158,19 @@ tpcf_status run_noalloc(tpcf_ctx* c, const float* xA, const float* yA, const flo
   const double span = std::max((double)ex, (double)ey);
   if (!c->opts.use_grid) cell = span * 2.0 + 1.0;
   while ((span / cell + 2.0) * (span / cell + 2.0) > (double)(1 << 24)) cell *= 1.5;
+  // The cell table (4 bytes per cell) may take at most an eighth of the
+  // scratch: a small theta_max over a wide field gets coarser cells here than
+  // in the regular entry points.  The results do not depend on the cell side.
+  while ((span / cell + 2.0) * (span / cell + 2.0) * 4.0 > (double)(kScratchBytes / 8)) cell *= 1.5;
   if (!(cell > 0)) cell = 1.0;
   const int ncx = std::max(1, (int)std::floor(ex / cell) + 1), ncy = std::max(1, (int)std::floor(ey / cell) + 1);
   const unsigned ncells = (unsigned)ncx * (unsigned)ncy;
   g.x0 = x0; g.y0 = y0; g.cell = (float)cell; g.inv_cell = (float)(1.0 / cell);
   g.ncx = ncx; g.ncy = ncy; g.n_valid = ns_valid;
   int* cs = (int*)cv.take(sizeof(int) * (ncells + 1));
-  SrcRec* rec = (SrcRec*)cv.take(sizeof(SrcRec) * std::max(ns_valid, 1));
+  const int n_chunks = std::max((ns_valid + kChunk - 1) / kChunk, 1);
+  SrcPair* pairs = (SrcPair*)cv.take(sizeof(SrcPair) * (kChunk / 2) * n_chunks);
+  ChunkMeta* cmeta = (ChunkMeta*)cv.take(sizeof(ChunkMeta) * n_chunks);
   if (nB > 0) {
     unsigned* k0 = (unsigned*)cv.take(sizeof(unsigned) * nB);
     unsigned* k1 = (unsigned*)cv.take(sizeof(unsigned) * nB);
@@ -180,12 +186,13 @@ tpcf_status run_noalloc(tpcf_ctx* c, const float* xA, const float* yA, const flo
     counted(c, launch_src_keys(xB, yB, zB, nB, x0, y0, g.inv_cell, ncx, ncy, mb, k0, i0, st), "src keys");
     check(sort_pairs_u32(tmp, tb, k0, k1, i0, i1, (int)nB, end_bit, st), "sort sources");
     counted(c, launch_cell_start(k1, nB, ncells, mb, cs, st), "cell start");
-    counted(c, launch_src_gather(i1, ns_valid, 0, xB, yB, zB, e1B, e2B, wB, mB, rec, st), "src gather");
+    counted(c, launch_src_pairs(i1, ns_valid, 0, xB, yB, zB, e1B, e2B, wB, mB, pairs, cmeta, st), "src gather");
   } else {
     check(cudaMemsetAsync(cs, 0, sizeof(int) * (ncells + 1), st), "memset cells");
   }
   g.cell_start = cs;
-  g.rec = rec;
+  g.pairs = pairs;
+  g.meta = cmeta;
   float margin = 0.f;
   for (int i = 0; i < 2; ++i)
     if (hcnt[i] > 0)
@@ -258,7 +265,7 @@ tpcf_status run_noalloc(tpcf_ctx* c, const float* xA, const float* yA, const flo
       P.eps = 4e-6f;
     }
     int grid = 0;
-    counted(c, launch_pairs(P, 0, has_m, has_z, logb, bt, 0, c->num_sms, st, &grid), "pair kernel");
+    counted(c, launch_pairs(P, 0, has_m, has_z, logb, bt, 4, 0, c->num_sms, st, &grid), "pair kernel");
     counted(c, launch_patch_reduce(item_sums, 0, pgroups, 1, nb, psum, st), "patch reduce");
   } else {
     check(cudaMemsetAsync(psum, 0, sizeof(double) * kQ * nb, st), "clear sums");

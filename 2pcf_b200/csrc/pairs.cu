@@ -4,21 +4,25 @@
 // (src/tpcf.f90:261-363) and scalar_kappa_tpcf (src/tpcf.f90:451-535).
 //
 // One thread block = one lens group (one lens per thread) against every source
-// row the group's theta_max neighbourhood touches.  Sources stream through
-// shared memory in tiles moved by the bulk-copy engine (cp.async.bulk +
-// mbarrier, double-buffered); every thread reads the same source (broadcast)
-// and bins the pair into its own FP32 histogram column in shared memory.  The
-// histogram is laid out [bin][quantity][thread], so a warp's 32 read-modify-
-// writes fall in 32 distinct banks whatever bins the lanes pick, and no
-// atomics are needed.  Every ~4096 sources the FP32 columns are folded into
-// FP64: per block (times the lens factors val*w or w) and, when per-lens output
-// is requested, per lens.
+// row the group's theta_max neighbourhood touches.  The source grid is stored
+// in HBM as 32-source sub-chunks already in the pair-interleaved form of the
+// packed FP32 instructions (SrcPair), each with its bounding box and sums
+// (ChunkMeta), so a tile is copied into shared memory by the bulk-copy engine
+// (cp.async.bulk + mbarrier) and used as it lands.  Tiles rotate through
+// several buffers and each warp consumes them at its own pace: a buffer is
+// refilled by the last warp to finish with it, so warps drift apart by up to
+// all-but-one buffers and there is no block-wide barrier per tile.  Every
+// thread reads the same source (broadcast) and bins its pairs into its own
+// FP32 histogram column in shared memory, laid out [bin][quantity][thread] so
+// that a warp's 32 read-modify-writes fall in 32 distinct banks whatever bins
+// the lanes pick, with no atomics.  Every ~4096 sources each warp folds its 32
+// columns into its own FP64 sums (times the lens factors val*w or w) and, when
+// per-lens output is requested, into per-lens FP64 columns.
 //
 // Most pairs never touch the histogram: per 32-source sub-chunk a lens whose
 // bin range (from the sub-chunk's box) is one bin or two adjacent bins sums in
 // registers and adds once per sub-chunk.  Those register paths run on sm_100's
-// packed FP32 instructions (two pairs per instruction), for which each copied
-// tile is rewritten in place into pair-interleaved SrcPair blocks.
+// packed FP32 instructions (two pairs per instruction).
 //
 // Binning.  The pair arithmetic is FP32.  For log spacing the bin comes from
 // t = log2(d2)*A + B (one MUFU.LG2 and one FFMA): bin = floor(t).  When t is
@@ -51,23 +55,28 @@ constexpr int kSingleUnroll = TPCF_SINGLE_UNROLL;  // and of the single-bin path
 // gives the compiler a register budget (up to 170 per thread) that it spends
 // on overlapping the packed FP32 chains of the register paths.
 constexpr int kPairMinBlocks = 3;
-// Coordinate of the null source that pads an odd sub-chunk in SrcPair form:
-// its d2 (~2e36) stays finite in FP32 and its weight and values are zero.
+// Coordinate of the null source that pads the last sub-chunk of a grid: its
+// d2 (~2e36) stays finite in FP32 and its weight and values are zero.
 constexpr float kNullPos = 1.0e18f;
+// Source bytes in flight per block: NBUF = kSrcRing / (TCH KB) tile buffers of
+// TCH sub-chunks (1 KB each) plus their ChunkMeta.
+constexpr int kSrcRing = 16384;
 
 // ------------------------------------------------------- shared-memory map --
 struct PairSmem {
-  size_t tiles, hist, bsum, e2s, fvw, fw, e2f, span0, span1, tpref, subbox, subsum, mbar, misc, total;
+  size_t tiles, meta, hist, bsum, e2s, fvw, fw, e2f, span0, span1, mbar, cnt, last, misc, total;
 };
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
-// bt here is the number of histogram columns (threads x lenses per thread).
-__host__ __device__ inline PairSmem pair_smem_layout(int nb, int qa, int bt) {
+// bt here is the number of histogram columns (threads), tch the sub-chunks per tile.
+__host__ __device__ inline PairSmem pair_smem_layout(int nb, int qa, int bt, int tch) {
+  const int nbuf = kSrcRing / (tch * kChunk * (int)sizeof(SrcRec));
   PairSmem s;
   size_t o = 0;
-  s.tiles = o; o += 2 * kTile * sizeof(SrcRec);
+  s.tiles = o; o += (size_t)nbuf * tch * kChunk * sizeof(SrcRec);
+  s.meta = o;  o += (size_t)nbuf * tch * sizeof(ChunkMeta);
   s.hist = o;  o += (size_t)nb * qa * bt * sizeof(float);
   o = align_up(o, 16);
-  s.bsum = o;  o += (size_t)kQ * nb * sizeof(double);
+  s.bsum = o;  o += (size_t)(bt / 32) * kQ * nb * sizeof(double);
   s.e2s = o;   o += (size_t)(nb + 1) * sizeof(double);
   s.fvw = o;   o += (size_t)bt * sizeof(double);
   s.fw = o;    o += (size_t)bt * sizeof(double);
@@ -75,11 +84,10 @@ __host__ __device__ inline PairSmem pair_smem_layout(int nb, int qa, int bt) {
   o = align_up(o, 16);
   s.span0 = o; o += kMaxRows * sizeof(int);
   s.span1 = o; o += kMaxRows * sizeof(int);
-  s.tpref = o; o += (kMaxRows + 1) * sizeof(int);
-  o = align_up(o, 16);
-  s.subbox = o; o += (kTile / 32) * sizeof(float4);
-  s.subsum = o; o += (kTile / 32) * sizeof(float4);
-  s.mbar = o;  o += 2 * sizeof(uint64_t);
+  o = align_up(o, 8);
+  s.mbar = o;  o += (size_t)nbuf * sizeof(uint64_t);
+  s.cnt = o;   o += (size_t)nbuf * sizeof(int);
+  s.last = o;  o += (size_t)nbuf * sizeof(int);
   s.misc = o;  o += 16;
   s.total = align_up(o, 128);
   return s;
@@ -132,8 +140,8 @@ __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const floa
 }
 
 // ---------------------------------------------------- sub-chunk fast paths --
-// A tile is cut into sub-chunks of 32 consecutive sources (spatially compact:
-// sources are sorted by cell, then Morton order inside the cell).  For each
+// Each sub-chunk holds 32 consecutive sources of the cell-sorted order
+// (spatially compact: cells in rows, Morton order inside a cell).  For each
 // lens and sub-chunk the bin range of the chunk's bounding box is bounded
 // conservatively (guard band eps on both ends):
 //   0  no pair of the chunk is in range        -> nothing to do
@@ -142,10 +150,16 @@ __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const floa
 //                                                  one edge, FP64 re-binning
 //                                                  inside its guard band
 //   3  anything else                           -> per-pair binning (do_pair)
-// A z cut (z_A > z_B skips the pair) is a per-pair mask inside all paths.
 // The path is chosen per warp (the largest class of its lanes), so lanes never
 // diverge inside a source loop.  Every pair still lands in its canonical bin:
 // in classes 1 and 2 the box bounds prove which bins are possible.
+//
+// A row span of the grid starts and ends anywhere inside a sub-chunk; its
+// first and last sub-chunks are "partial": only the sources [lo, hi) of the
+// sub-chunk belong to the span (the others belong to other cells and are
+// either out of reach or counted through another span).  The box of a partial
+// sub-chunk covers all its sources, so the bounds stay conservative; its pairs
+// carry a per-pair mask, as does a z cut (z_A > z_B skips the pair).
 
 // Per-pair quantities shared by the register paths, for the two sources of
 // one SrcPair at once (packed FP32: one instruction per operation for both
@@ -195,30 +209,49 @@ __device__ __forceinline__ void src_of(const SrcPair* __restrict__ S, int j, flo
   b = make_float4(f[8], f[10], f[12], 0.f);
 }
 
+// Which of the two sources of pair block k take part: the z cut and, in a
+// partial sub-chunk, the span [lo, hi).
+template <bool HAS_Z, bool PART>
+__device__ __forceinline__ float2 pair_mask(const SrcPair* __restrict__ S, int k, float lz, int lo, int hi, bool& a0,
+                                            bool& a1) {
+  a0 = true;
+  a1 = true;
+  if (HAS_Z) {
+    const float4 zn = S[k].zn;
+    a0 = lz <= zn.x;  // src/tpcf.f90:322 (a NaN z of a null source fails)
+    a1 = lz <= zn.y;
+  }
+  if (PART) {
+    a0 = a0 && (2 * k >= lo);
+    a1 = a1 && (2 * k + 1 < hi);
+  }
+  return make_float2(a0 ? 1.f : 0.f, a1 ? 1.f : 0.f);
+}
+
 // The register paths share the sub-chunk sums ss = {sum p, sum q, sum w,
-// sum K} over its sources: without a z cut, the w and K sums of every lens
-// are these (and, for scalar-scalar, so are the g_t and g_x sums, r = 1), so
-// they are not accumulated per pair.
+// sum K} over its sources: for a whole sub-chunk without a z cut, the w and K
+// sums of every lens are these (and, for scalar-scalar, so are the g_t and
+// g_x sums, r = 1), so they are not accumulated per pair.
 //
-// Class 1: every pair of the chunk is in bin `blo`.  With a z cut, a pair
-// with z_A > z_B (src/tpcf.f90:322) adds nothing.  An odd count is padded by
-// a null source (zero weight and values, far away, NaN z): it adds zero to
-// every sum, and the pair count is cnt (or the z-mask sum, which excludes it).
-template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int NC, int QA>
-__device__ __forceinline__ void chunk_single(const SrcPair* __restrict__ S, int cnt, const LensP& L, float lz,
+// Class 1: every pair of the chunk is in bin `blo`.  A masked pair (z cut,
+// outside the span) adds nothing.
+template <int MODE, bool HAS_M, bool HAS_Z, bool PART, bool LOGB, int NC, int QA>
+__device__ __forceinline__ void chunk_single(const SrcPair* __restrict__ S, int lo, int hi, const LensP& L, float lz,
                                              int cls, int blo, float* __restrict__ hcol, const float4 ss) {
-  constexpr bool LI = !HAS_Z;  // lens-independent sums come from ss
+  constexpr bool MK = HAS_Z || PART;
+  constexpr bool LI = !MK;  // lens-independent sums come from ss
   float2 sgt = dup2(0.f), sgx = dup2(0.f), sw = dup2(0.f), sdw = dup2(0.f), sk = dup2(0.f), sn = dup2(0.f);
-  const int np = (cnt + 1) >> 1;
+  const int k0 = PART ? (lo >> 1) : 0;
+  const int k1 = PART ? ((hi + 1) >> 1) : kChunk / 2;
 #pragma unroll kSingleUnroll
-  for (int k = 0; k < np; ++k) {
+  for (int k = k0; k < k1; ++k) {
     const float4 xy = S[k].xy, pq = S[k].pq, wk = S[k].wk;
     float2 d2, d, r, X, Y;
     pair_terms2<MODE, LOGB>(L, xy, pq, d2, d, r, X, Y);
     float2 w = lo2(wk), K = hi2(wk);
-    if (HAS_Z) {
-      const float4 zn = S[k].zn;
-      const float2 zm = make_float2(lz <= zn.x ? 1.f : 0.f, lz <= zn.y ? 1.f : 0.f);
+    if (MK) {
+      bool a0, a1;
+      const float2 zm = pair_mask<HAS_Z, PART>(S, k, lz, lo, hi, a0, a1);
       r = mul2(r, zm);
       w = mul2(w, zm);
       if (MODE == 0 && HAS_M) K = mul2(K, zm);
@@ -238,7 +271,7 @@ __device__ __forceinline__ void chunk_single(const SrcPair* __restrict__ S, int 
   acc[QGX] = (LI && MODE == 1) ? ss.y : sum2(sgx);
   acc[QW] = LI ? ss.z : sum2(sw);
   acc[QDW] = sum2(sdw);
-  acc[QN] = HAS_Z ? sum2(sn) : (float)cnt;
+  acc[QN] = MK ? sum2(sn) : (float)kChunk;
   if (MODE == 0 && HAS_M) acc[QK] = LI ? ss.w : sum2(sk);
   hist_add<QA, NC>(hcol, blo, acc);
 }
@@ -247,11 +280,12 @@ __device__ __forceinline__ void chunk_single(const SrcPair* __restrict__ S, int 
 // dropped); the edge between them is e2f[blo+1].  Sums over all pairs (s*)
 // and over the upper side (h*: the pair's r, w, K selected by d2 >= E, the
 // count as an integer); the lower side is their difference.
-template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int NC, int QA>
-__device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int cnt, const LensP& L, float lx, float ly,
-                                           float lz, int cls, int blo, float* __restrict__ hcol, const BinCtx& C,
-                                           const float4 ss) {
-  constexpr bool LI = !HAS_Z;
+template <int MODE, bool HAS_M, bool HAS_Z, bool PART, bool LOGB, int NC, int QA>
+__device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int lo, int hi, const LensP& L, float lx,
+                                           float ly, float lz, int cls, int blo, float* __restrict__ hcol,
+                                           const BinCtx& C, const float4 ss) {
+  constexpr bool MK = HAS_Z || PART;
+  constexpr bool LI = !MK;
   float2 sgt = dup2(0.f), sgx = dup2(0.f), sw = dup2(0.f), sdw = dup2(0.f), sk = dup2(0.f), sn = dup2(0.f);
   float2 hgt = dup2(0.f), hgx = dup2(0.f), hw = dup2(0.f), hdw = dup2(0.f), hk = dup2(0.f);
   int hn = 0;
@@ -260,27 +294,30 @@ __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int cn
   const float gE = (cls == 2) ? E * C.eps_rel : 0.f;
   const float2 nE = dup2(-E);
   bool near = false;  // some pair lies within the guard band of E
-  const int np = (cnt + 1) >> 1;
+  const int k0 = PART ? (lo >> 1) : 0;
+  const int k1 = PART ? ((hi + 1) >> 1) : kChunk / 2;
 #pragma unroll kDualUnroll
-  for (int k = 0; k < np; ++k) {
+  for (int k = k0; k < k1; ++k) {
     const float4 xy = S[k].xy, pq = S[k].pq, wk = S[k].wk;
     float2 d2, d, r, X, Y;
     pair_terms2<MODE, LOGB>(L, xy, pq, d2, d, r, X, Y);
     const float2 dE = add2(d2, nE);
-    near |= fabsf(dE.x) <= gE;
-    near |= fabsf(dE.y) <= gE;
     float2 w = lo2(wk), K = hi2(wk);
     bool u0 = d2.x >= E, u1 = d2.y >= E;
-    if (HAS_Z) {
-      const float4 zn = S[k].zn;
-      const bool z0 = lz <= zn.x, z1 = lz <= zn.y;
-      const float2 zm = make_float2(z0 ? 1.f : 0.f, z1 ? 1.f : 0.f);
+    if (MK) {
+      bool a0, a1;
+      const float2 zm = pair_mask<HAS_Z, PART>(S, k, lz, lo, hi, a0, a1);
       r = mul2(r, zm);
       w = mul2(w, zm);
       if (MODE == 0 && HAS_M) K = mul2(K, zm);
       sn = add2(sn, zm);
-      u0 = u0 && z0;
-      u1 = u1 && z1;
+      u0 = u0 && a0;
+      u1 = u1 && a1;
+      near |= a0 && fabsf(dE.x) <= gE;
+      near |= a1 && fabsf(dE.y) <= gE;
+    } else {
+      near |= fabsf(dE.x) <= gE;
+      near |= fabsf(dE.y) <= gE;
     }
     // products folded into the sums: one packed FFMA per quantity and side
     if (!(LI && MODE == 1)) {
@@ -304,43 +341,37 @@ __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int cn
     // rare (a pair within a relative 4e-6 of the edge): this lane's register
     // sums are dropped and the sub-chunk is binned pair by pair, each pair by
     // the canonical rule
-    for (int j = 0; j < cnt; ++j) {
+    for (int j = lo; j < hi; ++j) {
       float4 a, b;
       src_of(S, j, a, b);
       do_pair<MODE, HAS_M, HAS_Z, LOGB, NC, QA>(lx, ly, lz, a, b, hcol, C);
     }
     return;
   }
-  float tot[QA], hi[QA];
+  float tot[QA], up[QA];
   tot[QGT] = (LI && MODE == 1) ? ss.x : sum2(sgt);
   tot[QGX] = (LI && MODE == 1) ? ss.y : sum2(sgx);
   tot[QW] = LI ? ss.z : sum2(sw);
   tot[QDW] = sum2(sdw);
-  tot[QN] = HAS_Z ? sum2(sn) : (float)cnt;
-  hi[QGT] = sum2(hgt);
-  hi[QGX] = sum2(hgx);
-  hi[QW] = sum2(hw);
-  hi[QDW] = sum2(hdw);
-  hi[QN] = (float)hn;
+  tot[QN] = MK ? sum2(sn) : (float)kChunk;
+  up[QGT] = sum2(hgt);
+  up[QGX] = sum2(hgx);
+  up[QW] = sum2(hw);
+  up[QDW] = sum2(hdw);
+  up[QN] = (float)hn;
   if (MODE == 0 && HAS_M) {
     tot[QK] = LI ? ss.w : sum2(sk);
-    hi[QK] = sum2(hk);
-  }
-  if (!HAS_Z && (cnt & 1)) {
-    // the null source that pads an odd count counts on the upper side when
-    // its (huge) distance reaches E; it adds zero to every other sum
-    const float dxn = kNullPos - lx, dyn = kNullPos - ly;
-    if (fmaf(dyn, dyn, dxn * dxn) >= E) hi[QN] -= 1.f;
+    up[QK] = sum2(hk);
   }
   if (cls == 1) {
     hist_add<QA, NC>(hcol, blo, tot);
     return;
   }
-  float lo[QA];
+  float dn[QA];
 #pragma unroll
-  for (int q = 0; q < QA; ++q) lo[q] = tot[q] - hi[q];
-  if (blo >= 0) hist_add<QA, NC>(hcol, blo, lo);
-  if (blo + 1 < C.nb) hist_add<QA, NC>(hcol, blo + 1, hi);
+  for (int q = 0; q < QA; ++q) dn[q] = tot[q] - up[q];
+  if (blo >= 0) hist_add<QA, NC>(hcol, blo, dn);
+  if (blo + 1 < C.nb) hist_add<QA, NC>(hcol, blo + 1, up);
 }
 
 #ifdef TPCF_MODE_STATS
@@ -351,18 +382,105 @@ extern "C" int tpcf_debug_mode_stats(unsigned long long* out) {
 }
 #endif
 
+// ------------------------------------------------------------- tile ring --
+// Position of a tile in the row chunk of a work item: row `row` of the chunk,
+// tile `kk` within that row's span of sub-chunks.
+struct TilePos {
+  int row, kk;
+};
+// Sub-chunks [c0, c0 + n) of the tile at p, and the span bounds inside its
+// first and last sub-chunk.
+struct TileGeom {
+  int c0, n, lo0, hiL;
+};
+template <int TCH>
+__device__ __forceinline__ TileGeom tile_geom(const int* span0, const int* span1, TilePos p) {
+  const int s = span0[p.row], e = span1[p.row];
+  const int cA = s >> 5, cB = (e + kChunk - 1) >> 5;
+  TileGeom t;
+  t.c0 = cA + p.kk * TCH;
+  t.n = min(TCH, cB - t.c0);
+  t.lo0 = p.kk == 0 ? (s & (kChunk - 1)) : 0;
+  t.hiL = (t.c0 + t.n == cB && (e & (kChunk - 1))) ? (e & (kChunk - 1)) : kChunk;
+  return t;
+}
+template <int TCH>
+__device__ __forceinline__ int row_tiles(const int* span0, const int* span1, int r) {
+  const int s = span0[r], e = span1[r];
+  if (e <= s) return 0;
+  const int nc = ((e + kChunk - 1) >> 5) - (s >> 5);
+  return (nc + TCH - 1) / TCH;
+}
+// The next tile in row order (row == nr: none left).
+template <int TCH>
+__device__ __forceinline__ void next_tile(const int* span0, const int* span1, int nr, TilePos& p) {
+  if (++p.kk < row_tiles<TCH>(span0, span1, p.row)) return;
+  p.kk = 0;
+  for (++p.row; p.row < nr && row_tiles<TCH>(span0, span1, p.row) == 0; ++p.row) {
+  }
+}
+template <int TCH>
+__device__ __forceinline__ TilePos first_tile(const int* span0, const int* span1, int nr) {
+  TilePos p{0, 0};
+  while (p.row < nr && row_tiles<TCH>(span0, span1, p.row) == 0) ++p.row;
+  return p;
+}
+
+// Fold this warp's 32 histogram columns into its FP64 sums (times the lens
+// factors val*w or w) and, when lens_col is set, each lane's per-lens FP64
+// column; then clear the columns.  Called by all lanes of the warp.
+template <int QA, int BT>
+__device__ __forceinline__ void warp_fold(const float* hist, float* hcol, double* wsum, const double* fvw,
+                                          const double* fw, int nb, double* lens_col, size_t lens_stride, bool first,
+                                          int warp, int lane) {
+  __syncwarp();
+  if (lens_col) {
+    for (int q = 0; q < kQ; ++q) {
+      const int qa = (q == QK && QA == 5) ? QW : q;
+      for (int b = 0; b < nb; ++b) {
+        const double v = (double)hcol[(b * QA + qa) * BT];
+        double* p = lens_col + (size_t)(q * nb + b) * lens_stride;
+        *p = first ? v : *p + v;
+      }
+    }
+  }
+  const int cb = warp * 32;
+  for (int e = lane; e < kQ * nb; e += 32) {
+    const int q = e / nb, b = e - q * nb;
+    if (q == QK && QA == 5) continue;  // K == w: copied from the w row at item end
+    const float* row = hist + (b * QA + q) * BT + cb;
+    double s = 0.0;
+    if (q == QN) {
+      for (int l = 0; l < 32; ++l) s += (double)row[(l + lane) & 31];
+    } else {
+      const double* f = ((q == QGT || q == QGX) ? fvw : fw) + cb;
+      for (int l = 0; l < 32; ++l) {
+        const int c = (l + lane) & 31;
+        s = fma((double)row[c], f[c], s);
+      }
+    }
+    wsum[e] += s;
+  }
+  __syncwarp();
+  for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
+}
+
+// ------------------------------------------------------------ pair kernel --
 // PATH 0: sub-chunk classification with the register paths (default);
-// PATH 1: per-pair binning for every pair (kept for A/B measurement).
-template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int PATH>
+// PATH 1: per-pair binning for every pair in reach (for A/B measurement).
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int TCH, int PATH>
 __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P) {
   constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
   constexpr int NW = BT / 32;
+  constexpr int NBUF = kSrcRing / (TCH * kChunk * (int)sizeof(SrcRec));
+  static_assert(NBUF >= 2, "at least two tile buffers");
   const int nb = P.nb;
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   extern __shared__ __align__(128) unsigned char smem[];
-  const PairSmem L = pair_smem_layout(nb, QA, BT);
-  SrcRec* tiles = reinterpret_cast<SrcRec*>(smem + L.tiles);
+  const PairSmem L = pair_smem_layout(nb, QA, BT, TCH);
+  SrcPair* tiles = reinterpret_cast<SrcPair*>(smem + L.tiles);
+  ChunkMeta* meta = reinterpret_cast<ChunkMeta*>(smem + L.meta);
   float* hist = reinterpret_cast<float*>(smem + L.hist);
   double* bsum = reinterpret_cast<double*>(smem + L.bsum);
   double* e2s = reinterpret_cast<double*>(smem + L.e2s);
@@ -371,15 +489,19 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
   float* e2f = reinterpret_cast<float*>(smem + L.e2f);
   int* span0 = reinterpret_cast<int*>(smem + L.span0);
   int* span1 = reinterpret_cast<int*>(smem + L.span1);
-  int* tpref = reinterpret_cast<int*>(smem + L.tpref);
-  float4* subbox = reinterpret_cast<float4*>(smem + L.subbox);
-  float4* subsum = reinterpret_cast<float4*>(smem + L.subsum);
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + L.mbar);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.mbar);
+  int* cnt = reinterpret_cast<int*>(smem + L.cnt);    // warps done with the buffer's current tile
+  int* last = reinterpret_cast<int*>(smem + L.last);  // ring index of the buffer's last issued tile
   int* sh_item = reinterpret_cast<int*>(smem + L.misc);
+  volatile int* sh_abort = sh_item + 1;  // set by a warp whose bounded wait ran out
 
   if (tid == 0) {
-    mbar_init(&mbar[0], 1);
-    mbar_init(&mbar[1], 1);
+    for (int b = 0; b < NBUF; ++b) {
+      mbar_init(&full[b], 1);
+      cnt[b] = 0;
+      last[b] = -1;
+    }
+    *sh_abort = 0;
     mbar_fence_init();
   }
   for (int i = tid; i <= nb; i += BT) {
@@ -394,10 +516,11 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
   C.lo_g = e2f[0] * (1.f - P.eps);
   C.hi_g = e2f[nb] * (1.f + P.eps);
 
-  uint32_t phase = 0u;   // bit k: parity awaited next on buffer k
-  uint32_t tcount = 0u;  // tiles processed by this block so far
-  bool timed_out = false;
+  const uint32_t wait_limit = P.wait_limit ? P.wait_limit : kWaitPolls;
+  int tbase = 0;  // ring index of the first tile of the current row chunk
   float* __restrict__ hcol = hist + tid;
+  double* wsum = bsum + (size_t)warp * kQ * nb;
+  const int flush_src = P.flush_src > 0 ? P.flush_src : 4096;
 #ifdef TPCF_MODE_STATS
   __shared__ unsigned long long sh_stats[8];
   if (tid < 8) sh_stats[tid] = 0ull;
@@ -435,190 +558,140 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
     fvw[tid] = vw;
     fw[tid] = w;
     const size_t lens_stride = (size_t)LD.n_valid;
-    for (int e = tid; e < kQ * nb; e += BT) bsum[e] = 0.0;
+    for (int e = lane; e < kQ * nb; e += 32) wsum[e] = 0.0;
     bool first_flush = true;
     int since_flush = 0;
-    const int flush_src = P.flush_src > 0 ? P.flush_src : 4096;
     const float4 box = LD.group_box[g];
     int cy0, cy1;
     row_range(G, box, P.R, P.margin, cy0, cy1);
 
     for (int c0 = cy0; c0 <= cy1; c0 += kMaxRows) {
       const int nr = min(kMaxRows, cy1 - c0 + 1);
-      __syncthreads();
+      __syncthreads();  // every warp is done with the previous chunk's tiles and spans
       for (int r = tid; r < nr; r += BT) {
         const int2 sp = row_span(G, box, P.R, P.margin, c0 + r);
         span0[r] = sp.x;
         span1[r] = sp.y > sp.x ? sp.y : sp.x;
       }
       __syncthreads();
-      if (tid == 0) {
-        int acc = 0;
-        for (int r = 0; r < nr; ++r) {
-          tpref[r] = acc;
-          acc += (span1[r] - span0[r] + kTile - 1) / kTile;
+      // Ring of NBUF buffers: the tile with ring index t lives in buffer
+      // t % NBUF and completes phase (t / NBUF) & 1 of its full barrier.
+      auto issue = [&](TilePos p, int t) {
+        if (t + 1 == P.debug_skip_tile) return;  // fault injection (tests): this tile never lands
+        const TileGeom tg = tile_geom<TCH>(span0, span1, p);
+        const int b = t % NBUF;
+        const uint32_t nbytes = (uint32_t)tg.n * (kChunk * sizeof(SrcRec) + sizeof(ChunkMeta));
+        mbar_arrive_tx(&full[b], nbytes);
+        bulk_g2s(tiles + (size_t)b * TCH * (kChunk / 2), G.pairs + (size_t)tg.c0 * (kChunk / 2),
+                 (uint32_t)tg.n * kChunk * sizeof(SrcRec), &full[b]);
+        bulk_g2s(meta + (size_t)b * TCH, G.meta + tg.c0, (uint32_t)tg.n * sizeof(ChunkMeta), &full[b]);
+        last[b] = t;
+      };
+      if (tid == 0 && !*sh_abort) {
+        TilePos p = first_tile<TCH>(span0, span1, nr);
+        for (int k = 0; k < NBUF && p.row < nr; ++k) {
+          issue(p, tbase + k);
+          next_tile<TCH>(span0, span1, nr, p);
         }
-        tpref[nr] = acc;
       }
-      __syncthreads();
-      const int ntiles = tpref[nr];
-      int rc = 0, ri = 0;
-      if (tid == 0 && ntiles > 0) {
-        while (tpref[ri + 1] <= 0) ++ri;
-        const int s0 = span0[ri];
-        const int n0 = min(kTile, span1[ri] - s0);
-        const int bb = tcount & 1u;
-        mbar_arrive_tx(&mbar[bb], (uint32_t)(n0 * sizeof(SrcRec)));
-        bulk_g2s(tiles + bb * kTile, G.rec + s0, (uint32_t)(n0 * sizeof(SrcRec)), &mbar[bb]);
-      }
-      for (int k = 0; k < ntiles; ++k) {
-        if (tid == 0 && k + 1 < ntiles) {
-          while (tpref[ri + 1] <= k + 1) ++ri;
-          const int s1 = span0[ri] + (k + 1 - tpref[ri]) * kTile;
-          const int n1 = min(kTile, span1[ri] - s1);
-          const int bb = (tcount + k + 1) & 1u;
-          mbar_arrive_tx(&mbar[bb], (uint32_t)(n1 * sizeof(SrcRec)));
-          bulk_g2s(tiles + bb * kTile, G.rec + s1, (uint32_t)(n1 * sizeof(SrcRec)), &mbar[bb]);
-        }
-        while (tpref[rc + 1] <= k) ++rc;
-        const int s = span0[rc] + (k - tpref[rc]) * kTile;
-        const int n = min(kTile, span1[rc] - s);
-        const int bb = (tcount + k) & 1u;
-        const bool ok = mbar_wait_bounded(&mbar[bb], (phase >> bb) & 1u);
-        phase ^= (1u << bb);
-        // not __restrict__: the sub-chunk pass rewrites these bytes in place
-        const SrcRec* S = tiles + bb * kTile;
-        const int nsub = (n + 31) >> 5;
-        if (PATH == 0 && ok) {
-          // One warp per 32-source sub-chunk: its bounding box and sums, and the
-          // rewrite of its records into SrcPair form (lanes 2k, 2k+1 trade
-          // halves with one shuffle round; each lane stores only the 32 bytes
-          // of its own record, so the rewrite in place needs no ordering
-          // between lanes).  Slots past the tile's end get the null source.
-          for (int sc = warp; sc < nsub; sc += NW) {
-            const int j = sc * 32 + lane;
-            float4 a = make_float4(kNullPos, kNullPos, 0.f, 0.f);
-            float4 b = make_float4(0.f, 0.f, __int_as_float(0x7fc00000), 0.f);
-            float mnx = INFINITY, mny = INFINITY, mxx = -INFINITY, mxy = -INFINITY;
-            if (j < n) {
-              a = S[j].a;
-              b = S[j].b;
-              mnx = mxx = a.x;
-              mny = mxy = a.y;
-            }
-            const bool odd = lane & 1;
-            // even lane keeps {x, y, p, q} of both, odd lane {w, K, z}
-            const float r0 = __shfl_xor_sync(0xffffffffu, odd ? a.x : b.x, 1);
-            const float r1 = __shfl_xor_sync(0xffffffffu, odd ? a.y : b.y, 1);
-            const float r2 = __shfl_xor_sync(0xffffffffu, odd ? a.z : b.z, 1);
-            const float r3 = __shfl_xor_sync(0xffffffffu, a.w, 1);
-            float4* dst = reinterpret_cast<float4*>(tiles + bb * kTile + j);
-            if (!odd) {
-              dst[0] = make_float4(a.x, r0, a.y, r1);
-              dst[1] = make_float4(a.z, r2, a.w, r3);
-            } else {
-              dst[0] = make_float4(r0, b.x, r1, b.y);
-              dst[1] = make_float4(r2, b.z, 0.f, 0.f);
-            }
-            fence_proxy_async_smem();  // before the bulk copy that later refills this buffer
-#pragma unroll
-            for (int o = 16; o; o >>= 1) {
-              mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
-              mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
-              mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
-              mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
-            }
-            // sums of p, q, w, K over the sub-chunk (lens-independent)
-            float s0 = a.z, s1 = a.w, s2 = b.x, s3 = b.y;
-#pragma unroll
-            for (int o = 16; o; o >>= 1) {
-              s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-              s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-              s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-              s3 += __shfl_xor_sync(0xffffffffu, s3, o);
-            }
-            if (lane == 0) {
-              subbox[sc] = make_float4(mnx, mny, mxx, mxy);
-              subsum[sc] = make_float4(s0, s1, s2, s3);
-            }
-          }
-        }
-        if (__syncthreads_or(!ok)) timed_out = true;
-        if (!timed_out) {
-          if (PATH == 0) {
-            for (int sc = 0; sc < nsub; ++sc) {
-              const int base = sc * 32;
-              const int cnt = min(32, n - base);
-              int blo = 0;
-              const int cls = act ? classify<LOGB, HAS_Z, true>(lx, ly, subbox[sc], C, blo) : 0;
-              const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)cls);
+      TilePos p = first_tile<TCH>(span0, span1, nr);
+      int k = 0;
+      for (; p.row < nr; ++k) {
+        const int t = tbase + k;
+        const int b = t % NBUF;
+        const TileGeom tg = tile_geom<TCH>(span0, span1, p);
+        bool ok = !*sh_abort && mbar_wait_bounded(&full[b], (uint32_t)(t / NBUF) & 1u, wait_limit);
+        ok = __all_sync(0xffffffffu, ok);
+        if (!ok) *sh_abort = 1;  // stop consuming and issuing; the copies in flight are drained at exit
+        if (ok) {
+          const SrcPair* Tb = tiles + (size_t)b * TCH * (kChunk / 2);
+          const ChunkMeta* Mb = meta + (size_t)b * TCH;
+          for (int j = 0; j < tg.n; ++j) {
+            const int lo = j == 0 ? tg.lo0 : 0;
+            const int hi = j == tg.n - 1 ? tg.hiL : kChunk;
+            const bool part = lo > 0 || hi < kChunk;
+            const SrcPair* __restrict__ Sc = Tb + j * (kChunk / 2);
+            const float4 cbox = Mb[j].box;
+            int blo = 0;
+            int cls = act ? classify<LOGB, HAS_Z, true>(lx, ly, cbox, C, blo) : 0;
+            if (PATH == 1 && cls) cls = 3;
+            const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)cls);
 #ifdef TPCF_MODE_STATS
-              {
-                const unsigned nact = __popc(__ballot_sync(0xffffffffu, act));
-                if (lane == 0) {
-                  atomicAdd(&sh_stats[m], 1ull);
-                  atomicAdd(&sh_stats[4 + m], (unsigned long long)(cnt * nact));
-                }
+            {
+              const unsigned nact = __popc(__ballot_sync(0xffffffffu, act));
+              if (lane == 0) {
+                atomicAdd(&sh_stats[m], 1ull);
+                atomicAdd(&sh_stats[4 + m], (unsigned long long)((hi - lo) * nact));
               }
+            }
 #endif
-              if (m == 0) continue;
-              const SrcPair* __restrict__ Sc = reinterpret_cast<const SrcPair*>(S + base);
-              if (m == 1) {
-                chunk_single<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(Sc, cnt, LP, lz, cls, blo, hcol, subsum[sc]);
-              } else if (m == 2) {
-                chunk_dual<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(Sc, cnt, LP, lx, ly, lz, cls, blo, hcol, C, subsum[sc]);
-              } else if (act) {
-                for (int k = 0; k < (cnt >> 1); ++k) {
-                  const SrcPair sp = Sc[k];
-                  do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(
-                      lx, ly, lz, make_float4(sp.xy.x, sp.xy.z, sp.pq.x, sp.pq.z),
-                      make_float4(sp.wk.x, sp.wk.z, sp.zn.x, 0.f), hcol, C);
-                  do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(
-                      lx, ly, lz, make_float4(sp.xy.y, sp.xy.w, sp.pq.y, sp.pq.w),
-                      make_float4(sp.wk.y, sp.wk.w, sp.zn.y, 0.f), hcol, C);
-                }
-                if (cnt & 1) {
-                  float4 a, b;
-                  src_of(Sc, cnt - 1, a, b);
-                  do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, a, b, hcol, C);
-                }
+            if (m == 0) continue;
+            if (m == 1) {
+              const float4 ss = Mb[j].sum;
+              if (part)
+                chunk_single<MODE, HAS_M, HAS_Z, true, LOGB, BT, QA>(Sc, lo, hi, LP, lz, cls, blo, hcol, ss);
+              else
+                chunk_single<MODE, HAS_M, HAS_Z, false, LOGB, BT, QA>(Sc, 0, kChunk, LP, lz, cls, blo, hcol, ss);
+            } else if (m == 2) {
+              const float4 ss = Mb[j].sum;
+              if (part)
+                chunk_dual<MODE, HAS_M, HAS_Z, true, LOGB, BT, QA>(Sc, lo, hi, LP, lx, ly, lz, cls, blo, hcol, C,
+                                                                    ss);
+              else
+                chunk_dual<MODE, HAS_M, HAS_Z, false, LOGB, BT, QA>(Sc, 0, kChunk, LP, lx, ly, lz, cls, blo, hcol,
+                                                                     C, ss);
+            } else if (act) {
+              for (int jj = lo; jj < hi; ++jj) {
+                float4 a, bb;
+                src_of(Sc, jj, a, bb);
+                do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, a, bb, hcol, C);
               }
             }
-          } else if (act) {
-            int j = 0;
-            for (; j + 4 <= n; j += 4) {
-              float4 a[4], b[4];
-#pragma unroll
-              for (int u = 0; u < 4; ++u) {
-                a[u] = S[j + u].a;
-                b[u] = S[j + u].b;
-              }
-#pragma unroll
-              for (int u = 0; u < 4; ++u) do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, a[u], b[u], hcol, C);
-            }
-            for (; j < n; ++j) do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, S[j].a, S[j].b, hcol, C);
           }
         }
-        since_flush += n;
+        since_flush += tg.n * kChunk - tg.lo0 - (kChunk - tg.hiL);
+        // Release the buffer; the last warp to do so refills it with the tile
+        // NBUF places ahead.
+        __syncwarp();
+        if (lane == 0) {
+          __threadfence_block();
+          if (atomicAdd(&cnt[b], 1) == NW - 1) {
+            cnt[b] = 0;
+            __threadfence_block();
+            TilePos q = p;
+            for (int a = 0; a < NBUF && q.row < nr; ++a) next_tile<TCH>(span0, span1, nr, q);
+            if (q.row < nr && !*sh_abort) issue(q, t + NBUF);
+          }
+        }
         if (since_flush >= flush_src) {
-          flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
+          warp_fold<QA, BT>(hist, hcol, wsum, fvw, fw, nb, lens_col, lens_stride, first_flush, warp, lane);
           first_flush = false;
           since_flush = 0;
         }
-        __syncthreads();
+        next_tile<TCH>(span0, span1, nr, p);
       }
-      tcount += (uint32_t)ntiles;
+      tbase += k;
     }
-    flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
+    warp_fold<QA, BT>(hist, hcol, wsum, fvw, fw, nb, lens_col, lens_stride, first_flush, warp, lane);
     __syncthreads();
     double* out = P.item_sums + (size_t)(T.item_base + g) * kQ * nb;
     for (int e = tid; e < kQ * nb; e += BT) {
-      const int q = e / nb;
-      out[e] = (q == QK && QA == 5) ? bsum[e - (QK - QW) * nb] : bsum[e];
+      const int src = (e / nb == QK && QA == 5) ? e - (QK - QW) * nb : e;
+      double s = 0.0;
+      for (int ww = 0; ww < NW; ++ww) s += bsum[(size_t)ww * kQ * nb + src];
+      out[e] = s;
     }
     __syncthreads();
   }
-  if (timed_out && tid == 0) atomicOr(P.err, kErrTimeout);
+  // After a timed-out wait no tile was consumed or issued any more; wait
+  // (bounded) for the last copy issued into each buffer before the block's
+  // shared memory is released.
+  __syncthreads();
+  if (tid == 0 && *sh_abort) {
+    for (int b = 0; b < NBUF; ++b)
+      if (last[b] >= 0) mbar_wait_bounded(&full[b], (uint32_t)(last[b] / NBUF) & 1u, wait_limit);
+    atomicOr(P.err, kErrTimeout);
+  }
 #ifdef TPCF_MODE_STATS
   __syncthreads();
   if (tid < 8) atomicAdd(&g_mode_stats[tid], sh_stats[tid]);
@@ -764,25 +837,70 @@ __global__ void k_cell_start(const unsigned* __restrict__ keys, long long n, uns
   cell_start[c] = (int)lo;
 }
 
-// Packed, cell-sorted source records.  mode 0 shear, 1 scalar-scalar.
-__global__ void k_src_gather(const int* __restrict__ idx, int n_valid, int mode, const float* __restrict__ x,
-                             const float* __restrict__ y, const float* __restrict__ z,
-                             const float* __restrict__ f1, const float* __restrict__ f2,
-                             const float* __restrict__ w, const float* __restrict__ m, SrcRec* rec) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n_valid) return;
-  const int i = idx[s];
-  const float wi = w[i];
-  SrcRec r;
-  if (mode == 0) {
-    r.a = make_float4(x[i], y[i], -(f1[i] * wi), -(f2[i] * wi));
-    const float mi = m ? m[i] : 0.f;
-    r.b = make_float4(wi, wi * (1.0f + mi), z ? z[i] : 0.f, 0.f);
-  } else {
-    r.a = make_float4(x[i], y[i], f1[i] * wi, f2[i] * wi);
-    r.b = make_float4(wi, wi, 0.f, 0.f);
+// Cell-sorted source records in sub-chunk form: one warp per 32-source
+// sub-chunk gathers its sources (sorted positions 32c .. 32c+31, null sources
+// past n_valid) into 16 SrcPair blocks -- sources 2k and 2k+1 with their
+// fields interleaved, {x0 x1 y0 y1}{p0 p1 q0 q1}{w0 w1 K0 K1}{z0 z1 0 0} --
+// and writes the sub-chunk's bounding box and {p, q, w, K} sums.  Shear:
+// p = -e1 w, q = -e2 w, K = (1+m) w; scalar-scalar (mode 1): p = kE w,
+// q = kB w, K = w.
+__global__ void k_src_pairs(const int* __restrict__ idx, int n_valid, int n_chunks, int mode,
+                            const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+                            const float* __restrict__ f1, const float* __restrict__ f2,
+                            const float* __restrict__ w, const float* __restrict__ m, SrcPair* pairs,
+                            ChunkMeta* meta) {
+  const int c = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= n_chunks) return;  // whole warps
+  const int s = c * kChunk + lane;
+  float4 a = make_float4(kNullPos, kNullPos, 0.f, 0.f);
+  float4 b = make_float4(0.f, 0.f, __int_as_float(0x7fc00000), 0.f);
+  float mnx = INFINITY, mny = INFINITY, mxx = -INFINITY, mxy = -INFINITY;
+  if (s < n_valid) {
+    const int i = idx[s];
+    const float wi = w[i];
+    if (mode == 0) {
+      a = make_float4(x[i], y[i], -(f1[i] * wi), -(f2[i] * wi));
+      const float mi = m ? m[i] : 0.f;
+      b = make_float4(wi, wi * (1.0f + mi), z ? z[i] : 0.f, 0.f);
+    } else {
+      a = make_float4(x[i], y[i], f1[i] * wi, f2[i] * wi);
+      b = make_float4(wi, wi, 0.f, 0.f);
+    }
+    mnx = mxx = a.x;
+    mny = mxy = a.y;
   }
-  rec[s] = r;
+  const bool odd = lane & 1;
+  // lanes 2k, 2k+1 trade halves: the even lane writes {x, y, p, q} of both,
+  // the odd lane {w, K, z}
+  const float r0 = __shfl_xor_sync(0xffffffffu, odd ? a.x : b.x, 1);
+  const float r1 = __shfl_xor_sync(0xffffffffu, odd ? a.y : b.y, 1);
+  const float r2 = __shfl_xor_sync(0xffffffffu, odd ? a.z : b.z, 1);
+  const float r3 = __shfl_xor_sync(0xffffffffu, a.w, 1);
+  float4* dst = reinterpret_cast<float4*>(pairs + (size_t)c * (kChunk / 2) + (lane >> 1));
+  if (!odd) {
+    dst[0] = make_float4(a.x, r0, a.y, r1);
+    dst[1] = make_float4(a.z, r2, a.w, r3);
+  } else {
+    dst[2] = make_float4(r0, b.x, r1, b.y);
+    dst[3] = make_float4(r2, b.z, 0.f, 0.f);
+  }
+  float s0 = a.z, s1 = a.w, s2 = b.x, s3 = b.y;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+    mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+    mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+    mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    s3 += __shfl_xor_sync(0xffffffffu, s3, o);
+  }
+  if (lane == 0) {
+    meta[c].box = make_float4(mnx, mny, mxx, mxy);
+    meta[c].sum = make_float4(s0, s1, s2, s3);
+  }
 }
 
 __device__ __forceinline__ unsigned spread16(unsigned v) {
@@ -976,11 +1094,11 @@ __global__ void k_lens_outputs(const double* __restrict__ acc, const float4* __r
 }
 
 // --------------------------------------------------------- host launchers --
-template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int PATH>
+template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int TCH, int PATH>
 static cudaError_t launch_pairs_t(const PairParams& P, int num_sms, cudaStream_t st, int* grid_out) {
   constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
-  const size_t smem = pair_smem_layout(P.nb, QA, BT).total;
-  auto kern = k_pairs<MODE, HAS_M, HAS_Z, LOGB, BT, PATH>;
+  const size_t smem = pair_smem_layout(P.nb, QA, BT, TCH).total;
+  auto kern = k_pairs<MODE, HAS_M, HAS_Z, LOGB, BT, TCH, PATH>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
@@ -995,36 +1113,40 @@ static cudaError_t launch_pairs_t(const PairParams& P, int num_sms, cudaStream_t
   return cudaGetLastError();
 }
 
+// Tile shapes: bt lenses per block (128, 64 or 32) and tch sub-chunks per
+// source tile (4: four 1.1 KB tiles in flight; 2: eight 0.5 KB tiles, only
+// with 128 lenses).  variant 1 forces per-pair binning (A/B measurement).
 template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB>
-static cudaError_t launch_pairs_bt(const PairParams& P, int bt, int variant, int num_sms, cudaStream_t st,
+static cudaError_t launch_pairs_bt(const PairParams& P, int bt, int tch, int variant, int num_sms, cudaStream_t st,
                                    int* grid) {
   if (bt == 128) {
-    if (variant == 1 && MODE == 0 && !HAS_M && !HAS_Z && LOGB)  // per-pair path, for A/B measurement
-      return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 1>(P, num_sms, st, grid);
-    return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 0>(P, num_sms, st, grid);
+    if (variant == 1 && MODE == 0 && !HAS_M && !HAS_Z && LOGB)
+      return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 4, 1>(P, num_sms, st, grid);
+    if (tch == 2) return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 2, 0>(P, num_sms, st, grid);
+    return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 4, 0>(P, num_sms, st, grid);
   }
-  if (bt == 64) return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64, 0>(P, num_sms, st, grid);
-  return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 32, 0>(P, num_sms, st, grid);
+  if (bt == 64) return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64, 4, 0>(P, num_sms, st, grid);
+  return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 32, 4, 0>(P, num_sms, st, grid);
 }
 
-size_t pair_smem_bytes(int nb, int qa, int bt) { return pair_smem_layout(nb, qa, bt).total; }
+size_t pair_smem_bytes(int nb, int qa, int bt, int tch) { return pair_smem_layout(nb, qa, bt, tch).total; }
 
-cudaError_t launch_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int variant,
-                         int num_sms, cudaStream_t st, int* grid) {
+cudaError_t launch_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int tch,
+                         int variant, int num_sms, cudaStream_t st, int* grid) {
   if (mode == 1) {
-    return logb ? launch_pairs_bt<1, false, false, true>(P, bt, variant, num_sms, st, grid)
-                : launch_pairs_bt<1, false, false, false>(P, bt, variant, num_sms, st, grid);
+    return logb ? launch_pairs_bt<1, false, false, true>(P, bt, tch, variant, num_sms, st, grid)
+                : launch_pairs_bt<1, false, false, false>(P, bt, tch, variant, num_sms, st, grid);
   }
   if (has_m) {
-    if (has_z) return logb ? launch_pairs_bt<0, true, true, true>(P, bt, variant, num_sms, st, grid)
-                           : launch_pairs_bt<0, true, true, false>(P, bt, variant, num_sms, st, grid);
-    return logb ? launch_pairs_bt<0, true, false, true>(P, bt, variant, num_sms, st, grid)
-                : launch_pairs_bt<0, true, false, false>(P, bt, variant, num_sms, st, grid);
+    if (has_z) return logb ? launch_pairs_bt<0, true, true, true>(P, bt, tch, variant, num_sms, st, grid)
+                           : launch_pairs_bt<0, true, true, false>(P, bt, tch, variant, num_sms, st, grid);
+    return logb ? launch_pairs_bt<0, true, false, true>(P, bt, tch, variant, num_sms, st, grid)
+                : launch_pairs_bt<0, true, false, false>(P, bt, tch, variant, num_sms, st, grid);
   }
-  if (has_z) return logb ? launch_pairs_bt<0, false, true, true>(P, bt, variant, num_sms, st, grid)
-                         : launch_pairs_bt<0, false, true, false>(P, bt, variant, num_sms, st, grid);
-  return logb ? launch_pairs_bt<0, false, false, true>(P, bt, variant, num_sms, st, grid)
-              : launch_pairs_bt<0, false, false, false>(P, bt, variant, num_sms, st, grid);
+  if (has_z) return logb ? launch_pairs_bt<0, false, true, true>(P, bt, tch, variant, num_sms, st, grid)
+                         : launch_pairs_bt<0, false, true, false>(P, bt, tch, variant, num_sms, st, grid);
+  return logb ? launch_pairs_bt<0, false, false, true>(P, bt, tch, variant, num_sms, st, grid)
+              : launch_pairs_bt<0, false, false, false>(P, bt, tch, variant, num_sms, st, grid);
 }
 
 static inline unsigned gdim(long long n, int b) {
@@ -1058,10 +1180,13 @@ cudaError_t launch_cell_start(const unsigned* keys, long long n, unsigned ncells
   k_cell_start<<<(ncells + 1 + 255) / 256, 256, 0, st>>>(keys, n, ncells, mb, cell_start);
   return cudaGetLastError();
 }
-cudaError_t launch_src_gather(const int* idx, int n_valid, int mode, const float* x, const float* y, const float* z,
-                              const float* f1, const float* f2, const float* w, const float* m, SrcRec* rec,
-                              cudaStream_t st) {
-  if (n_valid > 0) k_src_gather<<<(n_valid + 255) / 256, 256, 0, st>>>(idx, n_valid, mode, x, y, z, f1, f2, w, m, rec);
+cudaError_t launch_src_pairs(const int* idx, int n_valid, int mode, const float* x, const float* y, const float* z,
+                             const float* f1, const float* f2, const float* w, const float* m, SrcPair* pairs,
+                             ChunkMeta* meta, cudaStream_t st) {
+  const int n_chunks = (n_valid + kChunk - 1) / kChunk;
+  if (n_chunks > 0)
+    k_src_pairs<<<(n_chunks + 7) / 8, 256, 0, st>>>(idx, n_valid, n_chunks, mode, x, y, z, f1, f2, w, m, pairs,
+                                                     meta);
   return cudaGetLastError();
 }
 cudaError_t launch_lens_keys(const float* x, const float* y, const float* z, const float* w, const int* patch,

@@ -2,6 +2,7 @@
 // host helpers shared by the C-ABI translation units.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <string>
@@ -16,6 +17,16 @@ struct Failure {
   tpcf_status status;
   std::string msg;
   Failure(tpcf_status s, std::string m) : status(s), msg(std::move(m)) {}
+};
+
+// NVTX range over one phase of a call (grid build, pair kernel, reduction,
+// k-means, resampling), visible in Nsight timelines; free when no tool is
+// attached.
+struct Phase {
+  explicit Phase(const char* name) { nvtxRangePushA(name); }
+  ~Phase() { nvtxRangePop(); }
+  Phase(const Phase&) = delete;
+  Phase& operator=(const Phase&) = delete;
 };
 
 // Grow-only device buffer.  A call takes slots in a fixed order, so repeated
@@ -44,6 +55,12 @@ struct tpcf_ctx {
   double last_pair_ms = 0.0;
   double last_call_ms = 0.0;
   int64_t last_pairs = 0;
+  // fault injection for tests (tpcf_debug_inject): the fail_alloc-th workspace
+  // allocation from now fails with TPCF_ERR_OOM (-1: none); pair-kernel tile
+  // whose copy is never issued (-1: none) and the poll limit of the waits
+  int64_t fail_alloc = -1;
+  int32_t skip_tile = -1;
+  uint32_t wait_limit = 0;
 };
 
 namespace tpcf {

@@ -2,8 +2,9 @@
 // host orchestration of libtpcf_b200.
 //
 // Layout in HBM (one call, many catalogues):
-//   source catalogue  -> cell grid: records sorted by row-major cell index
-//                        (SrcRec, 32 B each), cell_start[ncx*ncy+1]
+//   source catalogue  -> cell grid: records sorted by row-major cell index,
+//                        stored as 32-source sub-chunks (SrcPair form, 1 KB)
+//                        with one ChunkMeta each, cell_start[ncx*ncy+1]
 //   lens catalogue    -> lenses sorted by (patch, Morton code); groups of at
 //                        most BT consecutive lenses that never straddle a
 //                        patch; one bounding box per group
@@ -42,9 +43,9 @@ struct __align__(16) SrcRec {
 // Two consecutive sources (2k, 2k+1) of a 32-source sub-chunk in shared
 // memory with their fields interleaved, so that one 64-bit register pair holds
 // a field of both sources: the operand form of the sm_100 packed FP32
-// instructions (add/mul/fma .f32x2).  The planar pair kernel rewrites each
-// tile in place into this form (the same 64 bytes as the two SrcRec), after
-// the bulk copy.  p, q, w, K, z are a.z, a.w, b.x, b.y, b.z of SrcRec.
+// instructions (add/mul/fma .f32x2).  The planar source grid is built in this
+// form (the same 64 bytes as the two SrcRec).  p, q, w, K, z are a.z, a.w,
+// b.x, b.y, b.z of SrcRec.
 struct __align__(16) SrcPair {
   float4 xy;  // x0 x1 y0 y1
   float4 pq;  // p0 p1 q0 q1
@@ -53,6 +54,16 @@ struct __align__(16) SrcPair {
 };
 static_assert(sizeof(SrcPair) == 2 * sizeof(SrcRec), "a SrcPair rewrites two SrcRec in place");
 static_assert(kTile % 32 == 0, "tiles hold whole 32-source sub-chunks");
+
+// Sources per sub-chunk.  A planar source grid stores its cell-sorted records
+// as consecutive sub-chunks of 32 (16 SrcPair, 1 KB each; the last one padded
+// with null sources), aligned to multiples of 32 in the sorted order, with one
+// ChunkMeta per sub-chunk, so that the pair kernel copies them unchanged.
+constexpr int kChunk = 32;
+struct __align__(16) ChunkMeta {
+  float4 box;  // {xmin, ymin, xmax, ymax} of its real sources
+  float4 sum;  // {sum p, sum q, sum w, sum K} over its real sources
+};
 
 // A source on the sphere: the unit vector u of (lambda, phi) split into FP32
 // hi + lo parts (u = hi + lo to ~2^-48), so that u_B - u_A keeps full FP32
@@ -73,8 +84,10 @@ struct GridDesc {
   int n_valid;
   int pad;
   const int* cell_start;  // [ncx*ncy + 1]
-  const SrcRec* rec;      // [n_valid], sorted by cell (planar)
+  const SrcRec* rec;      // [n_valid], sorted by cell (lens grid of the adjoint)
   const SrcRecS* recs;    // [n_valid], sorted by cell (sphere), else nullptr
+  const SrcPair* pairs;   // planar sources: [ceil(n_valid/32) * 16] in sub-chunk form
+  const ChunkMeta* meta;  // [ceil(n_valid/32)]
 };
 
 struct LensDesc {
@@ -113,6 +126,11 @@ struct PairParams {
   float binA, binB;         // log spacing: t = lg2(d2)*binA + binB
   float eps;                // guard band half-width in t units (log) or relative (generic)
   int flush_src;            // FP32 histogram -> FP64 after this many sources (0: 4096)
+  // Fault injection for tests only (0 in every product call): 1 + the ring
+  // index of a source tile whose bulk copy is never issued, so that the waits
+  // on it run out (0: none), and the poll limit of the waits (0: kWaitPolls).
+  int debug_skip_tile;
+  unsigned wait_limit;
 };
 
 }  // namespace tpcf

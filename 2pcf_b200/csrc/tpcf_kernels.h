@@ -8,11 +8,11 @@
 
 namespace tpcf {
 
-size_t pair_smem_bytes(int nb, int qa, int bt);
-// bt = lenses per group; `variant` picks the thread shape of the main
-// configuration (0: bt threads x 1 lens; others: see pairs.cu).
-cudaError_t launch_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int variant,
-                         int num_sms, cudaStream_t st, int* grid);
+size_t pair_smem_bytes(int nb, int qa, int bt, int tch);
+// bt = lenses per group (threads per block), tch = 32-source sub-chunks per
+// source tile; variant 1 bins every pair one by one (A/B measurement).
+cudaError_t launch_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int tch,
+                         int variant, int num_sms, cudaStream_t st, int* grid);
 
 // Spherical pair kernel (sphere.cu); P.grids[*].recs and P.lenses[*].pos set.
 cudaError_t launch_pairs_sph(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int num_sms,
@@ -41,9 +41,11 @@ cudaError_t launch_src_keys(const float* x, const float* y, const float* z, long
                             float inv_cell, int ncx, int ncy, int mb, unsigned* keys, int* idx, cudaStream_t st);
 cudaError_t launch_cell_start(const unsigned* keys, long long n, unsigned ncells, int mb, int* cell_start,
                               cudaStream_t st);
-cudaError_t launch_src_gather(const int* idx, int n_valid, int mode, const float* x, const float* y,
-                              const float* z, const float* f1, const float* f2, const float* w, const float* m,
-                              SrcRec* rec, cudaStream_t st);
+// Planar source grid records in sub-chunk form: pairs [ceil(n_valid/32)*16],
+// meta [ceil(n_valid/32)].
+cudaError_t launch_src_pairs(const int* idx, int n_valid, int mode, const float* x, const float* y,
+                             const float* z, const float* f1, const float* f2, const float* w, const float* m,
+                             SrcPair* pairs, ChunkMeta* meta, cudaStream_t st);
 cudaError_t launch_lens_keys(const float* x, const float* y, const float* z, const float* w, const int* patch,
                              long long n, float4 box, unsigned long long* keys, int* idx, cudaStream_t st);
 cudaError_t launch_lens_gather(const int* idx, int n_valid, const float* x, const float* y, const float* z,

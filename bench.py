@@ -166,11 +166,12 @@ def cpu_baseline(w, seconds, nthreads, steps=1, warmup=0):
             "seconds": tot_t}
 
 
-def adjoint_timing(w, ctx, bins, pairs, pair_ms, stream):
+def adjoint_timing(w, ctx, bins, pairs, pair_ms, stream, peak):
     """The batched + adjoint form: xi_t and xi_x of all 25 tasks from one
     differentiable forward launch (raw per-lens sums kept on the device), a
-    chi^2 against a seeded target, and the backward (one adjoint call per
-    task), against the plain batched forward.  One untimed pass first."""
+    chi^2 against a seeded target, and the backward (one batched adjoint
+    launch over all tasks), against the plain batched forward.  One untimed
+    pass first."""
     import torch
     ag = importlib.import_module("2pcf_b200.autograd")
     d = lambda a: torch.from_numpy(a).cuda()
@@ -194,13 +195,18 @@ def adjoint_timing(w, ctx, bins, pairs, pair_ms, stream):
         e2.record(stream)
         torch.cuda.synchronize()
         t_fwd, t_all = e0.elapsed_time(e1), e0.elapsed_time(e2)
+        adj_ms = ctx.stats()["pair_kernel_ms"]   # the adjoint kernel of the backward launch
         del leaves, xi_t, loss
+    ach = pairs * ADJ_FLOP_PER_PAIR / (adj_ms * 1e-3) / 1e12
     return {"value": pairs / (t_all * 1e-3) / 1e9, "unit": UNIT,
             "forward_ms": t_fwd, "forward_plus_adjoint_ms": t_all,
             "fwd_adj_over_plain_fwd": t_all / pair_ms,
             "fwd_adj_over_fwd": t_all / t_fwd,
-            "note": "25 tasks in one differentiable forward launch (raw per-lens sums kept on the device), "
-                    "backward = one tpcf_shear_scalar_adjoint per task; plain forward = the pair kernel of "
+            "adjoint_roofline": {"bound": "fp32", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                                 "frac": ach / peak, "kernel": "k_adj", "kernel_ms": adj_ms,
+                                 "flop_per_pair": ADJ_FLOP_PER_PAIR},
+            "note": "25 tasks in one differentiable forward launch (raw per-lens sums kept on the device) and "
+                    "one backward launch (tpcf_batch_shear_scalar_adjoint); plain forward = the pair kernel of "
                     "the batched step"}
 
 
@@ -350,6 +356,205 @@ def widened_timing(tpcf, w, peak_fp32, stream, cpu_threads, with_cpu=True):
     return out
 
 
+# ------------------------------------------------------- configurations 1-4 --
+CONFIG_WORKLOADS = {
+    1: "config 1: shear-scalar + scalar-scalar, 20k x 20k uniform on 600' x 600', 15 log bins 1-100'",
+    2: "config 2: scalar-scalar auto-correlation, 1.0 M points on 600' x 600' (Gaussian random kappa, "
+       "P(k) ~ k^-1.5), w ~ U(0.5, 1.5), 30 log bins 0.5-250'",
+    3: "config 3: shear-scalar with errors, 2.0 M shear x 0.5 M scalar on 1200' x 1200', clustered, "
+       "100 k-means patches, 1000 resamples, 20 log bins 1-200'",
+    4: "config 4: differentiable xi_t on the clustered 2.0 M x 0.5 M catalogues, chi^2 against a seeded "
+       "target, forward + adjoint",
+}
+ADJ_FLOP_PER_PAIR = 20   # adjoint of a loss on xi_t, per binned pair (sources as owners)
+KAPPA_FLOP_PER_PAIR = 14
+
+
+def cpu_rate(mode, L, S, bins, seconds, nthreads, full=False):
+    """The FP32 OpenMP restatement of the reference loop (kd-tree) on every
+    k-th lens (k calibrated to about ``seconds`` of pair loop; all lenses when
+    ``full``) against all sources: binned pairs per second of pair loop."""
+    from oracle import oracle as O
+    lo, hi, nb = bins
+
+    def run(stride):
+        Ls = {k: np.ascontiguousarray(v[::stride]) for k, v in L.items()}
+        r = O.ref_pairs(mode, Ls, S, lo, hi, nb, num_threads=nthreads)
+        return int(r["n_pairs"].sum()), O.last_timing()[1], len(Ls["x"])
+
+    n = len(L["x"])
+    stride = 1
+    if not full:
+        cal = max(1, n // (200 if nthreads >= 4 else 20))
+        p0, t0, n0 = run(cal)
+        per_lens_s = t0 / max(n0, 1)
+        stride = max(1, int(n / max(1.0, seconds / max(per_lens_s, 1e-9))))
+    p, t, nl = run(stride)
+    return {"value": p / max(t, 1e-9) / 1e9, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": (f"all {nl} lenses" if stride == 1 else f"every {stride}-th lens ({nl})") +
+                      f" against all {len(S['x'])} sources; {p:.3e} binned pairs; rate over the OpenMP pair loop "
+                      f"({t:.1f} s), kd-tree build excluded"}
+
+
+def config_timing(k, tpcf, stream, peak, steps=3, warmup=2, with_cpu=True, cpu_seconds=8.0):
+    """One configuration of the benchmark suite at its stated size: `value` =
+    binned pairs per second of the whole step with inputs in HBM, `e2e` the same
+    step through the public API from pinned host arrays, the pair kernel's
+    roofline, the autotuned cell side and tile shape, and the CPU port on all
+    host threads and on one."""
+    import torch
+    synth = importlib.import_module("2pcf_b200.synth")
+    at = importlib.import_module("2pcf_b200.autotune")
+    w = synth.make_workload(k)
+    bins = tpcf.create_bins(*w["bins"])
+    ctx = tpcf.Context(0)
+    ctx.set_timing(True)
+    ctx.set_stream(stream.cuda_stream)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    L = w["lenses"]
+    S = w.get("shapes")
+    K = w.get("kappa_map")
+    lens_cat = [tpcf.LensCatalog(**{q: L[q] for q in ("x", "y", "val", "w", "z")})]
+    if k == 2:   # the kappa map is the lens catalogue itself (auto-correlation)
+        tune_src = [tpcf.ShapeCatalog(x=K["x"], y=K["y"], e1=K["kappa_E"], e2=K["kappa_B"], w=K["w"],
+                                      z=np.ones_like(K["x"]), m=np.zeros_like(K["x"]))]
+    else:
+        tune_src = [tpcf.ShapeCatalog(**{q: S[q] for q in ("x", "y", "e1", "e2", "w", "z", "m")})]
+    tune = at.autotune(lens_cat, tune_src, [(0, 0)], bins, ctx, corner=1.0 if k == 1 else 0.5)
+    n_patch = w.get("n_patch", 100)
+    wt = (0.01 + L["w"] / L["w"].max()).astype(np.float32)
+    kernel_ms, flops, adj_ms = [0.0], [0.0], [0.0]
+    state = {}
+
+    def shear(A, B, **kw):
+        return tpcf.tangential_shear_tpcf(A["x"], A["y"], A["z"], A["val"], A["w"], B["x"], B["y"], B["z"],
+                                          B["e1"], B["e2"], B["w"], B["m"], bins, calculate_marks=False,
+                                          ctx=ctx, **kw)
+
+    def kappa(A, B):
+        return tpcf.scalar_kappa_tpcf(A["x"], A["y"], A["val"], A["w"], B["x"], B["y"], B["kappa_E"],
+                                      B["kappa_B"], B["w"], bins, calculate_marks=False, ctx=ctx)
+
+    def step(A, B, C, U):
+        kernel_ms[0] = flops[0] = adj_ms[0] = 0.0
+        if k == 1:
+            r1 = shear(A, B)
+            k1 = ctx.stats()["pair_kernel_ms"]
+            r2 = kappa(A, C)
+            k2 = ctx.stats()["pair_kernel_ms"]
+            p1, p2 = int(r1.n_pairs.sum()), int(r2.n_pairs.sum())
+            kernel_ms[0], flops[0] = k1 + k2, p1 * FLOP_PER_PAIR + p2 * KAPPA_FLOP_PER_PAIR
+            return p1 + p2
+        if k == 2:
+            r = kappa(A, C)
+            p = int(r.n_pairs.sum())
+            kernel_ms[0], flops[0] = ctx.stats()["pair_kernel_ms"], p * KAPPA_FLOP_PER_PAIR
+            return p
+        if k == 3:
+            lab, _, _ = tpcf.partition_data(U[0], U[1], U[2], n_patch, ctx=ctx)
+            r = shear(A, B, patch_A=lab, n_patch=n_patch)
+            p = int(r.n_pairs.sum())
+            kernel_ms[0], flops[0] = ctx.stats()["pair_kernel_ms"], p * FLOP_PER_PAIR
+            tpcf.block_bootstrap(r.patch_sums, w["n_boot"], seed=1003, ctx=ctx)
+            return p
+        # k == 4: forward with raw per-lens sums, then the adjoint of the chi^2
+        r = shear(A, B, lens_raw=True)
+        p = int(r.n_pairs.sum())
+        kernel_ms[0], flops[0] = ctx.stats()["pair_kernel_ms"], p * FLOP_PER_PAIR
+        if state.get("forward_only"):
+            return p
+        xi = r.sum_gt / r.sum_K
+        if "target" not in state:
+            state["sig"] = np.abs(xi) * 0.1 + 1e-6
+            state["target"] = np.random.default_rng(1004).normal(xi, state["sig"])
+        lam = 2 * (xi - state["target"]) / state["sig"] ** 2
+        tpcf.tangential_shear_adjoint(A["x"], A["y"], A["z"], A["val"], A["w"], B["x"], B["y"], B["z"],
+                                      B["e1"], B["e2"], B["w"], B["m"], bins, r, lam, None, ctx=ctx)
+        adj_ms[0] = ctx.stats()["pair_kernel_ms"]
+        return p
+
+    def cats(to):
+        A = {q: to(v) for q, v in L.items()}
+        B = {q: to(v) for q, v in S.items()} if S is not None else None
+        C = {q: to(v) for q, v in K.items()} if K is not None else None
+        U = [to(L["x"]), to(L["y"]), to(wt)]
+        return A, B, C, U
+
+    def timed(A, B, C, U, n):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        kms = fl = ams = 0.0
+        e0.record(stream)
+        for _ in range(n):
+            pairs = step(A, B, C, U)
+            kms += kernel_ms[0]
+            fl += flops[0]
+            ams += adj_ms[0]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n, pairs, kms / n, fl / n, ams / n
+
+    Ad, Bd, Cd, Ud = cats(dev)
+    for _ in range(warmup):
+        step(Ad, Bd, Cd, Ud)
+    ms, pairs, kms, fl, ams = timed(Ad, Bd, Cd, Ud, steps)
+    Ah, Bh, Ch, Uh = cats(pin)
+    step(Ah, Bh, Ch, Uh)
+    ms_e2e, pairs_e2e, _, _, _ = timed(Ah, Bh, Ch, Uh, steps)
+    h2d = sum(int(t.numel()) * t.element_size() for d in (Ah, Bh, Ch) if d for t in d.values())
+    if k == 3:
+        h2d += sum(int(t.numel()) * t.element_size() for t in Uh)
+    ach = fl / (kms * 1e-3) / 1e12
+    out = {"workload": CONFIG_WORKLOADS[k], "value": pairs / (ms * 1e-3) / 1e9, "unit": UNIT,
+           "ms_per_step": ms, "steps": steps, "warmup": warmup, "binned_pairs": pairs,
+           "e2e": {"value": pairs_e2e / (ms_e2e * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": ms_e2e,
+                   "h2d_bytes_per_step": int(h2d)},
+           "roofline": {"bound": "fp32", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                        "kernel": "k_pairs", "kernel_ms": kms,
+                        "flop_per_pair": KAPPA_FLOP_PER_PAIR if k == 2 else
+                        ("26 shear, 14 scalar" if k == 1 else FLOP_PER_PAIR)},
+           "autotune_ms_per_gpair": {"cell": {f"theta_max/{d}": round(v, 3) for d, v in tune["cell"].items()},
+                                     "tile": {g: round(v, 3) for g, v in tune["tile"].items()},
+                                     "choice": tune["choice"]}}
+    if k == 4:
+        state["forward_only"] = True
+        fwd_ms, _, _, _, _ = timed(Ad, Bd, Cd, Ud, steps)
+        state["forward_only"] = False
+        adj_ach = pairs * ADJ_FLOP_PER_PAIR / (ams * 1e-3) / 1e12
+        out["forward_plus_adjoint_over_forward"] = ms / max(fwd_ms, 1e-9)
+        out["adjoint_roofline"] = {"bound": "fp32", "achieved": adj_ach, "peak": peak, "unit": "TFLOP/s",
+                                   "frac": adj_ach / peak, "kernel": "k_adj", "kernel_ms": ams,
+                                   "flop_per_pair": ADJ_FLOP_PER_PAIR}
+        out["forward_value"] = pairs / (fwd_ms * 1e-3) / 1e9
+    if with_cpu:
+        cw = w["bins"]
+        nt = host_threads()
+        if k == 1:
+            parts = [cpu_rate(O_SHEAR, L, S, cw, cpu_seconds, nt, full=True),
+                     cpu_rate(O_KAPPA, L, K, cw, cpu_seconds, nt, full=True)]
+            one = [cpu_rate(O_SHEAR, L, S, cw, cpu_seconds, 1, full=True)]
+        elif k == 2:
+            parts = [cpu_rate(O_KAPPA, L, K, cw, cpu_seconds, nt)]
+            one = [cpu_rate(O_KAPPA, L, K, cw, cpu_seconds / 2, 1)]
+        else:
+            parts = [cpu_rate(O_SHEAR, L, S, cw, cpu_seconds, nt)]
+            one = [cpu_rate(O_SHEAR, L, S, cw, cpu_seconds / 2, 1)]
+        cb = dict(parts[0])
+        if len(parts) > 1:
+            cb["value"] = float(np.mean([c["value"] for c in parts]))
+            cb["sample"] = "shear-scalar: " + parts[0]["sample"] + "; scalar-scalar: " + parts[1]["sample"] + \
+                           "; value = mean of the two rates"
+        cb["single_thread"] = {q: one[0][q] for q in ("value", "unit", "cores", "sample")}
+        out["cpu_baseline"] = cb
+        out["speedup_vs_cpu_all_threads"] = out["value"] / cb["value"]
+    ctx.close()
+    return out
+
+
+O_SHEAR, O_KAPPA = 0, 1   # oracle modes (oracle.SHEAR, oracle.KAPPA)
+
+
 def path_stats(tpcf, args):
     """One batched call on the diagnostic build; prints the share of warp
     sub-chunks and lane-pairs per path of k_pairs."""
@@ -376,6 +581,28 @@ def path_stats(tpcf, args):
         res[name] = {"warp_chunks": float(v[i] / v[:4].sum()), "lane_pairs": float(v[4 + i] / v[4:].sum())}
     res["computed_lane_pairs_per_binned_pair"] = float(v[5:].sum() / binned)
     print(json.dumps(res), flush=True)
+
+
+def config_line(tpcf, args, rank):
+    """`--config N` (1-4): that configuration's measurement as the one JSON line."""
+    import torch
+    stream = torch.cuda.current_stream()
+    ctx = tpcf.Context(0)
+    peak = ctx.measure_fp32_peak()
+    ctx.close()
+    with ClockSampler(0) as cs:
+        t0 = time.time()
+        r = config_timing(args.config, tpcf, stream, peak, steps=args.steps, warmup=args.warmup,
+                          with_cpu=not args.no_cpu_baseline, cpu_seconds=args.cpu_seconds / 2)
+        cs.window(t0, time.time())
+    line = {"metric": METRIC, "value": r.pop("value"), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r.pop("ms_per_step"), "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "accumulate": "f64", "data": "synthetic",
+            "config": {"workload": r.pop("workload"), "l2": "no flush between steps"}}
+    line.update(r)
+    line["clocks"] = cs.summary()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def host_threads():
@@ -427,6 +654,10 @@ def main():
                     help="grid cell side theta_max/D (64: the autotuner's usual choice on this workload)")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the cell side with 2pcf_b200.autotune on a corner of the field instead")
+    ap.add_argument("--config", type=int, default=5, choices=[1, 2, 3, 4, 5],
+                    help="5 (default): the tomography headline; 1-4: only that configuration's line")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the measurements of configurations 1-4 that the default run adds")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -445,6 +676,8 @@ def main():
     tpcf = importlib.import_module("2pcf_b200")
     if args.path_stats:
         return path_stats(tpcf, args)
+    if args.config != 5:
+        return config_line(tpcf, args, rank)
 
     w = workload(args.scale)
     if args.region > 0:
@@ -557,15 +790,15 @@ def main():
     d2h = (int(ux.size) * 4 + len(w["tasks"]) * bins.n_bin * (5 * 8 + 8 + 5 * 4 + n_patch * 6 * 8)
            + 2 * n_boot * len(w["tasks"]) * bins.n_bin * 8 + 2 * (len(w["tasks"]) * bins.n_bin) ** 2 * 8)
 
+    peak = ctx.measure_fp32_peak()
     adjoint = None
     if world == 1 and not args.no_adjoint and not sphere:
-        adjoint = adjoint_timing(w, ctx, bins, pairs, pair_ms, stream)
-    peak = ctx.measure_fp32_peak()
+        adjoint = adjoint_timing(w, ctx, bins, pairs, pair_ms, stream, peak)
     fpp = SPH_FLOP_PER_PAIR if sphere else FLOP_PER_PAIR
     achieved = pairs * fpp / (pair_ms * 1e-3) / 1e12
-    # DRAM bytes of one pair-kernel launch of this exact workload, from one ncu
-    # capture (profiles/k_pairs_tomography_10M_dram.md); other configurations
-    # were not captured
+    # DRAM bytes of one pair-kernel launch of this exact workload, from one
+    # one-pass ncu capture of dram__bytes_read.sum + dram__bytes_write.sum;
+    # other configurations were not captured
     default_cfg = not sphere and args.scale == 1.0 and args.region <= 0 and args.task < 0 and \
         abs(ctx.cell_size - bins.x_max / 64) < 1e-6
     traffic = K_PAIRS_DRAM_BYTES if default_cfg else None
@@ -603,6 +836,9 @@ def main():
         line["cpu_baseline"]["single_thread"] = {k: c1[k] for k in ("value", "unit", "cores", "sample")}
     if world == 1 and not args.no_widened and args.region <= 0 and args.task < 0 and not sphere:
         line["widened"] = widened_timing(tpcf, w, peak, stream, host_threads(), with_cpu=not args.no_cpu_baseline)
+    if world == 1 and not args.no_configs and args.region <= 0 and args.task < 0 and not sphere:
+        line["configs"] = {str(k): config_timing(k, tpcf, stream, peak, with_cpu=not args.no_cpu_baseline)
+                           for k in (1, 2, 3, 4)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -5,8 +5,8 @@
  * Every entry point is plain C: scalars by value, arrays as pointers plus
  * sizes, no C++ or torch types.  Each entry point names the reference routine
  * it replaces (file:line inside the reference project).  A Fortran caller
- * binds them through iso_c_binding (the interface module is given in
- * INTEGRATION.md); Python binds them through ctypes.
+ * binds them through an iso_c_binding interface module; Python binds them
+ * through ctypes.
  *
  * Conventions
  *   - Arrays are 0-based structure-of-arrays, the memory layout of the
@@ -77,7 +77,12 @@ typedef struct tpcf_opts {
                             must be summed over shards (one all-reduce);
                             normalised outputs are not written            */
   int32_t shard_count;   /* 0 or 1: no sharding                              */
-  int32_t reserved[5];
+  int32_t group_size;    /* planar pair kernel tile shape: lenses per group and
+                            threads per block (32, 64 or 128; 0 = 128, halved
+                            while the per-lens histogram would exceed 100 KB) */
+  int32_t tile_chunks;   /* 32-source sub-chunks per source tile (2 or 4 with
+                            128 lenses per group, else 4; 0 = 4)             */
+  int32_t reserved[3];
 } tpcf_opts;
 
 /* Per-call results.  Replaces type(shear_2pcf_results) (src/tpcf.f90:17-22)
@@ -177,6 +182,21 @@ tpcf_status tpcf_last_stats(const tpcf_ctx* ctx, tpcf_stats* stats);
 tpcf_status tpcf_set_cell_size(tpcf_ctx* ctx, double cell_size);
 /* Change the sharding of later calls (see tpcf_opts.shard_index). */
 tpcf_status tpcf_set_shard(tpcf_ctx* ctx, int32_t shard_index, int32_t shard_count);
+/* Tile shape of the planar pair kernel (tpcf_opts.group_size, tile_chunks;
+ * 0 = default).  Results do not depend on it, only speed (the autotuner in
+ * 2pcf_b200/autotune.py times the candidates).  No reference counterpart. */
+tpcf_status tpcf_set_tile_shape(tpcf_ctx* ctx, int32_t group_size, int32_t tile_chunks);
+
+/* Fault injection for tests of the failure paths; no reference counterpart
+ * (the reference stops the program: src/kdtree.f90:119-122, :265-267).
+ * fail_alloc >= 0: the fail_alloc-th device workspace allocation from now
+ * (0 = the next) fails as if cudaMalloc had, and the call returns
+ * TPCF_ERR_OOM.  skip_tile >= 0: the planar pair kernel never issues the copy
+ * of the source tile with that ring index in each block, so its bounded waits
+ * run out after wait_polls polls (0 = the product's 2^22) and the call
+ * returns TPCF_ERR_TIMEOUT; every copy that was issued has landed before the
+ * kernel exits.  -1 / 0 switch them off.  The context stays usable. */
+tpcf_status tpcf_debug_inject(tpcf_ctx* ctx, int64_t fail_alloc, int32_t skip_tile, uint32_t wait_polls);
 
 /* Roofline helper with no counterpart in the reference: measures this GPU's
  * FP32 FMA throughput (FLOP/s counting an FMA as 2) with a register-resident
@@ -349,6 +369,29 @@ tpcf_status tpcf_batch_shear_scalar(tpcf_ctx* ctx,
                                     const tpcf_bins* bins, int32_t n_patch,
                                     tpcf_result* outs);
 
+/* Scalar (kappa) catalogue of the scalar-scalar estimator (kappa_map,
+ * src/tpcf.f90:29-32): kappa_E and kappa_B per object. */
+typedef struct tpcf_kappa_catalog {
+  int64_t n;
+  const float* x;
+  const float* y;
+  const float* kE;
+  const float* kB;
+  const float* w;
+} tpcf_kappa_catalog;
+
+/* Batched scalar-scalar: n_task (scalar catalogue, kappa catalogue) pairs in
+ * one persistent launch, each as tpcf_scalar_scalar would compute it (the lens
+ * catalogues' z is not used).  Replaces the per-field loop around kappa_2pcf
+ * (src/main.f90:638-660). */
+tpcf_status tpcf_batch_scalar_scalar(tpcf_ctx* ctx,
+                                     int32_t n_lens_cat, const tpcf_lens_catalog* lenses,
+                                     int32_t n_kappa_cat, const tpcf_kappa_catalog* kappas,
+                                     int32_t n_task, const int32_t* task_lens,
+                                     const int32_t* task_kappa,
+                                     const tpcf_bins* bins, int32_t n_patch,
+                                     tpcf_result* outs);
+
 /* ------------------------------------------------------------ gradients -- */
 /* No counterpart in the reference (it has no gradients).  Adjoint of
  * tpcf_shear_scalar: given dL/dg_t and dL/dg_x per bin (g = the normalised
@@ -373,6 +416,45 @@ tpcf_status tpcf_shear_scalar_adjoint(tpcf_ctx* ctx,
                                       float* grad_valA, float* grad_wA,
                                       float* grad_e1B, float* grad_e2B, float* grad_wB, float* grad_mB);
 
+/* Gradient outputs of one catalogue of a batched backward pass (each array
+ * nullable, [n] of its catalogue). */
+typedef struct tpcf_lens_grad {
+  float* val;
+  float* w;
+} tpcf_lens_grad;
+typedef struct tpcf_shear_grad {
+  float* e1;
+  float* e2;
+  float* w;
+  float* m;
+} tpcf_shear_grad;
+/* The forward outputs and loss derivatives of one task of a batched backward
+ * pass: sum_gt, sum_gx (nullable), sum_K [n_bin] and lens_raw [nA][6][n_bin]
+ * of that task's forward (tpcf_batch_shear_scalar with lens_raw), dL/dg_t
+ * and dL/dg_x (nullable) [n_bin]. */
+typedef struct tpcf_adjoint_task {
+  const double* sum_gt;
+  const double* sum_gx;
+  const double* sum_K;
+  const double* lens_raw;
+  const double* dL_dgt;
+  const double* dL_dgx;
+} tpcf_adjoint_task;
+
+/* No counterpart in the reference.  Adjoint of tpcf_batch_shear_scalar: the
+ * gradients of every task at once, with one persistent launch over all
+ * (task, source group) work items, one lens grid per lens catalogue and one
+ * sorted copy of each source catalogue.  A catalogue used by several tasks
+ * receives the sum of their gradients (FP64, added in task order).  Each
+ * task's gradient is the one tpcf_shear_scalar_adjoint gives for it. */
+tpcf_status tpcf_batch_shear_scalar_adjoint(tpcf_ctx* ctx,
+                                            int32_t n_lens_cat, const tpcf_lens_catalog* lenses,
+                                            tpcf_lens_grad* lens_grads /* [n_lens_cat], nullable */,
+                                            int32_t n_src_cat, const tpcf_shear_catalog* sources,
+                                            tpcf_shear_grad* src_grads /* [n_src_cat], nullable */,
+                                            int32_t n_task, const int32_t* task_lens, const int32_t* task_src,
+                                            const tpcf_bins* bins, const tpcf_adjoint_task* task_in);
+
 /* -------------------------------------------------- patches and errors -- */
 /* Replaces partition_data (src/kmeans.f90:12-263) as called for Voronoi
  * blocks (equal_size = .false., weight_equalizer_scaling = 0,
@@ -382,8 +464,9 @@ tpcf_status tpcf_shear_scalar_adjoint(tpcf_ctx* ctx,
  * passes.  Distances are FP32 sqrt(dx*dx+dy*dy) with IEEE rounding; centroid
  * sums are 64-bit fixed point, so the labels are the same on every run.
  * labels_out [n] are 0-based; centroids_out [k][2] is nullable.  The
- * reference's equal-weight mode (distance penalty and rebalancing pass) is not
- * provided. */
+ * stopping rule is evaluated on the device, so the host waits once per batch
+ * of passes, not once per pass.  The reference's equal-weight mode (distance
+ * penalty and rebalancing pass) is tpcf_kmeans_equal below. */
 tpcf_status tpcf_kmeans(tpcf_ctx* ctx, const float* x, const float* y, const float* w, int64_t n,
                         int32_t k, int32_t max_iter, float reassign_tol,
                         int32_t* labels_out, float* centroids_out, int32_t* n_iter_out);

@@ -74,6 +74,9 @@ def lib():
         L.orc_last_timing.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.orc_canon_adjoint.argtypes = ([C.c_long] + [vp] * 5 + [C.c_long] + [vp] * 7 +
                                         [_f64p, C.c_int, _f64p, _f64p, C.c_int] + [_f64p] * 6)
+        L.orc_canon_adjoint_sel.argtypes = ([C.c_long] + [vp] * 5 + [C.c_long] + [vp] * 7 +
+                                            [_f64p, C.c_int] + [_f64p] * 5 + [vp, C.c_long, vp, C.c_long,
+                                                                               C.c_int] + [vp] * 6)
         L.orc_ref_sphere_f32.argtypes = ([C.c_int, C.c_long] + [vp] * 5 + [C.c_long] + [vp] * 7 +
                                          [C.c_float, C.c_float, C.c_int, C.c_int, C.c_float, C.c_int] +
                                          [vp] * 4)
@@ -186,7 +189,8 @@ def canon_pairs(mode, lens, src, edges_sq, num_threads=None, lens_idx=None):
 
     Returns a dict of per-bin FP64 arrays (CANON_Q) and, when ``lens_idx`` is
     given, ``lens`` = per-lens [n_sel][6][n_bin] sums (d*w, g_t, g_x, w, K, n)
-    for those lenses (and the per-bin sums cover only those lenses)."""
+    for those lenses (and the per-bin sums cover only those lenses), and
+    ``lens_abs`` = per-lens [n_sel][2][n_bin] sums of |g_t terms|, |g_x terms|."""
     f = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
     nA, nB = len(lens["x"]), len(src["x"])
     e2 = np.ascontiguousarray(edges_sq, np.float64)
@@ -200,7 +204,7 @@ def canon_pairs(mode, lens, src, edges_sq, num_threads=None, lens_idx=None):
         zB = mB = None
     sums = np.zeros(8 * n_bin)
     sel = None if lens_idx is None else np.ascontiguousarray(lens_idx, np.int64)
-    lens_out = None if sel is None else np.zeros((len(sel), 6, n_bin))
+    lens_out = None if sel is None else np.zeros((len(sel), 8, n_bin))
     nt = num_threads or os.cpu_count() or 1
     lib().orc_canon_pairs(mode, nA, _ptr(xA), _ptr(yA), _ptr(zA), _ptr(vA), _ptr(wA), nB, _ptr(xB),
                           _ptr(yB), _ptr(zB), _ptr(e1), _ptr(e2b), _ptr(wB), _ptr(mB), e2, n_bin,
@@ -208,7 +212,8 @@ def canon_pairs(mode, lens, src, edges_sq, num_threads=None, lens_idx=None):
     sums = sums.reshape(8, n_bin)
     out = {k: sums[i].copy() for i, k in enumerate(CANON_Q)}
     if lens_out is not None:
-        out["lens"] = lens_out
+        out["lens"] = np.ascontiguousarray(lens_out[:, :6])
+        out["lens_abs"] = np.ascontiguousarray(lens_out[:, 6:])  # sum|g_t terms|, sum|g_x terms|
     return out
 
 
@@ -226,6 +231,28 @@ def canon_adjoint(lens, src, edges_sq, lam_t, lam_x=None, num_threads=None):
     lib().orc_canon_adjoint(nA, *[_ptr(a) for a in A], nB, *[_ptr(b) for b in B],
                             np.ascontiguousarray(edges_sq, np.float64), nb, lt, lx,
                             num_threads or os.cpu_count() or 1, *out)
+    return dict(zip(("val_A", "w_A", "e1_B", "e2_B", "w_B", "m_B"), out))
+
+
+def canon_adjoint_sel(lens, src, edges_sq, totals, lam_t, lam_x, lens_sel, src_sel, num_threads=None):
+    """The FP64 brute-force gradient of canon_adjoint for selected lenses and
+    sources only, given the per-bin totals ``totals`` = (sum_gt, sum_gx,
+    sum_K) of the whole catalogue pair.  Returns val_A, w_A [len(lens_sel)]
+    and e1_B, e2_B, w_B, m_B [len(src_sel)]."""
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+    nA, nB = len(lens["x"]), len(src["x"])
+    nb = len(edges_sq) - 1
+    A = [f(lens[k]) for k in ("x", "y", "z", "val", "w")]
+    B = [f(src[k]) for k in ("x", "y", "z", "e1", "e2", "w", "m")]
+    d64 = lambda a: np.ascontiguousarray(a, np.float64)
+    ls = np.ascontiguousarray(lens_sel, np.int64)
+    ss = np.ascontiguousarray(src_sel, np.int64)
+    lx = np.zeros(nb) if lam_x is None else d64(lam_x)
+    out = [np.zeros(len(ls)), np.zeros(len(ls))] + [np.zeros(len(ss)) for _ in range(4)]
+    lib().orc_canon_adjoint_sel(nA, *[_ptr(a) for a in A], nB, *[_ptr(b) for b in B], d64(edges_sq), nb,
+                                d64(totals[0]), d64(totals[1]), d64(totals[2]), d64(lam_t), lx,
+                                ls.ctypes.data, len(ls), ss.ctypes.data, len(ss),
+                                num_threads or os.cpu_count() or 1, *[o.ctypes.data for o in out])
     return dict(zip(("val_A", "w_A", "e1_B", "e2_B", "w_B", "m_B"), out))
 
 

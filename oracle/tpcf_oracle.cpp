@@ -835,8 +835,8 @@ int orc_canon_pairs(int mode, long nA, const float* xA, const float* yA, const f
     for (long s = 0; s < n_sel; ++s) {
       const double* acc = all.data() + (size_t)s * NQ * nb;
       for (int q = 0; q < NQ * nb; ++q) sums[q] += acc[q];
-      if (lens_out)
-        for (int q = 0; q < 6 * nb; ++q) lens_out[(size_t)s * 6 * nb + q] = acc[q];
+      if (lens_out)  // all NQ rows: d*w, g_t, g_x, w, K, n, sum|g_t terms|, sum|g_x terms|
+        for (int q = 0; q < NQ * nb; ++q) lens_out[(size_t)s * NQ * nb + q] = acc[q];
     }
   }
   return 0;
@@ -908,6 +908,79 @@ int orc_canon_adjoint(long nA, const float* xA, const float* yA, const float* zA
     g_e2[j] = ge2;
     g_wB[j] = gw;
     g_m[j] = gm;
+  }
+  return 0;
+}
+
+// The gradient of orc_canon_adjoint for selected objects only, given the
+// per-bin totals sum_gt, sum_gx, sum_K of the whole catalogue pair (which a
+// caller may take from a full-size run): each selected lens against every
+// source, each selected source against every lens, in FP64 with the
+// canonical bins.  Outputs are [n_lsel] and [n_ssel].
+int orc_canon_adjoint_sel(long nA, const float* xA, const float* yA, const float* zA, const float* valA,
+                          const float* wA, long nB, const float* xB, const float* yB, const float* zB,
+                          const float* e1B, const float* e2B, const float* wB, const float* mB, const double* e2,
+                          int nb, const double* sgt, const double* sgx, const double* sK, const double* lt,
+                          const double* lx, const long* lsel, long n_lsel, const long* ssel, long n_ssel,
+                          int num_threads, double* g_val, double* g_wA, double* g_e1, double* g_e2, double* g_wB,
+                          double* g_m) {
+  std::vector<double> mu(nb, 0.0), mux(nb, 0.0), nu(nb, 0.0);
+  for (int b = 0; b < nb; ++b) {
+    const double K = sK[b];
+    if (K > 0) {
+      mu[b] = lt[b] / K;
+      mux[b] = lx[b] / K;
+      nu[b] = (lt[b] * (sgt[b] / K) + lx[b] * (sgx[b] / K)) / K;
+    }
+  }
+  auto pair = [&](long i, long j, int& b, double& c2, double& s2) -> bool {
+    if (wA[i] == 0.0f || zA[i] < 0.0f || zB[j] < 0.0f || zA[i] > zB[j]) return false;
+    const double d2 = canon::d2_of(xA[i], yA[i], xB[j], yB[j]);
+    b = canon::bin_of(d2, e2, nb);
+    if (b < 0) return false;
+    const double dx = (double)xA[i] - (double)xB[j], dy = (double)yA[i] - (double)yB[j];
+    const double d = sqrt(d2);
+    c2 = 2.0 * ((dx / d) * (dx / d)) - 1.0;
+    s2 = 2.0 * dx * dy / d2;
+    return true;
+  };
+#pragma omp parallel for schedule(dynamic, 1) num_threads(num_threads)
+  for (long k = 0; k < n_lsel; ++k) {
+    const long i = lsel[k];
+    double gv = 0, gw = 0;
+    for (long j = 0; j < nB; ++j) {
+      int b;
+      double c2, s2;
+      if (!pair(i, j, b, c2, s2)) continue;
+      const double e1 = e1B[j], ee2 = e2B[j], w = wB[j], m = mB ? mB[j] : 0.0;
+      const double t = -(e1 * c2 + ee2 * s2), x = -(-e1 * s2 + ee2 * c2);
+      const double a = mu[b] * t + mux[b] * x;
+      gv += a * w * (double)wA[i];
+      gw += a * w * (double)valA[i] - nu[b] * w * (1.0 + m);
+    }
+    g_val[k] = gv;
+    g_wA[k] = gw;
+  }
+  for (long k = 0; k < n_ssel; ++k) {
+    const long j = ssel[k];
+    const double e1 = e1B[j], ee2 = e2B[j], w = wB[j], m = mB ? mB[j] : 0.0;
+    double ge1 = 0, ge2 = 0, gw = 0, gm = 0;
+#pragma omp parallel for schedule(static) num_threads(num_threads) reduction(+ : ge1, ge2, gw, gm)
+    for (long i = 0; i < nA; ++i) {
+      int b;
+      double c2, s2;
+      if (!pair(i, j, b, c2, s2)) continue;
+      const double vw = (double)valA[i] * (double)wA[i];
+      const double t = -(e1 * c2 + ee2 * s2), x = -(-e1 * s2 + ee2 * c2);
+      ge1 += (mu[b] * (-c2) + mux[b] * s2) * w * vw;
+      ge2 += (mu[b] * (-s2) + mux[b] * (-c2)) * w * vw;
+      gw += (mu[b] * t + mux[b] * x) * vw - nu[b] * (1.0 + m) * (double)wA[i];
+      gm += -nu[b] * w * (double)wA[i];
+    }
+    g_e1[k] = ge1;
+    g_e2[k] = ge2;
+    g_wB[k] = gw;
+    g_m[k] = gm;
   }
   return 0;
 }

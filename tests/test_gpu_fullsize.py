@@ -2,10 +2,11 @@
 scalar bins, 25 tasks, 100 patches, 20 log bins over 1-300 arcmin) and the
 1 M-point scalar auto-correlation, through properties that hold at any size:
 
-- per-lens parity: the per-lens FP64 sums of randomly chosen lenses, computed
-  inside the full batched launch, against the oracle's FP64 brute force of
-  those lenses over the whole source catalogue (n_pairs bit-exact, sums to
-  1e-6 of sum|terms|);
+- per-lens parity in every one of the 25 tasks: the per-lens FP64 sums of 20
+  random lenses per task, computed inside the full batched launch, against
+  the oracle's FP64 brute force of those lenses over the task's whole source
+  catalogue (n_pairs bit-exact, sums to 1e-6 of the lens's sum|terms| per
+  bin; margins printed, tests/parity.py);
 - the per-patch sums add up to the totals (n_pairs exactly);
 - the batched launch equals single-task calls (n_pairs exactly);
 - two shards add up to the unsharded result (n_pairs exactly, sums to 1e-12);
@@ -14,6 +15,8 @@ scalar bins, 25 tasks, 100 patches, 20 log bins over 1-300 arcmin) and the
 """
 import numpy as np
 import pytest
+
+from parity import check_lens_sums
 
 pytestmark = pytest.mark.gpu
 
@@ -30,6 +33,7 @@ def cats(tpcf, w):
 
 
 def test_tomography_patches_batch_and_lens_parity(tpcf, oracle, tomo):
+    import torch
     ctx = tpcf.Context(0)
     ctx.set_cell_size(tomo["bins"][1] / 64)
     bins = tpcf.create_bins(*tomo["bins"])
@@ -40,27 +44,31 @@ def test_tomography_patches_batch_and_lens_parity(tpcf, oracle, tomo):
     lab, _, _ = tpcf.partition_data(ux, uy, (0.01 + uw / uw.max()).astype(np.float32), 100, ctx=ctx)
     offs = np.cumsum([0] + [len(l["x"]) for l in tomo["lens_bins"]])
     P = [lab[offs[i]:offs[i + 1]] for i in range(5)]
-    out = tpcf.batch_shear_2pcf(L, S, tomo["tasks"], bins, lens_patches=P, n_patch=100, ctx=ctx)
+    # one 25-task launch with per-lens FP64 rows kept in device memory
+    out = tpcf.batch_shear_2pcf(L, S, tomo["tasks"], bins, lens_patches=P, n_patch=100, lens_sums="device",
+                                ctx=ctx)
     total = sum(int(o.n_pairs.sum()) for o in out)
     assert total > 1.0e12
-    for o in out:
+    rng = np.random.default_rng(5)
+    for t, (li, si) in enumerate(tomo["tasks"]):
+        o = out[t]
         np.testing.assert_array_equal(o.patch_sums[:, 5].sum(0), o.n_pairs)
         np.testing.assert_allclose(o.patch_sums[:, 1].sum(0), o.sum_gt, rtol=1e-12, atol=1e-9)
-    # single-task calls with per-lens sums (scalar bin 1 = 0.1 M lenses against shear bin 5 = 4.0 M)
+        # 20 random lenses of this task against every source of its shear bin
+        Ld, Sd = tomo["lens_bins"][li], tomo["shape_bins"][si]
+        idx = np.sort(rng.choice(len(Ld["x"]), 20, replace=False))
+        got = o.lens_sums.index_select(0, torch.as_tensor(idx, device=o.lens_sums.device)).cpu().numpy()
+        can = oracle.canon_pairs(oracle.SHEAR, Ld, Sd, bins.bin_edges_sq, lens_idx=idx)
+        check_lens_sums(f"config5 task {t} (scalar bin {li + 1} x shear bin {si + 1}), 20 lenses", got, can,
+                        extra={"sources": int(len(Sd["x"]))})
+        o.lens_sums = None
+    # a single-task call agrees with its task of the batched launch
     t = tomo["tasks"].index((0, 4))
     Ld, Sd = tomo["lens_bins"][0], tomo["shape_bins"][4]
     one = tpcf.tangential_shear_tpcf(Ld["x"], Ld["y"], Ld["z"], Ld["val"], Ld["w"], Sd["x"], Sd["y"], Sd["z"],
-                                     Sd["e1"], Sd["e2"], Sd["w"], Sd["m"], bins, calculate_marks=False,
-                                     lens_sums=True, ctx=ctx)
+                                     Sd["e1"], Sd["e2"], Sd["w"], Sd["m"], bins, calculate_marks=False, ctx=ctx)
     np.testing.assert_array_equal(one.n_pairs, out[t].n_pairs)
-    rng = np.random.default_rng(5)
-    idx = np.sort(rng.choice(len(Ld["x"]), 150, replace=False))
-    can = oracle.canon_pairs(oracle.SHEAR, Ld, Sd, bins.bin_edges_sq, lens_idx=idx)
-    ref = can["lens"]                       # [150][6][n_bin]: d*w, g_t, g_x, w, K, n
-    got = one.lens_sums[idx]
-    np.testing.assert_array_equal(got[:, 5], ref[:, 5])
-    scale = np.abs(ref).sum(axis=2, keepdims=True) + 1e-300
-    assert np.all(np.abs(got[:, :5] - ref[:, :5]) <= 1e-6 * scale[:, :5])
+    np.testing.assert_allclose(one.sum_gt, out[t].sum_gt, rtol=1e-12, atol=1e-12 * np.abs(one.sum_gt).max())
     ctx.close()
 
 
@@ -98,8 +106,5 @@ def test_kappa_auto_1M_lens_parity(tpcf, oracle, synth):
     assert res.n_pairs.sum() > 1e11
     idx = np.sort(np.random.default_rng(6).choice(len(L["x"]), 120, replace=False))
     can = oracle.canon_pairs(oracle.KAPPA, L, K, bins.bin_edges_sq, lens_idx=idx)
-    ref, got = can["lens"], res.lens_sums[idx]
-    np.testing.assert_array_equal(got[:, 5], ref[:, 5])
-    scale = np.abs(ref).sum(axis=2, keepdims=True) + 1e-300
-    assert np.all(np.abs(got[:, :5] - ref[:, :5]) <= 1e-6 * scale[:, :5])
+    check_lens_sums("config2 kappa-kappa 1M auto, 120 lenses", res.lens_sums[idx], can)
     ctx.close()

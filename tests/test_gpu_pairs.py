@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 from conftest import uniform_shear
+from parity import check_sums
 
 pytestmark = pytest.mark.gpu
 
@@ -19,19 +20,9 @@ def canon(oracle, mode, L, S, bins, **kw):
     return oracle.canon_pairs(mode, L, S, bins.bin_edges_sq, **kw)
 
 
-def assert_parity(res, can, rtol=RTOL, kappa=False):
-    np.testing.assert_array_equal(res.n_pairs, can["n_pairs"].astype(np.int64))
-    for q, ref, scale in (("sum_gt", "sum_gt", "abs_gt"), ("sum_gx", "sum_gx", "abs_gx"),
-                          ("sum_w", "sum_w", "sum_w"), ("sum_K", "sum_K", "sum_K"),
-                          ("sum_dw", "sum_dw", "sum_dw")):
-        got, exp, sc = getattr(res, q), can[ref], np.abs(can[scale])
-        bad = np.abs(got - exp) > rtol * sc + 1e-300
-        assert not bad.any(), f"{q}: bins {np.nonzero(bad)[0]} got {got[bad]} expected {exp[bad]}"
-    K = can["sum_K"]
-    with np.errstate(invalid="ignore", divide="ignore"):
-        gt_ref = np.where(K > 0, can["sum_gt"] / K, 0.0)
-        tol = rtol * np.where(K > 0, can["abs_gt"] / K, 0.0) + 1e-7 * np.abs(gt_ref) + 1e-30
-    assert np.all(np.abs(res.g_t.astype(np.float64) - gt_ref) <= tol + np.abs(gt_ref) * 2e-7)
+def assert_parity(res, can, rtol=RTOL, kappa=False, name=None):
+    import inspect
+    check_sums(name or inspect.stack()[1].function, res, can, rtol=rtol)
 
 
 def test_shear_uniform(tpcf, oracle, ctx):
@@ -219,4 +210,41 @@ def test_cell_size_autotune_keeps_results(tpcf, oracle):
         ctx.set_cell_size(bins.x_max / d)
         r = tpcf.batch_shear_2pcf(lens, shp, [(0, 0)], bins, ctx=ctx)[0]
         assert_parity(r, can)
+    # every tile shape the tuner can pick gives the same pair sums
+    for g, t in ((128, 4), (128, 2), (64, 4), (32, 4)):
+        ctx.set_tile_shape(g, t)
+        r = tpcf.batch_shear_2pcf(lens, shp, [(0, 0)], bins, ctx=ctx)[0]
+        assert_parity(r, can, name=f"tile shape {g} lenses x {t} sub-chunks")
+    tuned = at.autotune(lens, shp, [(0, 0)], bins, ctx, divisors=(16, 48))
+    assert set(tuned["tile"]) == {"128x4", "128x2", "64x4"}
+    assert ctx.tile_shape == (tuned["choice"]["group_size"], tuned["choice"]["tile_chunks"])
     ctx.close()
+
+
+def test_batched_scalar_scalar_equals_single_calls(tpcf, oracle, ctx):
+    """tpcf_batch_scalar_scalar: every (scalar catalogue, kappa map) task of one
+    launch against the FP64 oracle and against tpcf_scalar_scalar."""
+    rng = np.random.default_rng(96)
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+    lens, kap, raw = [], [], []
+    for n, box in ((3000, 300.0), (1500, 250.0)):
+        L = dict(x=f(rng.uniform(0, box, n)), y=f(rng.uniform(0, box, n)), val=f(rng.normal(0, .02, n)),
+                 w=f(rng.uniform(.5, 1.5, n)))
+        K = dict(x=f(rng.uniform(0, box, 2 * n)), y=f(rng.uniform(0, box, 2 * n)),
+                 kappa_E=f(rng.normal(0, .02, 2 * n)), kappa_B=f(rng.normal(0, .01, 2 * n)),
+                 w=f(rng.uniform(.5, 1.5, 2 * n)))
+        raw.append((L, K))
+        lens.append(tpcf.LensCatalog(x=L["x"], y=L["y"], val=L["val"], w=L["w"]))
+        kap.append(tpcf.KappaMap(**K))
+    bins = tpcf.create_bins(0.5, 60.0, 16)
+    tasks = [(0, 0), (0, 1), (1, 0), (1, 1)]
+    outs = tpcf.batch_kappa_2pcf(lens, kap, tasks, bins, ctx=ctx)
+    for (i, j), r in zip(tasks, outs):
+        L, _ = raw[i]
+        _, K = raw[j]
+        can = oracle.canon_pairs(oracle.KAPPA, L, K, bins.bin_edges_sq)
+        assert_parity(r, can, name=f"batched scalar-scalar task ({i}, {j})")
+        one = tpcf.scalar_kappa_tpcf(L["x"], L["y"], L["val"], L["w"], K["x"], K["y"], K["kappa_E"], K["kappa_B"],
+                                     K["w"], bins, calculate_marks=False, ctx=ctx)
+        np.testing.assert_array_equal(one.n_pairs, r.n_pairs)
+        np.testing.assert_allclose(one.sum_gt, r.sum_gt, rtol=1e-13, atol=1e-13 * np.abs(one.sum_gt).max())

@@ -197,3 +197,24 @@ def test_equal_weight_kmeans_restatement_balances(oracle):
     assert abs((W.max() - W.min()) / W.mean() - dev) < 1e-5
     _, _, _, dev0 = oracle.kmeans_equal(x, y, w, 20, scaling=0.0, weight_tol=1e9, random_init=False)
     assert dev < 0.3 * dev0
+
+
+def test_subset_adjoint_equals_full_adjoint(oracle):
+    """canon_adjoint_sel (gradients of selected objects from given totals, used
+    at full sizes) equals the full brute-force gradient on those objects."""
+    rng = np.random.default_rng(1)
+    n = 400
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+    L = dict(x=f(rng.uniform(0, 100, n)), y=f(rng.uniform(0, 100, n)), z=f(rng.uniform(0, 1, n)),
+             val=f(rng.normal(0, 1, n)), w=f(rng.uniform(.5, 1.5, n)))
+    S = dict(x=f(rng.uniform(0, 100, n)), y=f(rng.uniform(0, 100, n)), z=f(rng.uniform(0.2, 1.2, n)),
+             e1=f(rng.normal(0, .3, n)), e2=f(rng.normal(0, .3, n)), w=f(rng.uniform(.5, 1.5, n)),
+             m=f(rng.normal(0, .05, n)))
+    _, e2 = oracle.canonical_edges(1.0, 50.0, 8)
+    lt, lx = rng.normal(size=8), rng.normal(size=8)
+    full = oracle.canon_adjoint(L, S, e2, lt, lx)
+    c = oracle.canon_pairs(oracle.SHEAR, L, S, e2)
+    ls, ss = np.array([3, 50, 399]), np.array([0, 7, 123, 250])
+    sel = oracle.canon_adjoint_sel(L, S, e2, (c["sum_gt"], c["sum_gx"], c["sum_K"]), lt, lx, ls, ss)
+    for k, idx in (("val_A", ls), ("w_A", ls), ("e1_B", ss), ("e2_B", ss), ("w_B", ss), ("m_B", ss)):
+        np.testing.assert_allclose(sel[k], full[k][idx], rtol=1e-12, atol=1e-15 * np.abs(full[k]).max())
