@@ -178,6 +178,12 @@ class Context:
         _check(lib().tpcf_measure_fp32_peak(self._h, C.byref(v)), self._h)
         return v.value
 
+    def measure_fp64_peak(self) -> float:
+        """Measured FP64 FMA throughput of this GPU in TFLOP/s."""
+        v = C.c_double()
+        _check(lib().tpcf_measure_fp64_peak(self._h, C.byref(v)), self._h)
+        return v.value
+
     def stats(self) -> dict:
         s = Stats()
         _check(lib().tpcf_last_stats(self._h, C.byref(s)), self._h)

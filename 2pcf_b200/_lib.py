@@ -57,7 +57,7 @@ class KappaCat(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("pair_kernel_ms", C.c_double), ("call_ms", C.c_double), ("n_pairs", C.c_int64),
-                ("h2d_bytes", C.c_int64), ("kernel_launches", C.c_int64)]
+                ("h2d_bytes", C.c_int64), ("kernel_launches", C.c_int64), ("workspace_bytes", C.c_int64)]
 
 
 class LensGrad(C.Structure):
@@ -117,6 +117,7 @@ def lib():
     _sig(L, "tpcf_set_tile_shape", st, [vp, i32, i32])
     _sig(L, "tpcf_debug_inject", st, [vp, i64, i32, C.c_uint32])
     _sig(L, "tpcf_measure_fp32_peak", st, [vp, C.POINTER(C.c_double)])
+    _sig(L, "tpcf_measure_fp64_peak", st, [vp, C.POINTER(C.c_double)])
     _sig(L, "tpcf_canonical_edges", st, [C.POINTER(Bins), vp, vp])
     _sig(L, "tpcf_bin_centers", st, [C.POINTER(Bins), vp])
     _sig(L, "tpcf_set_spherical", st, [vp, i32])

@@ -832,6 +832,31 @@ tpcf_status tpcf_measure_fp32_peak(tpcf_ctx* c, double* tflops) {
   }
 }
 
+tpcf_status tpcf_measure_fp64_peak(tpcf_ctx* c, double* tflops) {
+  if (!c || !tflops) return TPCF_ERR_INVALID_ARG;
+  try {
+    begin_call(c);
+    double* out = (double*)ws_alloc(c, 16);
+    const int threads = 256, blocks = c->num_sms * 8, iters = 1 << 14;
+    cudaEvent_t e0, e1;
+    check(cudaEventCreate(&e0), "event");
+    check(cudaEventCreate(&e1), "event");
+    counted(c, launch_dfma_peak(out, blocks, threads, 256, c->stream), "dfma warm-up");
+    check(cudaEventRecord(e0, c->stream), "event record");
+    counted(c, launch_dfma_peak(out, blocks, threads, iters, c->stream), "dfma peak");
+    check(cudaEventRecord(e1, c->stream), "event record");
+    check(cudaEventSynchronize(e1), "event sync");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *tflops = 2.0 * 8.0 * (double)iters * threads * blocks / (ms * 1e-3) / 1e12;
+    return TPCF_OK;
+  } catch (const Failure& f) {
+    return fail(c, f);
+  }
+}
+
 tpcf_status tpcf_last_stats(const tpcf_ctx* c, tpcf_stats* s) {
   if (!c || !s) return TPCF_ERR_INVALID_ARG;
   s->pair_kernel_ms = c->time_pairs ? c->last_pair_ms : 0.0;
@@ -839,6 +864,8 @@ tpcf_status tpcf_last_stats(const tpcf_ctx* c, tpcf_stats* s) {
   s->n_pairs = c->last_pairs;
   s->h2d_bytes = c->h2d_bytes;
   s->kernel_launches = c->launches;
+  s->workspace_bytes = 0;
+  for (const auto& sl : c->slots) s->workspace_bytes += (int64_t)sl.bytes;
   return TPCF_OK;
 }
 

@@ -9,9 +9,9 @@
 // only re-weights them, so this is a streaming pass over the marks (HBM-bound:
 // 12 bytes per lens and bin, plus 8 bytes per lens and map).
 //
-// One block = 256 lenses of one field and up to kMapGroup maps, staged 32 lenses
-// at a time in shared memory; FP64 accumulation, per-block partial sums in
-// scratch, then a fixed-order reduction over blocks (deterministic).
+// One block = 1024 lenses of one field and up to kMapGroup maps (register
+// sums per marks row, FP64), per-block partial sums in scratch, then a
+// fixed-order reduction over blocks (deterministic).
 
 #include <algorithm>
 #include <cmath>
@@ -27,7 +27,6 @@
 
 namespace tpcf {
 
-constexpr int kMarksChunk = 256;  // lenses per block
 constexpr int kMapGroup = 16;     // maps or resamples per pass over the marks
 
 struct MarksField {
@@ -70,83 +69,109 @@ struct MultFactors {  // resamples: vw = wm = multiplicity of the lens's unit
 };
 
 // partial[(blk * n_g + g) * R + r], R = 3 n_bin + 1 (E, B, K rows, weight).
-// The block's 256 lenses are taken 32 at a time: the tile's marks
-// (3 x 32 x n_bin floats, contiguous in HBM) and its lens factors for the n_g
-// maps are staged in shared memory with coalesced loads; then each sum
-// (map, quantity, bin) is owned by one thread and accumulated over the 32
-// lenses in lens order, in FP64 in shared memory (no atomics: deterministic).
-constexpr int kTileL = 32;
+//
+// A block is NG lens groups of TG = 32 ceil(R / 32) threads; thread r of a
+// group owns row r of the marks (xi_E, xi_B, K of bin r mod n_bin, or the
+// marks weight) and keeps the kMapGroup sums of that row in registers.  The
+// block takes kMarksLens lenses in tiles of kTileL: per tile the lens factors
+// of the n_g maps (FP64, zero for lenses left out) are staged in shared
+// memory, then group k takes lenses k, k + NG, ...: each thread loads its row
+// of the lens (the group's 32-lane loads cover the lens's contiguous marks)
+// and adds it times the n_g factors (FP64 FMA, one chain per map).  Streaming
+// the marks once per pass with all n_g maps applied keeps the pass near the
+// HBM roofline.  The groups are summed in fixed order at the end
+// (deterministic, no atomics).
+constexpr int kTileL = 64;
+constexpr int kMarksLens = 1024;  // lenses per block
 template <class Fac>
-__global__ void __launch_bounds__(256) k_marks_partials(const MarksField* __restrict__ fields, int n_field,
-                                                         const Fac fac, int n_g, int n_bin,
-                                                         double* __restrict__ partial) {
+__global__ void __launch_bounds__(512, 2) k_marks_partials(const MarksField* __restrict__ fields, int n_field,
+                                                            const Fac fac, int n_g, int n_bin, int tg,
+                                                            double* __restrict__ partial) {
   extern __shared__ __align__(16) unsigned char sm[];
   const int R = 3 * n_bin + 1;
-  double* acc = reinterpret_cast<double*>(sm);                       // [n_g][R]
-  double* fvw = acc + (size_t)n_g * R;                               // [n_g][kTileL]
-  double* fwm = fvw + (size_t)n_g * kTileL;                          // [n_g][kTileL]
-  float* mk = reinterpret_cast<float*>(fwm + (size_t)n_g * kTileL);  // [3][kTileL * n_bin]
-  float* mw = mk + 3 * kTileL * n_bin;                               // [kTileL]
+  const int ng = blockDim.x / tg;
+  double* fac_s = reinterpret_cast<double*>(sm);  // [kTileL][kMapGroup] factors of the E and B rows
+  double* fw_s = fac_s + kTileL * kMapGroup;      // [kTileL][kMapGroup] factors of K and the weight
   const int blk = blockIdx.x;
   int fi = 0;
   while (fi + 1 < n_field && fields[fi + 1].chunk0 <= blk) ++fi;
   const MarksField F = fields[fi];
-  const long long j0 = (long long)(blk - F.chunk0) * kMarksChunk;
-  const long long j1 = min(F.n, j0 + kMarksChunk);
+  const long long j0 = (long long)(blk - F.chunk0) * kMarksLens;
+  const long long j1 = min(F.n, j0 + kMarksLens);
   const int tid = threadIdx.x;
-  for (int c = tid; c < n_g * R; c += blockDim.x) acc[c] = 0.0;
+  const int grp = tid / tg, r = tid % tg;
+  const int q = r / n_bin, bb = r - q * n_bin;  // q = 3: the marks weight row
+  const float* row = q == 0 ? F.xiE + bb : q == 1 ? F.xiB + bb : q == 2 ? F.K + bb : F.mw;
+  const long long rs = q < 3 ? n_bin : 1;       // stride of the row from lens to lens
+  const bool live = r < R;
+  const double* fsel = q < 2 ? fac_s : fw_s;
+  double acc[kMapGroup];
+#pragma unroll
+  for (int g = 0; g < kMapGroup; ++g) acc[g] = 0.0;
   for (long long t0 = j0; t0 < j1; t0 += kTileL) {
     const int nt = (int)min((long long)kTileL, j1 - t0);
-    __syncthreads();
-    const size_t off = (size_t)t0 * n_bin;
-    for (int e = tid; e < nt * n_bin; e += blockDim.x) {
-      mk[e] = F.xiE[off + e];
-      mk[kTileL * n_bin + e] = F.xiB[off + e];
-      mk[2 * kTileL * n_bin + e] = F.K[off + e];
-    }
-    for (int e = tid; e < n_g * kTileL; e += blockDim.x) {
-      const int g = e / kTileL, jj = e % kTileL;
+    __syncthreads();  // the previous tile's factors are no longer read
+    for (int e = tid; e < kTileL * kMapGroup; e += blockDim.x) {
+      const int jj = e / kMapGroup, g = e - jj * kMapGroup;
       double vw = 0.0, wm = 0.0;
-      if (jj < nt) {
+      if (jj < nt && g < n_g) {
         const long long j = t0 + jj;
         fac.get(F, g, j, vw, wm);
         if (!fac.keep(F.mw[j], wm)) vw = wm = 0.0;  // left out: contributes nothing
       }
-      fvw[e] = vw;
-      fwm[e] = wm;
+      fac_s[e] = vw;
+      fw_s[e] = wm;
     }
-    for (int jj = tid; jj < kTileL; jj += blockDim.x) mw[jj] = jj < nt ? F.mw[t0 + jj] : 0.f;
     __syncthreads();
-    for (int c = tid; c < n_g * R; c += blockDim.x) {
-      const int g = c / R, r = c % R;
-      const double* fv = fvw + g * kTileL;
-      const double* fw = fwm + g * kTileL;
-      double a = acc[c];
-      if (r < 3 * n_bin) {
-        const int q = r / n_bin, bb = r % n_bin;
-        const float* m = mk + q * kTileL * n_bin + bb;
-        const double* f = q < 2 ? fv : fw;
-        for (int jj = 0; jj < nt; ++jj) a = fma((double)m[jj * n_bin], f[jj], a);
-      } else {
-        for (int jj = 0; jj < nt; ++jj) a = fma((double)mw[jj], fw[jj], a);
+    if (live) {
+      const float* base = row + t0 * rs;
+#pragma unroll 4
+      for (int jj = grp; jj < nt; jj += ng) {
+        const double m = (double)__ldg(base + jj * rs);
+        const double2* f2 = reinterpret_cast<const double2*>(fsel + jj * kMapGroup);
+#pragma unroll
+        for (int h = 0; h < kMapGroup / 2; ++h) {
+          const double2 f = f2[h];
+          acc[2 * h] = fma(m, f.x, acc[2 * h]);
+          acc[2 * h + 1] = fma(m, f.y, acc[2 * h + 1]);
+        }
       }
-      acc[c] = a;
     }
   }
-  __syncthreads();
-  for (int c = tid; c < n_g * R; c += blockDim.x) partial[(size_t)blk * n_g * R + c] = acc[c];
+  // groups 1.. add their sums into group 0's, in group order
+  double* red = fac_s;  // [tg][kMapGroup]
+  for (int k = 1; k < ng; ++k) {
+    __syncthreads();
+    if (grp == k) {
+#pragma unroll
+      for (int g = 0; g < kMapGroup; ++g) red[r * kMapGroup + g] = acc[g];
+    }
+    __syncthreads();
+    if (grp == 0) {
+#pragma unroll
+      for (int g = 0; g < kMapGroup; ++g) acc[g] += red[r * kMapGroup + g];
+    }
+  }
+  if (grp == 0 && live) {
+#pragma unroll
+    for (int g = 0; g < kMapGroup; ++g)
+      if (g < n_g) partial[((size_t)blk * n_g + g) * R + r] = acc[g];
+  }
 }
 
-size_t marks_smem(int n_g, int n_bin) {
-  const int R = 3 * n_bin + 1;
-  return sizeof(double) * ((size_t)n_g * R + 2 * (size_t)n_g * kTileL) + sizeof(float) * (3 * kTileL * n_bin + kTileL);
+// Threads per lens group (one per marks row, whole warps) and per block.
+int marks_group_threads(int n_bin) { return (3 * n_bin + 1 + 31) / 32 * 32; }
+int marks_block_threads(int n_bin) {
+  const int tg = marks_group_threads(n_bin);
+  return tg >= 256 ? tg : (256 / tg) * tg;
 }
-// maps or resamples per pass: at most kMapGroup, and the shared memory within 96 KB
-int marks_group(int n_bin) {
-  int g = kMapGroup;
-  while (g > 1 && marks_smem(g, n_bin) > 96 * 1024) --g;
-  return g;
+size_t marks_smem(int n_bin) {
+  const size_t fac = 2 * sizeof(double) * kTileL * kMapGroup;
+  const size_t red = sizeof(double) * (size_t)marks_group_threads(n_bin) * kMapGroup;
+  return std::max(fac, red);
 }
+// maps or resamples per pass over the marks
+int marks_group(int) { return kMapGroup; }
 
 // Multiplicities of G resamples s0.. over n_units units: n_draw draws each,
 // counter (d/4, s, 0x2BCF, 0), word d%4, index by multiply-shift (the stream
@@ -231,7 +256,7 @@ extern "C" tpcf_status tpcf_xi_from_marks(tpcf_ctx* c, int32_t n_field, const tp
       F.n_bin = nb;
       F.chunk0 = nblk;
       F.lens0 = 0;
-      nblk += (int)((n + kMarksChunk - 1) / kMarksChunk);
+      nblk += (int)((n + kMarksLens - 1) / kMarksLens);
       F.mw = stage(c, m.w, n);
       F.xiE = stage(c, m.xi_E, n * nb);
       F.xiB = stage(c, m.xi_B, n * nb);
@@ -268,13 +293,14 @@ extern "C" tpcf_status tpcf_xi_from_marks(tpcf_ctx* c, int32_t n_field, const tp
     double* part = (double*)ws_alloc(c, sizeof(double) * (size_t)std::max(nblk, 1) * kMapGroup * R);
     double* dout = (double*)ws_alloc(c, sizeof(double) * (size_t)kMapGroup * n_field * R);
     const int MG = marks_group(nb);
-    const size_t msm = marks_smem(MG, nb);
+    const size_t msm = marks_smem(nb);
     check(cudaFuncSetAttribute(k_marks_partials<MapFactors>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm),
           "smem attr");
     for (int m0 = 0; m0 < n_map; m0 += MG) {
       const int g = std::min(MG, n_map - m0);
       if (nblk > 0) {
-        k_marks_partials<MapFactors><<<nblk, 256, marks_smem(g, nb), st>>>(df, n_field, MapFactors{m0}, g, nb, part);
+        k_marks_partials<MapFactors><<<nblk, marks_block_threads(nb), msm, st>>>(df, n_field, MapFactors{m0}, g, nb,
+                                                                                marks_group_threads(nb), part);
         counted(c, cudaGetLastError(), "marks partials");
       }
       const int tot = g * n_field * R;
@@ -349,7 +375,7 @@ extern "C" tpcf_status tpcf_marks_bootstrap(tpcf_ctx* c, int32_t n_field, const 
       F.chunk0 = nblk;
       F.lens0 = off;
       off += m.n;
-      nblk += (int)((m.n + kMarksChunk - 1) / kMarksChunk);
+      nblk += (int)((m.n + kMarksLens - 1) / kMarksLens);
       F.mw = stage(c, m.w, m.n);
       F.xiE = stage(c, m.xi_E, m.n * nb);
       F.xiB = stage(c, m.xi_B, m.n * nb);
@@ -381,7 +407,7 @@ extern "C" tpcf_status tpcf_marks_bootstrap(tpcf_ctx* c, int32_t n_field, const 
     std::vector<double> sums((size_t)n_boot * n_field * R, 0.0);
     const int MG = marks_group(nb);
     check(cudaFuncSetAttribute(k_marks_partials<MultFactors>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)marks_smem(MG, nb)), "smem attr");
+                               (int)marks_smem(nb)), "smem attr");
     for (int s0 = 0; s0 < n_boot; s0 += MG) {
       const int G = std::min(MG, n_boot - s0);
       const int* mult;
@@ -396,9 +422,8 @@ extern "C" tpcf_status tpcf_marks_bootstrap(tpcf_ctx* c, int32_t n_field, const 
         mult = mbuf;
       }
       if (nblk > 0) {
-        k_marks_partials<MultFactors><<<nblk, 256, marks_smem(G, nb), st>>>(df, n_field,
-                                                                            MultFactors{mult, dunit, n_units}, G,
-                                                                            nb, part);
+        k_marks_partials<MultFactors><<<nblk, marks_block_threads(nb), marks_smem(nb), st>>>(
+            df, n_field, MultFactors{mult, dunit, n_units}, G, nb, marks_group_threads(nb), part);
         counted(c, cudaGetLastError(), "bootstrap partials");
         const int tot = G * n_field * R;
         k_marks_reduce<<<(tot + 255) / 256, 256, 0, st>>>(part, df, n_field, nblk, G, R, dout);

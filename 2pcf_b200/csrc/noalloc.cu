@@ -48,7 +48,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 std::mutex g_addr_mu;
 void* g_addr[kMaxDevices] = {};
 
-// Device address of g_noalloc_scratch on the current device (looked up once).
+// Device address of g_noalloc_scratch on the current device (looked up once
+// per device; it stays valid as long as the device's primary context does, so
+// cudaDeviceReset between calls is not supported).
 void* scratch_base(int device) {
   if (device < 0 || device >= kMaxDevices) throw Failure(TPCF_ERR_INVALID_ARG, "device index too large");
   std::lock_guard<std::mutex> lk(g_addr_mu);

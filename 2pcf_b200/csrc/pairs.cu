@@ -1031,6 +1031,21 @@ __global__ void k_ffma_peak(float* out, int iters, float a, float b) {
   if (s == 12345.678f) out[0] = s;  // keeps the loop alive, never true in practice
 }
 
+// FP64 FMA throughput probe: 8 independent DFMA chains per thread.
+__global__ void k_dfma_peak(double* out, int iters, double a, double b) {
+  double r[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r[k] = threadIdx.x * 1e-3 + k;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r[k] = fma(r[k], a, b);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += r[k];
+  if (s == 12345.678) out[0] = s;  // keeps the loop alive, never true in practice
+}
+
 // Per-patch FP64 sums from item sums, fixed order (deterministic).
 // patch_groups[p] .. patch_groups[p+1] are the groups of patch p.
 __global__ void k_patch_reduce(const double* __restrict__ item_sums, int item_base, const int* __restrict__ patch_groups,
@@ -1221,6 +1236,10 @@ cudaError_t launch_permute_items(const int2* items, const int* order, int n, int
 }
 cudaError_t launch_ffma_peak(float* out, int blocks, int threads, int iters, cudaStream_t st) {
   k_ffma_peak<<<blocks, threads, 0, st>>>(out, iters, 0.999999f, 1e-7f);
+  return cudaGetLastError();
+}
+cudaError_t launch_dfma_peak(double* out, int blocks, int threads, int iters, cudaStream_t st) {
+  k_dfma_peak<<<blocks, threads, 0, st>>>(out, iters, 0.999999999, 1e-13);
   return cudaGetLastError();
 }
 cudaError_t launch_patch_reduce(const double* item_sums, int item_base, const int* patch_groups, int n_patch, int nb,

@@ -60,6 +60,7 @@ cudaError_t launch_item_cost(const int2* items, int n_items, const TaskDesc* tas
 cudaError_t launch_permute_items(const int2* items, const int* order, int n, int index, int count, int2* out,
                                  cudaStream_t st);
 cudaError_t launch_ffma_peak(float* out, int blocks, int threads, int iters, cudaStream_t st);
+cudaError_t launch_dfma_peak(double* out, int blocks, int threads, int iters, cudaStream_t st);
 cudaError_t launch_patch_reduce(const double* item_sums, int item_base, const int* patch_groups, int n_patch,
                                 int nb, double* patch_sums, cudaStream_t st);
 cudaError_t launch_lens_outputs(const double* acc, const float4* rec, const int* perm, int n_valid, int nb,

@@ -316,7 +316,9 @@ def widened_timing(tpcf, w, peak_fp32, stream, cpu_threads, with_cpu=True):
     mctx = tpcf.Context(0)
     mctx.set_stream(stream.cuda_stream)
     _, ms = timed(lambda: tpcf.calculate_tpcf_from_marks([mk], [val], [wm], ctx=mctx))
-    byt = (n_map + 3) // 4 * (3 * 4 * n * nbm + 4 * n) + n_map * 8 * n
+    # algorithmic bytes: the marks once (xi_E, xi_B, K [n][n_bin] and the marks
+    # weight, FP32) and the maps' val and w [n_map][n] (FP32)
+    byt = (3 * 4 * n * nbm + 4 * n) + n_map * 8 * n
     hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"] \
         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
     out["marks_reweight"] = {"maps": n_map, "lenses": n, "n_bin": nbm, "call_ms": ms,
@@ -324,10 +326,14 @@ def widened_timing(tpcf, w, peak_fp32, stream, cpu_threads, with_cpu=True):
                                           "unit": "GB/s", "frac": byt / (ms * 1e-3) / 1e9 / hbm,
                                           "bytes": byt}}
     _, ms = timed(lambda: tpcf.marks_bootstrap([mk], 1000, seed=5, covariance=True, ctx=mctx))
-    byt = 250 * (3 * 4 * n * nbm + 4 * n)
+    # each resample re-weights every lens's 3 n_bin + 1 marks: one FP64 FMA
+    # each (the multiplicities are drawn on the device), so FP64-bound
+    flop = 1000 * n * (3 * nbm + 1) * 2
+    p64 = mctx.measure_fp64_peak()
     out["marks_bootstrap"] = {"resamples": 1000, "lenses": n, "call_ms": ms,
-                              "roofline": {"bound": "hbm", "achieved": byt / (ms * 1e-3) / 1e9, "peak": hbm,
-                                           "unit": "GB/s", "frac": byt / (ms * 1e-3) / 1e9 / hbm, "bytes": byt}}
+                              "roofline": {"bound": "fp64", "achieved": flop / (ms * 1e-3) / 1e12, "peak": p64,
+                                           "unit": "TFLOP/s", "frac": flop / (ms * 1e-3) / 1e12 / p64,
+                                           "flop": flop, "peak_source": "FP64 FMA loop measured in this run"}}
     del mk, val, wm
 
     # equal-weight k-means on all lens positions, 100 blocks

@@ -174,6 +174,8 @@ typedef struct tpcf_stats {
   int64_t n_pairs;          /* sum of n_pairs over all bins and tasks       */
   int64_t h2d_bytes;        /* bytes copied host->device by the last call   */
   int64_t kernel_launches;  /* kernels launched by this context so far      */
+  int64_t workspace_bytes;  /* device workspace this context holds (grown by
+                               cudaMalloc on demand, freed by tpcf_destroy)  */
 } tpcf_stats;
 tpcf_status tpcf_set_timing(tpcf_ctx* ctx, int32_t enable);
 tpcf_status tpcf_last_stats(const tpcf_ctx* ctx, tpcf_stats* stats);
@@ -202,6 +204,9 @@ tpcf_status tpcf_debug_inject(tpcf_ctx* ctx, int64_t fail_alloc, int32_t skip_ti
  * FP32 FMA throughput (FLOP/s counting an FMA as 2) with a register-resident
  * FFMA loop timed by CUDA events on the context stream. */
 tpcf_status tpcf_measure_fp32_peak(tpcf_ctx* ctx, double* tflops);
+/* The same for FP64 FMA (a register-resident DFMA loop); no counterpart in the
+ * reference.  The roofline of the FP64-bound resampling passes. */
+tpcf_status tpcf_measure_fp64_peak(tpcf_ctx* ctx, double* tflops);
 
 /* Canonical FP64 edges [n_bin+1] and squared edges [n_bin+1]: the bin rule of
  * every pair kernel.  A pair with d2 = dx*dx + dy*dy (FP64, from the FP32
@@ -520,8 +525,13 @@ tpcf_status tpcf_bootstrap(tpcf_ctx* ctx, const double* patch_sums, int32_t n_ta
  * (what must start at zero is cleared by each call): calls that overlap on the
  * GPU, from two host threads or two streams, race.  Patches and per-lens
  * outputs are not available (those fields of `out` must be NULL).  A call that
- * needs more than the 64 MiB (roughly 600 thousand objects in all) fails with
- * TPCF_ERR_OVERFLOW before any pair work. */
+ * needs more than the 64 MiB fails with TPCF_ERR_OVERFLOW before any pair
+ * work: about 100 bytes per object of either catalogue, i.e. roughly 600
+ * thousand objects in all (the cell table is kept within an eighth of the
+ * array by coarsening the cells when theta_max is small against the field, so
+ * the field's extent does not lower the limit).  The cached address is only
+ * valid for the device context that looked it up: do not call
+ * cudaDeviceReset between calls. */
 tpcf_status tpcf_shear_scalar_noalloc(tpcf_ctx* ctx,
                                       const float* xA, const float* yA, const float* zA,
                                       const float* valA, const float* wA, int64_t nA,
