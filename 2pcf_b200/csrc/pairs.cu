@@ -45,6 +45,9 @@
 #ifndef TPCF_SINGLE_UNROLL
 #define TPCF_SINGLE_UNROLL 4
 #endif
+#ifndef TPCF_GUARD_ALU
+#define TPCF_GUARD_ALU 0
+#endif
 
 namespace tpcf {
 
@@ -292,7 +295,13 @@ __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int lo
   // lanes of class 1 (or 0) keep an edge no pair reaches
   const float E = (cls == 2) ? C.e2f[blo + 1] : 3.0e38f;
   const float gE = (cls == 2) ? E * C.eps_rel : 0.f;
+#if TPCF_GUARD_ALU
+  // guard band [E - gE, E + gE] by two compares (integer pipe); outside it
+  // d2 >= E and d2 > E + gE agree
+  const float Elo = E - gE, Ehi = E + gE;
+#else
   const float2 nE = dup2(-E);
+#endif
   bool near = false;  // some pair lies within the guard band of E
   const int k0 = PART ? (lo >> 1) : 0;
   const int k1 = PART ? ((hi + 1) >> 1) : kChunk / 2;
@@ -301,9 +310,15 @@ __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int lo
     const float4 xy = S[k].xy, pq = S[k].pq, wk = S[k].wk;
     float2 d2, d, r, X, Y;
     pair_terms2<MODE, LOGB>(L, xy, pq, d2, d, r, X, Y);
+#if TPCF_GUARD_ALU
+    bool u0 = d2.x > Ehi, u1 = d2.y > Ehi;
+    const bool n0 = d2.x >= Elo && !u0, n1 = d2.y >= Elo && !u1;
+#else
     const float2 dE = add2(d2, nE);
-    float2 w = lo2(wk), K = hi2(wk);
     bool u0 = d2.x >= E, u1 = d2.y >= E;
+    const bool n0 = fabsf(dE.x) <= gE, n1 = fabsf(dE.y) <= gE;
+#endif
+    float2 w = lo2(wk), K = hi2(wk);
     if (MK) {
       bool a0, a1;
       const float2 zm = pair_mask<HAS_Z, PART>(S, k, lz, lo, hi, a0, a1);
@@ -313,11 +328,9 @@ __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int lo
       sn = add2(sn, zm);
       u0 = u0 && a0;
       u1 = u1 && a1;
-      near |= a0 && fabsf(dE.x) <= gE;
-      near |= a1 && fabsf(dE.y) <= gE;
+      near |= (a0 && n0) || (a1 && n1);
     } else {
-      near |= fabsf(dE.x) <= gE;
-      near |= fabsf(dE.y) <= gE;
+      near |= n0 || n1;
     }
     // products folded into the sums: one packed FFMA per quantity and side
     if (!(LI && MODE == 1)) {

@@ -574,6 +574,7 @@ def path_stats(tpcf, args):
     S = [tpcf.ShapeCatalog(**{k: dev(s[k]) for k in ("x", "y", "e1", "e2", "w", "z", "m")})
          for s in w["shape_bins"]]
     ctx = tpcf.Context(0)
+    ctx.set_cell_size(bins.x_max / (args.cell_divisor or 64))
     lib = tpcf._lib.lib()
     st = (C.c_ulonglong * 8)()
     lib.tpcf_debug_mode_stats(st)
@@ -656,10 +657,9 @@ def main():
                          "pair kernel instead")
     ap.add_argument("--no-widened", action="store_true",
                     help="skip the spherical, marks, bootstrap, k-means and reader measurements")
-    ap.add_argument("--cell-divisor", type=int, default=64,
-                    help="grid cell side theta_max/D (64: the autotuner's usual choice on this workload)")
-    ap.add_argument("--autotune", action="store_true",
-                    help="pick the cell side with 2pcf_b200.autotune on a corner of the field instead")
+    ap.add_argument("--cell-divisor", type=int, default=0,
+                    help="fix the grid cell side at theta_max/D and the default tile shape instead of running "
+                         "the autotuner (2pcf_b200.autotune) once before the warm-up")
     ap.add_argument("--config", type=int, default=5, choices=[1, 2, 3, 4, 5],
                     help="5 (default): the tomography headline; 1-4: only that configuration's line")
     ap.add_argument("--no-configs", action="store_true",
@@ -705,17 +705,18 @@ def main():
     ctx.set_timing(True)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
-    # cell side picked by the autotuner (trial calls on a density-preserving corner)
-    if not args.autotune:
+    # cell side and tile shape picked once by the autotuner (trial calls on a
+    # density-preserving corner of the field, before the warm-up), or fixed
+    if args.cell_divisor > 0:
         ctx.set_cell_size(bins.x_max / args.cell_divisor)
-        tune = {}
+        tune = None
     else:
         at = importlib.import_module("2pcf_b200.autotune")
-        tune = at.autotune_cell_size(
+        tune = at.autotune(
             [tpcf.LensCatalog(**{k: l[k] for k in ("x", "y", "val", "w", "z")}) for l in w["lens_bins"]],
             [tpcf.ShapeCatalog(**{k: s_[k] for k in ("x", "y", "e1", "e2", "w", "z", "m")})
              for s_ in w["shape_bins"]],
-            w["tasks"], bins, ctx, spherical_coords=sphere)
+            w["tasks"], bins, ctx, corner=0.4, spherical_coords=sphere)
     if world > 1:
         ctx.set_shard(rank, world)
     n_boot = w["n_boot"]
@@ -819,7 +820,10 @@ def main():
                    "parallelism": f"work items sharded over {world} rank(s)" if world > 1 else "single GPU",
                    "l2": "inputs (280 MB of catalogues) larger than L2 (126 MB); no flush",
                    "cell_size": ctx.cell_size,
-                   "autotune_ms_per_gpair": {f"theta_max/{d}": round(v, 2) for d, v in tune.items()},
+                   "tile_shape": {"group_size": ctx.tile_shape[0] or 128, "tile_chunks": ctx.tile_shape[1] or 4},
+                   "autotune_ms_per_gpair": None if tune is None else {
+                       "cell": {f"theta_max/{d}": round(v, 3) for d, v in tune["cell"].items()},
+                       "tile": {g: round(v, 3) for g, v in tune["tile"].items()}, "choice": tune["choice"]},
                    "step": "k-means (100 patches, all 2.4 M lens positions) + grid build + one 25-task "
                            "pair launch + per-patch sums + 1000-resample bootstrap with the joint "
                            "500x500 covariance"},
