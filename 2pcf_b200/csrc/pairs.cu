@@ -45,9 +45,6 @@
 #ifndef TPCF_SINGLE_UNROLL
 #define TPCF_SINGLE_UNROLL 4
 #endif
-#ifndef TPCF_GUARD_ALU
-#define TPCF_GUARD_ALU 0
-#endif
 
 namespace tpcf {
 
@@ -295,13 +292,7 @@ __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int lo
   // lanes of class 1 (or 0) keep an edge no pair reaches
   const float E = (cls == 2) ? C.e2f[blo + 1] : 3.0e38f;
   const float gE = (cls == 2) ? E * C.eps_rel : 0.f;
-#if TPCF_GUARD_ALU
-  // guard band [E - gE, E + gE] by two compares (integer pipe); outside it
-  // d2 >= E and d2 > E + gE agree
-  const float Elo = E - gE, Ehi = E + gE;
-#else
   const float2 nE = dup2(-E);
-#endif
   bool near = false;  // some pair lies within the guard band of E
   const int k0 = PART ? (lo >> 1) : 0;
   const int k1 = PART ? ((hi + 1) >> 1) : kChunk / 2;
@@ -310,14 +301,9 @@ __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int lo
     const float4 xy = S[k].xy, pq = S[k].pq, wk = S[k].wk;
     float2 d2, d, r, X, Y;
     pair_terms2<MODE, LOGB>(L, xy, pq, d2, d, r, X, Y);
-#if TPCF_GUARD_ALU
-    bool u0 = d2.x > Ehi, u1 = d2.y > Ehi;
-    const bool n0 = d2.x >= Elo && !u0, n1 = d2.y >= Elo && !u1;
-#else
     const float2 dE = add2(d2, nE);
     bool u0 = d2.x >= E, u1 = d2.y >= E;
     const bool n0 = fabsf(dE.x) <= gE, n1 = fabsf(dE.y) <= gE;
-#endif
     float2 w = lo2(wk), K = hi2(wk);
     if (MK) {
       bool a0, a1;
@@ -388,8 +374,9 @@ __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int lo
 }
 
 #ifdef TPCF_MODE_STATS
-// Diagnostic build only: warp-level path counts [4] and lane-pairs per path [4].
-__device__ unsigned long long g_mode_stats[8];
+// Diagnostic build only: warp-level path counts [4], lane-pairs per warp path
+// [4], and lane-pairs per lane class [4] (active lanes only).
+__device__ unsigned long long g_mode_stats[12];
 extern "C" int tpcf_debug_mode_stats(unsigned long long* out) {
   return (int)cudaMemcpyFromSymbol(out, g_mode_stats, sizeof(g_mode_stats));
 }
@@ -535,8 +522,8 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
   double* wsum = bsum + (size_t)warp * kQ * nb;
   const int flush_src = P.flush_src > 0 ? P.flush_src : 4096;
 #ifdef TPCF_MODE_STATS
-  __shared__ unsigned long long sh_stats[8];
-  if (tid < 8) sh_stats[tid] = 0ull;
+  __shared__ unsigned long long sh_stats[12];
+  if (tid < 12) sh_stats[tid] = 0ull;
   __syncthreads();
 #endif
   for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
@@ -632,9 +619,12 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
 #ifdef TPCF_MODE_STATS
             {
               const unsigned nact = __popc(__ballot_sync(0xffffffffu, act));
+              unsigned ncls[4];
+              for (int cc = 0; cc < 4; ++cc) ncls[cc] = __popc(__ballot_sync(0xffffffffu, act && cls == cc));
               if (lane == 0) {
                 atomicAdd(&sh_stats[m], 1ull);
                 atomicAdd(&sh_stats[4 + m], (unsigned long long)((hi - lo) * nact));
+                for (int cc = 0; cc < 4; ++cc) atomicAdd(&sh_stats[8 + cc], (unsigned long long)((hi - lo) * ncls[cc]));
               }
             }
 #endif
@@ -707,7 +697,7 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
   }
 #ifdef TPCF_MODE_STATS
   __syncthreads();
-  if (tid < 8) atomicAdd(&g_mode_stats[tid], sh_stats[tid]);
+  if (tid < 12) atomicAdd(&g_mode_stats[tid], sh_stats[tid]);
 #endif
 }
 

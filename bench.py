@@ -576,7 +576,7 @@ def path_stats(tpcf, args):
     ctx = tpcf.Context(0)
     ctx.set_cell_size(bins.x_max / (args.cell_divisor or 64))
     lib = tpcf._lib.lib()
-    st = (C.c_ulonglong * 8)()
+    st = (C.c_ulonglong * 12)()
     lib.tpcf_debug_mode_stats(st)
     base = np.array(st[:])
     outs = tpcf.batch_shear_2pcf(L, S, w["tasks"], bins, ctx=ctx)
@@ -585,8 +585,11 @@ def path_stats(tpcf, args):
     binned = sum(int(o.n_pairs.sum()) for o in outs)
     res = {"binned_pairs": binned}
     for i, name in enumerate(("skip", "single_bin", "one_edge", "per_pair")):
-        res[name] = {"warp_chunks": float(v[i] / v[:4].sum()), "lane_pairs": float(v[4 + i] / v[4:].sum())}
-    res["computed_lane_pairs_per_binned_pair"] = float(v[5:].sum() / binned)
+        res[name] = {"warp_chunks": float(v[i] / v[:4].sum()), "lane_pairs": float(v[4 + i] / v[4:8].sum())}
+    res["computed_lane_pairs_per_binned_pair"] = float(v[5:8].sum() / binned)
+    res["lane_class_of_active_lane_pairs"] = {name: float(v[8 + i] / v[8:12].sum())
+                                              for i, name in enumerate(("out_of_range", "single_bin", "one_edge",
+                                                                        "per_pair"))}
     print(json.dumps(res), flush=True)
 
 
