@@ -157,9 +157,10 @@ class Context:
         self.cell_size = float(cell_size)
 
     def set_tile_shape(self, group_size: int = 0, tile_chunks: int = 0):
-        """Planar pair kernel tile shape for later calls: lenses per group
-        (32, 64, 128) and 32-source sub-chunks per source tile (2, 4); 0 keeps
-        the default.  Changes speed only, never results."""
+        """Planar pair kernel tile shape for later calls: threads per block
+        (32, 64, 128; every warp takes 32-lens work items of its own) and
+        32-source sub-chunks per source tile (1, 2); 0 keeps the default.
+        Changes speed only, never results."""
         _check(lib().tpcf_set_tile_shape(self._h, int(group_size), int(tile_chunks)), self._h)
         self.tile_shape = (int(group_size), int(tile_chunks))
 

@@ -3,9 +3,10 @@
 The grid cell side trades the area scanned around each lens group (smaller
 cells hug the theta_max disc more tightly) against per-row overhead and
 partial sub-chunks at the ends of shorter source runs.  The tile shape is the
-number of lenses per group (threads per block: 128 or 64) and the number of
-32-source sub-chunks per source tile (4 or 2: fewer, larger copies against
-more tiles in flight between the warps).  ``autotune`` times the pair kernel
+number of threads per block (128 or 64: warps, each with its own 32-lens work
+items, sharing one block's shared memory) and the number of 32-source
+sub-chunks per source tile (2 or 1: fewer, larger copies against more tiles
+in flight in each warp's ring).  ``autotune`` times the pair kernel
 (CUDA events on the launch stream, via tpcf_last_stats) on a corner of the
 field that keeps the object density: first every cell side theta_max/d with
 the default shape, then every shape with the best cell side, and sets the
@@ -19,7 +20,7 @@ import numpy as np
 from . import Context, batch_shear_2pcf
 
 DIVISORS = (16, 24, 32, 48, 64, 96)
-SHAPES = ((128, 4), (128, 2), (64, 4))   # (lenses per group, sub-chunks per tile)
+SHAPES = ((128, 2), (128, 1), (64, 2))   # (threads per block, sub-chunks per tile)
 
 
 def _corner(cats, x_cut, y_cut):

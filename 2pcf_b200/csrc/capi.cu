@@ -311,9 +311,12 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
   const int qa = has_m ? 6 : 5;
   int bt = 128;
   while (bt > 32 && (size_t)nb * qa * bt * 4 > 100 * 1024) bt /= 2;
-  int tch = 4;
+  // planar: bt threads per block, each warp one 32-lens group at a time, tiles
+  // of tch sub-chunks; sphere: one bt-lens group per block
+  int tch = 2;
   if (!sph && c->opts.group_size > 0 && c->opts.group_size <= bt) bt = c->opts.group_size;
-  if (!sph && bt == 128 && c->opts.tile_chunks == 2) tch = 2;
+  if (!sph && c->opts.tile_chunks == 1) tch = 1;
+  const int lens_group = sph ? bt : 32;
 
   const double Rd = bins->x_max;
   float R = (float)(Rd * (1.0 + 1e-6));
@@ -388,7 +391,7 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
   if (sph) margin = (float)(2.0 * M_PI + M_PI);  // reduced longitudes and latitudes
   margin = (float)(1e-5 * (margin + Rd) + 1e-4 * maxcell);
 
-  // ---- lens catalogues: sort by (patch, Morton), groups of <= bt lenses
+  // ---- lens catalogues: sort by (patch, Morton), groups of <= lens_group lenses
   std::vector<LensBuilt> lb(nL);
   std::vector<LensDesc> ldesc(nL);
   for (int i = 0; i < nL; ++i) {
@@ -425,7 +428,7 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     B.patch_groups.assign(n_patch_eff + 1, 0);
     for (int p = 0; p < n_patch_eff; ++p) {
       B.patch_groups[p] = (int)gstart.size();
-      for (int s0 = off[p]; s0 < off[p + 1]; s0 += bt) gstart.push_back(s0);
+      for (int s0 = off[p]; s0 < off[p + 1]; s0 += lens_group) gstart.push_back(s0);
     }
     B.patch_groups[n_patch_eff] = (int)gstart.size();
     B.n_groups = (int)gstart.size();
@@ -528,12 +531,13 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
       P.binA = P.binB = 0.f;
       P.eps = 4e-6f;
     }
-    // FP32 histogram folded into FP64 every 4096 sources: each histogram cell
-    // then holds at most 128 register sums of 32 pairs (measured: the parity
-    // bar of 1e-6 of sum|terms| holds at 1024, 2048 and 4096; 4096 is 4%
-    // faster than 1024, and 18% with per-lens outputs, whose FP64 columns are
-    // updated at every fold)
-    P.flush_src = 4096;
+    // FP32 histogram folded into FP64 every 4096 sources (each histogram cell
+    // then holds at most 128 register sums of 32 pairs): the per-bin sums of
+    // the call stay within 1e-6 of sum|terms|.  Per-lens outputs are sums of
+    // far fewer terms per cell, so their FP32 partials are folded every 1024
+    // sources (at 4096 one lens and bin of the 2 M x 0.5 M clustered
+    // workload reached 1.05e-6 of its sum|terms|)
+    P.flush_src = lens_acc ? 1024 : 4096;
     P.debug_skip_tile = c->skip_tile + 1;
     P.wait_limit = c->wait_limit;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -758,7 +762,7 @@ tpcf_status tpcf_debug_inject(tpcf_ctx* c, int64_t fail_alloc, int32_t skip_tile
 
 tpcf_status tpcf_set_tile_shape(tpcf_ctx* c, int32_t group_size, int32_t tile_chunks) {
   if (!c || (group_size != 0 && group_size != 32 && group_size != 64 && group_size != 128) ||
-      (tile_chunks != 0 && tile_chunks != 2 && tile_chunks != 4))
+      (tile_chunks != 0 && tile_chunks != 1 && tile_chunks != 2))
     return TPCF_ERR_INVALID_ARG;
   c->opts.group_size = group_size;
   c->opts.tile_chunks = tile_chunks;

@@ -202,7 +202,7 @@ tpcf_status run_noalloc(tpcf_ctx* c, const float* xA, const float* yA, const flo
                                     std::fabs(hbox[8 * i + 3]));
   margin = (float)(1e-5 * (margin + Rd) + 1e-4 * g.cell);
 
-  // lenses: sorted by Morton code, groups of bt (one patch)
+  // lenses: sorted by Morton code, groups of 32 (one per warp of the pair kernel; one patch)
   const int nl_valid = (int)hcnt[0];
   float4* lrec = (float4*)cv.take(sizeof(float4) * std::max(nl_valid, 1));
   float* zs = (float*)cv.take(sizeof(float) * std::max(nl_valid, 1));
@@ -220,7 +220,8 @@ tpcf_status run_noalloc(tpcf_ctx* c, const float* xA, const float* yA, const flo
     check(sort_pairs_u64(tmp, tb, k0, k1, i0, i1, (int)nA, st), "sort lenses");
     counted(c, launch_lens_gather(i1, nl_valid, xA, yA, zA, valA, wA, lrec, zs, perm, st), "lens gather");
   }
-  const int n_groups = (nl_valid + bt - 1) / bt;
+  constexpr int kGroup = 32;
+  const int n_groups = (nl_valid + kGroup - 1) / kGroup;
   int* gstart = (int*)cv.take(sizeof(int) * (n_groups + 1));
   int2* items = (int2*)cv.take(sizeof(int2) * std::max(n_groups, 1));
   int* pgroups = (int*)cv.take(sizeof(int) * 2);
@@ -235,7 +236,7 @@ tpcf_status run_noalloc(tpcf_ctx* c, const float* xA, const float* yA, const flo
   int* head = (int*)cv.take(sizeof(int) * 4);
   unsigned* err = (unsigned*)(head + 1);
 
-  k_na_groups<<<(n_groups + 1 + 255) / 256, 256, 0, st>>>(gstart, n_groups, nl_valid, bt, items, pgroups);
+  k_na_groups<<<(n_groups + 1 + 255) / 256, 256, 0, st>>>(gstart, n_groups, nl_valid, kGroup, items, pgroups);
   counted(c, cudaGetLastError(), "groups");
   counted(c, launch_group_box(lrec, gstart, n_groups, gbox, st), "group box");
   TaskDesc td{};
@@ -267,7 +268,7 @@ tpcf_status run_noalloc(tpcf_ctx* c, const float* xA, const float* yA, const flo
       P.eps = 4e-6f;
     }
     int grid = 0;
-    counted(c, launch_pairs(P, 0, has_m, has_z, logb, bt, 4, 0, c->num_sms, st, &grid), "pair kernel");
+    counted(c, launch_pairs(P, 0, has_m, has_z, logb, bt, 2, 0, c->num_sms, st, &grid), "pair kernel");
     counted(c, launch_patch_reduce(item_sums, 0, pgroups, 1, nb, psum, st), "patch reduce");
   } else {
     check(cudaMemsetAsync(psum, 0, sizeof(double) * kQ * nb, st), "clear sums");

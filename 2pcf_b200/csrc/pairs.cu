@@ -58,36 +58,36 @@ constexpr int kPairMinBlocks = 3;
 // Coordinate of the null source that pads the last sub-chunk of a grid: its
 // d2 (~2e36) stays finite in FP32 and its weight and values are zero.
 constexpr float kNullPos = 1.0e18f;
-// Source bytes in flight per block: NBUF = kSrcRing / (TCH KB) tile buffers of
-// TCH sub-chunks (1 KB each) plus their ChunkMeta.
-constexpr int kSrcRing = 16384;
+// Source bytes in flight per warp: NBUF = kWarpRing / (TCH KB) tile buffers
+// of TCH sub-chunks (1 KB each) plus their ChunkMeta.
+constexpr int kWarpRing = 4096;
+constexpr int kRowsPerPass = 32;  // cell rows whose spans a warp holds at once (one per lane)
 
 // ------------------------------------------------------- shared-memory map --
 struct PairSmem {
-  size_t tiles, meta, hist, bsum, e2s, fvw, fw, e2f, span0, span1, mbar, cnt, last, misc, total;
+  size_t ring, hist, bsum, e2s, fvw, fw, e2f, mbar, misc, total;
 };
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
-// bt here is the number of histogram columns (threads), tch the sub-chunks per tile.
+// Bytes of one ring buffer: TCH sub-chunks and their metadata.
+__host__ __device__ inline size_t ring_buffer_bytes(int tch) {
+  return (size_t)tch * (kChunk * sizeof(SrcRec) + sizeof(ChunkMeta));
+}
+// bt is the number of threads (histogram columns), tch the sub-chunks per tile.
 __host__ __device__ inline PairSmem pair_smem_layout(int nb, int qa, int bt, int tch) {
-  const int nbuf = kSrcRing / (tch * kChunk * (int)sizeof(SrcRec));
+  const int nw = bt / 32;
+  const int nbuf = kWarpRing / (tch * kChunk * (int)sizeof(SrcRec));
   PairSmem s;
   size_t o = 0;
-  s.tiles = o; o += (size_t)nbuf * tch * kChunk * sizeof(SrcRec);
-  s.meta = o;  o += (size_t)nbuf * tch * sizeof(ChunkMeta);
+  s.ring = o;  o += (size_t)nw * nbuf * ring_buffer_bytes(tch);
   s.hist = o;  o += (size_t)nb * qa * bt * sizeof(float);
   o = align_up(o, 16);
-  s.bsum = o;  o += (size_t)(bt / 32) * kQ * nb * sizeof(double);
+  s.bsum = o;  o += (size_t)nw * kQ * nb * sizeof(double);
   s.e2s = o;   o += (size_t)(nb + 1) * sizeof(double);
   s.fvw = o;   o += (size_t)bt * sizeof(double);
   s.fw = o;    o += (size_t)bt * sizeof(double);
   s.e2f = o;   o += (size_t)(nb + 1) * sizeof(float);
-  o = align_up(o, 16);
-  s.span0 = o; o += kMaxRows * sizeof(int);
-  s.span1 = o; o += kMaxRows * sizeof(int);
   o = align_up(o, 8);
-  s.mbar = o;  o += (size_t)nbuf * sizeof(uint64_t);
-  s.cnt = o;   o += (size_t)nbuf * sizeof(int);
-  s.last = o;  o += (size_t)nbuf * sizeof(int);
+  s.mbar = o;  o += (size_t)nw * nbuf * sizeof(uint64_t);
   s.misc = o;  o += 16;
   s.total = align_up(o, 128);
   return s;
@@ -383,47 +383,36 @@ extern "C" int tpcf_debug_mode_stats(unsigned long long* out) {
 #endif
 
 // ------------------------------------------------------------- tile ring --
-// Position of a tile in the row chunk of a work item: row `row` of the chunk,
-// tile `kk` within that row's span of sub-chunks.
-struct TilePos {
-  int row, kk;
-};
-// Sub-chunks [c0, c0 + n) of the tile at p, and the span bounds inside its
-// first and last sub-chunk.
+// Each warp walks the cell rows of its work item 32 at a time, lane r holding
+// the source span [s0, s1) of row c0 + r.  A row's span covers the sub-chunks
+// [s0 / 32, ceil(s1 / 32)); its first and last sub-chunks are partial when s0
+// or s1 is not a multiple of 32.  Tile k of the pass is the (k - first)-th
+// group of TCH sub-chunks of the row whose prefix of tile counts contains k.
 struct TileGeom {
   int c0, n, lo0, hiL;
 };
 template <int TCH>
-__device__ __forceinline__ TileGeom tile_geom(const int* span0, const int* span1, TilePos p) {
-  const int s = span0[p.row], e = span1[p.row];
-  const int cA = s >> 5, cB = (e + kChunk - 1) >> 5;
-  TileGeom t;
-  t.c0 = cA + p.kk * TCH;
-  t.n = min(TCH, cB - t.c0);
-  t.lo0 = p.kk == 0 ? (s & (kChunk - 1)) : 0;
-  t.hiL = (t.c0 + t.n == cB && (e & (kChunk - 1))) ? (e & (kChunk - 1)) : kChunk;
-  return t;
-}
-template <int TCH>
-__device__ __forceinline__ int row_tiles(const int* span0, const int* span1, int r) {
-  const int s = span0[r], e = span1[r];
+__device__ __forceinline__ int tiles_of_span(int s, int e) {
   if (e <= s) return 0;
   const int nc = ((e + kChunk - 1) >> 5) - (s >> 5);
   return (nc + TCH - 1) / TCH;
 }
-// The next tile in row order (row == nr: none left).
+// Called by all 32 lanes with the same k (0 <= k < the pass's tile count);
+// incl = this lane's inclusive prefix of tile counts, s0/s1 its row's span.
 template <int TCH>
-__device__ __forceinline__ void next_tile(const int* span0, const int* span1, int nr, TilePos& p) {
-  if (++p.kk < row_tiles<TCH>(span0, span1, p.row)) return;
-  p.kk = 0;
-  for (++p.row; p.row < nr && row_tiles<TCH>(span0, span1, p.row) == 0; ++p.row) {
-  }
-}
-template <int TCH>
-__device__ __forceinline__ TilePos first_tile(const int* span0, const int* span1, int nr) {
-  TilePos p{0, 0};
-  while (p.row < nr && row_tiles<TCH>(span0, span1, p.row) == 0) ++p.row;
-  return p;
+__device__ __forceinline__ TileGeom tile_of(int k, int incl, int ntr, int s0, int s1) {
+  const int r = __popc(__ballot_sync(0xffffffffu, incl <= k));  // first row with incl > k
+  const int s = __shfl_sync(0xffffffffu, s0, r);
+  const int e = __shfl_sync(0xffffffffu, s1, r);
+  const int first = __shfl_sync(0xffffffffu, incl - ntr, r);
+  const int kk = k - first;
+  const int cA = s >> 5, cB = (e + kChunk - 1) >> 5;
+  TileGeom t;
+  t.c0 = cA + kk * TCH;
+  t.n = min(TCH, cB - t.c0);
+  t.lo0 = kk == 0 ? (s & (kChunk - 1)) : 0;
+  t.hiL = (t.c0 + t.n == cB && (e & (kChunk - 1))) ? (e & (kChunk - 1)) : kChunk;
+  return t;
 }
 
 // Fold this warp's 32 histogram columns into its FP64 sums (times the lens
@@ -466,42 +455,41 @@ __device__ __forceinline__ void warp_fold(const float* hist, float* hcol, double
 }
 
 // ------------------------------------------------------------ pair kernel --
+// Every warp is independent: it takes its own work items (32 lenses, one per
+// lane, against every source row the group's theta_max neighbourhood touches)
+// from the queue and streams their tiles through its own ring of NBUF buffers
+// in shared memory (bulk copies issued by lane 0, one mbarrier per buffer,
+// bounded waits); no barrier and no shared state ties it to the other warps
+// of the block, so a warp never waits for another's share of work.  The
+// block's warps share only the launch (occupancy, the bin edges).
 // PATH 0: sub-chunk classification with the register paths (default);
 // PATH 1: per-pair binning for every pair in reach (for A/B measurement).
 template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int TCH, int PATH>
 __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P) {
   constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
-  constexpr int NW = BT / 32;
-  constexpr int NBUF = kSrcRing / (TCH * kChunk * (int)sizeof(SrcRec));
-  static_assert(NBUF >= 2, "at least two tile buffers");
+  constexpr int NBUF = kWarpRing / (TCH * kChunk * (int)sizeof(SrcRec));
+  static_assert(NBUF >= 2, "at least two tile buffers per warp");
+  constexpr size_t BUFB = (size_t)TCH * (kChunk * sizeof(SrcRec) + sizeof(ChunkMeta));
   const int nb = P.nb;
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   extern __shared__ __align__(128) unsigned char smem[];
   const PairSmem L = pair_smem_layout(nb, QA, BT, TCH);
-  SrcPair* tiles = reinterpret_cast<SrcPair*>(smem + L.tiles);
-  ChunkMeta* meta = reinterpret_cast<ChunkMeta*>(smem + L.meta);
+  unsigned char* wring = smem + L.ring + (size_t)warp * NBUF * BUFB;
   float* hist = reinterpret_cast<float*>(smem + L.hist);
   double* bsum = reinterpret_cast<double*>(smem + L.bsum);
   double* e2s = reinterpret_cast<double*>(smem + L.e2s);
   double* fvw = reinterpret_cast<double*>(smem + L.fvw);
   double* fw = reinterpret_cast<double*>(smem + L.fw);
   float* e2f = reinterpret_cast<float*>(smem + L.e2f);
-  int* span0 = reinterpret_cast<int*>(smem + L.span0);
-  int* span1 = reinterpret_cast<int*>(smem + L.span1);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.mbar);
-  int* cnt = reinterpret_cast<int*>(smem + L.cnt);    // warps done with the buffer's current tile
-  int* last = reinterpret_cast<int*>(smem + L.last);  // ring index of the buffer's last issued tile
-  int* sh_item = reinterpret_cast<int*>(smem + L.misc);
-  volatile int* sh_abort = sh_item + 1;  // set by a warp whose bounded wait ran out
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.mbar) + (size_t)warp * NBUF;
+  auto tile_ptr = [&](int b) { return reinterpret_cast<SrcPair*>(wring + (size_t)b * BUFB); };
+  auto meta_ptr = [&](int b) {
+    return reinterpret_cast<ChunkMeta*>(wring + (size_t)b * BUFB + (size_t)TCH * kChunk * sizeof(SrcRec));
+  };
 
-  if (tid == 0) {
-    for (int b = 0; b < NBUF; ++b) {
-      mbar_init(&full[b], 1);
-      cnt[b] = 0;
-      last[b] = -1;
-    }
-    *sh_abort = 0;
+  if (lane == 0) {
+    for (int b = 0; b < NBUF; ++b) mbar_init(&full[b], 1);
     mbar_fence_init();
   }
   for (int i = tid; i <= nb; i += BT) {
@@ -517,7 +505,9 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
   C.hi_g = e2f[nb] * (1.f + P.eps);
 
   const uint32_t wait_limit = P.wait_limit ? P.wait_limit : kWaitPolls;
-  int tbase = 0;  // ring index of the first tile of the current row chunk
+  int ring_t = 0;         // ring index of the next tile this warp consumes
+  int issued_end = 0;     // ring index one past the last tile this warp issued
+  bool aborted = false;   // a bounded wait ran out: consume and issue nothing more
   float* __restrict__ hcol = hist + tid;
   double* wsum = bsum + (size_t)warp * kQ * nb;
   const int flush_src = P.flush_src > 0 ? P.flush_src : 4096;
@@ -528,10 +518,10 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
 #endif
   for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
 
-  for (;;) {
-    if (tid == 0) *sh_item = atomicAdd(P.queue_head, 1);
-    __syncthreads();
-    const int item = *sh_item;
+  while (!aborted) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(P.queue_head, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= P.n_items) break;
     const int2 it = P.items[item];
     const TaskDesc T = P.tasks[it.x];
@@ -540,17 +530,17 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
     const int g = it.y;
     const int gs = LD.group_start[g];
     const int nl = LD.group_start[g + 1] - gs;
-    const bool act = tid < nl;
+    const bool act = lane < nl;
     float lx = 0.f, ly = 0.f, lz = 0.f;
     double vw = 0.0, w = 0.0;
     double* lens_col = nullptr;
     if (act) {
-      const float4 r = LD.rec[gs + tid];
+      const float4 r = LD.rec[gs + lane];
       lx = r.x; ly = r.y;
       vw = (double)r.z * (double)r.w;
       w = (double)r.w;
-      if (HAS_Z) lz = LD.z[gs + tid];
-      if (P.lens_acc && T.lens_acc_off >= 0) lens_col = P.lens_acc + T.lens_acc_off + gs + tid;
+      if (HAS_Z) lz = LD.z[gs + lane];
+      if (P.lens_acc && T.lens_acc_off >= 0) lens_col = P.lens_acc + T.lens_acc_off + gs + lane;
     }
     LensP LP;
     LP.nlx = dup2(-lx);
@@ -565,135 +555,123 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
     int cy0, cy1;
     row_range(G, box, P.R, P.margin, cy0, cy1);
 
-    for (int c0 = cy0; c0 <= cy1; c0 += kMaxRows) {
-      const int nr = min(kMaxRows, cy1 - c0 + 1);
-      __syncthreads();  // every warp is done with the previous chunk's tiles and spans
-      for (int r = tid; r < nr; r += BT) {
-        const int2 sp = row_span(G, box, P.R, P.margin, c0 + r);
-        span0[r] = sp.x;
-        span1[r] = sp.y > sp.x ? sp.y : sp.x;
+    for (int c0 = cy0; c0 <= cy1 && !aborted; c0 += kRowsPerPass) {
+      const int nr = min(kRowsPerPass, cy1 - c0 + 1);
+      int s0 = 0, s1 = 0;
+      if (lane < nr) {
+        const int2 sp = row_span(G, box, P.R, P.margin, c0 + lane);
+        s0 = sp.x;
+        s1 = sp.y > sp.x ? sp.y : sp.x;
       }
-      __syncthreads();
-      // Ring of NBUF buffers: the tile with ring index t lives in buffer
-      // t % NBUF and completes phase (t / NBUF) & 1 of its full barrier.
-      auto issue = [&](TilePos p, int t) {
+      const int ntr = tiles_of_span<TCH>(s0, s1);
+      int incl = ntr;  // inclusive prefix of the tile counts over the lanes (rows)
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int ntiles = __shfl_sync(0xffffffffu, incl, 31);
+      // Ring: the tile with ring index t lives in buffer t % NBUF and completes
+      // phase (t / NBUF) & 1 of that buffer's barrier.  The pass's tile k has
+      // ring index ring_t + k; each consumed buffer is refilled at once with
+      // the tile NBUF places ahead.
+      auto issue = [&](int k) {
+        const TileGeom tg = tile_of<TCH>(k, incl, ntr, s0, s1);  // all lanes (shuffles)
+        const int t = ring_t + k;
+        issued_end = t + 1;
         if (t + 1 == P.debug_skip_tile) return;  // fault injection (tests): this tile never lands
-        const TileGeom tg = tile_geom<TCH>(span0, span1, p);
-        const int b = t % NBUF;
-        const uint32_t nbytes = (uint32_t)tg.n * (kChunk * sizeof(SrcRec) + sizeof(ChunkMeta));
-        mbar_arrive_tx(&full[b], nbytes);
-        bulk_g2s(tiles + (size_t)b * TCH * (kChunk / 2), G.pairs + (size_t)tg.c0 * (kChunk / 2),
-                 (uint32_t)tg.n * kChunk * sizeof(SrcRec), &full[b]);
-        bulk_g2s(meta + (size_t)b * TCH, G.meta + tg.c0, (uint32_t)tg.n * sizeof(ChunkMeta), &full[b]);
-        last[b] = t;
-      };
-      if (tid == 0 && !*sh_abort) {
-        TilePos p = first_tile<TCH>(span0, span1, nr);
-        for (int k = 0; k < NBUF && p.row < nr; ++k) {
-          issue(p, tbase + k);
-          next_tile<TCH>(span0, span1, nr, p);
+        if (lane == 0) {
+          const int b = t % NBUF;
+          mbar_arrive_tx(&full[b], (uint32_t)(tg.n * (kChunk * sizeof(SrcRec) + sizeof(ChunkMeta))));
+          bulk_g2s(tile_ptr(b), G.pairs + (size_t)tg.c0 * (kChunk / 2), (uint32_t)tg.n * kChunk * sizeof(SrcRec),
+                   &full[b]);
+          bulk_g2s(meta_ptr(b), G.meta + tg.c0, (uint32_t)tg.n * sizeof(ChunkMeta), &full[b]);
         }
-      }
-      TilePos p = first_tile<TCH>(span0, span1, nr);
-      int k = 0;
-      for (; p.row < nr; ++k) {
-        const int t = tbase + k;
+      };
+      for (int k = 0; k < NBUF && k < ntiles; ++k) issue(k);
+      for (int k = 0; k < ntiles; ++k) {
+        const int t = ring_t + k;
         const int b = t % NBUF;
-        const TileGeom tg = tile_geom<TCH>(span0, span1, p);
-        bool ok = !*sh_abort && mbar_wait_bounded(&full[b], (uint32_t)(t / NBUF) & 1u, wait_limit);
-        ok = __all_sync(0xffffffffu, ok);
-        if (!ok) *sh_abort = 1;  // stop consuming and issuing; the copies in flight are drained at exit
-        if (ok) {
-          const SrcPair* Tb = tiles + (size_t)b * TCH * (kChunk / 2);
-          const ChunkMeta* Mb = meta + (size_t)b * TCH;
-          for (int j = 0; j < tg.n; ++j) {
-            const int lo = j == 0 ? tg.lo0 : 0;
-            const int hi = j == tg.n - 1 ? tg.hiL : kChunk;
-            const bool part = lo > 0 || hi < kChunk;
-            const SrcPair* __restrict__ Sc = Tb + j * (kChunk / 2);
-            const float4 cbox = Mb[j].box;
-            int blo = 0;
-            int cls = act ? classify<LOGB, HAS_Z, true>(lx, ly, cbox, C, blo) : 0;
-            if (PATH == 1 && cls) cls = 3;
-            const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)cls);
+        const TileGeom tg = tile_of<TCH>(k, incl, ntr, s0, s1);
+        const bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(&full[b], (uint32_t)(t / NBUF) & 1u, wait_limit));
+        if (!ok) {  // stop: drain this warp's copies in flight below, report the timeout
+          aborted = true;
+          ring_t = t;
+          break;
+        }
+        const SrcPair* Tb = tile_ptr(b);
+        const ChunkMeta* Mb = meta_ptr(b);
+        for (int j = 0; j < tg.n; ++j) {
+          const int lo = j == 0 ? tg.lo0 : 0;
+          const int hi = j == tg.n - 1 ? tg.hiL : kChunk;
+          const bool part = lo > 0 || hi < kChunk;
+          const SrcPair* __restrict__ Sc = Tb + j * (kChunk / 2);
+          const float4 cbox = Mb[j].box;
+          int blo = 0;
+          int cls = act ? classify<LOGB, HAS_Z, true>(lx, ly, cbox, C, blo) : 0;
+          if (PATH == 1 && cls) cls = 3;
+          const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)cls);
 #ifdef TPCF_MODE_STATS
-            {
-              const unsigned nact = __popc(__ballot_sync(0xffffffffu, act));
-              unsigned ncls[4];
-              for (int cc = 0; cc < 4; ++cc) ncls[cc] = __popc(__ballot_sync(0xffffffffu, act && cls == cc));
-              if (lane == 0) {
-                atomicAdd(&sh_stats[m], 1ull);
-                atomicAdd(&sh_stats[4 + m], (unsigned long long)((hi - lo) * nact));
-                for (int cc = 0; cc < 4; ++cc) atomicAdd(&sh_stats[8 + cc], (unsigned long long)((hi - lo) * ncls[cc]));
-              }
+          {
+            const unsigned nact = __popc(__ballot_sync(0xffffffffu, act));
+            unsigned ncls[4];
+            for (int cc = 0; cc < 4; ++cc) ncls[cc] = __popc(__ballot_sync(0xffffffffu, act && cls == cc));
+            if (lane == 0) {
+              atomicAdd(&sh_stats[m], 1ull);
+              atomicAdd(&sh_stats[4 + m], (unsigned long long)((hi - lo) * nact));
+              for (int cc = 0; cc < 4; ++cc) atomicAdd(&sh_stats[8 + cc], (unsigned long long)((hi - lo) * ncls[cc]));
             }
+          }
 #endif
-            if (m == 0) continue;
-            if (m == 1) {
-              const float4 ss = Mb[j].sum;
-              if (part)
-                chunk_single<MODE, HAS_M, HAS_Z, true, LOGB, BT, QA>(Sc, lo, hi, LP, lz, cls, blo, hcol, ss);
-              else
-                chunk_single<MODE, HAS_M, HAS_Z, false, LOGB, BT, QA>(Sc, 0, kChunk, LP, lz, cls, blo, hcol, ss);
-            } else if (m == 2) {
-              const float4 ss = Mb[j].sum;
-              if (part)
-                chunk_dual<MODE, HAS_M, HAS_Z, true, LOGB, BT, QA>(Sc, lo, hi, LP, lx, ly, lz, cls, blo, hcol, C,
-                                                                    ss);
-              else
-                chunk_dual<MODE, HAS_M, HAS_Z, false, LOGB, BT, QA>(Sc, 0, kChunk, LP, lx, ly, lz, cls, blo, hcol,
-                                                                     C, ss);
-            } else if (act) {
-              for (int jj = lo; jj < hi; ++jj) {
-                float4 a, bb;
-                src_of(Sc, jj, a, bb);
-                do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, a, bb, hcol, C);
-              }
+          if (m == 0) continue;
+          if (m == 1) {
+            const float4 ss = Mb[j].sum;
+            if (part)
+              chunk_single<MODE, HAS_M, HAS_Z, true, LOGB, BT, QA>(Sc, lo, hi, LP, lz, cls, blo, hcol, ss);
+            else
+              chunk_single<MODE, HAS_M, HAS_Z, false, LOGB, BT, QA>(Sc, 0, kChunk, LP, lz, cls, blo, hcol, ss);
+          } else if (m == 2) {
+            const float4 ss = Mb[j].sum;
+            if (part)
+              chunk_dual<MODE, HAS_M, HAS_Z, true, LOGB, BT, QA>(Sc, lo, hi, LP, lx, ly, lz, cls, blo, hcol, C, ss);
+            else
+              chunk_dual<MODE, HAS_M, HAS_Z, false, LOGB, BT, QA>(Sc, 0, kChunk, LP, lx, ly, lz, cls, blo, hcol, C,
+                                                                   ss);
+          } else if (act) {
+            for (int jj = lo; jj < hi; ++jj) {
+              float4 a, bb;
+              src_of(Sc, jj, a, bb);
+              do_pair<MODE, HAS_M, HAS_Z, LOGB, BT, QA>(lx, ly, lz, a, bb, hcol, C);
             }
           }
         }
         since_flush += tg.n * kChunk - tg.lo0 - (kChunk - tg.hiL);
-        // Release the buffer; the last warp to do so refills it with the tile
-        // NBUF places ahead.
-        __syncwarp();
-        if (lane == 0) {
-          __threadfence_block();
-          if (atomicAdd(&cnt[b], 1) == NW - 1) {
-            cnt[b] = 0;
-            __threadfence_block();
-            TilePos q = p;
-            for (int a = 0; a < NBUF && q.row < nr; ++a) next_tile<TCH>(span0, span1, nr, q);
-            if (q.row < nr && !*sh_abort) issue(q, t + NBUF);
-          }
-        }
+        __syncwarp();  // every lane is done reading buffer b
+        if (k + NBUF < ntiles) issue(k + NBUF);
         if (since_flush >= flush_src) {
           warp_fold<QA, BT>(hist, hcol, wsum, fvw, fw, nb, lens_col, lens_stride, first_flush, warp, lane);
           first_flush = false;
           since_flush = 0;
         }
-        next_tile<TCH>(span0, span1, nr, p);
       }
-      tbase += k;
+      if (!aborted) ring_t += ntiles;
     }
+    if (aborted) break;
     warp_fold<QA, BT>(hist, hcol, wsum, fvw, fw, nb, lens_col, lens_stride, first_flush, warp, lane);
-    __syncthreads();
     double* out = P.item_sums + (size_t)(T.item_base + g) * kQ * nb;
-    for (int e = tid; e < kQ * nb; e += BT) {
+    for (int e = lane; e < kQ * nb; e += 32) {
       const int src = (e / nb == QK && QA == 5) ? e - (QK - QW) * nb : e;
-      double s = 0.0;
-      for (int ww = 0; ww < NW; ++ww) s += bsum[(size_t)ww * kQ * nb + src];
-      out[e] = s;
+      out[e] = wsum[src];
     }
-    __syncthreads();
+    __syncwarp();
   }
-  // After a timed-out wait no tile was consumed or issued any more; wait
-  // (bounded) for the last copy issued into each buffer before the block's
-  // shared memory is released.
-  __syncthreads();
-  if (tid == 0 && *sh_abort) {
-    for (int b = 0; b < NBUF; ++b)
-      if (last[b] >= 0) mbar_wait_bounded(&full[b], (uint32_t)(last[b] / NBUF) & 1u, wait_limit);
-    atomicOr(P.err, kErrTimeout);
+  if (aborted) {
+    // No tile is consumed or issued any more; wait (bounded) for the copies
+    // this warp issued and did not consume, so that none is in flight when
+    // the block's shared memory is released.
+    for (int t = ring_t; t < issued_end; ++t)
+      if (t + 1 != P.debug_skip_tile) mbar_wait_bounded(&full[t % NBUF], (uint32_t)(t / NBUF) & 1u, wait_limit);
+    if (lane == 0) atomicOr(P.err, kErrTimeout);
   }
 #ifdef TPCF_MODE_STATS
   __syncthreads();
@@ -1124,27 +1102,29 @@ static cudaError_t launch_pairs_t(const PairParams& P, int num_sms, cudaStream_t
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   int grid = per_sm * num_sms;
-  if (grid > P.n_items) grid = P.n_items;
+  const int need = (P.n_items + BT / 32 - 1) / (BT / 32);  // each warp takes items of its own
+  if (grid > need) grid = need;
   if (grid < 1) grid = 1;
   *grid_out = grid;
   kern<<<grid, BT, smem, st>>>(P);
   return cudaGetLastError();
 }
 
-// Tile shapes: bt lenses per block (128, 64 or 32) and tch sub-chunks per
-// source tile (4: four 1.1 KB tiles in flight; 2: eight 0.5 KB tiles, only
-// with 128 lenses).  variant 1 forces per-pair binning (A/B measurement).
+// Tile shapes: bt threads per block (128, 64 or 32; each warp takes 32-lens
+// work items of its own) and tch sub-chunks per source tile (2: two 2.1 KB
+// buffers per warp; 1: four 1.1 KB buffers).  variant 1 forces per-pair binning
+// (A/B measurement).
 template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB>
 static cudaError_t launch_pairs_bt(const PairParams& P, int bt, int tch, int variant, int num_sms, cudaStream_t st,
                                    int* grid) {
   if (bt == 128) {
     if (variant == 1 && MODE == 0 && !HAS_M && !HAS_Z && LOGB)
-      return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 4, 1>(P, num_sms, st, grid);
-    if (tch == 2) return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 2, 0>(P, num_sms, st, grid);
-    return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 4, 0>(P, num_sms, st, grid);
+      return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 2, 1>(P, num_sms, st, grid);
+    if (tch == 1) return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 1, 0>(P, num_sms, st, grid);
+    return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 2, 0>(P, num_sms, st, grid);
   }
-  if (bt == 64) return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64, 4, 0>(P, num_sms, st, grid);
-  return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 32, 4, 0>(P, num_sms, st, grid);
+  if (bt == 64) return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64, 2, 0>(P, num_sms, st, grid);
+  return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 32, 2, 0>(P, num_sms, st, grid);
 }
 
 size_t pair_smem_bytes(int nb, int qa, int bt, int tch) { return pair_smem_layout(nb, qa, bt, tch).total; }

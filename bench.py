@@ -823,7 +823,7 @@ def main():
                    "parallelism": f"work items sharded over {world} rank(s)" if world > 1 else "single GPU",
                    "l2": "inputs (280 MB of catalogues) larger than L2 (126 MB); no flush",
                    "cell_size": ctx.cell_size,
-                   "tile_shape": {"group_size": ctx.tile_shape[0] or 128, "tile_chunks": ctx.tile_shape[1] or 4},
+                   "tile_shape": {"threads_per_block": ctx.tile_shape[0] or 128, "tile_chunks": ctx.tile_shape[1] or 2},
                    "autotune_ms_per_gpair": None if tune is None else {
                        "cell": {f"theta_max/{d}": round(v, 3) for d, v in tune["cell"].items()},
                        "tile": {g: round(v, 3) for g, v in tune["tile"].items()}, "choice": tune["choice"]},

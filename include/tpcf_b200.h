@@ -77,11 +77,12 @@ typedef struct tpcf_opts {
                             must be summed over shards (one all-reduce);
                             normalised outputs are not written            */
   int32_t shard_count;   /* 0 or 1: no sharding                              */
-  int32_t group_size;    /* planar pair kernel tile shape: lenses per group and
-                            threads per block (32, 64 or 128; 0 = 128, halved
-                            while the per-lens histogram would exceed 100 KB) */
-  int32_t tile_chunks;   /* 32-source sub-chunks per source tile (2 or 4 with
-                            128 lenses per group, else 4; 0 = 4)             */
+  int32_t group_size;    /* planar pair kernel tile shape: threads per block
+                            (32, 64 or 128; 0 = 128, halved while the
+                            per-lens histogram would exceed 100 KB); each
+                            warp takes 32-lens work items of its own         */
+  int32_t tile_chunks;   /* 32-source sub-chunks per source tile (1 or 2;
+                            0 = 2), in a 4 KB ring per warp                 */
   int32_t reserved[3];
 } tpcf_opts;
 
