@@ -196,16 +196,21 @@ __global__ void k_unit_mult(unsigned long long seed, long long n_units, long lon
 }
 
 // Field sums: out[(g * n_field + fi) * R + r] = sum over the field's blocks.
+// One warp per output: lane l adds blocks l, l + 32, ... of the field, then
+// the lanes are combined by a fixed shuffle tree (the same order every run).
 __global__ void k_marks_reduce(const double* __restrict__ partial, const MarksField* __restrict__ fields,
                                int n_field, int n_blocks, int n_map_g, int R, double* __restrict__ out) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n_map_g * n_field * R) return;
+  const int t = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (t >= n_map_g * n_field * R) return;  // whole warps
   const int r = t % R, fi = (t / R) % n_field, g = t / (R * n_field);
   const int c0 = fields[fi].chunk0;
   const int c1 = fi + 1 < n_field ? fields[fi + 1].chunk0 : n_blocks;
   double s = 0.0;
-  for (int c = c0; c < c1; ++c) s += partial[((size_t)c * n_map_g + g) * R + r];
-  out[t] = s;
+  for (int c = c0 + lane; c < c1; c += 32) s += partial[((size_t)c * n_map_g + g) * R + r];
+#pragma unroll
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) out[t] = s;
 }
 
 // Flags a unit label outside [0, n_units).
@@ -305,7 +310,7 @@ extern "C" tpcf_status tpcf_xi_from_marks(tpcf_ctx* c, int32_t n_field, const tp
       }
       const int tot = g * n_field * R;
       if (nblk > 0) {
-        k_marks_reduce<<<(tot + 255) / 256, 256, 0, st>>>(part, df, n_field, nblk, g, R, dout);
+        k_marks_reduce<<<(tot + 7) / 8, 256, 0, st>>>(part, df, n_field, nblk, g, R, dout);
         counted(c, cudaGetLastError(), "marks reduce");
       } else {
         check(cudaMemsetAsync(dout, 0, sizeof(double) * tot, st), "memset");
@@ -426,7 +431,7 @@ extern "C" tpcf_status tpcf_marks_bootstrap(tpcf_ctx* c, int32_t n_field, const 
             df, n_field, MultFactors{mult, dunit, n_units}, G, nb, marks_group_threads(nb), part);
         counted(c, cudaGetLastError(), "bootstrap partials");
         const int tot = G * n_field * R;
-        k_marks_reduce<<<(tot + 255) / 256, 256, 0, st>>>(part, df, n_field, nblk, G, R, dout);
+        k_marks_reduce<<<(tot + 7) / 8, 256, 0, st>>>(part, df, n_field, nblk, G, R, dout);
         counted(c, cudaGetLastError(), "bootstrap reduce");
         check(cudaMemcpyAsync(sums.data() + (size_t)s0 * n_field * R, dout, sizeof(double) * tot,
                               cudaMemcpyDeviceToHost, st), "D2H sums");

@@ -370,7 +370,7 @@ CONFIG_WORKLOADS = {
     3: "config 3: shear-scalar with errors, 2.0 M shear x 0.5 M scalar on 1200' x 1200', clustered, "
        "100 k-means patches, 1000 resamples, 20 log bins 1-200'",
     4: "config 4: differentiable xi_t on the clustered 2.0 M x 0.5 M catalogues, chi^2 against a seeded "
-       "target, forward + adjoint",
+       "target, forward + adjoint (torch.autograd, device tensors)",
 }
 ADJ_FLOP_PER_PAIR = 20   # adjoint of a loss on xi_t, per binned pair (sources as owners)
 KAPPA_FLOP_PER_PAIR = 14
@@ -464,21 +464,25 @@ def config_timing(k, tpcf, stream, peak, steps=3, warmup=2, with_cpu=True, cpu_s
             kernel_ms[0], flops[0] = ctx.stats()["pair_kernel_ms"], p * FLOP_PER_PAIR
             tpcf.block_bootstrap(r.patch_sums, w["n_boot"], seed=1003, ctx=ctx)
             return p
-        # k == 4: forward with raw per-lens sums, then the adjoint of the chi^2
-        r = shear(A, B, lens_raw=True)
-        p = int(r.n_pairs.sum())
-        kernel_ms[0], flops[0] = ctx.stats()["pair_kernel_ms"], p * FLOP_PER_PAIR
+        # k == 4: the differentiable form (torch.autograd on device tensors: the
+        # raw per-lens sums stay in device memory), chi^2 against a seeded
+        # target, backward through the adjoint; the loss is read back
+        ag = importlib.import_module("2pcf_b200.autograd")
+        cu = lambda t: t if t.is_cuda else t.cuda(non_blocking=True)
+        g = {q: cu(t) for q, t in A.items()}
+        h = {q: cu(t) for q, t in B.items()}
+        geo = dict(x_A=g["x"], y_A=g["y"], z_A=g["z"], x_B=h["x"], y_B=h["y"], z_B=h["z"], m_B=h["m"])
+        leaves = [t.detach().requires_grad_(True) for t in (g["val"], g["w"], h["e1"], h["e2"], h["w"])]
+        xi_t, _ = ag.xi_shear(*leaves, geo, bins, ctx)
+        kernel_ms[0], flops[0] = ctx.stats()["pair_kernel_ms"], state["pairs"] * FLOP_PER_PAIR
         if state.get("forward_only"):
-            return p
-        xi = r.sum_gt / r.sum_K
-        if "target" not in state:
-            state["sig"] = np.abs(xi) * 0.1 + 1e-6
-            state["target"] = np.random.default_rng(1004).normal(xi, state["sig"])
-        lam = 2 * (xi - state["target"]) / state["sig"] ** 2
-        tpcf.tangential_shear_adjoint(A["x"], A["y"], A["z"], A["val"], A["w"], B["x"], B["y"], B["z"],
-                                      B["e1"], B["e2"], B["w"], B["m"], bins, r, lam, None, ctx=ctx)
+            xi_t.sum().item()
+            return state["pairs"]
+        loss = (((xi_t - state["target"]) / state["sig"]) ** 2).sum()
+        loss.backward()
         adj_ms[0] = ctx.stats()["pair_kernel_ms"]
-        return p
+        loss.item()
+        return state["pairs"]
 
     def cats(to):
         A = {q: to(v) for q, v in L.items()}
@@ -502,6 +506,13 @@ def config_timing(k, tpcf, stream, peak, steps=3, warmup=2, with_cpu=True, cpu_s
         return e0.elapsed_time(e1) / n, pairs, kms / n, fl / n, ams / n
 
     Ad, Bd, Cd, Ud = cats(dev)
+    if k == 4:  # binned pairs and the seeded target, from one plain forward call
+        r = shear(Ad, Bd)
+        state["pairs"] = int(r.n_pairs.sum())
+        xi = r.sum_gt / r.sum_K
+        sig = np.abs(xi) * 0.1 + 1e-6
+        state["sig"] = torch.from_numpy(sig).cuda()
+        state["target"] = torch.from_numpy(np.random.default_rng(1004).normal(xi, sig)).cuda()
     for _ in range(warmup):
         step(Ad, Bd, Cd, Ud)
     ms, pairs, kms, fl, ams = timed(Ad, Bd, Cd, Ud, steps)

@@ -181,7 +181,11 @@ def last_timing():
 
 
 # ----------------------------------------------------------------- canonical --
-CANON_Q = ("sum_dw", "sum_gt", "sum_gx", "sum_w", "sum_K", "n_pairs", "abs_gt", "abs_gx")
+# abs_*: sums of |term|; norm_*: sums of the bound on a term before its
+# rotation (w_B |val_A w_A| |(e1, e2)| for shear, |term| for scalar fields), the
+# scale of an FP32 evaluation's error in one rotated term.
+CANON_Q = ("sum_dw", "sum_gt", "sum_gx", "sum_w", "sum_K", "n_pairs", "abs_gt", "abs_gx", "norm_gt", "norm_gx")
+NQ = len(CANON_Q)
 
 
 def canon_pairs(mode, lens, src, edges_sq, num_threads=None, lens_idx=None):
@@ -190,7 +194,8 @@ def canon_pairs(mode, lens, src, edges_sq, num_threads=None, lens_idx=None):
     Returns a dict of per-bin FP64 arrays (CANON_Q) and, when ``lens_idx`` is
     given, ``lens`` = per-lens [n_sel][6][n_bin] sums (d*w, g_t, g_x, w, K, n)
     for those lenses (and the per-bin sums cover only those lenses), and
-    ``lens_abs`` = per-lens [n_sel][2][n_bin] sums of |g_t terms|, |g_x terms|."""
+    ``lens_abs`` = per-lens [n_sel][2][n_bin] sums of |g_t terms|, |g_x terms|
+    and ``lens_norm`` the per-lens norm_gt, norm_gx rows."""
     f = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
     nA, nB = len(lens["x"]), len(src["x"])
     e2 = np.ascontiguousarray(edges_sq, np.float64)
@@ -202,18 +207,19 @@ def canon_pairs(mode, lens, src, edges_sq, num_threads=None, lens_idx=None):
     else:
         xB, yB, e1, e2b, wB = (f(src[k]) for k in ("x", "y", "kappa_E", "kappa_B", "w"))
         zB = mB = None
-    sums = np.zeros(8 * n_bin)
+    sums = np.zeros(NQ * n_bin)
     sel = None if lens_idx is None else np.ascontiguousarray(lens_idx, np.int64)
-    lens_out = None if sel is None else np.zeros((len(sel), 8, n_bin))
+    lens_out = None if sel is None else np.zeros((len(sel), NQ, n_bin))
     nt = num_threads or os.cpu_count() or 1
     lib().orc_canon_pairs(mode, nA, _ptr(xA), _ptr(yA), _ptr(zA), _ptr(vA), _ptr(wA), nB, _ptr(xB),
                           _ptr(yB), _ptr(zB), _ptr(e1), _ptr(e2b), _ptr(wB), _ptr(mB), e2, n_bin,
                           nt, sums, _ptr(sel), 0 if sel is None else len(sel), _ptr(lens_out))
-    sums = sums.reshape(8, n_bin)
+    sums = sums.reshape(NQ, n_bin)
     out = {k: sums[i].copy() for i, k in enumerate(CANON_Q)}
     if lens_out is not None:
         out["lens"] = np.ascontiguousarray(lens_out[:, :6])
-        out["lens_abs"] = np.ascontiguousarray(lens_out[:, 6:])  # sum|g_t terms|, sum|g_x terms|
+        out["lens_abs"] = np.ascontiguousarray(lens_out[:, 6:8])  # sum|g_t terms|, sum|g_x terms|
+        out["lens_norm"] = np.ascontiguousarray(lens_out[:, 8:10])
     return out
 
 
@@ -299,11 +305,11 @@ def canon_sphere(mode, lens, src, edges_sq_chord, num_threads=None):
     else:
         xB, yB, e1, e2b, wB = (f(src[k]) for k in ("x", "y", "kappa_E", "kappa_B", "w"))
         zB = mB = None
-    sums = np.zeros(8 * nb)
+    sums = np.zeros(NQ * nb)
     lib().orc_canon_sphere(mode, nA, _ptr(xA), _ptr(yA), _ptr(zA), _ptr(vA), _ptr(wA), nB, _ptr(xB),
                            _ptr(yB), _ptr(zB), _ptr(e1), _ptr(e2b), _ptr(wB), _ptr(mB), e2, nb,
                            num_threads or os.cpu_count() or 1, sums)
-    sums = sums.reshape(8, nb)
+    sums = sums.reshape(NQ, nb)
     return {k: sums[i].copy() for i, k in enumerate(CANON_Q)}
 
 

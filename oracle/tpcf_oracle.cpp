@@ -648,7 +648,11 @@ inline double d2_of(float xa, float ya, float xb, float yb) {
   return a + b;
 }
 
-enum { Q_DW = 0, Q_GT, Q_GX, Q_W, Q_K, Q_N, Q_AGT, Q_AGX, NQ };
+// Q_AGT/Q_AGX: sums of |g_t term|, |g_x term|.  Q_NGT/Q_NGX: sums of the
+// bound on each term's size before the rotation, w_B |val_A w_A| |(e1, e2)|
+// for shear (both rows) and |term| for scalar fields: an FP32 evaluation of
+// the rotated term errs by a few ulps of that bound, not of the term itself.
+enum { Q_DW = 0, Q_GT, Q_GX, Q_W, Q_K, Q_N, Q_AGT, Q_AGX, Q_NGT, Q_NGX, NQ };
 
 // One lens against all sources, FP64, canonical binning.  acc is [NQ][n_bin].
 inline void lens_row(int mode, float xa, float ya, float za, float va, float wa,
@@ -693,6 +697,9 @@ inline void lens_row(int mode, float xa, float ya, float za, float va, float wa,
     a[Q_N * nb + b] += 1.0;
     a[Q_AGT * nb + b] += fabs(tt);
     a[Q_AGX * nb + b] += fabs(tx);
+    const double nt = mode == 0 ? hypot((double)e1B[j], (double)e2B[j]) * w * fabs(vw) : fabs(tt);
+    a[Q_NGT * nb + b] += nt;
+    a[Q_NGX * nb + b] += mode == 0 ? nt : fabs(tx);
   }
 }
 
@@ -793,9 +800,10 @@ REF_PAIR_EXPORT(orc_ref_pairs_f32, float)
 REF_PAIR_EXPORT(orc_ref_pairs_f64, double)
 
 // Canonical FP64 pair sums.
-//   sums: [8][n_bin] = (sum d*wA*wB, sum g_t terms, sum g_x terms, sum wA*wB,
-//                       sum K terms, n_pairs, sum |g_t terms|, sum |g_x terms|)
-//   lens_idx/lens_out (optional): per-lens [n_sel][6][n_bin] of the first six
+//   sums: [10][n_bin] = (sum d*wA*wB, sum g_t terms, sum g_x terms, sum wA*wB,
+//                        sum K terms, n_pairs, sum |g_t terms|, sum |g_x terms|,
+//                        the two term-bound rows Q_NGT, Q_NGX)
+//   lens_idx/lens_out (optional): per-lens [n_sel][10][n_bin] of the same
 //   quantities for the listed lens indices.
 // Summation order is fixed (per lens over sources in index order, then lenses
 // in blocks of 64 in index order), so results do not depend on num_threads.
@@ -835,7 +843,7 @@ int orc_canon_pairs(int mode, long nA, const float* xA, const float* yA, const f
     for (long s = 0; s < n_sel; ++s) {
       const double* acc = all.data() + (size_t)s * NQ * nb;
       for (int q = 0; q < NQ * nb; ++q) sums[q] += acc[q];
-      if (lens_out)  // all NQ rows: d*w, g_t, g_x, w, K, n, sum|g_t terms|, sum|g_x terms|
+      if (lens_out)  // all NQ rows: d*w, g_t, g_x, w, K, n, sum|g_t terms|, sum|g_x terms|, the two bound rows
         for (int q = 0; q < NQ * nb; ++q) lens_out[(size_t)s * NQ * nb + q] = acc[q];
     }
   }
@@ -1171,6 +1179,9 @@ int orc_canon_sphere(int mode, long nA, const float* xA, const float* yA, const 
         acc[canon::Q_N * nb + b] += 1.0;
         acc[canon::Q_AGT * nb + b] += fabs(tt);
         acc[canon::Q_AGX * nb + b] += fabs(tx);
+        const double nt = mode == 0 ? hypot((double)e1B[j], (double)e2B[j]) * w * fabs(vw) : fabs(tt);
+        acc[canon::Q_NGT * nb + b] += nt;
+        acc[canon::Q_NGX * nb + b] += mode == 0 ? nt : fabs(tx);
       }
     }
   }
