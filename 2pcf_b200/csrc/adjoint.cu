@@ -897,7 +897,8 @@ tpcf_status run_adjoint_batch(tpcf_ctx* c, std::vector<AdjLensIn> lens, std::vec
     int2* items0 = (int2*)ws_alloc(c, sizeof(int2) * n_items);
     int2* d_items = (int2*)ws_alloc(c, sizeof(int2) * n_items);
     check(cudaMemcpyAsync(items0, items.data(), sizeof(int2) * n_items, cudaMemcpyHostToDevice, st), "H2D items");
-    // longest items first: cost = lenses in the rows of each source group
+    // costliest items first (in cost bands, space order inside a band): cost =
+    // lenses in the rows of each source group
     unsigned long long* ck0 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * n_items);
     unsigned long long* ck1 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * n_items);
     int* o0 = (int*)ws_alloc(c, sizeof(int) * n_items);

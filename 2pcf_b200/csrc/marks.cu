@@ -42,30 +42,61 @@ struct MarksField {
   const float* w;           // maps: [n_map][n]
 };
 
-// Lens factors of resample/map g for lens j of field F: numerator factor vw,
-// K factor wm, and whether the lens takes part.
+// 4-byte asynchronous copy global -> shared (cp.async); with valid == false
+// nothing is read and the destination is zero-filled.
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(
+                   static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+               "l"(src), "r"(valid ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Lens factors of resample/map g for lens jj of a tile.  stage() starts the
+// copies of the raw inputs of entry e = (g, jj) into shared memory; factors()
+// turns the landed raw values into the numerator factor vw and the K factor
+// wm (both 0 for a lens that takes no part).
 struct MapFactors {  // foreground maps: vw = val w, wm = w
   int map0;
-  __device__ __forceinline__ void get(const MarksField& F, int g, long long j, double& vw, double& wm) const {
-    const size_t o = (size_t)(map0 + g) * (size_t)F.n + (size_t)j;
-    wm = (double)F.w[o];
-    vw = (double)F.val[o] * wm;
+  static constexpr size_t kRawBytes = sizeof(float) * (2 * kMapGroup + 1) * 64;
+  // raw: val [kMapGroup][64], w [kMapGroup][64], marks weight [64]
+  __device__ __forceinline__ void stage(const MarksField& F, int g, int jj, long long j, bool valid,
+                                        unsigned char* raw, int e) const {
+    float* rv = reinterpret_cast<float*>(raw);
+    const size_t o = valid ? (size_t)(map0 + g) * (size_t)F.n + (size_t)j : 0;
+    cp_async4(rv + e, F.val + o, valid);
+    cp_async4(rv + kMapGroup * 64 + e, F.w + o, valid);
+    if (g == 0) cp_async4(rv + 2 * kMapGroup * 64 + jj, F.mw + (valid ? j : 0), valid);
   }
-  // calculate_tpcf_from_marks drops lenses with marks weight x weight <= 0
-  __device__ __forceinline__ bool keep(float mw, double wm) const { return (double)mw * wm > 0.0; }
+  __device__ __forceinline__ void factors(const unsigned char* raw, int e, int jj, double& vw, double& wm) const {
+    const float* rv = reinterpret_cast<const float*>(raw);
+    wm = (double)rv[kMapGroup * 64 + e];
+    vw = (double)rv[e] * wm;
+    // calculate_tpcf_from_marks drops lenses with marks weight x weight <= 0
+    if (!((double)rv[2 * kMapGroup * 64 + jj] * wm > 0.0)) vw = wm = 0.0;
+  }
 };
 struct MultFactors {  // resamples: vw = wm = multiplicity of the lens's unit
   const int* mult;    // [G][n_units]
   const int* unit;    // unit of each lens (all fields concatenated), or nullptr: the lens itself
   long long n_units;
-  __device__ __forceinline__ void get(const MarksField& F, int g, long long j, double& vw, double& wm) const {
-    const long long gl = F.lens0 + j;
-    const long long u = unit ? (long long)unit[gl] : gl;
-    wm = (double)mult[(size_t)g * (size_t)n_units + (size_t)u];
-    vw = wm;
+  static constexpr size_t kRawBytes = sizeof(int) * kMapGroup * 64;
+  __device__ __forceinline__ void stage(const MarksField& F, int g, int, long long j, bool valid,
+                                        unsigned char* raw, int e) const {
+    size_t o = 0;
+    if (valid) {
+      const long long gl = F.lens0 + j;
+      const long long u = unit ? (long long)__ldg(unit + gl) : gl;
+      o = (size_t)g * (size_t)n_units + (size_t)u;
+    }
+    cp_async4(reinterpret_cast<int*>(raw) + e, mult + o, valid);
   }
   // the bootstraps take every drawn lens (src/tpcf.f90:601, :917, :1248)
-  __device__ __forceinline__ bool keep(float, double wm) const { return wm > 0.0; }
+  __device__ __forceinline__ void factors(const unsigned char* raw, int e, int, double& vw, double& wm) const {
+    const int m = reinterpret_cast<const int*>(raw)[e];
+    wm = m > 0 ? (double)m : 0.0;
+    vw = wm;
+  }
 };
 
 // partial[(blk * n_g + g) * R + r], R = 3 n_bin + 1 (E, B, K rows, weight).
@@ -73,29 +104,40 @@ struct MultFactors {  // resamples: vw = wm = multiplicity of the lens's unit
 // A block is NG lens groups of TG = 32 ceil(R / 32) threads; thread r of a
 // group owns row r of the marks (xi_E, xi_B, K of bin r mod n_bin, or the
 // marks weight) and keeps the kMapGroup sums of that row in registers.  The
-// block takes kMarksLens lenses in tiles of kTileL: per tile the lens factors
-// of the n_g maps (FP64, zero for lenses left out) are staged in shared
-// memory, then group k takes lenses k, k + NG, ...: each thread loads its row
-// of the lens (the group's 32-lane loads cover the lens's contiguous marks)
-// and adds it times the n_g factors (FP64 FMA, one chain per map).  Streaming
-// the marks once per pass with all n_g maps applied keeps the pass near the
-// HBM roofline.  The groups are summed in fixed order at the end
-// (deterministic, no atomics).
+// block takes kMarksLens lenses in tiles of kTileL.  While the block sums one
+// tile, the raw inputs of the next tile's lens factors (per map and lens;
+// consecutive threads copy consecutive lenses of one map) are already being
+// copied into shared memory (cp.async), so no load latency is exposed and no
+// register holds them; after a barrier they become the FP64 factors (zero for
+// lenses left out) of the next tile.  Group k takes lenses k, k + NG, ...:
+// each thread loads its row of the lens (the group's 32-lane loads cover the
+// lens's contiguous marks) and adds it times the n_g factors (FP64 FMA, one
+// chain per map).  Streaming the marks once per pass with all n_g maps
+// applied keeps the pass near the FP64 roofline.  The groups are summed in
+// fixed order at the end (deterministic, no atomics).
+//
+// A factor row of 16 doubles is stored with its columns XOR-swizzled by
+// 2 (jj & 7): pairs (2h, 2h+1) stay adjacent and in order (read as one
+// double2 at pair index h ^ (jj & 7)), and the 32 lanes of one conversion
+// store (one map, 32 lenses) spread over 16 banks instead of 2.
 constexpr int kTileL = 64;
 constexpr int kMarksLens = 1024;  // lenses per block
+static_assert(kTileL == 64, "the raw staging areas hold 64 lenses");
 template <class Fac>
 __global__ void __launch_bounds__(512, 2) k_marks_partials(const MarksField* __restrict__ fields, int n_field,
                                                             const Fac fac, int n_g, int n_bin, int tg,
                                                             double* __restrict__ partial) {
   extern __shared__ __align__(16) unsigned char sm[];
+  constexpr int TF = kTileL * kMapGroup;
   const int R = 3 * n_bin + 1;
   const int ng = blockDim.x / tg;
   double* fac_s = reinterpret_cast<double*>(sm);  // [kTileL][kMapGroup] factors of the E and B rows
-  double* fw_s = fac_s + kTileL * kMapGroup;      // [kTileL][kMapGroup] factors of K and the weight
+  double* fw_s = fac_s + TF;                      // [kTileL][kMapGroup] factors of K and the weight
+  unsigned char* raw = sm + 2 * TF * sizeof(double);
   const int blk = blockIdx.x;
   int fi = 0;
   while (fi + 1 < n_field && fields[fi + 1].chunk0 <= blk) ++fi;
-  const MarksField F = fields[fi];
+  const MarksField& F = fields[fi];  // read where used: its pointers need no registers across the loop
   const long long j0 = (long long)(blk - F.chunk0) * kMarksLens;
   const long long j1 = min(F.n, j0 + kMarksLens);
   const int tid = threadIdx.x;
@@ -105,37 +147,57 @@ __global__ void __launch_bounds__(512, 2) k_marks_partials(const MarksField* __r
   const long long rs = q < 3 ? n_bin : 1;       // stride of the row from lens to lens
   const bool live = r < R;
   const double* fsel = q < 2 ? fac_s : fw_s;
+
+  auto stage_tile = [&](long long t0) {
+    const int nt = (int)min((long long)kTileL, j1 - t0);
+    for (int e = tid; e < TF; e += blockDim.x) {
+      const int g = e / kTileL, jj = e - g * kTileL;
+      fac.stage(F, g, jj, t0 + jj, jj < nt && g < n_g, raw, e);
+    }
+  };
+  auto convert_tile = [&]() {
+    for (int e = tid; e < TF; e += blockDim.x) {
+      const int g = e / kTileL, jj = e - g * kTileL;
+      double vw, wm;
+      fac.factors(raw, e, jj, vw, wm);
+      const int o = jj * kMapGroup + (g ^ ((jj & 7) << 1));
+      fac_s[o] = vw;
+      fw_s[o] = wm;
+    }
+  };
+
   double acc[kMapGroup];
 #pragma unroll
   for (int g = 0; g < kMapGroup; ++g) acc[g] = 0.0;
+  if (j0 < j1) stage_tile(j0);
+  cp_async_wait_all();
+  __syncthreads();
+  if (j0 < j1) convert_tile();
+  __syncthreads();
   for (long long t0 = j0; t0 < j1; t0 += kTileL) {
     const int nt = (int)min((long long)kTileL, j1 - t0);
-    __syncthreads();  // the previous tile's factors are no longer read
-    for (int e = tid; e < kTileL * kMapGroup; e += blockDim.x) {
-      const int jj = e / kMapGroup, g = e - jj * kMapGroup;
-      double vw = 0.0, wm = 0.0;
-      if (jj < nt && g < n_g) {
-        const long long j = t0 + jj;
-        fac.get(F, g, j, vw, wm);
-        if (!fac.keep(F.mw[j], wm)) vw = wm = 0.0;  // left out: contributes nothing
-      }
-      fac_s[e] = vw;
-      fw_s[e] = wm;
-    }
-    __syncthreads();
+    const bool more = t0 + kTileL < j1;
+    if (more) stage_tile(t0 + kTileL);  // the raw area was read before the last barrier
     if (live) {
       const float* base = row + t0 * rs;
-#pragma unroll 4
+#pragma unroll 2
       for (int jj = grp; jj < nt; jj += ng) {
         const double m = (double)__ldg(base + jj * rs);
         const double2* f2 = reinterpret_cast<const double2*>(fsel + jj * kMapGroup);
+        const int sw = jj & 7;
 #pragma unroll
         for (int h = 0; h < kMapGroup / 2; ++h) {
-          const double2 f = f2[h];
+          const double2 f = f2[h ^ sw];
           acc[2 * h] = fma(m, f.x, acc[2 * h]);
           acc[2 * h + 1] = fma(m, f.y, acc[2 * h + 1]);
         }
       }
+    }
+    cp_async_wait_all();
+    __syncthreads();  // the next tile's raw inputs landed; this tile's factors are no longer read
+    if (more) {
+      convert_tile();
+      __syncthreads();
     }
   }
   // groups 1.. add their sums into group 0's, in group order
@@ -159,14 +221,16 @@ __global__ void __launch_bounds__(512, 2) k_marks_partials(const MarksField* __r
   }
 }
 
-// Threads per lens group (one per marks row, whole warps) and per block.
+// Threads per lens group (one per marks row, whole warps) and per block: as
+// many groups as fit in 512 threads.
 int marks_group_threads(int n_bin) { return (3 * n_bin + 1 + 31) / 32 * 32; }
 int marks_block_threads(int n_bin) {
   const int tg = marks_group_threads(n_bin);
-  return tg >= 256 ? tg : (256 / tg) * tg;
+  return tg > 256 ? tg : (512 / tg) * tg;
 }
 size_t marks_smem(int n_bin) {
-  const size_t fac = 2 * sizeof(double) * kTileL * kMapGroup;
+  const size_t fac = 2 * sizeof(double) * kTileL * kMapGroup +
+                     std::max(MapFactors::kRawBytes, MultFactors::kRawBytes);
   const size_t red = sizeof(double) * (size_t)marks_group_threads(n_bin) * kMapGroup;
   return std::max(fac, red);
 }

@@ -3,24 +3,24 @@
 // Replaces the OpenMP pair loops of tangential_shear_tpcf
 // (src/tpcf.f90:261-363) and scalar_kappa_tpcf (src/tpcf.f90:451-535).
 //
-// One thread block = one lens group (one lens per thread) against every source
-// row the group's theta_max neighbourhood touches.  The source grid is stored
-// in HBM as 32-source sub-chunks already in the pair-interleaved form of the
-// packed FP32 instructions (SrcPair), each with its bounding box and sums
-// (ChunkMeta), so a tile is copied into shared memory by the bulk-copy engine
-// (cp.async.bulk + mbarrier) and used as it lands.  Tiles rotate through
-// several buffers and each warp consumes them at its own pace: a buffer is
-// refilled by the last warp to finish with it, so warps drift apart by up to
-// all-but-one buffers and there is no block-wide barrier per tile.  Every
-// thread reads the same source (broadcast) and bins its pairs into its own
-// FP32 histogram column in shared memory, laid out [bin][quantity][thread] so
-// that a warp's 32 read-modify-writes fall in 32 distinct banks whatever bins
-// the lanes pick, with no atomics.  Every ~4096 sources each warp folds its 32
-// columns into its own FP64 sums (times the lens factors val*w or w) and, when
-// per-lens output is requested, into per-lens FP64 columns.
+// Every warp works on its own: it takes work items of 32 lenses (one per
+// lane) from an atomic queue and walks the source rows of the items'
+// theta_max neighbourhood.  The source grid is stored in HBM as 32-source
+// sub-chunks already in the pair-interleaved form of the packed FP32
+// instructions (SrcPair), each with its bounding box and sums (ChunkMeta), so
+// a tile is copied into shared memory by the bulk-copy engine (cp.async.bulk
+// + mbarrier, issued by lane 0) and used as it lands.  Each warp owns a ring
+// of tile buffers; no barrier or shared state ties it to the other warps of
+// its block.  Every lane reads the same source (broadcast) and bins its
+// pairs into its own FP32 histogram column in shared memory, laid out
+// [bin][quantity][thread] so that a warp's 32 read-modify-writes fall in 32
+// distinct banks whatever bins the lanes pick, with no atomics.  Every ~4096
+// sources (1024 with per-lens output) the warp folds its 32 columns into its
+// FP64 sums (times the lens factors val*w or w) and, when per-lens output is
+// requested, into per-lens FP64 columns.
 //
 // Most pairs never touch the histogram: per 32-source sub-chunk a lens whose
-// bin range (from the sub-chunk's box) is one bin or two adjacent bins sums in
+// bin range (from the sub-chunk's box) spans at most three bins sums in
 // registers and adds once per sub-chunk.  Those register paths run on sm_100's
 // packed FP32 instructions (two pairs per instruction).
 //
@@ -48,7 +48,7 @@
 
 namespace tpcf {
 
-constexpr int kDualUnroll = TPCF_DUAL_UNROLL;      // source-loop unrolling of the one-edge path
+constexpr int kDualUnroll = TPCF_DUAL_UNROLL;      // source-loop unrolling of the edge paths
 constexpr int kSingleUnroll = TPCF_SINGLE_UNROLL;  // and of the single-bin path
 // Blocks per SM that the pair kernel is compiled for: the shared-memory
 // occupancy of 128 threads at 20 bins (51 KB histogram + tiles).  Declaring it
@@ -146,13 +146,14 @@ __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const floa
 // conservatively (guard band eps on both ends):
 //   0  no pair of the chunk is in range        -> nothing to do
 //   1  every pair is in one bin `blo`           -> register sums, no binning
-//   2  pairs fall in bins blo and blo+1 only    -> register sums split at the
-//                                                  one edge, FP64 re-binning
-//                                                  inside its guard band
-//   3  anything else                           -> per-pair binning (do_pair)
+//   2  pairs fall in bins blo, blo+1            -> register sums split at the
+//   3  pairs fall in bins blo .. blo+2             one or two edges, FP64
+//                                                  re-binning inside a guard
+//                                                  band
+//   4  anything else                           -> per-pair binning (do_pair)
 // The path is chosen per warp (the largest class of its lanes), so lanes never
 // diverge inside a source loop.  Every pair still lands in its canonical bin:
-// in classes 1 and 2 the box bounds prove which bins are possible.
+// in classes 1 to 3 the box bounds prove which bins are possible.
 //
 // A row span of the grid starts and ends anywhere inside a sub-chunk; its
 // first and last sub-chunks are "partial": only the sources [lo, hi) of the
@@ -276,24 +277,34 @@ __device__ __forceinline__ void chunk_single(const SrcPair* __restrict__ S, int 
   hist_add<QA, NC>(hcol, blo, acc);
 }
 
-// Class 2: pairs in bins blo and blo+1 (either may be out of range, then it is
-// dropped); the edge between them is e2f[blo+1].  Sums over all pairs (s*)
-// and over the upper side (h*: the pair's r, w, K selected by d2 >= E, the
-// count as an integer); the lower side is their difference.
-template <int MODE, bool HAS_M, bool HAS_Z, bool PART, bool LOGB, int NC, int QA>
-__device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int lo, int hi, const LensP& L, float lx,
-                                           float ly, float lz, int cls, int blo, float* __restrict__ hcol,
-                                           const BinCtx& C, const float4 ss) {
+// Classes 2 and 3: the pairs of the chunk fall in bins blo .. blo + NE across
+// NE = 1 or 2 edges (a bin outside [0, nb) is dropped); edge e is
+// e2f[blo + 1 + e].  Sums over all pairs (s*) and, per edge, over the pairs on
+// its far side (h*[e]: d2 >= E_e); bin blo + j receives h[j-1] - h[j] with
+// h[-1] = all and h[NE] = 0.  The side of a pair is a 1.0/0.0 mask from one
+// FP32 compare, applied by multiplication.  Each edge is tested at
+// E (1 - eps) and E (1 + eps): a pair between the two lies within the guard
+// band, and then this lane drops its register sums and bins the sub-chunk
+// pair by pair by the canonical rule (rare).  A lane with fewer edges than NE
+// (class 1, or class 2 in a class-3 warp) keeps 3e38 on its unused edges.
+template <int MODE, bool HAS_M, bool HAS_Z, bool PART, bool LOGB, int NC, int QA, int NE>
+__device__ __forceinline__ void chunk_edges(const SrcPair* __restrict__ S, int lo, int hi, const LensP& L, float lx,
+                                            float ly, float lz, int cls, int blo, float* __restrict__ hcol,
+                                            const BinCtx& C, const float4 ss) {
   constexpr bool MK = HAS_Z || PART;
   constexpr bool LI = !MK;
   float2 sgt = dup2(0.f), sgx = dup2(0.f), sw = dup2(0.f), sdw = dup2(0.f), sk = dup2(0.f), sn = dup2(0.f);
-  float2 hgt = dup2(0.f), hgx = dup2(0.f), hw = dup2(0.f), hdw = dup2(0.f), hk = dup2(0.f);
-  int hn = 0;
-  // lanes of class 1 (or 0) keep an edge no pair reaches
-  const float E = (cls == 2) ? C.e2f[blo + 1] : 3.0e38f;
-  const float gE = (cls == 2) ? E * C.eps_rel : 0.f;
-  const float2 nE = dup2(-E);
-  bool near = false;  // some pair lies within the guard band of E
+  float2 hgt[NE], hgx[NE], hw[NE], hdw[NE], hk[NE], hn[NE];
+  float Elo[NE], Ehi[NE];
+  float2 nc = dup2(0.f);  // pairs inside a guard band (counted, masked)
+#pragma unroll
+  for (int e = 0; e < NE; ++e) {
+    hgt[e] = hgx[e] = hw[e] = hdw[e] = hk[e] = hn[e] = dup2(0.f);
+    const bool on = e < cls - 1;
+    const float E = C.e2f[min(max(blo + 1 + e, 0), C.nb)];
+    Elo[e] = on ? E * (1.f - C.eps_rel) : 3.0e38f;
+    Ehi[e] = on ? E * (1.f + C.eps_rel) : 3.0e38f;
+  }
   const int k0 = PART ? (lo >> 1) : 0;
   const int k1 = PART ? ((hi + 1) >> 1) : kChunk / 2;
 #pragma unroll kDualUnroll
@@ -301,22 +312,15 @@ __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int lo
     const float4 xy = S[k].xy, pq = S[k].pq, wk = S[k].wk;
     float2 d2, d, r, X, Y;
     pair_terms2<MODE, LOGB>(L, xy, pq, d2, d, r, X, Y);
-    const float2 dE = add2(d2, nE);
-    bool u0 = d2.x >= E, u1 = d2.y >= E;
-    const bool n0 = fabsf(dE.x) <= gE, n1 = fabsf(dE.y) <= gE;
     float2 w = lo2(wk), K = hi2(wk);
+    float2 zm = dup2(1.f);
     if (MK) {
       bool a0, a1;
-      const float2 zm = pair_mask<HAS_Z, PART>(S, k, lz, lo, hi, a0, a1);
+      zm = pair_mask<HAS_Z, PART>(S, k, lz, lo, hi, a0, a1);
       r = mul2(r, zm);
       w = mul2(w, zm);
       if (MODE == 0 && HAS_M) K = mul2(K, zm);
       sn = add2(sn, zm);
-      u0 = u0 && a0;
-      u1 = u1 && a1;
-      near |= (a0 && n0) || (a1 && n1);
-    } else {
-      near |= n0 || n1;
     }
     // products folded into the sums: one packed FFMA per quantity and side
     if (!(LI && MODE == 1)) {
@@ -326,20 +330,28 @@ __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int lo
     if (!LI) sw = add2(sw, w);
     sdw = fma2(d, w, sdw);
     if (MODE == 0 && HAS_M && !LI) sk = add2(sk, K);
-    const float2 rm = make_float2(u0 ? r.x : 0.f, u1 ? r.y : 0.f);
-    const float2 wm = make_float2(u0 ? w.x : 0.f, u1 ? w.y : 0.f);
-    hgt = fma2(rm, X, hgt);
-    hgx = fma2(rm, Y, hgx);
-    hw = add2(hw, wm);
-    hdw = fma2(d, wm, hdw);
-    hn += (int)u0 + (int)u1;
-    if (MODE == 0 && HAS_M) hk = add2(hk, make_float2(u0 ? K.x : 0.f, u1 ? K.y : 0.f));
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+      float2 mh = make_float2(d2.x >= Ehi[e] ? 1.f : 0.f, d2.y >= Ehi[e] ? 1.f : 0.f);
+      const float2 ml = make_float2(d2.x >= Elo[e] ? 1.f : 0.f, d2.y >= Elo[e] ? 1.f : 0.f);
+      if (MK) {
+        nc = fma2(add2(ml, make_float2(-mh.x, -mh.y)), zm, nc);
+        mh = mul2(mh, zm);
+      } else {
+        nc = add2(nc, add2(ml, make_float2(-mh.x, -mh.y)));
+      }
+      const float2 rm = mul2(r, mh);
+      const float2 wm = mul2(w, mh);
+      hgt[e] = fma2(rm, X, hgt[e]);
+      hgx[e] = fma2(rm, Y, hgx[e]);
+      hw[e] = add2(hw[e], wm);
+      hdw[e] = fma2(d, wm, hdw[e]);
+      hn[e] = add2(hn[e], mh);
+      if (MODE == 0 && HAS_M) hk[e] = fma2(K, mh, hk[e]);
+    }
   }
   if (cls == 0) return;
-  if (near) {
-    // rare (a pair within a relative 4e-6 of the edge): this lane's register
-    // sums are dropped and the sub-chunk is binned pair by pair, each pair by
-    // the canonical rule
+  if (sum2(nc) != 0.f) {
     for (int j = lo; j < hi; ++j) {
       float4 a, b;
       src_of(S, j, a, b);
@@ -347,36 +359,43 @@ __device__ __forceinline__ void chunk_dual(const SrcPair* __restrict__ S, int lo
     }
     return;
   }
-  float tot[QA], up[QA];
-  tot[QGT] = (LI && MODE == 1) ? ss.x : sum2(sgt);
-  tot[QGX] = (LI && MODE == 1) ? ss.y : sum2(sgx);
-  tot[QW] = LI ? ss.z : sum2(sw);
-  tot[QDW] = sum2(sdw);
-  tot[QN] = MK ? sum2(sn) : (float)kChunk;
-  up[QGT] = sum2(hgt);
-  up[QGX] = sum2(hgx);
-  up[QW] = sum2(hw);
-  up[QDW] = sum2(hdw);
-  up[QN] = (float)hn;
-  if (MODE == 0 && HAS_M) {
-    tot[QK] = LI ? ss.w : sum2(sk);
-    up[QK] = sum2(hk);
-  }
-  if (cls == 1) {
-    hist_add<QA, NC>(hcol, blo, tot);
-    return;
-  }
-  float dn[QA];
+  float prev[QA];
+  prev[QGT] = (LI && MODE == 1) ? ss.x : sum2(sgt);
+  prev[QGX] = (LI && MODE == 1) ? ss.y : sum2(sgx);
+  prev[QW] = LI ? ss.z : sum2(sw);
+  prev[QDW] = sum2(sdw);
+  prev[QN] = MK ? sum2(sn) : (float)kChunk;
+  if (MODE == 0 && HAS_M) prev[QK] = LI ? ss.w : sum2(sk);
 #pragma unroll
-  for (int q = 0; q < QA; ++q) dn[q] = tot[q] - up[q];
-  if (blo >= 0) hist_add<QA, NC>(hcol, blo, dn);
-  if (blo + 1 < C.nb) hist_add<QA, NC>(hcol, blo + 1, up);
+  for (int j = 0; j <= NE; ++j) {
+    float up[QA];
+    if (j < NE) {
+      up[QGT] = sum2(hgt[j]);
+      up[QGX] = sum2(hgx[j]);
+      up[QW] = sum2(hw[j]);
+      up[QDW] = sum2(hdw[j]);
+      up[QN] = sum2(hn[j]);
+      if (MODE == 0 && HAS_M) up[QK] = sum2(hk[j]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < QA; ++q) up[q] = 0.f;
+    }
+    const int bin = blo + j;
+    if (j <= cls - 1 && bin >= 0 && bin < C.nb) {
+      float v[QA];
+#pragma unroll
+      for (int q = 0; q < QA; ++q) v[q] = prev[q] - up[q];
+      hist_add<QA, NC>(hcol, bin, v);
+    }
+#pragma unroll
+    for (int q = 0; q < QA; ++q) prev[q] = up[q];
+  }
 }
 
 #ifdef TPCF_MODE_STATS
 // Diagnostic build only: warp-level path counts [4], lane-pairs per warp path
 // [4], and lane-pairs per lane class [4] (active lanes only).
-__device__ unsigned long long g_mode_stats[12];
+__device__ unsigned long long g_mode_stats[15];
 extern "C" int tpcf_debug_mode_stats(unsigned long long* out) {
   return (int)cudaMemcpyFromSymbol(out, g_mode_stats, sizeof(g_mode_stats));
 }
@@ -512,8 +531,8 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
   double* wsum = bsum + (size_t)warp * kQ * nb;
   const int flush_src = P.flush_src > 0 ? P.flush_src : 4096;
 #ifdef TPCF_MODE_STATS
-  __shared__ unsigned long long sh_stats[12];
-  if (tid < 12) sh_stats[tid] = 0ull;
+  __shared__ unsigned long long sh_stats[15];
+  if (tid < 15) sh_stats[tid] = 0ull;
   __syncthreads();
 #endif
   for (int e = 0; e < nb * QA; ++e) hcol[e * BT] = 0.f;
@@ -608,35 +627,43 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
           const SrcPair* __restrict__ Sc = Tb + j * (kChunk / 2);
           const float4 cbox = Mb[j].box;
           int blo = 0;
-          int cls = act ? classify<LOGB, HAS_Z, true>(lx, ly, cbox, C, blo) : 0;
-          if (PATH == 1 && cls) cls = 3;
+          int cls = act ? classify_edges<LOGB>(lx, ly, cbox, C, blo) : 0;
+          if (PATH == 1 && cls) cls = 4;
           const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)cls);
 #ifdef TPCF_MODE_STATS
           {
             const unsigned nact = __popc(__ballot_sync(0xffffffffu, act));
-            unsigned ncls[4];
-            for (int cc = 0; cc < 4; ++cc) ncls[cc] = __popc(__ballot_sync(0xffffffffu, act && cls == cc));
+            unsigned ncls[5];
+            for (int cc = 0; cc < 5; ++cc) ncls[cc] = __popc(__ballot_sync(0xffffffffu, act && cls == cc));
             if (lane == 0) {
               atomicAdd(&sh_stats[m], 1ull);
-              atomicAdd(&sh_stats[4 + m], (unsigned long long)((hi - lo) * nact));
-              for (int cc = 0; cc < 4; ++cc) atomicAdd(&sh_stats[8 + cc], (unsigned long long)((hi - lo) * ncls[cc]));
+              atomicAdd(&sh_stats[5 + m], (unsigned long long)((hi - lo) * nact));
+              for (int cc = 0; cc < 5; ++cc)
+                atomicAdd(&sh_stats[10 + cc], (unsigned long long)((hi - lo) * ncls[cc]));
             }
           }
 #endif
           if (m == 0) continue;
+          const float4 ss = Mb[j].sum;
           if (m == 1) {
-            const float4 ss = Mb[j].sum;
             if (part)
               chunk_single<MODE, HAS_M, HAS_Z, true, LOGB, BT, QA>(Sc, lo, hi, LP, lz, cls, blo, hcol, ss);
             else
               chunk_single<MODE, HAS_M, HAS_Z, false, LOGB, BT, QA>(Sc, 0, kChunk, LP, lz, cls, blo, hcol, ss);
           } else if (m == 2) {
-            const float4 ss = Mb[j].sum;
             if (part)
-              chunk_dual<MODE, HAS_M, HAS_Z, true, LOGB, BT, QA>(Sc, lo, hi, LP, lx, ly, lz, cls, blo, hcol, C, ss);
+              chunk_edges<MODE, HAS_M, HAS_Z, true, LOGB, BT, QA, 1>(Sc, lo, hi, LP, lx, ly, lz, cls, blo, hcol, C,
+                                                                     ss);
             else
-              chunk_dual<MODE, HAS_M, HAS_Z, false, LOGB, BT, QA>(Sc, 0, kChunk, LP, lx, ly, lz, cls, blo, hcol, C,
-                                                                   ss);
+              chunk_edges<MODE, HAS_M, HAS_Z, false, LOGB, BT, QA, 1>(Sc, 0, kChunk, LP, lx, ly, lz, cls, blo, hcol,
+                                                                      C, ss);
+          } else if (m == 3) {
+            if (part)
+              chunk_edges<MODE, HAS_M, HAS_Z, true, LOGB, BT, QA, 2>(Sc, lo, hi, LP, lx, ly, lz, cls, blo, hcol, C,
+                                                                     ss);
+            else
+              chunk_edges<MODE, HAS_M, HAS_Z, false, LOGB, BT, QA, 2>(Sc, 0, kChunk, LP, lx, ly, lz, cls, blo, hcol,
+                                                                      C, ss);
           } else if (act) {
             for (int jj = lo; jj < hi; ++jj) {
               float4 a, bb;
@@ -675,7 +702,7 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
   }
 #ifdef TPCF_MODE_STATS
   __syncthreads();
-  if (tid < 12) atomicAdd(&g_mode_stats[tid], sh_stats[tid]);
+  if (tid < 15) atomicAdd(&g_mode_stats[tid], sh_stats[tid]);
 #endif
 }
 
@@ -984,7 +1011,7 @@ __global__ void k_item_cost(const int2* __restrict__ items, int n_items, const T
     if (sp.y > sp.x) s += (unsigned long long)(sp.y - sp.x);
   }
   const unsigned long long nl = (unsigned long long)(L.group_start[it.y + 1] - L.group_start[it.y]);
-  cost[i] = s * nl + 1;
+  cost[i] = item_key(s * nl + 1, i);
   order[i] = i;
 }
 
@@ -1028,16 +1055,31 @@ __global__ void k_dfma_peak(double* out, int iters, double a, double b) {
 }
 
 // Per-patch FP64 sums from item sums, fixed order (deterministic).
-// patch_groups[p] .. patch_groups[p+1] are the groups of patch p.
-__global__ void k_patch_reduce(const double* __restrict__ item_sums, int item_base, const int* __restrict__ patch_groups,
-                               int n_patch, int nb, double* patch_sums) {
+// patch_groups[p] .. patch_groups[p+1] are the groups of patch p.  Block
+// (p, c) covers the 32 sums e = 32 c + lane of patch p: warp w adds the groups
+// g0 + w, g0 + w + 8, ... (lane-contiguous loads), then the 8 warp sums are
+// added in warp order.
+constexpr int kReduceWarps = 8;
+__global__ void __launch_bounds__(32 * kReduceWarps) k_patch_reduce(const double* __restrict__ item_sums, int item_base,
+                                                                   const int* __restrict__ patch_groups, int n_patch,
+                                                                   int nb, double* patch_sums) {
+  __shared__ double part[kReduceWarps][32];
   const int p = blockIdx.x;
-  if (p >= n_patch) return;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int e = blockIdx.y * 32 + lane;
+  const int ne = kQ * nb;
   const int g0 = patch_groups[p], g1 = patch_groups[p + 1];
-  for (int e = threadIdx.x; e < kQ * nb; e += blockDim.x) {
-    double s = 0.0;
-    for (int g = g0; g < g1; ++g) s += item_sums[(size_t)(item_base + g) * kQ * nb + e];
-    patch_sums[(size_t)p * kQ * nb + e] = s;
+  double s = 0.0;
+  if (e < ne) {
+#pragma unroll 4
+    for (int g = g0 + w; g < g1; g += kReduceWarps) s += item_sums[(size_t)(item_base + g) * ne + e];
+  }
+  part[w][lane] = s;
+  __syncthreads();
+  if (w == 0 && e < ne) {
+    double t = part[0][lane];
+    for (int k = 1; k < kReduceWarps; ++k) t += part[k][lane];
+    patch_sums[(size_t)p * ne + e] = t;
   }
 }
 
@@ -1227,7 +1269,9 @@ cudaError_t launch_dfma_peak(double* out, int blocks, int threads, int iters, cu
 }
 cudaError_t launch_patch_reduce(const double* item_sums, int item_base, const int* patch_groups, int n_patch, int nb,
                                 double* patch_sums, cudaStream_t st) {
-  if (n_patch > 0) k_patch_reduce<<<n_patch, 128, 0, st>>>(item_sums, item_base, patch_groups, n_patch, nb, patch_sums);
+  if (n_patch > 0)
+    k_patch_reduce<<<dim3(n_patch, (kQ * nb + 31) / 32), 32 * kReduceWarps, 0, st>>>(item_sums, item_base, patch_groups,
+                                                                                    n_patch, nb, patch_sums);
   return cudaGetLastError();
 }
 cudaError_t launch_lens_outputs(const double* acc, const float4* rec, const int* perm, int n_valid, int nb,

@@ -841,7 +841,7 @@ __global__ void k_item_cost_sph(const int2* __restrict__ items, int n_items, con
       if (sp[j].y > sp[j].x) s += (unsigned long long)(sp[j].y - sp[j].x);
   }
   const unsigned long long nl = (unsigned long long)(L.group_start[it.y + 1] - L.group_start[it.y]);
-  cost[i] = s * nl + 1;
+  cost[i] = item_key(s * nl + 1, i);
   order[i] = i;
 }
 

@@ -94,6 +94,17 @@ __device__ __forceinline__ int2 row_span(const GridDesc& G, float4 box, float R,
   return make_int2(G.cell_start[base + cx0], G.cell_start[base + cx1 + 1]);
 }
 
+// Sort key of work item i (items are built in task, then lens-group order,
+// and lens groups follow (patch, Morton) order): the item's cost in bands of
+// 2^(1/8) (about 9%) on top, the item index below.  Sorted descending, the
+// costliest items start first (load balance), and inside one band the items
+// run in task and space order, so that the warps resident at one time read
+// the same rows of one source grid and those stay in L2.
+__device__ __forceinline__ unsigned long long item_key(unsigned long long cost, int i) {
+  const unsigned band = (unsigned)(__log2f((float)cost) * 8.f);
+  return ((unsigned long long)band << 32) | (unsigned)i;
+}
+
 // ------------------------------------------------------------ binning -------
 // Canonical FP64 bin of the pair (rare path: pairs inside the guard band).
 static __device__ __noinline__ int slow_bin(float lx, float ly, float sx, float sy, const double* e2, int nb) {
@@ -174,6 +185,36 @@ __device__ __forceinline__ int classify(float lx, float ly, const float4 box, co
   if (b0 == b1) return 1;
   if (b1 == b0 + 1) return 2;
   return 3;
+}
+
+// Class of a box for the planar pair kernel: 0 when no pair can be in range,
+// else 1 + the number of bin edges its distance range [dmin, dmax] may cross
+// (guard band eps on both ends) for up to two edges, 4 beyond (per-pair
+// binning).  blo = the lowest bin, -1 when the range starts below the first
+// edge; bins below 0 and from nb up are all dropped, so the range is clamped
+// to [-1, nb] first and every edge blo + 1 + e it names is in [0, nb].
+template <bool LOGB>
+__device__ __forceinline__ int classify_edges(float lx, float ly, const float4 box, const BinCtx& C, int& blo) {
+  const float dxl = fmaxf(fmaxf(box.x - lx, lx - box.z), 0.f);
+  const float dyl = fmaxf(fmaxf(box.y - ly, ly - box.w), 0.f);
+  const float dxh = fmaxf(lx - box.x, box.z - lx);
+  const float dyh = fmaxf(ly - box.y, box.w - ly);
+  const float dmin2 = fmaf(dyl, dyl, dxl * dxl);
+  const float dmax2 = fmaf(dyh, dyh, dxh * dxh);
+  int b0, b1;
+  if (LOGB) {
+    b0 = __float2int_rd(fmaf(__log2f(dmin2), C.A, C.B) - C.eps);
+    b1 = __float2int_rd(fmaf(__log2f(dmax2), C.A, C.B) + C.eps);
+  } else {
+    b0 = edge_index_f32(dmin2 * (1.f - C.eps), C.e2f, C.nb);
+    b1 = edge_index_f32(dmax2 * (1.f + C.eps), C.e2f, C.nb);
+  }
+  if (b1 < 0 || b0 >= C.nb) return 0;
+  b0 = max(b0, -1);
+  b1 = min(b1, C.nb);
+  blo = b0;
+  const int e = b1 - b0;
+  return e <= 2 ? 1 + e : 4;
 }
 
 }  // namespace tpcf

@@ -587,7 +587,7 @@ def path_stats(tpcf, args):
     ctx = tpcf.Context(0)
     ctx.set_cell_size(bins.x_max / (args.cell_divisor or 64))
     lib = tpcf._lib.lib()
-    st = (C.c_ulonglong * 12)()
+    st = (C.c_ulonglong * 15)()
     lib.tpcf_debug_mode_stats(st)
     base = np.array(st[:])
     outs = tpcf.batch_shear_2pcf(L, S, w["tasks"], bins, ctx=ctx)
@@ -595,12 +595,12 @@ def path_stats(tpcf, args):
     v = np.array(st[:]) - base
     binned = sum(int(o.n_pairs.sum()) for o in outs)
     res = {"binned_pairs": binned}
-    for i, name in enumerate(("skip", "single_bin", "one_edge", "per_pair")):
-        res[name] = {"warp_chunks": float(v[i] / v[:4].sum()), "lane_pairs": float(v[4 + i] / v[4:8].sum())}
-    res["computed_lane_pairs_per_binned_pair"] = float(v[5:8].sum() / binned)
-    res["lane_class_of_active_lane_pairs"] = {name: float(v[8 + i] / v[8:12].sum())
-                                              for i, name in enumerate(("out_of_range", "single_bin", "one_edge",
-                                                                        "per_pair"))}
+    names = ("skip", "single_bin", "one_edge", "two_edges", "per_pair")
+    for i, name in enumerate(names):
+        res[name] = {"warp_chunks": float(v[i] / v[:5].sum()), "lane_pairs": float(v[5 + i] / v[5:10].sum())}
+    res["computed_lane_pairs_per_binned_pair"] = float(v[6:10].sum() / binned)
+    res["lane_class_of_active_lane_pairs"] = {("out_of_range" if i == 0 else name): float(v[10 + i] / v[10:15].sum())
+                                              for i, name in enumerate(names)}
     print(json.dumps(res), flush=True)
 
 
