@@ -220,6 +220,61 @@ def sky_patch(x, y, box, lam0_deg=40.0, phi0_deg=-30.0):
     return lam.astype(np.float32), phi.astype(np.float32)
 
 
+def marks_timing(tpcf, stream, nb):
+    """xi from precomputed marks for 16 maps over 1.0 M lenses (HBM roofline
+    on the algorithmic bytes) and a 1000-resample marks bootstrap (FP64 FMA
+    roofline); CUDA events on the launch stream, each timed call after an
+    untimed one."""
+    import torch
+    out = {}
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, e0.elapsed_time(e1)
+
+    # xi from marks: 1.0 M lenses x 20 bins, 16 maps
+    rng = np.random.default_rng(77)
+    n, nbm, n_map = 1_000_000, nb, 16
+    mk = tpcf.MarksField(x=dev(rng.normal(size=n).astype(np.float32)), y=dev(rng.normal(size=n).astype(np.float32)),
+                         w=dev(rng.uniform(0.5, 1.5, n).astype(np.float32)),
+                         xi_E=dev(rng.normal(size=(n, nbm)).astype(np.float32)),
+                         xi_B=dev(rng.normal(size=(n, nbm)).astype(np.float32)),
+                         K=dev(rng.uniform(0.5, 1.5, (n, nbm)).astype(np.float32)))
+    val = dev(rng.normal(size=(n_map, n)).astype(np.float32))
+    wm = dev(rng.uniform(0.5, 1.5, (n_map, n)).astype(np.float32))
+    mctx = tpcf.Context(0)
+    mctx.set_stream(stream.cuda_stream)
+    _, ms = timed(lambda: tpcf.calculate_tpcf_from_marks([mk], [val], [wm], ctx=mctx))
+    # algorithmic bytes: the marks once (xi_E, xi_B, K [n][n_bin] and the marks
+    # weight, FP32) and the maps' val and w [n_map][n] (FP32)
+    byt = (3 * 4 * n * nbm + 4 * n) + n_map * 8 * n
+    hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"] \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    out["marks_reweight"] = {"maps": n_map, "lenses": n, "n_bin": nbm, "call_ms": ms,
+                             "roofline": {"bound": "hbm", "achieved": byt / (ms * 1e-3) / 1e9, "peak": hbm,
+                                          "unit": "GB/s", "frac": byt / (ms * 1e-3) / 1e9 / hbm,
+                                          "bytes": byt}}
+    _, ms = timed(lambda: tpcf.marks_bootstrap([mk], 1000, seed=5, covariance=True, ctx=mctx))
+    # each resample re-weights every lens's 3 n_bin + 1 marks: one FP64 FMA
+    # each (the multiplicities are drawn on the device), so FP64-bound
+    flop = 1000 * n * (3 * nbm + 1) * 2
+    p64 = mctx.measure_fp64_peak()
+    out["marks_bootstrap"] = {"resamples": 1000, "lenses": n, "call_ms": ms,
+                              "roofline": {"bound": "fp64", "achieved": flop / (ms * 1e-3) / 1e12, "peak": p64,
+                                           "unit": "TFLOP/s", "frac": flop / (ms * 1e-3) / 1e12 / p64,
+                                           "flop": flop, "peak_source": "FP64 FMA loop measured in this run"}}
+    del mk, val, wm
+    mctx.close()
+    return out
+
+
 def widened_timing(tpcf, w, peak_fp32, stream, cpu_threads, with_cpu=True):
     """Measurements of the rows around the pair sum: the spherical pair sum on
     the tomography catalogues projected onto a sky patch, xi from precomputed
@@ -303,38 +358,7 @@ def widened_timing(tpcf, w, peak_fp32, stream, cpu_threads, with_cpu=True):
     sctx.close()
     del Ls, Ss
 
-    # xi from marks: 1.0 M lenses x 20 bins, 16 maps
-    rng = np.random.default_rng(77)
-    n, nbm, n_map = 1_000_000, nb, 16
-    mk = tpcf.MarksField(x=dev(rng.normal(size=n).astype(np.float32)), y=dev(rng.normal(size=n).astype(np.float32)),
-                         w=dev(rng.uniform(0.5, 1.5, n).astype(np.float32)),
-                         xi_E=dev(rng.normal(size=(n, nbm)).astype(np.float32)),
-                         xi_B=dev(rng.normal(size=(n, nbm)).astype(np.float32)),
-                         K=dev(rng.uniform(0.5, 1.5, (n, nbm)).astype(np.float32)))
-    val = dev(rng.normal(size=(n_map, n)).astype(np.float32))
-    wm = dev(rng.uniform(0.5, 1.5, (n_map, n)).astype(np.float32))
-    mctx = tpcf.Context(0)
-    mctx.set_stream(stream.cuda_stream)
-    _, ms = timed(lambda: tpcf.calculate_tpcf_from_marks([mk], [val], [wm], ctx=mctx))
-    # algorithmic bytes: the marks once (xi_E, xi_B, K [n][n_bin] and the marks
-    # weight, FP32) and the maps' val and w [n_map][n] (FP32)
-    byt = (3 * 4 * n * nbm + 4 * n) + n_map * 8 * n
-    hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"] \
-        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
-    out["marks_reweight"] = {"maps": n_map, "lenses": n, "n_bin": nbm, "call_ms": ms,
-                             "roofline": {"bound": "hbm", "achieved": byt / (ms * 1e-3) / 1e9, "peak": hbm,
-                                          "unit": "GB/s", "frac": byt / (ms * 1e-3) / 1e9 / hbm,
-                                          "bytes": byt}}
-    _, ms = timed(lambda: tpcf.marks_bootstrap([mk], 1000, seed=5, covariance=True, ctx=mctx))
-    # each resample re-weights every lens's 3 n_bin + 1 marks: one FP64 FMA
-    # each (the multiplicities are drawn on the device), so FP64-bound
-    flop = 1000 * n * (3 * nbm + 1) * 2
-    p64 = mctx.measure_fp64_peak()
-    out["marks_bootstrap"] = {"resamples": 1000, "lenses": n, "call_ms": ms,
-                              "roofline": {"bound": "fp64", "achieved": flop / (ms * 1e-3) / 1e12, "peak": p64,
-                                           "unit": "TFLOP/s", "frac": flop / (ms * 1e-3) / 1e12 / p64,
-                                           "flop": flop, "peak_source": "FP64 FMA loop measured in this run"}}
-    del mk, val, wm
+    out.update(marks_timing(tpcf, stream, nb))
 
     # equal-weight k-means on all lens positions, 100 blocks
     ux = np.concatenate([l["x"] for l in w["lens_bins"]])
@@ -342,6 +366,8 @@ def widened_timing(tpcf, w, peak_fp32, stream, cpu_threads, with_cpu=True):
     uw = np.concatenate([l["w"] for l in w["lens_bins"]])
     uw = (0.01 + uw / uw.max()).astype(np.float32)
     U = [dev(a) for a in (ux, uy, uw)]
+    mctx = tpcf.Context(0)
+    mctx.set_stream(stream.cuda_stream)
     (lab, _, it, devw), ms = timed(lambda: tpcf.partition_data_equal(U[0], U[1], U[2], 100, seed=3, ctx=mctx))
     out["kmeans_equal"] = {"points": int(len(ux)), "k": 100, "iterations": it, "max_weight_deviation": devw,
                            "call_ms": ms}
@@ -669,6 +695,8 @@ def main():
     ap.add_argument("--geometry", default="plane", choices=["plane", "sphere"],
                     help="profiling: 'sphere' projects the catalogues onto a sky patch and times the spherical "
                          "pair kernel instead")
+    ap.add_argument("--marks-only", action="store_true",
+                    help="profiling: only the xi-from-marks and marks-bootstrap measurements, as one JSON line")
     ap.add_argument("--no-widened", action="store_true",
                     help="skip the spherical, marks, bootstrap, k-means and reader measurements")
     ap.add_argument("--cell-divisor", type=int, default=0,
@@ -698,6 +726,11 @@ def main():
         return path_stats(tpcf, args)
     if args.config != 5:
         return config_line(tpcf, args, rank)
+    if args.marks_only:
+        res = marks_timing(tpcf, torch.cuda.current_stream(), 20)
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+        return 0
 
     w = workload(args.scale)
     if args.region > 0:
