@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(BT, kAdjMinBlocks) k_adj(const AdjParams P) {
 }
 
 // --------------------------------------------------------------- prep -------
-// Lens grid keys (lens validity: finite, w != 0, z >= 0), cell + Morton inside.
+// Lens grid keys (lens validity: finite, w != 0, z >= 0), cell + Hilbert index inside.
 __global__ void k_adj_lens_keys(const float* __restrict__ x, const float* __restrict__ y,
                                 const float* __restrict__ z, const float* __restrict__ w, long long n, float x0,
                                 float y0, float inv_cell, int ncx, int ncy, int mb, unsigned* keys, int* idx) {
@@ -484,9 +484,7 @@ __global__ void k_adj_lens_keys(const float* __restrict__ x, const float* __rest
       if (half > 0) {
         unsigned qx = (unsigned)clamp_floor((fx - (float)cx) * q, 0, (1 << half) - 1);
         unsigned qy = (unsigned)clamp_floor((fy - (float)cy) * q, 0, (1 << half) - 1);
-        unsigned m = 0;
-        for (int b = 0; b < half; ++b) m |= (((qx >> b) & 1u) << (2 * b)) | (((qy >> b) & 1u) << (2 * b + 1));
-        key |= m;
+        key |= hilbert_index(qx, qy, half);
       }
     }
     keys[i] = key;
@@ -506,7 +504,7 @@ __global__ void k_adj_lens_gather(const int* __restrict__ idx, int n_valid, cons
   rec[s] = r;
 }
 
-// Source Morton keys over the source box (source validity: finite, z >= 0).
+// Source Hilbert keys over the source box (source validity: finite, z >= 0).
 __global__ void k_adj_src_keys(const float* __restrict__ x, const float* __restrict__ y,
                                const float* __restrict__ z, long long n, float4 box, unsigned long long* keys,
                                int* idx) {
@@ -518,9 +516,7 @@ __global__ void k_adj_src_keys(const float* __restrict__ x, const float* __restr
     if (v) {
       const unsigned qx = (unsigned)clamp_floor((xi - box.x) * sxs, 0, 65535);
       const unsigned qy = (unsigned)clamp_floor((yi - box.y) * sys, 0, 65535);
-      unsigned m = 0;
-      for (int b = 0; b < 16; ++b) m |= (((qx >> b) & 1u) << (2 * b)) | (((qy >> b) & 1u) << (2 * b + 1));
-      key = m;
+      key = hilbert_index(qx, qy, 16);
     }
     keys[i] = key;
     idx[i] = (int)i;

@@ -357,7 +357,7 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
       int* i1 = (int*)ws_alloc(c, sizeof(int) * s.n);
       int cell_bits = 1;
       while (cell_bits < 32 && (1ull << cell_bits) <= (unsigned long long)ncells) ++cell_bits;
-      const int mb = std::min(16, (32 - cell_bits) & ~1);  // within-cell Morton bits
+      const int mb = std::min(16, (32 - cell_bits) & ~1);  // within-cell Hilbert bits
       counted(c, launch_src_keys(s.x, s.y, s.z, s.n, x0, y0, g.inv_cell, ncx, ncy, mb, k0, i0, st), "src keys");
       const int end_bit = cell_bits + mb;
       size_t tb = 0;
@@ -391,7 +391,7 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
   if (sph) margin = (float)(2.0 * M_PI + M_PI);  // reduced longitudes and latitudes
   margin = (float)(1e-5 * (margin + Rd) + 1e-4 * maxcell);
 
-  // ---- lens catalogues: sort by (patch, Morton), groups of <= lens_group lenses
+  // ---- lens catalogues: sort by (patch, Hilbert index), groups of <= lens_group lenses
   std::vector<LensBuilt> lb(nL);
   std::vector<LensDesc> ldesc(nL);
   for (int i = 0; i < nL; ++i) {

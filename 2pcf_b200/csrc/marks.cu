@@ -122,9 +122,21 @@ struct MultFactors {  // resamples: vw = wm = multiplicity of the lens's unit
 // store (one map, 32 lenses) spread over 16 banks instead of 2.
 constexpr int kTileL = 64;
 constexpr int kMarksLens = 1024;  // lenses per block
+// Threads per block at most: one group of 3 kMaxBins + 1 = 385 rows fits, and
+// two blocks per SM leave 78 registers per thread (the 16 FP64 sums and the
+// staged factor pairs in flight without spilling).
+constexpr int kMarksThreads = 416;
 static_assert(kTileL == 64, "the raw staging areas hold 64 lenses");
-template <class Fac>
-__global__ void __launch_bounds__(512, 2) k_marks_partials(const MarksField* __restrict__ fields, int n_field,
+// With STAGE the marks of the next tile (xi_E, xi_B, K [kTileL][n_bin] and the
+// marks weight [kTileL], as laid out in HBM) are copied into shared memory by
+// cp.async together with the factors' raw inputs, into the other of two
+// buffers, so the summing loop reads only shared memory and no global load
+// latency is exposed; for wide binnings (marks_stage_floats too large) the
+// loop loads the marks from HBM itself.
+int marks_stage_floats(int n_bin) { return 3 * kTileL * n_bin + kTileL; }
+constexpr int kMaxStageFloats = 3 * kTileL * 32 + kTileL;  // n_bin <= 32
+template <class Fac, bool STAGE>
+__global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const MarksField* __restrict__ fields, int n_field,
                                                             const Fac fac, int n_g, int n_bin, int tg,
                                                             double* __restrict__ partial) {
   extern __shared__ __align__(16) unsigned char sm[];
@@ -134,6 +146,8 @@ __global__ void __launch_bounds__(512, 2) k_marks_partials(const MarksField* __r
   double* fac_s = reinterpret_cast<double*>(sm);  // [kTileL][kMapGroup] factors of the E and B rows
   double* fw_s = fac_s + TF;                      // [kTileL][kMapGroup] factors of K and the weight
   unsigned char* raw = sm + 2 * TF * sizeof(double);
+  float* mk = reinterpret_cast<float*>(raw + std::max(MapFactors::kRawBytes, MultFactors::kRawBytes));
+  const int MS = 3 * kTileL * n_bin + kTileL;  // floats per marks buffer
   const int blk = blockIdx.x;
   int fi = 0;
   while (fi + 1 < n_field && fields[fi + 1].chunk0 <= blk) ++fi;
@@ -143,16 +157,30 @@ __global__ void __launch_bounds__(512, 2) k_marks_partials(const MarksField* __r
   const int tid = threadIdx.x;
   const int grp = tid / tg, r = tid % tg;
   const int q = r / n_bin, bb = r - q * n_bin;  // q = 3: the marks weight row
-  const float* row = q == 0 ? F.xiE + bb : q == 1 ? F.xiB + bb : q == 2 ? F.K + bb : F.mw;
-  const long long rs = q < 3 ? n_bin : 1;       // stride of the row from lens to lens
   const bool live = r < R;
   const double* fsel = q < 2 ? fac_s : fw_s;
+  // this thread's marks row: in HBM (lens stride rs) or in a staged buffer
+  const float* row = q == 0 ? F.xiE + bb : q == 1 ? F.xiB + bb : q == 2 ? F.K + bb : F.mw;
+  const long long rs = q < 3 ? n_bin : 1;
+  const int srow = q < 3 ? q * kTileL * n_bin + bb : 3 * kTileL * n_bin;
 
-  auto stage_tile = [&](long long t0) {
+  auto stage_tile = [&](long long t0, int buf) {
     const int nt = (int)min((long long)kTileL, j1 - t0);
     for (int e = tid; e < TF; e += blockDim.x) {
       const int g = e / kTileL, jj = e - g * kTileL;
       fac.stage(F, g, jj, t0 + jj, jj < nt && g < n_g, raw, e);
+    }
+    if (STAGE) {
+      float* mb = mk + buf * MS;
+      const int ne = nt * n_bin;
+      const size_t o = (size_t)t0 * n_bin;
+      for (int e = tid; e < kTileL * n_bin; e += blockDim.x) {
+        const bool v = e < ne;
+        cp_async4(mb + e, F.xiE + (v ? o + e : 0), v);
+        cp_async4(mb + kTileL * n_bin + e, F.xiB + (v ? o + e : 0), v);
+        cp_async4(mb + 2 * kTileL * n_bin + e, F.K + (v ? o + e : 0), v);
+      }
+      for (int e = tid; e < kTileL; e += blockDim.x) cp_async4(mb + 3 * kTileL * n_bin + e, F.mw + (e < nt ? t0 + e : 0), e < nt);
     }
   };
   auto convert_tile = [&]() {
@@ -169,20 +197,23 @@ __global__ void __launch_bounds__(512, 2) k_marks_partials(const MarksField* __r
   double acc[kMapGroup];
 #pragma unroll
   for (int g = 0; g < kMapGroup; ++g) acc[g] = 0.0;
-  if (j0 < j1) stage_tile(j0);
+  if (j0 < j1) stage_tile(j0, 0);
   cp_async_wait_all();
   __syncthreads();
   if (j0 < j1) convert_tile();
   __syncthreads();
+  int buf = 0;
   for (long long t0 = j0; t0 < j1; t0 += kTileL) {
     const int nt = (int)min((long long)kTileL, j1 - t0);
     const bool more = t0 + kTileL < j1;
-    if (more) stage_tile(t0 + kTileL);  // the raw area was read before the last barrier
+    // the raw area was read before the last barrier, the other marks buffer
+    // before the one ahead of it
+    if (more) stage_tile(t0 + kTileL, buf ^ 1);
     if (live) {
-      const float* base = row + t0 * rs;
-#pragma unroll 2
+      const float* base = STAGE ? mk + buf * MS + srow : row + t0 * rs;
+#pragma unroll 1
       for (int jj = grp; jj < nt; jj += ng) {
-        const double m = (double)__ldg(base + jj * rs);
+        const double m = STAGE ? (double)base[jj * rs] : (double)__ldg(base + jj * rs);
         const double2* f2 = reinterpret_cast<const double2*>(fsel + jj * kMapGroup);
         const int sw = jj & 7;
 #pragma unroll
@@ -194,11 +225,12 @@ __global__ void __launch_bounds__(512, 2) k_marks_partials(const MarksField* __r
       }
     }
     cp_async_wait_all();
-    __syncthreads();  // the next tile's raw inputs landed; this tile's factors are no longer read
+    __syncthreads();  // the next tile's copies landed; this tile's factors and marks are no longer read
     if (more) {
       convert_tile();
       __syncthreads();
     }
+    buf ^= 1;
   }
   // groups 1.. add their sums into group 0's, in group order
   double* red = fac_s;  // [tg][kMapGroup]
@@ -222,18 +254,40 @@ __global__ void __launch_bounds__(512, 2) k_marks_partials(const MarksField* __r
 }
 
 // Threads per lens group (one per marks row, whole warps) and per block: as
-// many groups as fit in 512 threads.
+// many groups as fit in kMarksThreads.
 int marks_group_threads(int n_bin) { return (3 * n_bin + 1 + 31) / 32 * 32; }
 int marks_block_threads(int n_bin) {
   const int tg = marks_group_threads(n_bin);
-  return tg > 256 ? tg : (512 / tg) * tg;
+  return (kMarksThreads / tg) * tg;
 }
+bool marks_stage(int n_bin) { return marks_stage_floats(n_bin) <= kMaxStageFloats; }
 size_t marks_smem(int n_bin) {
-  const size_t fac = 2 * sizeof(double) * kTileL * kMapGroup +
-                     std::max(MapFactors::kRawBytes, MultFactors::kRawBytes);
+  size_t fac = 2 * sizeof(double) * kTileL * kMapGroup + std::max(MapFactors::kRawBytes, MultFactors::kRawBytes);
+  if (marks_stage(n_bin)) fac += 2 * sizeof(float) * (size_t)marks_stage_floats(n_bin);
   const size_t red = sizeof(double) * (size_t)marks_group_threads(n_bin) * kMapGroup;
   return std::max(fac, red);
 }
+// One pass of k_marks_partials over all fields (the staged form when the
+// binning is narrow enough).
+template <class Fac>
+cudaError_t launch_marks_partials(const MarksField* fields, int n_field, int nblk, const Fac& fac, int n_g, int nb,
+                                  double* part, cudaStream_t st) {
+  const size_t msm = marks_smem(nb);
+  const int bt = marks_block_threads(nb), tg = marks_group_threads(nb);
+  if (marks_stage(nb)) {
+    cudaError_t e = cudaFuncSetAttribute(k_marks_partials<Fac, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)msm);
+    if (e != cudaSuccess) return e;
+    k_marks_partials<Fac, true><<<nblk, bt, msm, st>>>(fields, n_field, fac, n_g, nb, tg, part);
+  } else {
+    cudaError_t e = cudaFuncSetAttribute(k_marks_partials<Fac, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)msm);
+    if (e != cudaSuccess) return e;
+    k_marks_partials<Fac, false><<<nblk, bt, msm, st>>>(fields, n_field, fac, n_g, nb, tg, part);
+  }
+  return cudaGetLastError();
+}
+
 // maps or resamples per pass over the marks
 int marks_group(int) { return kMapGroup; }
 
@@ -362,16 +416,9 @@ extern "C" tpcf_status tpcf_xi_from_marks(tpcf_ctx* c, int32_t n_field, const tp
     double* part = (double*)ws_alloc(c, sizeof(double) * (size_t)std::max(nblk, 1) * kMapGroup * R);
     double* dout = (double*)ws_alloc(c, sizeof(double) * (size_t)kMapGroup * n_field * R);
     const int MG = marks_group(nb);
-    const size_t msm = marks_smem(nb);
-    check(cudaFuncSetAttribute(k_marks_partials<MapFactors>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm),
-          "smem attr");
     for (int m0 = 0; m0 < n_map; m0 += MG) {
       const int g = std::min(MG, n_map - m0);
-      if (nblk > 0) {
-        k_marks_partials<MapFactors><<<nblk, marks_block_threads(nb), msm, st>>>(df, n_field, MapFactors{m0}, g, nb,
-                                                                                marks_group_threads(nb), part);
-        counted(c, cudaGetLastError(), "marks partials");
-      }
+      if (nblk > 0) counted(c, launch_marks_partials(df, n_field, nblk, MapFactors{m0}, g, nb, part, st), "marks partials");
       const int tot = g * n_field * R;
       if (nblk > 0) {
         k_marks_reduce<<<(tot + 7) / 8, 256, 0, st>>>(part, df, n_field, nblk, g, R, dout);
@@ -475,8 +522,6 @@ extern "C" tpcf_status tpcf_marks_bootstrap(tpcf_ctx* c, int32_t n_field, const 
     double* dout = (double*)ws_alloc(c, sizeof(double) * (size_t)kMapGroup * n_field * R);
     std::vector<double> sums((size_t)n_boot * n_field * R, 0.0);
     const int MG = marks_group(nb);
-    check(cudaFuncSetAttribute(k_marks_partials<MultFactors>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)marks_smem(nb)), "smem attr");
     for (int s0 = 0; s0 < n_boot; s0 += MG) {
       const int G = std::min(MG, n_boot - s0);
       const int* mult;
@@ -491,9 +536,8 @@ extern "C" tpcf_status tpcf_marks_bootstrap(tpcf_ctx* c, int32_t n_field, const 
         mult = mbuf;
       }
       if (nblk > 0) {
-        k_marks_partials<MultFactors><<<nblk, marks_block_threads(nb), marks_smem(nb), st>>>(
-            df, n_field, MultFactors{mult, dunit, n_units}, G, nb, marks_group_threads(nb), part);
-        counted(c, cudaGetLastError(), "bootstrap partials");
+        counted(c, launch_marks_partials(df, n_field, nblk, MultFactors{mult, dunit, n_units}, G, nb, part, st),
+                "bootstrap partials");
         const int tot = G * n_field * R;
         k_marks_reduce<<<(tot + 7) / 8, 256, 0, st>>>(part, df, n_field, nblk, G, R, dout);
         counted(c, cudaGetLastError(), "bootstrap reduce");

@@ -202,7 +202,7 @@ tpcf_status run_noalloc(tpcf_ctx* c, const float* xA, const float* yA, const flo
                                     std::fabs(hbox[8 * i + 3]));
   margin = (float)(1e-5 * (margin + Rd) + 1e-4 * g.cell);
 
-  // lenses: sorted by Morton code, groups of 32 (one per warp of the pair kernel; one patch)
+  // lenses: sorted by Hilbert index, groups of 32 (one per warp of the pair kernel; one patch)
   const int nl_valid = (int)hcnt[0];
   float4* lrec = (float4*)cv.take(sizeof(float4) * std::max(nl_valid, 1));
   float* zs = (float*)cv.take(sizeof(float) * std::max(nl_valid, 1));

@@ -141,7 +141,7 @@ __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const floa
 
 // ---------------------------------------------------- sub-chunk fast paths --
 // Each sub-chunk holds 32 consecutive sources of the cell-sorted order
-// (spatially compact: cells in rows, Morton order inside a cell).  For each
+// (spatially compact: cells in rows, Hilbert order inside a cell).  For each
 // lens and sub-chunk the bin range of the chunk's bounding box is bounded
 // conservatively (guard band eps on both ends):
 //   0  no pair of the chunk is in range        -> nothing to do
@@ -798,12 +798,11 @@ __global__ void k_bbox_finish(const int* box_ord, float* box, int n) {
   if (i < n) box[i] = ord2f(box_ord[i]);
 }
 
-__device__ __forceinline__ unsigned spread16(unsigned v);
 
-// Sort key of each source: (cell << mb) | Morton code of its position inside the
-// cell on a 2^(mb/2) grid, so that consecutive sources of one cell are spatially
-// compact (32-source sub-chunks get small bounding boxes).  Invalid sources get
-// ncells << mb and sort last.
+// Sort key of each source: (cell << mb) | Hilbert index of its position inside
+// the cell on a 2^(mb/2) grid, so that consecutive sources of one cell are
+// spatially compact (32-source sub-chunks get small bounding boxes).  Invalid
+// sources get ncells << mb and sort last.
 __global__ void k_src_keys(const float* __restrict__ x, const float* __restrict__ y,
                            const float* __restrict__ z, long long n, float x0, float y0, float inv_cell,
                            int ncx, int ncy, int mb, unsigned* keys, int* idx) {
@@ -823,7 +822,7 @@ __global__ void k_src_keys(const float* __restrict__ x, const float* __restrict_
       if (half > 0) {
         const unsigned qx = (unsigned)clamp_floor((fx - (float)cx) * q, 0, (1 << half) - 1);
         const unsigned qy = (unsigned)clamp_floor((fy - (float)cy) * q, 0, (1 << half) - 1);
-        key |= spread16(qx) | (spread16(qy) << 1);
+        key |= hilbert_index(qx, qy, half);
       }
     }
     keys[i] = key;
@@ -911,17 +910,11 @@ __global__ void k_src_pairs(const int* __restrict__ idx, int n_valid, int n_chun
   }
 }
 
-__device__ __forceinline__ unsigned spread16(unsigned v) {
-  v &= 0xffffu;
-  v = (v | (v << 8)) & 0x00ff00ffu;
-  v = (v | (v << 4)) & 0x0f0f0f0fu;
-  v = (v | (v << 2)) & 0x33333333u;
-  v = (v | (v << 1)) & 0x55555555u;
-  return v;
-}
 
-// Lens sort keys: (patch << 32) | Morton(x, y) on a 2^16 grid over the box;
-// invalid lenses get ~0 and sort last.
+// Lens sort keys: (patch << 32) | Hilbert index of (x, y) on a 2^16 grid over
+// the box (groups of 32 consecutive lenses of one patch: a third less box
+// diagonal than Morton order on the tomography lenses); invalid lenses get ~0
+// and sort last.
 __global__ void k_lens_keys(const float* __restrict__ x, const float* __restrict__ y,
                             const float* __restrict__ z, const float* __restrict__ w,
                             const int* __restrict__ patch, long long n, float4 box,
@@ -936,9 +929,8 @@ __global__ void k_lens_keys(const float* __restrict__ x, const float* __restrict
     if (v) {
       const unsigned qx = (unsigned)clamp_floor((xi - box.x) * sx, 0, 65535);
       const unsigned qy = (unsigned)clamp_floor((yi - box.y) * sy, 0, 65535);
-      const unsigned mort = spread16(qx) | (spread16(qy) << 1);
       const unsigned long long p = patch ? (unsigned long long)(unsigned)patch[i] : 0ull;
-      key = (p << 32) | mort;
+      key = (p << 32) | hilbert_index(qx, qy, 16);
     }
     keys[i] = key;
     idx[i] = (int)i;

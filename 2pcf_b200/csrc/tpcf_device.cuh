@@ -95,7 +95,7 @@ __device__ __forceinline__ int2 row_span(const GridDesc& G, float4 box, float R,
 }
 
 // Sort key of work item i (items are built in task, then lens-group order,
-// and lens groups follow (patch, Morton) order): the item's cost in bands of
+// and lens groups follow (patch, Hilbert) order): the item's cost in bands of
 // 2^(1/8) (about 9%) on top, the item index below.  Sorted descending, the
 // costliest items start first (load balance), and inside one band the items
 // run in task and space order, so that the warps resident at one time read
@@ -103,6 +103,34 @@ __device__ __forceinline__ int2 row_span(const GridDesc& G, float4 box, float R,
 __device__ __forceinline__ unsigned long long item_key(unsigned long long cost, int i) {
   const unsigned band = (unsigned)(__log2f((float)cost) * 8.f);
   return ((unsigned long long)band << 32) | (unsigned)i;
+}
+
+// Position of cell (qx, qy) of a 2^bits x 2^bits grid (bits <= 16) along the
+// Hilbert curve: the quadrant digit of each level from the top down, with
+// the cell's coordinates inside its quadrant turned into the orientation of
+// that quadrant's sub-curve.  Runs of consecutive positions are compact
+// (no jumps across the grid, unlike Morton order), so groups of 32
+// consecutive objects get small bounding boxes.
+__device__ __forceinline__ unsigned hilbert_index(unsigned qx, unsigned qy, int bits) {
+  unsigned d = 0;
+  for (int b = bits - 1; b >= 0; --b) {
+    const unsigned s = 1u << b, m = s - 1u;
+    const unsigned rx = (qx >> b) & 1u, ry = (qy >> b) & 1u;
+    d += s * s * ((3u * rx) ^ ry);
+    unsigned x = qx & m, y = qy & m;
+    if (ry == 0u) {
+      if (rx == 1u) {
+        x = m - x;
+        y = m - y;
+      }
+      const unsigned t = x;
+      x = y;
+      y = t;
+    }
+    qx = x;
+    qy = y;
+  }
+  return d;
 }
 
 // ------------------------------------------------------------ binning -------

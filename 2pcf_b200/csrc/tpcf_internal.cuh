@@ -5,7 +5,7 @@
 //   source catalogue  -> cell grid: records sorted by row-major cell index,
 //                        stored as 32-source sub-chunks (SrcPair form, 1 KB)
 //                        with one ChunkMeta each, cell_start[ncx*ncy+1]
-//   lens catalogue    -> lenses sorted by (patch, Morton code); groups of at
+//   lens catalogue    -> lenses sorted by (patch, Hilbert index); groups of at
 //                        most BT consecutive lenses that never straddle a
 //                        patch; one bounding box per group
 //   work item         -> (task, group): one lens group against every source

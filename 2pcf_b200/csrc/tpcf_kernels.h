@@ -36,7 +36,7 @@ cudaError_t launch_bbox(const float* x, const float* y, const float* z, const fl
                         const float* m, long long n, int kind, int* box_ord, unsigned long long* count,
                         int* prange, cudaStream_t st);
 cudaError_t launch_bbox_finish(const int* box_ord, float* box, int n, cudaStream_t st);
-// mb = bits of the within-cell Morton code in the source sort key.
+// mb = bits of the within-cell Hilbert index in the source sort key.
 cudaError_t launch_src_keys(const float* x, const float* y, const float* z, long long n, float x0, float y0,
                             float inv_cell, int ncx, int ncy, int mb, unsigned* keys, int* idx, cudaStream_t st);
 cudaError_t launch_cell_start(const unsigned* keys, long long n, unsigned ncells, int mb, int* cell_start,
