@@ -33,7 +33,7 @@ __all__ = [
     "partition_data_equal", "block_bootstrap", "TPCFError", "rotate_data_from_poles_and_meridian",
     "unit_vectors", "read_table", "load_standard_shape_catalog", "load_standard_kappa_map",
     "load_standard_lens_catalog", "write_result_table", "MarksField", "save_marks", "load_survey_marks",
-    "calculate_tpcf_from_marks", "marks_bootstrap",
+    "calculate_tpcf_from_marks", "marks_bootstrap", "BatchPlan",
 ]
 
 
@@ -450,6 +450,102 @@ def batch_shear_2pcf(lenses: Sequence[LensCatalog], shapes: Sequence[ShapeCatalo
                                        int(n_patch) if lens_patches is not None else 0, outs)
     _check(st, ctx.handle)
     return [_finish(r, nb) for r in pyouts]
+
+
+class BatchPlan:
+    """A prepared batch_shear_2pcf call (tpcf_plan_shear_scalar): the grids,
+    lens groups and sorted work items are built once; ``launch()`` enqueues
+    only the persistent pair kernel and the per-patch reductions on the plan's
+    stream (no host synchronisation or allocation, so it can be recorded into
+    a CUDA graph, see ``capture``), ``results()`` waits and returns the same
+    Shear2pcfResults list as batch_shear_2pcf (identical sums).  Device
+    inputs are used in place and are kept referenced by the plan."""
+
+    def __init__(self, lenses, shapes, tasks, bins, lens_patches=None, n_patch=0, lens_sums=False,
+                 ctx: Context = None, stream=None):
+        ctx = _resolve_ctx(ctx)
+        self._keep = []
+        lc = (LensCat * len(lenses))()
+        for i, L in enumerate(lenses):
+            arrs = [_Arr(a) for a in (L.x, L.y, L.z, L.val, L.w)]
+            p = _Arr(None if lens_patches is None else lens_patches[i], np.int32)
+            self._keep += arrs + [p]
+            lc[i] = LensCat(arrs[0].n, *[a.ptr for a in arrs], p.ptr)
+        sc = (ShearCat * len(shapes))()
+        for i, S in enumerate(shapes):
+            arrs = [_Arr(a) for a in (S.x, S.y, S.z, S.e1, S.e2, S.w, S.m)]
+            self._keep += arrs
+            sc[i] = ShearCat(arrs[0].n, *[a.ptr for a in arrs])
+        tl = np.ascontiguousarray([t[0] for t in tasks], np.int32)
+        ts = np.ascontiguousarray([t[1] for t in tasks], np.int32)
+        self.n_bin = bins.n_bin
+        self._n_lens = [lenses[t[0]].n for t in tasks]
+        self._lens_sums = lens_sums
+        self._n_patch = int(n_patch) if lens_patches is not None else 0
+        shape = (Result * len(tasks))()
+        for t in range(len(tasks)):
+            _, shape[t] = _alloc_result(self.n_bin, 1, False, bool(lens_sums), 0)
+        cb = bins.c_struct()
+        h = C.c_void_p()
+        st = lib().tpcf_plan_shear_scalar(ctx.handle, len(lenses), lc, len(shapes), sc, len(tasks),
+                                          tl.ctypes.data, ts.ctypes.data, C.byref(cb), self._n_patch, shape,
+                                          C.byref(h))
+        _check(st, ctx.handle)
+        self.handle = h
+        self.n_task = len(tasks)
+        if stream is not None:
+            self.set_stream(stream)
+
+    def _err(self, st):
+        if st != 0:
+            raise TPCFError(st, lib().tpcf_plan_last_error(self.handle).decode())
+
+    def set_stream(self, stream):
+        """Launch on this CUDA stream (a torch.cuda.Stream or a raw handle)."""
+        raw = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        self._err(lib().tpcf_plan_set_stream(self.handle, C.c_void_p(raw)))
+
+    def launch(self):
+        self._err(lib().tpcf_plan_launch(self.handle))
+
+    def capture(self):
+        """Records launch() into a torch.cuda.CUDAGraph on the current torch
+        stream (the plan launches on it) and returns the graph; graph.replay()
+        then re-runs the pair kernel and the reductions."""
+        import torch
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            self.set_stream(s)
+            self.launch()  # warm-up outside the graph
+            with torch.cuda.graph(g, stream=s):
+                self.launch()
+        torch.cuda.current_stream().wait_stream(s)
+        self.set_stream(torch.cuda.current_stream())
+        return g
+
+    def results(self):
+        nb = self.n_bin
+        outs = (Result * self.n_task)()
+        pyouts = []
+        for t in range(self.n_task):
+            r, cres = _alloc_result(nb, self._n_lens[t], False, self._lens_sums, self._n_patch)
+            outs[t] = cres
+            pyouts.append(r)
+        self._err(lib().tpcf_plan_results(self.handle, outs))
+        return [_finish(r, nb) for r in pyouts]
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().tpcf_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def batch_kappa_2pcf(lenses: Sequence[LensCatalog], kappas: Sequence[KappaMap], tasks: Sequence[tuple],

@@ -138,6 +138,13 @@ def lib():
          [C.POINTER(Bins), vp, i32, C.POINTER(Result)])
     _sig(L, "tpcf_batch_shear_scalar", st, [vp, i32, C.POINTER(LensCat), i32, C.POINTER(ShearCat),
                                             i32, vp, vp, C.POINTER(Bins), i32, C.POINTER(Result)])
+    _sig(L, "tpcf_plan_shear_scalar", st, [vp, i32, C.POINTER(LensCat), i32, C.POINTER(ShearCat),
+                                           i32, vp, vp, C.POINTER(Bins), i32, C.POINTER(Result), C.POINTER(vp)])
+    _sig(L, "tpcf_plan_launch", st, [vp])
+    _sig(L, "tpcf_plan_results", st, [vp, C.POINTER(Result)])
+    _sig(L, "tpcf_plan_set_stream", st, [vp, vp])
+    _sig(L, "tpcf_plan_last_error", C.c_char_p, [vp])
+    _sig(L, "tpcf_plan_destroy", st, [vp])
     _sig(L, "tpcf_shear_scalar_noalloc", st, [vp] + [vp] * 5 + [i64] + [vp] * 7 + [i64] +
          [C.POINTER(Bins), C.POINTER(Result)])
     _sig(L, "tpcf_shear_scalar_adjoint", st, [vp] + [vp] * 5 + [i64] + [vp] * 7 + [i64] +

@@ -872,6 +872,7 @@ tpcf_status run_adjoint_batch(tpcf_ctx* c, std::vector<AdjLensIn> lens, std::vec
     a.dsum = dsum[t];
     // item cost: the source groups play the lens-group role, the lens grid the source grid
     tdesc[t].lens_cat = si; tdesc[t].src_cat = li; tdesc[t].item_base = 0; tdesc[t].lens_acc_off = -1;
+    tdesc[t].margin = margin;
     if (hc[li] > 0)
       for (int g = 0; g < ngroups[si]; ++g) items.push_back(make_int2(t, g));
   }
@@ -899,7 +900,7 @@ tpcf_status run_adjoint_batch(tpcf_ctx* c, std::vector<AdjLensIn> lens, std::vec
     unsigned long long* ck1 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * n_items);
     int* o0 = (int*)ws_alloc(c, sizeof(int) * n_items);
     int* o1 = (int*)ws_alloc(c, sizeof(int) * n_items);
-    counted(c, launch_item_cost(items0, n_items, d_td, d_gd, d_lg, R, margin, ck0, o0, st), "item cost");
+    counted(c, launch_item_cost(items0, n_items, d_td, d_gd, d_lg, R, ck0, o0, st), "item cost");
     size_t tb = 0;
     check(sort_pairs_u64_desc(nullptr, tb, ck0, ck1, o0, o1, n_items, st), "sort size");
     void* tmp = ws_alloc(c, tb);

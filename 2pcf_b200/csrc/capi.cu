@@ -199,11 +199,33 @@ struct SrcBuilt {
   GridDesc g{};
 };
 
-// Everything one batched call needs; outs[t] receives task t.
-tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vector<SrcIn> srcs,
-                      const std::vector<int>& tl, const std::vector<int>& ts, const tpcf_bins* bins, int n_patch,
-                      tpcf_result* outs) {
-  auto t_start = std::chrono::steady_clock::now();
+// One prepared batch: every device buffer of the call (in the context's
+// workspace) and what the launch and the outputs need.  batch_setup builds
+// the grids, lens groups and the sorted work items; batch_launch enqueues the
+// pair kernel and the per-patch reductions (no host synchronisation, no
+// allocation); batch_finish writes the per-lens outputs, waits and forms the
+// totals and normalised outputs.
+struct Batch {
+  int mode = 0;
+  bool sph = false, sharded = false, use_patch_any = false, has_m = false, has_z = false, logb = false;
+  int nb = 0, n_patch = 0, n_patch_eff = 1, bt = 128, tch = 2, variant = 0, nT = 0;
+  std::vector<int> tl;
+  std::vector<int64_t> lens_n;  // input size of each lens catalogue
+  std::vector<LensBuilt> lb;
+  std::vector<TaskDesc> tdesc;
+  std::vector<char> want_lens;
+  int n_items = 0, grid = 0;
+  PairParams P{};
+  PairLaunch L{};
+  int* head = nullptr;  // [0] queue head, [1] error flags
+  double* item_sums = nullptr;
+  double* lens_acc = nullptr;
+  long long lens_acc_elems = 0;
+  std::vector<double*> dpatch;
+};
+
+void batch_setup(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vector<SrcIn> srcs, const std::vector<int>& tl,
+                 const std::vector<int>& ts, const tpcf_bins* bins, int n_patch, const tpcf_result* outs, Batch& B) {
   begin_call(c);
   cudaStream_t st = c->stream;
   const int nb = bins->n_bin;
@@ -380,30 +402,34 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     g.pairs = pairs;
     g.meta = cmeta;
   }
-  float margin = 0.f;
+  // FP32 guard on the reach of a task's rows and cells: the rounding scale of
+  // the coordinates its two catalogues hold, so that a task's tiles (and its
+  // sums, bit for bit) do not depend on the other tasks of a batch
+  std::vector<double> extent(ncat, 0.0);
   for (int i = 0; i < ncat; ++i) {
     const float* b = &hbox[8 * i];
     if (hcnt[i] == 0) continue;
-    margin = std::max(margin, std::fabs(b[0]) + std::fabs(b[1]) + std::fabs(b[2]) + std::fabs(b[3]));
+    extent[i] = std::fabs(b[0]) + std::fabs(b[1]) + std::fabs(b[2]) + std::fabs(b[3]);
+    if (sph) extent[i] = 2.0 * M_PI + M_PI;  // reduced longitudes and latitudes
   }
-  float maxcell = 0.f;
-  for (auto& g : grids) maxcell = std::max(maxcell, g.cell);
-  if (sph) margin = (float)(2.0 * M_PI + M_PI);  // reduced longitudes and latitudes
-  margin = (float)(1e-5 * (margin + Rd) + 1e-4 * maxcell);
+  auto task_margin = [&](int li, int si) {
+    return (float)(1e-5 * (std::max(extent[li], extent[nL + si]) + Rd) + 1e-4 * grids[si].cell);
+  };
 
   // ---- lens catalogues: sort by (patch, Hilbert index), groups of <= lens_group lenses
-  std::vector<LensBuilt> lb(nL);
+  std::vector<LensBuilt>& lb = B.lb;
+  lb.assign(nL, LensBuilt{});
   std::vector<LensDesc> ldesc(nL);
   for (int i = 0; i < nL; ++i) {
     const LensIn& l = lens[i];
-    LensBuilt& B = lb[i];
-    B.n_valid = (int)hcnt[i];
+    LensBuilt& LB = lb[i];
+    LB.n_valid = (int)hcnt[i];
     const float* b = &hbox[8 * i];
-    B.rec = (float4*)ws_alloc(c, sizeof(float4) * std::max(B.n_valid, 1));
-    B.zs = mode == 0 ? (float*)ws_alloc(c, sizeof(float) * std::max(B.n_valid, 1)) : nullptr;
-    B.perm = (int*)ws_alloc(c, sizeof(int) * std::max(B.n_valid, 1));
+    LB.rec = (float4*)ws_alloc(c, sizeof(float4) * std::max(LB.n_valid, 1));
+    LB.zs = mode == 0 ? (float*)ws_alloc(c, sizeof(float) * std::max(LB.n_valid, 1)) : nullptr;
+    LB.perm = (int*)ws_alloc(c, sizeof(int) * std::max(LB.n_valid, 1));
     std::vector<int> off(n_patch_eff + 1, 0);
-    if (l.n > 0 && B.n_valid > 0) {
+    if (l.n > 0 && LB.n_valid > 0) {
       unsigned long long* k0 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * l.n);
       unsigned long long* k1 = (unsigned long long*)ws_alloc(c, sizeof(unsigned long long) * l.n);
       int* i0 = (int*)ws_alloc(c, sizeof(int) * l.n);
@@ -414,61 +440,63 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
       check(sort_pairs_u64(nullptr, tb, k0, k1, i0, i1, (int)l.n, st), "sort size");
       void* tmp = ws_alloc(c, tb);
       check(sort_pairs_u64(tmp, tb, k0, k1, i0, i1, (int)l.n, st), "sort lenses");
-      counted(c, launch_lens_gather(i1, B.n_valid, l.x, l.y, l.z, l.val, l.w, B.rec, B.zs, B.perm, st), "lens gather");
+      counted(c, launch_lens_gather(i1, LB.n_valid, l.x, l.y, l.z, l.val, l.w, LB.rec, LB.zs, LB.perm, st), "lens gather");
       if (l.patch) {
         int* doff = (int*)ws_alloc(c, sizeof(int) * (n_patch_eff + 1));
-        counted(c, launch_patch_offsets(k1, B.n_valid, n_patch_eff, doff, st), "patch offsets");
+        counted(c, launch_patch_offsets(k1, LB.n_valid, n_patch_eff, doff, st), "patch offsets");
         check(cudaMemcpyAsync(off.data(), doff, sizeof(int) * (n_patch_eff + 1), cudaMemcpyDeviceToHost, st), "D2H off");
         check(cudaStreamSynchronize(st), "sync offsets");
       } else {
-        for (int p = 1; p <= n_patch_eff; ++p) off[p] = B.n_valid;
+        for (int p = 1; p <= n_patch_eff; ++p) off[p] = LB.n_valid;
       }
     }
     std::vector<int> gstart;
-    B.patch_groups.assign(n_patch_eff + 1, 0);
+    LB.patch_groups.assign(n_patch_eff + 1, 0);
     for (int p = 0; p < n_patch_eff; ++p) {
-      B.patch_groups[p] = (int)gstart.size();
+      LB.patch_groups[p] = (int)gstart.size();
       for (int s0 = off[p]; s0 < off[p + 1]; s0 += lens_group) gstart.push_back(s0);
     }
-    B.patch_groups[n_patch_eff] = (int)gstart.size();
-    B.n_groups = (int)gstart.size();
-    gstart.push_back(B.n_valid);
-    B.group_start = (int*)ws_alloc(c, sizeof(int) * gstart.size());
-    check(cudaMemcpyAsync(B.group_start, gstart.data(), sizeof(int) * gstart.size(), cudaMemcpyHostToDevice, st), "H2D groups");
-    B.d_patch_groups = (int*)ws_alloc(c, sizeof(int) * (n_patch_eff + 1));
-    check(cudaMemcpyAsync(B.d_patch_groups, B.patch_groups.data(), sizeof(int) * (n_patch_eff + 1),
+    LB.patch_groups[n_patch_eff] = (int)gstart.size();
+    LB.n_groups = (int)gstart.size();
+    gstart.push_back(LB.n_valid);
+    LB.group_start = (int*)ws_alloc(c, sizeof(int) * gstart.size());
+    check(cudaMemcpyAsync(LB.group_start, gstart.data(), sizeof(int) * gstart.size(), cudaMemcpyHostToDevice, st), "H2D groups");
+    LB.d_patch_groups = (int*)ws_alloc(c, sizeof(int) * (n_patch_eff + 1));
+    check(cudaMemcpyAsync(LB.d_patch_groups, LB.patch_groups.data(), sizeof(int) * (n_patch_eff + 1),
                           cudaMemcpyHostToDevice, st), "H2D patch groups");
     float4* pos = nullptr;
     if (sph) {
-      pos = (float4*)ws_alloc(c, sizeof(float4) * 2 * std::max(B.n_valid, 1));
-      if (B.n_valid > 0) counted(c, launch_lens_pos_sph(B.perm, B.n_valid, lamL[i], l.y, pos, st), "lens pos");
+      pos = (float4*)ws_alloc(c, sizeof(float4) * 2 * std::max(LB.n_valid, 1));
+      if (LB.n_valid > 0) counted(c, launch_lens_pos_sph(LB.perm, LB.n_valid, lamL[i], l.y, pos, st), "lens pos");
     }
-    B.group_box = (float4*)ws_alloc(c, sizeof(float4) * std::max(B.n_groups, 1));
-    counted(c, launch_group_box(B.rec, B.group_start, B.n_groups, B.group_box, st), "group box");
+    LB.group_box = (float4*)ws_alloc(c, sizeof(float4) * std::max(LB.n_groups, 1));
+    counted(c, launch_group_box(LB.rec, LB.group_start, LB.n_groups, LB.group_box, st), "group box");
     check(cudaStreamSynchronize(st), "sync groups");  // host vectors above must outlive the async copies
     LensDesc& d = ldesc[i];
-    d.rec = B.rec; d.z = B.zs; d.group_start = B.group_start; d.group_box = B.group_box;
-    d.n_valid = B.n_valid; d.n_groups = B.n_groups;
+    d.rec = LB.rec; d.z = LB.zs; d.group_start = LB.group_start; d.group_box = LB.group_box;
+    d.n_valid = LB.n_valid; d.n_groups = LB.n_groups;
     d.pos = pos;
   }
 
   // ---- tasks and work items
-  Phase ph_items("tpcf: work items + pair kernel");
-  std::vector<TaskDesc> tdesc(nT);
+  Phase ph_items("tpcf: work items");
+  std::vector<TaskDesc>& tdesc = B.tdesc;
+  tdesc.assign(nT, TaskDesc{});
   std::vector<int2> items;
-  std::vector<char> want_lens(nT, 0);
+  B.want_lens.assign(nT, 0);
   long long lens_acc_elems = 0;
   for (int t = 0; t < nT; ++t) {
     TaskDesc& d = tdesc[t];
     d.lens_cat = tl[t];
     d.src_cat = ts[t];
+    d.margin = task_margin(tl[t], ts[t]);
     d.item_base = (int)items.size();
     for (int g = 0; g < lb[tl[t]].n_groups; ++g) items.push_back(make_int2(t, g));
     const tpcf_result& o = outs[t];
-    want_lens[t] =
+    B.want_lens[t] =
         (o.xi_E_marks || o.xi_B_marks || o.K_marks || o.w_marks || o.marks_weight || o.lens_sums || o.lens_raw) ? 1 : 0;
     d.lens_acc_off = -1;
-    if (want_lens[t]) {
+    if (B.want_lens[t]) {
       d.lens_acc_off = lens_acc_elems;
       lens_acc_elems += (long long)kQ * nb * std::max(lb[tl[t]].n_valid, 1);
     }
@@ -490,10 +518,9 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
   for (int i = 0; i <= nb; ++i) e2f[i] = (float)e2[i];
   check(cudaMemcpyAsync(d_e2, e2.data(), sizeof(double) * (nb + 1), cudaMemcpyHostToDevice, st), "H2D edges");
   check(cudaMemcpyAsync(d_e2f, e2f.data(), sizeof(float) * (nb + 1), cudaMemcpyHostToDevice, st), "H2D edges f");
-  check(cudaMemsetAsync(head, 0, sizeof(int) * 4, st), "memset head");
 
   int2* d_items = (int2*)ws_alloc(c, sizeof(int2) * std::max(n_items, 1));
-  int grid = 0;
+  int n_run = 0;
   if (n_items > 0) {
     int2* d_items0 = (int2*)ws_alloc(c, sizeof(int2) * n_items);
     check(cudaMemcpyAsync(d_items0, items.data(), sizeof(int2) * n_items, cudaMemcpyHostToDevice, st), "H2D items");
@@ -502,10 +529,10 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     int* o0 = (int*)ws_alloc(c, sizeof(int) * n_items);
     int* o1 = (int*)ws_alloc(c, sizeof(int) * n_items);
     if (sph)
-      counted(c, launch_item_cost_sph(d_items0, n_items, d_tasks, d_lens, d_grids, R, margin, ck0, o0, st),
+      counted(c, launch_item_cost_sph(d_items0, n_items, d_tasks, d_lens, d_grids, R, ck0, o0, st),
               "item cost");
     else
-      counted(c, launch_item_cost(d_items0, n_items, d_tasks, d_lens, d_grids, R, margin, ck0, o0, st), "item cost");
+      counted(c, launch_item_cost(d_items0, n_items, d_tasks, d_lens, d_grids, R, ck0, o0, st), "item cost");
     size_t tb = 0;
     check(sort_pairs_u64_desc(nullptr, tb, ck0, ck1, o0, o1, n_items, st), "sort size");
     void* tmp = ws_alloc(c, tb);
@@ -513,72 +540,109 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     const int sc = c->opts.shard_count > 1 ? c->opts.shard_count : 1;
     const int si = sc > 1 ? c->opts.shard_index : 0;
     counted(c, launch_permute_items(d_items0, o1, n_items, si, sc, d_items, st), "permute items");
-    const int n_run = sc > 1 ? (n_items - si + sc - 1) / sc : n_items;
-    if (sc > 1) check(cudaMemsetAsync(item_sums, 0, sizeof(double) * kQ * nb * n_items, st), "memset items");
-    if (sc > 1 && lens_acc) check(cudaMemsetAsync(lens_acc, 0, sizeof(double) * lens_acc_elems, st), "memset lens");
+    n_run = sc > 1 ? (n_items - si + sc - 1) / sc : n_items;
+  }
+  PairParams& P = B.P;
+  P = PairParams{};
+  P.tasks = d_tasks; P.lenses = d_lens; P.grids = d_grids; P.items = d_items; P.n_items = n_run;
+  P.nb = nb; P.queue_head = head; P.item_sums = item_sums; P.lens_acc = lens_acc; P.err = err;
+  P.e2 = d_e2; P.e2f = d_e2f; P.R = R;
+  if (logb) {  // t = log2(theta^2) A + B (planar: theta^2 = d2)
+    const double l0 = std::log2(e[0] * e[0]), l1 = std::log2(e[nb] * e[nb]);
+    const double A = nb / (l1 - l0);
+    P.binA = (float)A;
+    P.binB = (float)(-l0 * A);
+    P.eps = 1.0f / 32768.0f;
+  } else {
+    P.binA = P.binB = 0.f;
+    P.eps = 4e-6f;
+  }
+  // FP32 histogram folded into FP64 every 4096 sources (each histogram cell
+  // then holds at most 128 register sums of 32 pairs): the per-bin sums of
+  // the call stay within 1e-6 of sum|terms|.  Per-lens outputs are sums of
+  // far fewer terms per cell, so their FP32 partials are folded every 1024
+  // sources (at 4096 one lens and bin of the 2 M x 0.5 M clustered
+  // workload reached 1.05e-6 of its sum|terms|)
+  P.flush_src = lens_acc ? 1024 : 4096;
+  P.debug_skip_tile = c->skip_tile + 1;
+  P.wait_limit = c->wait_limit;
+  const char* var_env = std::getenv("TPCF_PAIR_VARIANT");
+  B.variant = var_env ? std::atoi(var_env) : 0;
+  if (n_items > 0 && !sph)
+    counted(c, prepare_pairs(P, mode, has_m, has_z, logb, bt, tch, B.variant, c->num_sms, &B.L), "pair kernel");
 
-    PairParams P{};
-    P.tasks = d_tasks; P.lenses = d_lens; P.grids = d_grids; P.items = d_items; P.n_items = n_run;
-    P.nb = nb; P.queue_head = head; P.item_sums = item_sums; P.lens_acc = lens_acc; P.err = err;
-    P.e2 = d_e2; P.e2f = d_e2f; P.R = R; P.margin = margin;
-    if (logb) {  // t = log2(theta^2) A + B (planar: theta^2 = d2)
-      const double l0 = std::log2(e[0] * e[0]), l1 = std::log2(e[nb] * e[nb]);
-      const double A = nb / (l1 - l0);
-      P.binA = (float)A;
-      P.binB = (float)(-l0 * A);
-      P.eps = 1.0f / 32768.0f;
-    } else {
-      P.binA = P.binB = 0.f;
-      P.eps = 4e-6f;
+  B.mode = mode; B.sph = sph; B.sharded = sharded; B.use_patch_any = use_patch_any;
+  B.has_m = has_m; B.has_z = has_z; B.logb = logb;
+  B.nb = nb; B.n_patch = n_patch; B.n_patch_eff = n_patch_eff; B.bt = bt; B.tch = tch; B.nT = nT;
+  B.tl = tl;
+  B.lens_n.assign(nL, 0);
+  for (int i = 0; i < nL; ++i) B.lens_n[i] = lens[i].n;
+  B.n_items = n_items;
+  B.head = head;
+  B.item_sums = item_sums;
+  B.lens_acc = lens_acc;
+  B.lens_acc_elems = lens_acc_elems;
+  B.dpatch.assign(nT, nullptr);
+  for (int t = 0; t < nT; ++t) B.dpatch[t] = (double*)ws_alloc(c, sizeof(double) * kQ * nb * n_patch_eff);
+}
+
+// The pair kernel and the per-patch reductions of a prepared batch: device
+// work only, in stream order (a CUDA graph may record it).  The queue head and
+// the error flags are cleared first, so a batch may be launched again.
+void batch_launch(tpcf_ctx* c, Batch& B, bool timed) {
+  Phase ph("tpcf: pair kernel + patch reduction");
+  cudaStream_t st = c->stream;
+  const int nb = B.nb;
+  check(cudaMemsetAsync(B.head, 0, sizeof(int) * 4, st), "memset head");
+  if (B.n_items > 0) {
+    if (B.sharded) {
+      check(cudaMemsetAsync(B.item_sums, 0, sizeof(double) * kQ * nb * B.n_items, st), "memset items");
+      if (B.lens_acc) check(cudaMemsetAsync(B.lens_acc, 0, sizeof(double) * B.lens_acc_elems, st), "memset lens");
     }
-    // FP32 histogram folded into FP64 every 4096 sources (each histogram cell
-    // then holds at most 128 register sums of 32 pairs): the per-bin sums of
-    // the call stay within 1e-6 of sum|terms|.  Per-lens outputs are sums of
-    // far fewer terms per cell, so their FP32 partials are folded every 1024
-    // sources (at 4096 one lens and bin of the 2 M x 0.5 M clustered
-    // workload reached 1.05e-6 of its sum|terms|)
-    P.flush_src = lens_acc ? 1024 : 4096;
-    P.debug_skip_tile = c->skip_tile + 1;
-    P.wait_limit = c->wait_limit;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    if (c->time_pairs) {
+    if (timed) {
       check(cudaEventCreate(&ev0), "event");
       check(cudaEventCreate(&ev1), "event");
       check(cudaEventRecord(ev0, st), "event record");
     }
-    const char* var_env = std::getenv("TPCF_PAIR_VARIANT");
-    const int variant = var_env ? std::atoi(var_env) : 0;
-    if (sph)
-      counted(c, launch_pairs_sph(P, mode, has_m, has_z, logb, bt, c->num_sms, st, &grid), "pair kernel");
-    else
-      counted(c, launch_pairs(P, mode, has_m, has_z, logb, bt, tch, variant, c->num_sms, st, &grid), "pair kernel");
-    if (c->time_pairs) {
+    if (B.sph) {
+      counted(c, launch_pairs_sph(B.P, B.mode, B.has_m, B.has_z, B.logb, B.bt, c->num_sms, st, &B.grid),
+              "pair kernel");
+    } else {
+      B.grid = B.L.grid;
+      counted(c, launch_prepared(B.L, B.P, st), "pair kernel");
+    }
+    if (timed) {
       check(cudaEventRecord(ev1, st), "event record");
       c->pending_ev0 = ev0;
       c->pending_ev1 = ev1;
     }
   }
-  vlog(c, "mode=%d tasks=%d items=%d grid=%d bt=%d has_m=%d has_z=%d", mode, nT, n_items, grid, bt, (int)has_m,
-       (int)has_z);
-
-  // ---- per-patch sums and per-lens outputs
-  Phase ph_reduce("tpcf: patch reduction + outputs");
-  std::vector<std::vector<double>> hpatch(nT);
-  std::vector<double*> dpatch(nT);
-  for (int t = 0; t < nT; ++t) {
-    const LensBuilt& B = lb[tl[t]];
-    dpatch[t] = (double*)ws_alloc(c, sizeof(double) * kQ * nb * n_patch_eff);
-    if (n_items > 0 && B.n_groups > 0)
-      counted(c, launch_patch_reduce(item_sums, tdesc[t].item_base, B.d_patch_groups, n_patch_eff, nb, dpatch[t], st),
-              "patch reduce");
+  for (int t = 0; t < B.nT; ++t) {
+    const LensBuilt& LB = B.lb[B.tl[t]];
+    if (B.n_items > 0 && LB.n_groups > 0)
+      counted(c, launch_patch_reduce(B.item_sums, B.tdesc[t].item_base, LB.d_patch_groups, B.n_patch_eff, nb,
+                                     B.dpatch[t], st), "patch reduce");
     else
-      check(cudaMemsetAsync(dpatch[t], 0, sizeof(double) * kQ * nb * n_patch_eff, st), "memset patch");
+      check(cudaMemsetAsync(B.dpatch[t], 0, sizeof(double) * kQ * nb * B.n_patch_eff, st), "memset patch");
+  }
+}
+
+// Per-lens outputs, the wait for the launch, and the totals and normalised
+// outputs of every task (host, fixed order).
+void batch_finish(tpcf_ctx* c, Batch& B, const tpcf_bins* bins, tpcf_result* outs) {
+  Phase ph_reduce("tpcf: outputs");
+  cudaStream_t st = c->stream;
+  const int nb = B.nb, nT = B.nT, n_patch_eff = B.n_patch_eff, n_patch = B.n_patch;
+  std::vector<std::vector<double>> hpatch(nT);
+  for (int t = 0; t < nT; ++t) {
+    const LensBuilt& LB = B.lb[B.tl[t]];
     hpatch[t].resize((size_t)kQ * nb * n_patch_eff);
-    check(cudaMemcpyAsync(hpatch[t].data(), dpatch[t], sizeof(double) * kQ * nb * n_patch_eff,
+    check(cudaMemcpyAsync(hpatch[t].data(), B.dpatch[t], sizeof(double) * kQ * nb * n_patch_eff,
                           cudaMemcpyDeviceToHost, st), "D2H patch");
-    if (want_lens[t]) {
+    if (B.want_lens[t]) {
       const tpcf_result& o = outs[t];
-      const int64_t nA = lens[tl[t]].n;
+      const int64_t nA = B.lens_n[B.tl[t]];
       auto dev_out = [&](void* user, size_t bytes) -> void* {
         if (!user) return nullptr;
         void* d = is_device_ptr(user) ? user : ws_alloc(c, bytes);
@@ -596,9 +660,9 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
       const bool marks_all = xE && xB && Km && wm;
       if (!marks_all && (xE || xB || Km || wm))
         throw Failure(TPCF_ERR_INVALID_ARG, "xi_E_marks, xi_B_marks, K_marks and w_marks go together");
-      if (B.n_valid > 0 && n_items > 0)
-        counted(c, launch_lens_outputs(lens_acc + tdesc[t].lens_acc_off, B.rec, B.perm, B.n_valid, nb, xE, xB, Km,
-                                       wm, mw, ls, lr, st), "lens outputs");
+      if (LB.n_valid > 0 && B.n_items > 0 && B.lens_acc)
+        counted(c, launch_lens_outputs(B.lens_acc + B.tdesc[t].lens_acc_off, LB.rec, LB.perm, LB.n_valid, nb, xE,
+                                       xB, Km, wm, mw, ls, lr, st), "lens outputs");
       if (xE && xE != (void*)o.xi_E_marks) copy_out(c, o.xi_E_marks, xE, mb);
       if (xB && xB != (void*)o.xi_B_marks) copy_out(c, o.xi_B_marks, xB, mb);
       if (Km && Km != (void*)o.K_marks) copy_out(c, o.K_marks, Km, mb);
@@ -609,7 +673,7 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     }
   }
   unsigned herr = 0;
-  check(cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "D2H err");
+  check(cudaMemcpyAsync(&herr, B.head + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "D2H err");
   check(cudaStreamSynchronize(st), "sync results");
   if (herr & kErrTimeout) throw Failure(TPCF_ERR_TIMEOUT, "a bounded device wait timed out in the pair kernel");
   if (herr) throw Failure(TPCF_ERR_CUDA, "device error flags " + std::to_string(herr));
@@ -651,13 +715,13 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     copy_out(c, o.sum_K, sK.data(), sizeof(double) * nb);
     copy_out(c, o.n_pairs, np.data(), sizeof(int64_t) * nb);
     copy_out(c, o.theta, centers.data(), sizeof(float) * nb);
-    if (!sharded) {
+    if (!B.sharded) {
       copy_out(c, o.mean_theta, mt.data(), sizeof(float) * nb);
       copy_out(c, o.g_t, gt.data(), sizeof(float) * nb);
       copy_out(c, o.g_x, gx.data(), sizeof(float) * nb);
       copy_out(c, o.weights, ww.data(), sizeof(float) * nb);
     }
-    if (o.patch_sums && use_patch_any) {
+    if (o.patch_sums && B.use_patch_any) {
       std::vector<double> ps((size_t)n_patch * 6 * nb);
       for (int p = 0; p < n_patch; ++p)
         for (int r = 0; r < 6; ++r)
@@ -667,6 +731,19 @@ tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vect
     }
     check(cudaStreamSynchronize(st), "sync outputs");  // host staging vectors are freed at scope exit
   }
+}
+
+// Everything one batched call needs; outs[t] receives task t.
+tpcf_status run_batch(tpcf_ctx* c, int mode, std::vector<LensIn> lens, std::vector<SrcIn> srcs,
+                      const std::vector<int>& tl, const std::vector<int>& ts, const tpcf_bins* bins, int n_patch,
+                      tpcf_result* outs) {
+  auto t_start = std::chrono::steady_clock::now();
+  Batch B;
+  batch_setup(c, mode, std::move(lens), std::move(srcs), tl, ts, bins, n_patch, outs, B);
+  batch_launch(c, B, c->time_pairs);
+  vlog(c, "mode=%d tasks=%d items=%d grid=%d bt=%d has_m=%d has_z=%d", mode, B.nT, B.n_items, B.grid, B.bt,
+       (int)B.has_m, (int)B.has_z);
+  batch_finish(c, B, bins, outs);
   c->last_call_ms =
       std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
   vlog(c, "call %.3f ms, pairs %lld", c->last_call_ms, (long long)c->last_pairs);
@@ -938,6 +1015,114 @@ tpcf_status tpcf_batch_shear_scalar(tpcf_ctx* c, int32_t n_lens_cat, const tpcf_
   } catch (const Failure& f) {
     return fail(c, f);
   }
+}
+
+// ------------------------------------------------------------ plans --------
+// A prepared batched call: the grids, lens groups and sorted work items of
+// one tpcf_batch_shear_scalar call, built once and kept in the plan's own
+// workspace, so that the pair kernel and the per-patch reductions can be
+// enqueued again (and recorded into a CUDA graph) without host work.
+}  // extern "C"
+
+struct tpcf_plan {
+  tpcf_ctx* ctx = nullptr;  // the plan's own context; its stream is the caller's
+  Batch B;
+  tpcf_bins bins{};
+  std::vector<tpcf_result> shape;  // which outputs each task has (non-null fields)
+  size_t slot_mark = 0;            // workspace slots of the batch; later ones are the outputs' scratch
+};
+
+extern "C" {
+
+tpcf_status tpcf_plan_shear_scalar(tpcf_ctx* c, int32_t n_lens_cat, const tpcf_lens_catalog* lenses,
+                                   int32_t n_src_cat, const tpcf_shear_catalog* sources, int32_t n_task,
+                                   const int32_t* task_lens, const int32_t* task_src, const tpcf_bins* bins,
+                                   int32_t n_patch, const tpcf_result* outs, tpcf_plan** plan) {
+  if (!c || !bins || !outs || !plan || n_lens_cat < 1 || n_src_cat < 1 || n_task < 1 || !lenses || !sources ||
+      !task_lens || !task_src)
+    return TPCF_ERR_INVALID_ARG;
+  *plan = nullptr;
+  if (c->opts.spherical) {
+    c->err = "plans are planar";
+    return TPCF_ERR_NOT_SUPPORTED;
+  }
+  tpcf_ctx* pc = nullptr;
+  tpcf_status st = tpcf_create(&pc, c->device, &c->opts);
+  if (st != TPCF_OK) return st;
+  pc->stream = c->stream;
+  tpcf_plan* pl = new tpcf_plan();
+  pl->ctx = pc;
+  pl->bins = *bins;
+  pl->shape.assign(outs, outs + n_task);
+  try {
+    std::vector<LensIn> L;
+    for (int i = 0; i < n_lens_cat; ++i) {
+      const tpcf_lens_catalog& l = lenses[i];
+      L.push_back({l.n, l.x, l.y, l.z, l.val, l.w, l.patch});
+    }
+    std::vector<SrcIn> S;
+    for (int i = 0; i < n_src_cat; ++i) {
+      const tpcf_shear_catalog& s = sources[i];
+      S.push_back({s.n, s.x, s.y, s.z, s.e1, s.e2, s.w, s.m});
+    }
+    std::vector<int> tl(task_lens, task_lens + n_task), ts(task_src, task_src + n_task);
+    batch_setup(pc, 0, L, S, tl, ts, bins, n_patch, outs, pl->B);
+    check(cudaStreamSynchronize(pc->stream), "sync plan");
+    pl->slot_mark = pc->next_slot;
+  } catch (const Failure& f) {
+    c->err = f.msg;
+    tpcf_destroy(pc);
+    delete pl;
+    return f.status;
+  }
+  *plan = pl;
+  return TPCF_OK;
+}
+
+tpcf_status tpcf_plan_launch(tpcf_plan* pl) {
+  if (!pl) return TPCF_ERR_INVALID_ARG;
+  try {
+    batch_launch(pl->ctx, pl->B, false);
+  } catch (const Failure& f) {
+    return fail(pl->ctx, f);
+  }
+  return TPCF_OK;
+}
+
+tpcf_status tpcf_plan_results(tpcf_plan* pl, tpcf_result* outs) {
+  if (!pl || !outs) return TPCF_ERR_INVALID_ARG;
+  for (int t = 0; t < pl->B.nT; ++t) {  // the per-lens outputs must be the ones the plan was made for
+    const tpcf_result& a = pl->shape[t];
+    const tpcf_result& b = outs[t];
+    if (!a.xi_E_marks != !b.xi_E_marks || !a.xi_B_marks != !b.xi_B_marks || !a.K_marks != !b.K_marks ||
+        !a.w_marks != !b.w_marks || !a.marks_weight != !b.marks_weight || !a.lens_sums != !b.lens_sums ||
+        !a.lens_raw != !b.lens_raw) {
+      pl->ctx->err = "per-lens outputs differ from the plan's";
+      return TPCF_ERR_INVALID_ARG;
+    }
+  }
+  try {
+    pl->ctx->next_slot = pl->slot_mark;  // the outputs' staging reuses the same slots every time
+    batch_finish(pl->ctx, pl->B, &pl->bins, outs);
+  } catch (const Failure& f) {
+    return fail(pl->ctx, f);
+  }
+  return TPCF_OK;
+}
+
+tpcf_status tpcf_plan_set_stream(tpcf_plan* pl, void* stream) {
+  if (!pl) return TPCF_ERR_INVALID_ARG;
+  pl->ctx->stream = stream ? (cudaStream_t)stream : pl->ctx->own_stream;
+  return TPCF_OK;
+}
+
+const char* tpcf_plan_last_error(const tpcf_plan* pl) { return pl ? pl->ctx->err.c_str() : ""; }
+
+tpcf_status tpcf_plan_destroy(tpcf_plan* pl) {
+  if (!pl) return TPCF_OK;
+  tpcf_destroy(pl->ctx);
+  delete pl;
+  return TPCF_OK;
 }
 
 tpcf_status tpcf_batch_scalar_scalar(tpcf_ctx* c, int32_t n_lens_cat, const tpcf_lens_catalog* lenses,

@@ -234,7 +234,27 @@ __global__ void __launch_bounds__(1024) k_km_sweep_eq(const float* __restrict__ 
     W[j] = wfix[j];
   }
   unsigned long long re = 0;
+  // this thread's point of the next chunk, loaded while the current one is
+  // assigned (a point's label is written only by its own thread)
+  float nx = 0.f, ny = 0.f, nw = 0.f;
+  int nl = -1;
+  const bool lane_in = (int)threadIdx.x < chunk;
+  if (lane_in && (long long)threadIdx.x < n) {
+    nx = x[threadIdx.x];
+    ny = y[threadIdx.x];
+    nw = w[threadIdx.x];
+    nl = labels[threadIdx.x];
+  }
   for (long long base = 0; base < n; base += chunk) {
+    const float xi = nx, yi = ny, wi = nw;
+    const int old = nl;
+    const long long inext = base + chunk + threadIdx.x;
+    if (lane_in && inext < n) {
+      nx = x[inext];
+      ny = y[inext];
+      nw = w[inext];
+      nl = labels[inext];
+    }
     __syncthreads();
     for (int j = threadIdx.x; j < k; j += blockDim.x) {
       // 1 + (W_j / W_mean - 1) * s in FP32 as written (kmeans.f90:174)
@@ -244,12 +264,20 @@ __global__ void __launch_bounds__(1024) k_km_sweep_eq(const float* __restrict__ 
     __syncthreads();
     const long long i = base + threadIdx.x;
     if (threadIdx.x < chunk && i < n) {
-      const float xi = x[i], yi = y[i];
       float best = min_init, cm = 0.f;
       int bi = -1, ci = -1;
+      // A cluster can change the outcome only if its scaled distance d is
+      // below T = max(best, cm * best) (candidates) or best.  The exact d
+      // (correctly rounded sqrt, as the reference) is formed only when
+      // f^2 (dx^2 + dy^2) <= T^2 (1 + 1e-5): outside that margin d > T for
+      // certain, whatever the FP32 roundings, so the labels do not change.
+      float tsq = __fmul_rn(min_init, min_init) * 1.00001f;
       for (int j = 0; j < k; ++j) {
         const float dx = __fsub_rn(xi, c[j].x), dy = __fsub_rn(yi, c[j].y);
-        const float d = __fmul_rn(f[j], __fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy))));
+        const float q = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+        const float fj = f[j];
+        if (fj > 0.f && fj * fj * q > tsq) continue;  // (f <= 0 gives d <= 0: always formed)
+        const float d = __fmul_rn(fj, __fsqrt_rn(q));
         if (candidates && d > 0.0f) {
           if (d < best) {
             cm = __fdiv_rn(best, d);
@@ -259,21 +287,26 @@ __global__ void __launch_bounds__(1024) k_km_sweep_eq(const float* __restrict__ 
           } else if (d < __fmul_rn(cm, best)) {
             cm = __fdiv_rn(d, best);
             ci = j;
+          } else {
+            continue;
           }
         } else if (d < best) {
           best = d;
           bi = j;
+        } else {
+          continue;
         }
+        const float t = candidates ? fmaxf(best, __fmul_rn(cm, best)) : best;
+        tsq = __fmul_rn(t, t) * 1.00001f;
       }
       if (candidates) {
         cand[i] = ci;
         memb[i] = cm;
       }
-      const int old = labels[i];
       if (bi != old) {
         labels[i] = bi;
         ++re;
-        const long long wf = __double2ll_rn(ldexp((double)w[i], sw));
+        const long long wf = __double2ll_rn(ldexp((double)wi, sw));
         if (old >= 0) atomicAdd((unsigned long long*)&W[old], (unsigned long long)(-wf));
         if (bi >= 0) atomicAdd((unsigned long long*)&W[bi], (unsigned long long)wf);
       }

@@ -240,7 +240,7 @@ tpcf_status run_noalloc(tpcf_ctx* c, const float* xA, const float* yA, const flo
   counted(c, cudaGetLastError(), "groups");
   counted(c, launch_group_box(lrec, gstart, n_groups, gbox, st), "group box");
   TaskDesc td{};
-  td.lens_cat = 0; td.src_cat = 0; td.item_base = 0; td.lens_acc_off = -1;
+  td.lens_cat = 0; td.src_cat = 0; td.item_base = 0; td.lens_acc_off = -1; td.margin = margin;
   LensDesc ld{};
   ld.rec = lrec; ld.z = zs; ld.group_start = gstart; ld.group_box = gbox; ld.n_valid = nl_valid;
   ld.n_groups = n_groups;
@@ -256,7 +256,7 @@ tpcf_status run_noalloc(tpcf_ctx* c, const float* xA, const float* yA, const flo
     PairParams P{};
     P.tasks = d_task; P.lenses = d_lens; P.grids = d_grid; P.items = items; P.n_items = n_groups;
     P.nb = nb; P.queue_head = head; P.item_sums = item_sums; P.lens_acc = nullptr; P.err = err;
-    P.e2 = d_e2; P.e2f = d_e2f; P.R = R; P.margin = margin;
+    P.e2 = d_e2; P.e2f = d_e2f; P.R = R;
     if (logb) {
       const double l0 = std::log2(e2[0]), l1 = std::log2(e2[nb]);
       const double A = nb / (l1 - l0);

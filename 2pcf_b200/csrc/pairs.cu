@@ -572,13 +572,13 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
     int since_flush = 0;
     const float4 box = LD.group_box[g];
     int cy0, cy1;
-    row_range(G, box, P.R, P.margin, cy0, cy1);
+    row_range(G, box, P.R, T.margin, cy0, cy1);
 
     for (int c0 = cy0; c0 <= cy1 && !aborted; c0 += kRowsPerPass) {
       const int nr = min(kRowsPerPass, cy1 - c0 + 1);
       int s0 = 0, s1 = 0;
       if (lane < nr) {
-        const int2 sp = row_span(G, box, P.R, P.margin, c0 + lane);
+        const int2 sp = row_span(G, box, P.R, T.margin, c0 + lane);
         s0 = sp.x;
         s1 = sp.y > sp.x ? sp.y : sp.x;
       }
@@ -987,7 +987,7 @@ __global__ void k_group_box(const float4* __restrict__ rec, const int* __restric
 // descending sort (longest items first).
 __global__ void k_item_cost(const int2* __restrict__ items, int n_items, const TaskDesc* __restrict__ tasks,
                             const LensDesc* __restrict__ lenses, const GridDesc* __restrict__ grids, float R,
-                            float margin, unsigned long long* cost, int* order) {
+                            unsigned long long* cost, int* order) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_items) return;
   const int2 it = items[i];
@@ -996,10 +996,10 @@ __global__ void k_item_cost(const int2* __restrict__ items, int n_items, const T
   const GridDesc G = grids[T.src_cat];
   const float4 box = L.group_box[it.y];
   int cy0, cy1;
-  row_range(G, box, R, margin, cy0, cy1);
+  row_range(G, box, R, T.margin, cy0, cy1);
   unsigned long long s = 0;
   for (int cy = cy0; cy <= cy1; ++cy) {
-    const int2 sp = row_span(G, box, R, margin, cy);
+    const int2 sp = row_span(G, box, R, T.margin, cy);
     if (sp.y > sp.x) s += (unsigned long long)(sp.y - sp.x);
   }
   const unsigned long long nl = (unsigned long long)(L.group_start[it.y + 1] - L.group_start[it.y]);
@@ -1124,8 +1124,12 @@ __global__ void k_lens_outputs(const double* __restrict__ acc, const float4* __r
 }
 
 // --------------------------------------------------------- host launchers --
+// prepare_*: sets the kernel's shared-memory attribute and sizes its grid
+// (persistent: the occupancy times the SM count, at most one warp per work
+// item); the launch itself is a plain cudaLaunchKernel of the result, so that
+// a prepared launch can be recorded into a CUDA graph.
 template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB, int BT, int TCH, int PATH>
-static cudaError_t launch_pairs_t(const PairParams& P, int num_sms, cudaStream_t st, int* grid_out) {
+static cudaError_t prepare_pairs_t(const PairParams& P, int num_sms, PairLaunch* L) {
   constexpr int QA = (MODE == 0 && HAS_M) ? 6 : 5;
   const size_t smem = pair_smem_layout(P.nb, QA, BT, TCH).total;
   auto kern = k_pairs<MODE, HAS_M, HAS_Z, LOGB, BT, TCH, PATH>;
@@ -1139,9 +1143,11 @@ static cudaError_t launch_pairs_t(const PairParams& P, int num_sms, cudaStream_t
   const int need = (P.n_items + BT / 32 - 1) / (BT / 32);  // each warp takes items of its own
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
-  *grid_out = grid;
-  kern<<<grid, BT, smem, st>>>(P);
-  return cudaGetLastError();
+  L->func = reinterpret_cast<const void*>(kern);
+  L->grid = grid;
+  L->block = BT;
+  L->smem = smem;
+  return cudaSuccess;
 }
 
 // Tile shapes: bt threads per block (128, 64 or 32; each warp takes 32-lens
@@ -1149,36 +1155,49 @@ static cudaError_t launch_pairs_t(const PairParams& P, int num_sms, cudaStream_t
 // buffers per warp; 1: four 1.1 KB buffers).  variant 1 forces per-pair binning
 // (A/B measurement).
 template <int MODE, bool HAS_M, bool HAS_Z, bool LOGB>
-static cudaError_t launch_pairs_bt(const PairParams& P, int bt, int tch, int variant, int num_sms, cudaStream_t st,
-                                   int* grid) {
+static cudaError_t prepare_pairs_bt(const PairParams& P, int bt, int tch, int variant, int num_sms, PairLaunch* L) {
   if (bt == 128) {
     if (variant == 1 && MODE == 0 && !HAS_M && !HAS_Z && LOGB)
-      return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 2, 1>(P, num_sms, st, grid);
-    if (tch == 1) return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 1, 0>(P, num_sms, st, grid);
-    return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 2, 0>(P, num_sms, st, grid);
+      return prepare_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 2, 1>(P, num_sms, L);
+    if (tch == 1) return prepare_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 1, 0>(P, num_sms, L);
+    return prepare_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 128, 2, 0>(P, num_sms, L);
   }
-  if (bt == 64) return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64, 2, 0>(P, num_sms, st, grid);
-  return launch_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 32, 2, 0>(P, num_sms, st, grid);
+  if (bt == 64) return prepare_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 64, 2, 0>(P, num_sms, L);
+  return prepare_pairs_t<MODE, HAS_M, HAS_Z, LOGB, 32, 2, 0>(P, num_sms, L);
 }
 
 size_t pair_smem_bytes(int nb, int qa, int bt, int tch) { return pair_smem_layout(nb, qa, bt, tch).total; }
 
-cudaError_t launch_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int tch,
-                         int variant, int num_sms, cudaStream_t st, int* grid) {
+cudaError_t prepare_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int tch,
+                          int variant, int num_sms, PairLaunch* L) {
   if (mode == 1) {
-    return logb ? launch_pairs_bt<1, false, false, true>(P, bt, tch, variant, num_sms, st, grid)
-                : launch_pairs_bt<1, false, false, false>(P, bt, tch, variant, num_sms, st, grid);
+    return logb ? prepare_pairs_bt<1, false, false, true>(P, bt, tch, variant, num_sms, L)
+                : prepare_pairs_bt<1, false, false, false>(P, bt, tch, variant, num_sms, L);
   }
   if (has_m) {
-    if (has_z) return logb ? launch_pairs_bt<0, true, true, true>(P, bt, tch, variant, num_sms, st, grid)
-                           : launch_pairs_bt<0, true, true, false>(P, bt, tch, variant, num_sms, st, grid);
-    return logb ? launch_pairs_bt<0, true, false, true>(P, bt, tch, variant, num_sms, st, grid)
-                : launch_pairs_bt<0, true, false, false>(P, bt, tch, variant, num_sms, st, grid);
+    if (has_z) return logb ? prepare_pairs_bt<0, true, true, true>(P, bt, tch, variant, num_sms, L)
+                           : prepare_pairs_bt<0, true, true, false>(P, bt, tch, variant, num_sms, L);
+    return logb ? prepare_pairs_bt<0, true, false, true>(P, bt, tch, variant, num_sms, L)
+                : prepare_pairs_bt<0, true, false, false>(P, bt, tch, variant, num_sms, L);
   }
-  if (has_z) return logb ? launch_pairs_bt<0, false, true, true>(P, bt, tch, variant, num_sms, st, grid)
-                         : launch_pairs_bt<0, false, true, false>(P, bt, tch, variant, num_sms, st, grid);
-  return logb ? launch_pairs_bt<0, false, false, true>(P, bt, tch, variant, num_sms, st, grid)
-              : launch_pairs_bt<0, false, false, false>(P, bt, tch, variant, num_sms, st, grid);
+  if (has_z) return logb ? prepare_pairs_bt<0, false, true, true>(P, bt, tch, variant, num_sms, L)
+                         : prepare_pairs_bt<0, false, true, false>(P, bt, tch, variant, num_sms, L);
+  return logb ? prepare_pairs_bt<0, false, false, true>(P, bt, tch, variant, num_sms, L)
+              : prepare_pairs_bt<0, false, false, false>(P, bt, tch, variant, num_sms, L);
+}
+
+cudaError_t launch_prepared(const PairLaunch& L, const PairParams& P, cudaStream_t st) {
+  void* args[] = {const_cast<PairParams*>(&P)};
+  return cudaLaunchKernel(L.func, dim3((unsigned)L.grid), dim3((unsigned)L.block), args, L.smem, st);
+}
+
+cudaError_t launch_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int tch,
+                         int variant, int num_sms, cudaStream_t st, int* grid) {
+  PairLaunch L;
+  cudaError_t e = prepare_pairs(P, mode, has_m, has_z, logb, bt, tch, variant, num_sms, &L);
+  if (e != cudaSuccess) return e;
+  *grid = L.grid;
+  return launch_prepared(L, P, st);
 }
 
 static inline unsigned gdim(long long n, int b) {
@@ -1240,10 +1259,10 @@ cudaError_t launch_group_box(const float4* rec, const int* gstart, int n_groups,
   return cudaGetLastError();
 }
 cudaError_t launch_item_cost(const int2* items, int n_items, const TaskDesc* tasks, const LensDesc* lenses,
-                             const GridDesc* grids, float R, float margin, unsigned long long* cost, int* order,
+                             const GridDesc* grids, float R, unsigned long long* cost, int* order,
                              cudaStream_t st) {
   if (n_items > 0)
-    k_item_cost<<<(n_items + 127) / 128, 128, 0, st>>>(items, n_items, tasks, lenses, grids, R, margin, cost, order);
+    k_item_cost<<<(n_items + 127) / 128, 128, 0, st>>>(items, n_items, tasks, lenses, grids, R, cost, order);
   return cudaGetLastError();
 }
 cudaError_t launch_permute_items(const int2* items, const int* order, int n, int index, int count, int2* out,

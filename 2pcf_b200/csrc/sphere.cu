@@ -593,10 +593,10 @@ __global__ void __launch_bounds__(BT, 3) k_pairs_sph(const PairParams P) {
     int since_flush = 0;
     const float4 box = LD.group_box[g];
     int cy0, cy1;
-    row_range(G, box, P.R, P.margin, cy0, cy1);
+    row_range(G, box, P.R, T.margin, cy0, cy1);
     float dl;
     bool full;
-    sph_reach(G, box, P.R, P.margin, dl, full);
+    sph_reach(G, box, P.R, T.margin, dl, full);
 
     for (int c0 = cy0; c0 <= cy1; c0 += kRowsS) {
       const int nr = min(kRowsS, cy1 - c0 + 1);
@@ -604,7 +604,7 @@ __global__ void __launch_bounds__(BT, 3) k_pairs_sph(const PairParams P) {
       __syncthreads();
       for (int r = tid; r < nr; r += BT) {
         int2 sp[3];
-        const int k = sph_row_spans(G, box, P.R, P.margin, c0 + r, dl, full, sp);
+        const int k = sph_row_spans(G, box, P.R, T.margin, c0 + r, dl, full, sp);
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
           const int2 v = j < k ? sp[j] : make_int2(0, 0);
@@ -820,7 +820,7 @@ __global__ void k_unit_vectors(const float* __restrict__ lam, const float* __res
 
 __global__ void k_item_cost_sph(const int2* __restrict__ items, int n_items, const TaskDesc* __restrict__ tasks,
                                 const LensDesc* __restrict__ lenses, const GridDesc* __restrict__ grids, float R,
-                                float margin, unsigned long long* cost, int* order) {
+                                unsigned long long* cost, int* order) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n_items) return;
   const int2 it = items[i];
@@ -829,14 +829,14 @@ __global__ void k_item_cost_sph(const int2* __restrict__ items, int n_items, con
   const GridDesc G = grids[T.src_cat];
   const float4 box = L.group_box[it.y];
   int cy0, cy1;
-  row_range(G, box, R, margin, cy0, cy1);
+  row_range(G, box, R, T.margin, cy0, cy1);
   float dl;
   bool full;
-  sph_reach(G, box, R, margin, dl, full);
+  sph_reach(G, box, R, T.margin, dl, full);
   unsigned long long s = 0;
   for (int cy = cy0; cy <= cy1; ++cy) {
     int2 sp[3];
-    const int k = sph_row_spans(G, box, R, margin, cy, dl, full, sp);
+    const int k = sph_row_spans(G, box, R, T.margin, cy, dl, full, sp);
     for (int j = 0; j < k; ++j)
       if (sp[j].y > sp[j].x) s += (unsigned long long)(sp[j].y - sp[j].x);
   }
@@ -919,10 +919,10 @@ cudaError_t launch_unit_vectors(const float* lam, const float* phi, long long n,
   return cudaGetLastError();
 }
 cudaError_t launch_item_cost_sph(const int2* items, int n_items, const TaskDesc* tasks, const LensDesc* lenses,
-                                 const GridDesc* grids, float R, float margin, unsigned long long* cost, int* order,
+                                 const GridDesc* grids, float R, unsigned long long* cost, int* order,
                                  cudaStream_t st) {
   if (n_items > 0)
-    k_item_cost_sph<<<(n_items + 127) / 128, 128, 0, st>>>(items, n_items, tasks, lenses, grids, R, margin, cost,
+    k_item_cost_sph<<<(n_items + 127) / 128, 128, 0, st>>>(items, n_items, tasks, lenses, grids, R, cost,
                                                             order);
   return cudaGetLastError();
 }

@@ -104,7 +104,7 @@ struct TaskDesc {
   int lens_cat;
   int src_cat;
   int item_base;            // row of (task, group 0) in item_sums
-  int pad;
+  float margin;             // FP32 guard on the reach of this task's rows and cells
   long long lens_acc_off;   // element offset of this task's per-lens sums, -1 = none
 };
 
@@ -122,7 +122,6 @@ struct PairParams {
   const double* e2;         // canonical squared edges [nb+1]
   const float* e2f;         // FP32 squared edges [nb+1] (generic spacing)
   float R;                  // search radius: theta_max with a relative margin
-  float margin;             // absolute margin for cell-boundary rounding
   float binA, binB;         // log spacing: t = lg2(d2)*binA + binB
   float eps;                // guard band half-width in t units (log) or relative (generic)
   int flush_src;            // FP32 histogram -> FP64 after this many sources (0: 4096)

@@ -13,6 +13,17 @@ size_t pair_smem_bytes(int nb, int qa, int bt, int tch);
 // source tile; variant 1 bins every pair one by one (A/B measurement).
 cudaError_t launch_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int tch,
                          int variant, int num_sms, cudaStream_t st, int* grid);
+// The same in two steps: prepare_pairs picks the kernel instantiation, sets
+// its shared-memory attribute and sizes the grid; launch_prepared is one
+// cudaLaunchKernel (no other API call, so it may be recorded into a graph).
+struct PairLaunch {
+  const void* func = nullptr;
+  int grid = 0, block = 0;
+  size_t smem = 0;
+};
+cudaError_t prepare_pairs(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int tch,
+                          int variant, int num_sms, PairLaunch* L);
+cudaError_t launch_prepared(const PairLaunch& L, const PairParams& P, cudaStream_t st);
 
 // Spherical pair kernel (sphere.cu); P.grids[*].recs and P.lenses[*].pos set.
 cudaError_t launch_pairs_sph(const PairParams& P, int mode, bool has_m, bool has_z, bool logb, int bt, int num_sms,
@@ -26,7 +37,7 @@ cudaError_t launch_lens_pos_sph(const int* perm, int n_valid, const float* lam, 
 cudaError_t launch_unit_vectors(const float* lam, const float* phi, long long n, float* hi, float* lo,
                                 cudaStream_t st);
 cudaError_t launch_item_cost_sph(const int2* items, int n_items, const TaskDesc* tasks, const LensDesc* lenses,
-                                 const GridDesc* grids, float R, float margin, unsigned long long* cost, int* order,
+                                 const GridDesc* grids, float R, unsigned long long* cost, int* order,
                                  cudaStream_t st);
 
 cudaError_t launch_bbox_init(int* box_ord, unsigned long long* count, int* prange, int n, cudaStream_t st);
@@ -55,7 +66,7 @@ cudaError_t launch_patch_offsets(const unsigned long long* keys, int n_valid, in
                                  cudaStream_t st);
 cudaError_t launch_group_box(const float4* rec, const int* gstart, int n_groups, float4* box, cudaStream_t st);
 cudaError_t launch_item_cost(const int2* items, int n_items, const TaskDesc* tasks, const LensDesc* lenses,
-                             const GridDesc* grids, float R, float margin, unsigned long long* cost, int* order,
+                             const GridDesc* grids, float R, unsigned long long* cost, int* order,
                              cudaStream_t st);
 cudaError_t launch_permute_items(const int2* items, const int* order, int n, int index, int count, int2* out,
                                  cudaStream_t st);

@@ -38,7 +38,10 @@ sys.path.insert(0, ROOT)
 METRIC = "Gpairs/s for xi_t at 10M objects, plain vs batched+adjoint form at 1e-6 rel. error"
 UNIT = "Gpairs/s"
 FLOP_PER_PAIR = 26  # shear-scalar, FMA = 2, MUFU = 1 (per binned pair)
-K_PAIRS_DRAM_BYTES = 63.414e9 + 135.05e6  # read + written by one launch of the default workload (ncu, one pass)
+# DRAM bytes read + written by one pair-kernel launch of the default workload,
+# per grid cell side theta_max/D (one-pass ncu captures of
+# dram__bytes_read.sum + dram__bytes_write.sum)
+K_PAIRS_DRAM_BYTES = {24: 87.957e9 + 0.406e9}
 SPH_FLOP_PER_PAIR = 52  # spherical shear-scalar: hi/lo unit-vector differences, east/north projection, angle series
 WORKLOAD_DESC = ("tomography: 5 shear bins (0.2,0.5,1.0,1.9,4.0 M) x 5 scalar bins "
                  "(0.1,0.2,0.4,0.7,1.0 M) = 10.0 M objects, 25 cross-pairs in one launch, "
@@ -850,12 +853,13 @@ def main():
         adjoint = adjoint_timing(w, ctx, bins, pairs, pair_ms, stream, peak)
     fpp = SPH_FLOP_PER_PAIR if sphere else FLOP_PER_PAIR
     achieved = pairs * fpp / (pair_ms * 1e-3) / 1e12
-    # DRAM bytes of one pair-kernel launch of this exact workload, from one
-    # one-pass ncu capture of dram__bytes_read.sum + dram__bytes_write.sum;
-    # other configurations were not captured
-    default_cfg = not sphere and args.scale == 1.0 and args.region <= 0 and args.task < 0 and \
-        abs(ctx.cell_size - bins.x_max / 64) < 1e-6
-    traffic = K_PAIRS_DRAM_BYTES if default_cfg else None
+    # DRAM bytes of one pair-kernel launch of this exact workload at a captured
+    # cell side; other configurations were not captured
+    traffic = None
+    if not sphere and args.scale == 1.0 and args.region <= 0 and args.task < 0:
+        for d, byt in K_PAIRS_DRAM_BYTES.items():
+            if abs(ctx.cell_size - bins.x_max / d) < 1e-6:
+                traffic = byt
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -398,6 +398,39 @@ tpcf_status tpcf_batch_scalar_scalar(tpcf_ctx* ctx,
                                      const tpcf_bins* bins, int32_t n_patch,
                                      tpcf_result* outs);
 
+/* ------------------------------------------------------------ plans ------ */
+/* A prepared tpcf_batch_shear_scalar call (planar).  tpcf_plan_shear_scalar
+ * takes the same arguments and builds, once, everything that depends only on
+ * the catalogues' positions, weights and values as they are now: the source
+ * grids and sub-chunk records, the lens groups, the sorted work items.
+ * Device input arrays are used in place and must stay alive and unchanged
+ * while the plan exists.  `outs` only tells which per-lens outputs each task
+ * has (non-null fields; the pointers are not kept).
+ *
+ * tpcf_plan_launch enqueues the persistent pair kernel and the per-patch
+ * reductions on the plan's stream (the context's stream when the plan was
+ * made, or tpcf_plan_set_stream): no host synchronisation, no allocation and
+ * no other API call, so the sequence may be recorded into a CUDA graph
+ * (stream capture) and replayed.  tpcf_plan_results waits for the last launch
+ * and writes the outputs of every task, as tpcf_batch_shear_scalar would
+ * (same sums bit for bit); its outs must have the per-lens outputs the plan
+ * was made with.  The plan keeps its own device workspace; the context it was
+ * made from stays free for other calls.  Spherical contexts return
+ * TPCF_ERR_NOT_SUPPORTED. */
+typedef struct tpcf_plan tpcf_plan;
+tpcf_status tpcf_plan_shear_scalar(tpcf_ctx* ctx,
+                                   int32_t n_lens_cat, const tpcf_lens_catalog* lenses,
+                                   int32_t n_src_cat, const tpcf_shear_catalog* sources,
+                                   int32_t n_task, const int32_t* task_lens,
+                                   const int32_t* task_src,
+                                   const tpcf_bins* bins, int32_t n_patch,
+                                   const tpcf_result* outs, tpcf_plan** plan);
+tpcf_status tpcf_plan_launch(tpcf_plan* plan);
+tpcf_status tpcf_plan_results(tpcf_plan* plan, tpcf_result* outs);
+tpcf_status tpcf_plan_set_stream(tpcf_plan* plan, void* cuda_stream);
+const char* tpcf_plan_last_error(const tpcf_plan* plan);
+tpcf_status tpcf_plan_destroy(tpcf_plan* plan);
+
 /* ------------------------------------------------------------ gradients -- */
 /* No counterpart in the reference (it has no gradients).  Adjoint of
  * tpcf_shear_scalar: given dL/dg_t and dL/dg_x per bin (g = the normalised
