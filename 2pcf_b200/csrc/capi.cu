@@ -595,10 +595,9 @@ void batch_launch(tpcf_ctx* c, Batch& B, bool timed) {
   const int nb = B.nb;
   check(cudaMemsetAsync(B.head, 0, sizeof(int) * 4, st), "memset head");
   if (B.n_items > 0) {
-    if (B.sharded) {
-      check(cudaMemsetAsync(B.item_sums, 0, sizeof(double) * kQ * nb * B.n_items, st), "memset items");
-      if (B.lens_acc) check(cudaMemsetAsync(B.lens_acc, 0, sizeof(double) * B.lens_acc_elems, st), "memset lens");
-    }
+    if (B.sharded) check(cudaMemsetAsync(B.item_sums, 0, sizeof(double) * kQ * nb * B.n_items, st), "memset items");
+    // the kernel adds only the non-zero cells of each per-lens fold
+    if (B.lens_acc) check(cudaMemsetAsync(B.lens_acc, 0, sizeof(double) * B.lens_acc_elems, st), "memset lens");
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     if (timed) {
       check(cudaEventCreate(&ev0), "event");

@@ -42,36 +42,76 @@ struct MarksField {
   const float* w;           // maps: [n_map][n]
 };
 
-// 4-byte asynchronous copy global -> shared (cp.async); with valid == false
-// nothing is read and the destination is zero-filled.
+// Asynchronous copies global -> shared (cp.async) of 4 or 16 bytes; with
+// valid == false nothing is read and the destination is zero-filled.
 __device__ __forceinline__ void cp_async4(void* dst, const void* src, bool valid) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(
                    static_cast<unsigned>(__cvta_generic_to_shared(dst))),
                "l"(src), "r"(valid ? 4 : 0)
                : "memory");
 }
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                   static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+               "l"(src), "r"(valid ? 16 : 0)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Copies `rows` runs of 64 consecutive 4-byte values, run k from src(k) (a
+// device pointer to the run's first value), into dst[k * 64 ..], by all
+// threads of the block: valid values are the first nt of each run of the
+// first live_rows runs, the rest is zero-filled.  16-byte chunks when the
+// tile is whole and every run starts on a 16-byte boundary (vec), else 4-byte
+// copies.
+template <class SrcOf>
+__device__ __forceinline__ void stage_runs(void* dst, int rows, int live_rows, int nt, bool vec, SrcOf src, int tid,
+                                           int nthr) {
+  unsigned char* d = reinterpret_cast<unsigned char*>(dst);
+  if (vec) {
+    for (int e = tid; e < rows * 16; e += nthr) {
+      const int k = e >> 4, c = e & 15;
+      const bool v = k < live_rows;
+      cp_async16(d + (size_t)(k * 64 + 4 * c) * 4, v ? reinterpret_cast<const unsigned char*>(src(k)) + 16 * c
+                                                        : reinterpret_cast<const unsigned char*>(src(0)), v);
+    }
+  } else {
+    for (int e = tid; e < rows * 64; e += nthr) {
+      const int k = e >> 6, jj = e & 63;
+      const bool v = k < live_rows && jj < nt;
+      cp_async4(d + (size_t)e * 4, v ? reinterpret_cast<const unsigned char*>(src(k)) + 4 * jj
+                                      : reinterpret_cast<const unsigned char*>(src(0)), v);
+    }
+  }
+}
 
 // Lens factors of resample/map g for lens jj of a tile.  stage() starts the
-// copies of the raw inputs of entry e = (g, jj) into shared memory; factors()
-// turns the landed raw values into the numerator factor vw and the K factor
-// wm (both 0 for a lens that takes no part).
+// copies of the raw inputs of one tile into shared memory (all threads);
+// factors() turns the landed raw values into the numerator factor vw and the
+// K factor wm (both 0 for a lens that takes no part).
 struct MapFactors {  // foreground maps: vw = val w, wm = w
   int map0;
   static constexpr size_t kRawBytes = sizeof(float) * (2 * kMapGroup + 1) * 64;
   // raw: val [kMapGroup][64], w [kMapGroup][64], marks weight [64]
-  __device__ __forceinline__ void stage(const MarksField& F, int g, int jj, long long j, bool valid,
-                                        unsigned char* raw, int e) const {
+  __device__ __forceinline__ void stage(const MarksField& F, long long t0, int nt, int n_g, unsigned char* raw,
+                                        int tid, int nthr) const {
     float* rv = reinterpret_cast<float*>(raw);
-    const size_t o = valid ? (size_t)(map0 + g) * (size_t)F.n + (size_t)j : 0;
-    cp_async4(rv + e, F.val + o, valid);
-    cp_async4(rv + kMapGroup * 64 + e, F.w + o, valid);
-    if (g == 0) cp_async4(rv + 2 * kMapGroup * 64 + jj, F.mw + (valid ? j : 0), valid);
+    const bool vec = nt == 64 && al16(F.val) && al16(F.w) && al16(F.mw) && (F.n & 3) == 0 && (t0 & 3) == 0;
+    const size_t o = (size_t)map0 * (size_t)F.n + (size_t)t0;
+    const float* val = F.val;
+    const float* w = F.w;
+    const long long n = F.n;
+    stage_runs(rv, kMapGroup, n_g, nt, vec, [&](int k) { return val + o + (size_t)k * n; }, tid, nthr);
+    stage_runs(rv + kMapGroup * 64, kMapGroup, n_g, nt, vec, [&](int k) { return w + o + (size_t)k * n; }, tid,
+               nthr);
+    const float* mw = F.mw + t0;
+    stage_runs(rv + 2 * kMapGroup * 64, 1, 1, nt, vec, [&](int) { return mw; }, tid, nthr);
   }
-  __device__ __forceinline__ void factors(const unsigned char* raw, int e, int jj, double& vw, double& wm) const {
+  __device__ __forceinline__ void factors(const unsigned char* raw, int g, int jj, double& vw, double& wm) const {
     const float* rv = reinterpret_cast<const float*>(raw);
-    wm = (double)rv[kMapGroup * 64 + e];
-    vw = (double)rv[e] * wm;
+    wm = (double)rv[kMapGroup * 64 + g * 64 + jj];
+    vw = (double)rv[g * 64 + jj] * wm;
     // calculate_tpcf_from_marks drops lenses with marks weight x weight <= 0
     if (!((double)rv[2 * kMapGroup * 64 + jj] * wm > 0.0)) vw = wm = 0.0;
   }
@@ -81,19 +121,27 @@ struct MultFactors {  // resamples: vw = wm = multiplicity of the lens's unit
   const int* unit;    // unit of each lens (all fields concatenated), or nullptr: the lens itself
   long long n_units;
   static constexpr size_t kRawBytes = sizeof(int) * kMapGroup * 64;
-  __device__ __forceinline__ void stage(const MarksField& F, int g, int, long long j, bool valid,
-                                        unsigned char* raw, int e) const {
-    size_t o = 0;
-    if (valid) {
-      const long long gl = F.lens0 + j;
-      const long long u = unit ? (long long)__ldg(unit + gl) : gl;
-      o = (size_t)g * (size_t)n_units + (size_t)u;
+  __device__ __forceinline__ void stage(const MarksField& F, long long t0, int nt, int n_g, unsigned char* raw,
+                                        int tid, int nthr) const {
+    int* rm = reinterpret_cast<int*>(raw);
+    const long long gl0 = F.lens0 + t0;
+    if (!unit) {  // each lens its own unit: runs of consecutive multiplicities
+      const bool vec = nt == 64 && al16(mult) && (n_units & 3) == 0 && (gl0 & 3) == 0;
+      const int* m = mult + gl0;
+      const long long nu = n_units;
+      stage_runs(rm, kMapGroup, n_g, nt, vec, [&](int k) { return m + (size_t)k * nu; }, tid, nthr);
+      return;
     }
-    cp_async4(reinterpret_cast<int*>(raw) + e, mult + o, valid);
+    for (int e = tid; e < kMapGroup * 64; e += nthr) {  // gathered through the unit labels
+      const int g = e >> 6, jj = e & 63;
+      const bool v = g < n_g && jj < nt;
+      const size_t o = v ? (size_t)g * (size_t)n_units + (size_t)__ldg(unit + gl0 + jj) : 0;
+      cp_async4(rm + e, mult + o, v);
+    }
   }
   // the bootstraps take every drawn lens (src/tpcf.f90:601, :917, :1248)
-  __device__ __forceinline__ void factors(const unsigned char* raw, int e, int, double& vw, double& wm) const {
-    const int m = reinterpret_cast<const int*>(raw)[e];
+  __device__ __forceinline__ void factors(const unsigned char* raw, int g, int jj, double& vw, double& wm) const {
+    const int m = reinterpret_cast<const int*>(raw)[g * 64 + jj];
     wm = m > 0 ? (double)m : 0.0;
     vw = wm;
   }
@@ -116,11 +164,11 @@ struct MultFactors {  // resamples: vw = wm = multiplicity of the lens's unit
 // applied keeps the pass near the FP64 roofline.  The groups are summed in
 // fixed order at the end (deterministic, no atomics).
 //
-// A factor row of 16 doubles is stored with its columns XOR-swizzled by
-// 2 (jj & 7): pairs (2h, 2h+1) stay adjacent and in order (read as one
-// double2 at pair index h ^ (jj & 7)), and the 32 lanes of one conversion
-// store (one map, 32 lenses) spread over 16 banks instead of 2.
+// A factor row of 16 doubles is stored with a stride of 18 (kFacStride): the
+// summing loop reads it as 8 aligned double2, and the 32 lanes of one
+// conversion store (one map, 32 lenses) spread over 16 banks instead of 2.
 constexpr int kTileL = 64;
+constexpr int kFacStride = kMapGroup + 2;
 constexpr int kMarksLens = 1024;  // lenses per block
 // Threads per block at most: one group of 3 kMaxBins + 1 = 385 rows fits, and
 // two blocks per SM leave 78 registers per thread (the 16 FP64 sums and the
@@ -140,11 +188,11 @@ __global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const Marks
                                                             const Fac fac, int n_g, int n_bin, int tg,
                                                             double* __restrict__ partial) {
   extern __shared__ __align__(16) unsigned char sm[];
-  constexpr int TF = kTileL * kMapGroup;
+  constexpr int TF = kTileL * kFacStride;
   const int R = 3 * n_bin + 1;
   const int ng = blockDim.x / tg;
-  double* fac_s = reinterpret_cast<double*>(sm);  // [kTileL][kMapGroup] factors of the E and B rows
-  double* fw_s = fac_s + TF;                      // [kTileL][kMapGroup] factors of K and the weight
+  double* fac_s = reinterpret_cast<double*>(sm);  // [kTileL][kFacStride] factors of the E and B rows
+  double* fw_s = fac_s + TF;                      // [kTileL][kFacStride] factors of K and the weight
   unsigned char* raw = sm + 2 * TF * sizeof(double);
   float* mk = reinterpret_cast<float*>(raw + std::max(MapFactors::kRawBytes, MultFactors::kRawBytes));
   const int MS = 3 * kTileL * n_bin + kTileL;  // floats per marks buffer
@@ -154,7 +202,7 @@ __global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const Marks
   const MarksField& F = fields[fi];  // read where used: its pointers need no registers across the loop
   const long long j0 = (long long)(blk - F.chunk0) * kMarksLens;
   const long long j1 = min(F.n, j0 + kMarksLens);
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, nthr = blockDim.x;
   const int grp = tid / tg, r = tid % tg;
   const int q = r / n_bin, bb = r - q * n_bin;  // q = 3: the marks weight row
   const bool live = r < R;
@@ -166,31 +214,33 @@ __global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const Marks
 
   auto stage_tile = [&](long long t0, int buf) {
     const int nt = (int)min((long long)kTileL, j1 - t0);
-    for (int e = tid; e < TF; e += blockDim.x) {
-      const int g = e / kTileL, jj = e - g * kTileL;
-      fac.stage(F, g, jj, t0 + jj, jj < nt && g < n_g, raw, e);
-    }
+    fac.stage(F, t0, nt, n_g, raw, tid, nthr);
     if (STAGE) {
+      // the tile's marks as laid out in HBM: [nt][n_bin] of each quantity, the weights
       float* mb = mk + buf * MS;
-      const int ne = nt * n_bin;
       const size_t o = (size_t)t0 * n_bin;
-      for (int e = tid; e < kTileL * n_bin; e += blockDim.x) {
-        const bool v = e < ne;
-        cp_async4(mb + e, F.xiE + (v ? o + e : 0), v);
-        cp_async4(mb + kTileL * n_bin + e, F.xiB + (v ? o + e : 0), v);
-        cp_async4(mb + 2 * kTileL * n_bin + e, F.K + (v ? o + e : 0), v);
+      const int nq = nt * n_bin, cap = kTileL * n_bin;
+      const bool vec = nt == kTileL && al16(F.xiE + o) && al16(F.xiB + o) && al16(F.K + o);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float* src = (k == 0 ? F.xiE : k == 1 ? F.xiB : F.K) + o;
+        if (vec) {
+          for (int e = tid; e < cap / 4; e += nthr) cp_async16(mb + k * cap + 4 * e, src + 4 * e, true);
+        } else {
+          for (int e = tid; e < cap; e += nthr) cp_async4(mb + k * cap + e, src + (e < nq ? e : 0), e < nq);
+        }
       }
-      for (int e = tid; e < kTileL; e += blockDim.x) cp_async4(mb + 3 * kTileL * n_bin + e, F.mw + (e < nt ? t0 + e : 0), e < nt);
+      const float* mw = F.mw + t0;
+      stage_runs(mb + 3 * cap, 1, 1, nt, nt == kTileL && al16(mw), [&](int) { return mw; }, tid, nthr);
     }
   };
   auto convert_tile = [&]() {
-    for (int e = tid; e < TF; e += blockDim.x) {
-      const int g = e / kTileL, jj = e - g * kTileL;
+    for (int e = tid; e < kTileL * kMapGroup; e += nthr) {
+      const int g = e >> 6, jj = e & 63;
       double vw, wm;
-      fac.factors(raw, e, jj, vw, wm);
-      const int o = jj * kMapGroup + (g ^ ((jj & 7) << 1));
-      fac_s[o] = vw;
-      fw_s[o] = wm;
+      fac.factors(raw, g, jj, vw, wm);
+      fac_s[jj * kFacStride + g] = vw;
+      fw_s[jj * kFacStride + g] = wm;
     }
   };
 
@@ -214,11 +264,10 @@ __global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const Marks
 #pragma unroll 1
       for (int jj = grp; jj < nt; jj += ng) {
         const double m = STAGE ? (double)base[jj * rs] : (double)__ldg(base + jj * rs);
-        const double2* f2 = reinterpret_cast<const double2*>(fsel + jj * kMapGroup);
-        const int sw = jj & 7;
+        const double2* f2 = reinterpret_cast<const double2*>(fsel + jj * kFacStride);
 #pragma unroll
         for (int h = 0; h < kMapGroup / 2; ++h) {
-          const double2 f = f2[h ^ sw];
+          const double2 f = f2[h];
           acc[2 * h] = fma(m, f.x, acc[2 * h]);
           acc[2 * h + 1] = fma(m, f.y, acc[2 * h + 1]);
         }
@@ -262,7 +311,7 @@ int marks_block_threads(int n_bin) {
 }
 bool marks_stage(int n_bin) { return marks_stage_floats(n_bin) <= kMaxStageFloats; }
 size_t marks_smem(int n_bin) {
-  size_t fac = 2 * sizeof(double) * kTileL * kMapGroup + std::max(MapFactors::kRawBytes, MultFactors::kRawBytes);
+  size_t fac = 2 * sizeof(double) * kTileL * kFacStride + std::max(MapFactors::kRawBytes, MultFactors::kRawBytes);
   if (marks_stage(n_bin)) fac += 2 * sizeof(float) * (size_t)marks_stage_floats(n_bin);
   const size_t red = sizeof(double) * (size_t)marks_group_threads(n_bin) * kMapGroup;
   return std::max(fac, red);

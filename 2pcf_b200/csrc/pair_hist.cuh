@@ -17,11 +17,12 @@ __device__ __forceinline__ void hist_add(float* hcol, int bin, const float* v) {
 }
 
 // Fold the FP32 histogram into FP64: the block sums (times the lens factors
-// val*w or w) and, when lens_col is set, this thread's per-lens FP64 column.
-// Then clear this thread's column.  Called by all threads.
+// val*w or w) and, when lens_col is set, this thread's per-lens FP64 column
+// (zeroed before the launch: only non-zero cells are added).  Then clear this
+// thread's column.  Called by all threads.
 template <int QA, int BT>
 __device__ __forceinline__ void flush_hist(float* hist, double* bsum, const double* fvw, const double* fw,
-                                           int nb, double* lens_col, size_t lens_stride, bool first) {
+                                           int nb, double* lens_col, size_t lens_stride) {
   const int tid = threadIdx.x;
   __syncthreads();
   float* hcol = hist + tid;
@@ -29,9 +30,11 @@ __device__ __forceinline__ void flush_hist(float* hist, double* bsum, const doub
     for (int q = 0; q < kQ; ++q) {
       const int qa = (q == QK && QA == 5) ? QW : q;
       for (int b = 0; b < nb; ++b) {
-        const double v = (double)hcol[(b * QA + qa) * BT];
-        double* p = lens_col + (size_t)(q * nb + b) * lens_stride;
-        *p = first ? v : *p + v;
+        const float v = hcol[(b * QA + qa) * BT];
+        if (v != 0.f) {  // the column was zeroed before the launch
+          double* p = lens_col + (size_t)(q * nb + b) * lens_stride;
+          *p += (double)v;
+        }
       }
     }
   }

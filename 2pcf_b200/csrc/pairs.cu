@@ -436,19 +436,24 @@ __device__ __forceinline__ TileGeom tile_of(int k, int incl, int ntr, int s0, in
 
 // Fold this warp's 32 histogram columns into its FP64 sums (times the lens
 // factors val*w or w) and, when lens_col is set, each lane's per-lens FP64
-// column; then clear the columns.  Called by all lanes of the warp.
+// column (zeroed before the launch; a lens's pairs between two folds fall in
+// few bins, so only its non-zero cells are added: most of the column's
+// read-modify-writes, and for lanes of one warp mostly the same ones, are
+// skipped); then clear the columns.  Called by all lanes of the warp.
 template <int QA, int BT>
 __device__ __forceinline__ void warp_fold(const float* hist, float* hcol, double* wsum, const double* fvw,
-                                          const double* fw, int nb, double* lens_col, size_t lens_stride, bool first,
-                                          int warp, int lane) {
+                                          const double* fw, int nb, double* lens_col, size_t lens_stride, int warp,
+                                          int lane) {
   __syncwarp();
   if (lens_col) {
     for (int q = 0; q < kQ; ++q) {
       const int qa = (q == QK && QA == 5) ? QW : q;
       for (int b = 0; b < nb; ++b) {
-        const double v = (double)hcol[(b * QA + qa) * BT];
-        double* p = lens_col + (size_t)(q * nb + b) * lens_stride;
-        *p = first ? v : *p + v;
+        const float v = hcol[(b * QA + qa) * BT];
+        if (v != 0.f) {
+          double* p = lens_col + (size_t)(q * nb + b) * lens_stride;
+          *p += (double)v;
+        }
       }
     }
   }
@@ -568,7 +573,6 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
     fw[tid] = w;
     const size_t lens_stride = (size_t)LD.n_valid;
     for (int e = lane; e < kQ * nb; e += 32) wsum[e] = 0.0;
-    bool first_flush = true;
     int since_flush = 0;
     const float4 box = LD.group_box[g];
     int cy0, cy1;
@@ -676,15 +680,14 @@ __global__ void __launch_bounds__(BT, kPairMinBlocks) k_pairs(const PairParams P
         __syncwarp();  // every lane is done reading buffer b
         if (k + NBUF < ntiles) issue(k + NBUF);
         if (since_flush >= flush_src) {
-          warp_fold<QA, BT>(hist, hcol, wsum, fvw, fw, nb, lens_col, lens_stride, first_flush, warp, lane);
-          first_flush = false;
+          warp_fold<QA, BT>(hist, hcol, wsum, fvw, fw, nb, lens_col, lens_stride, warp, lane);
           since_flush = 0;
         }
       }
       if (!aborted) ring_t += ntiles;
     }
     if (aborted) break;
-    warp_fold<QA, BT>(hist, hcol, wsum, fvw, fw, nb, lens_col, lens_stride, first_flush, warp, lane);
+    warp_fold<QA, BT>(hist, hcol, wsum, fvw, fw, nb, lens_col, lens_stride, warp, lane);
     double* out = P.item_sums + (size_t)(T.item_base + g) * kQ * nb;
     for (int e = lane; e < kQ * nb; e += 32) {
       const int src = (e / nb == QK && QA == 5) ? e - (QK - QW) * nb : e;

@@ -589,7 +589,6 @@ __global__ void __launch_bounds__(BT, 3) k_pairs_sph(const PairParams P) {
     fw[tid] = w;
     const size_t lens_stride = (size_t)LD.n_valid;
     for (int e = tid; e < kQ * nb; e += BT) bsum[e] = 0.0;
-    bool first_flush = true;
     int since_flush = 0;
     const float4 box = LD.group_box[g];
     int cy0, cy1;
@@ -736,15 +735,14 @@ __global__ void __launch_bounds__(BT, 3) k_pairs_sph(const PairParams P) {
         }
         since_flush += n;
         if (since_flush >= (P.flush_src > 0 ? P.flush_src : kFlushSrcS)) {
-          flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
-          first_flush = false;
+          flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride);
           since_flush = 0;
         }
         __syncthreads();
       }
       tcount += (uint32_t)ntiles;
     }
-    flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride, first_flush);
+    flush_hist<QA, BT>(hist, bsum, fvw, fw, nb, lens_col, lens_stride);
     __syncthreads();
     double* out = P.item_sums + (size_t)(T.item_base + g) * kQ * nb;
     for (int e = tid; e < kQ * nb; e += BT) {
