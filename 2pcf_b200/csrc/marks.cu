@@ -91,6 +91,7 @@ __device__ __forceinline__ void stage_runs(void* dst, int rows, int live_rows, i
 // factors() turns the landed raw values into the numerator factor vw and the
 // K factor wm (both 0 for a lens that takes no part).
 struct MapFactors {  // foreground maps: vw = val w, wm = w
+  static constexpr bool kSame = false;  // vw and wm differ: two factor arrays
   int map0;
   static constexpr size_t kRawBytes = sizeof(float) * (2 * kMapGroup + 1) * 64;
   // raw: val [kMapGroup][64], w [kMapGroup][64], marks weight [64]
@@ -117,6 +118,7 @@ struct MapFactors {  // foreground maps: vw = val w, wm = w
   }
 };
 struct MultFactors {  // resamples: vw = wm = multiplicity of the lens's unit
+  static constexpr bool kSame = true;  // one factor array serves every row
   const int* mult;    // [G][n_units]
   const int* unit;    // unit of each lens (all fields concatenated), or nullptr: the lens itself
   long long n_units;
@@ -164,11 +166,14 @@ struct MultFactors {  // resamples: vw = wm = multiplicity of the lens's unit
 // applied keeps the pass near the FP64 roofline.  The groups are summed in
 // fixed order at the end (deterministic, no atomics).
 //
-// A factor row of 16 doubles is stored with a stride of 18 (kFacStride): the
-// summing loop reads it as 8 aligned double2, and the 32 lanes of one
-// conversion store (one map, 32 lenses) spread over 16 banks instead of 2.
+// The factors of one lens are stored as [vw of the 16 maps | 2 pad | wm of
+// the 16 maps | 2 pad] (kLensStride doubles): the summing loop reads its
+// half as 8 aligned double2, and a warp whose rows read both halves (E/B rows
+// and K/weight rows) hits disjoint banks, as do the 32 lanes of one
+// conversion store (one map, 32 lenses).
 constexpr int kTileL = 64;
-constexpr int kFacStride = kMapGroup + 2;
+constexpr int kLensStride = 2 * (kMapGroup + 2);
+constexpr int kWmOffset = kMapGroup + 2;
 constexpr int kMarksLens = 1024;  // lenses per block
 // Threads per block at most: one group of 3 kMaxBins + 1 = 385 rows fits, and
 // two blocks per SM leave 78 registers per thread (the 16 FP64 sums and the
@@ -188,12 +193,11 @@ __global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const Marks
                                                             const Fac fac, int n_g, int n_bin, int tg,
                                                             double* __restrict__ partial) {
   extern __shared__ __align__(16) unsigned char sm[];
-  constexpr int TF = kTileL * kFacStride;
+  constexpr int TF = kTileL * kLensStride;
   const int R = 3 * n_bin + 1;
   const int ng = blockDim.x / tg;
-  double* fac_s = reinterpret_cast<double*>(sm);  // [kTileL][kFacStride] factors of the E and B rows
-  double* fw_s = fac_s + TF;                      // [kTileL][kFacStride] factors of K and the weight
-  unsigned char* raw = sm + 2 * TF * sizeof(double);
+  double* fac_s = reinterpret_cast<double*>(sm);  // [kTileL][kLensStride] factors of every row
+  unsigned char* raw = sm + TF * sizeof(double);
   float* mk = reinterpret_cast<float*>(raw + std::max(MapFactors::kRawBytes, MultFactors::kRawBytes));
   const int MS = 3 * kTileL * n_bin + kTileL;  // floats per marks buffer
   const int blk = blockIdx.x;
@@ -206,7 +210,7 @@ __global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const Marks
   const int grp = tid / tg, r = tid % tg;
   const int q = r / n_bin, bb = r - q * n_bin;  // q = 3: the marks weight row
   const bool live = r < R;
-  const double* fsel = q < 2 ? fac_s : fw_s;
+  const double* fsel = (q < 2 || Fac::kSame) ? fac_s : fac_s + kWmOffset;
   // this thread's marks row: in HBM (lens stride rs) or in a staged buffer
   const float* row = q == 0 ? F.xiE + bb : q == 1 ? F.xiB + bb : q == 2 ? F.K + bb : F.mw;
   const long long rs = q < 3 ? n_bin : 1;
@@ -239,8 +243,8 @@ __global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const Marks
       const int g = e >> 6, jj = e & 63;
       double vw, wm;
       fac.factors(raw, g, jj, vw, wm);
-      fac_s[jj * kFacStride + g] = vw;
-      fw_s[jj * kFacStride + g] = wm;
+      fac_s[jj * kLensStride + g] = vw;
+      if (!Fac::kSame) fac_s[jj * kLensStride + kWmOffset + g] = wm;
     }
   };
 
@@ -264,7 +268,7 @@ __global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const Marks
 #pragma unroll 1
       for (int jj = grp; jj < nt; jj += ng) {
         const double m = STAGE ? (double)base[jj * rs] : (double)__ldg(base + jj * rs);
-        const double2* f2 = reinterpret_cast<const double2*>(fsel + jj * kFacStride);
+        const double2* f2 = reinterpret_cast<const double2*>(fsel + jj * kLensStride);
 #pragma unroll
         for (int h = 0; h < kMapGroup / 2; ++h) {
           const double2 f = f2[h];
@@ -311,7 +315,7 @@ int marks_block_threads(int n_bin) {
 }
 bool marks_stage(int n_bin) { return marks_stage_floats(n_bin) <= kMaxStageFloats; }
 size_t marks_smem(int n_bin) {
-  size_t fac = 2 * sizeof(double) * kTileL * kFacStride + std::max(MapFactors::kRawBytes, MultFactors::kRawBytes);
+  size_t fac = sizeof(double) * kTileL * kLensStride + std::max(MapFactors::kRawBytes, MultFactors::kRawBytes);
   if (marks_stage(n_bin)) fac += 2 * sizeof(float) * (size_t)marks_stage_floats(n_bin);
   const size_t red = sizeof(double) * (size_t)marks_group_threads(n_bin) * kMapGroup;
   return std::max(fac, red);

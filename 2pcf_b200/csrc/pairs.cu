@@ -43,7 +43,7 @@
 #define TPCF_DUAL_UNROLL 4
 #endif
 #ifndef TPCF_SINGLE_UNROLL
-#define TPCF_SINGLE_UNROLL 4
+#define TPCF_SINGLE_UNROLL 8
 #endif
 
 namespace tpcf {

@@ -177,6 +177,8 @@ __device__ __forceinline__ int classify_s(const LensS& L, const float4 mn, const
     b1 = edge_index_f32(dmax2 * (1.f + C.eps), C.e2f, C.nb);
   }
   if (b1 < 0 || b0 >= C.nb) return 0;
+  b0 = max(b0, -1);  // every bin below 0 or from nb up is dropped alike
+  b1 = min(b1, C.nb);
   blo = b0;
   if (b0 == b1) return 1;  // a z cut is applied inside the register paths
   if (b1 == b0 + 1) return 2;
@@ -292,24 +294,24 @@ __device__ __forceinline__ void sph_terms2(const LensS2& L, const SrcPairS& s, f
 // Register sums of one lens over a sub-chunk: all pairs (s*) and, in the
 // one-edge path, the upper side (h*).
 struct SphAcc {
-  float2 sgt, sgx, sw, sdw, sk, sn, hgt, hgx, hw, hdw, hk;
-  int hn;
+  float2 sgt, sgx, sw, sdw, sk, sn, hgt, hgx, hw, hdw, hk, hn, nc;
 };
 __device__ __forceinline__ void sph_acc_zero(SphAcc& A) {
   A.sgt = A.sgx = A.sw = A.sdw = A.sk = A.sn = dup2(0.f);
-  A.hgt = A.hgx = A.hw = A.hdw = A.hk = dup2(0.f);
-  A.hn = 0;
+  A.hgt = A.hgx = A.hw = A.hdw = A.hk = A.hn = A.nc = dup2(0.f);
 }
 
 // The two pairs of one SrcPairS against a lens (TAIL: only the first; the
 // second half is a copy, masked out).  With a z cut a pair with z_A > z_B
 // (src/tpcf.f90:322) adds nothing.  DUAL also forms the upper-side sums
-// (d2 >= E, selected) and the guard-band flag.  Without a z cut the w and K
-// sums of all pairs (and, scalar-scalar, the g sums) are the sub-chunk's
-// totals, so they are not accumulated here.
+// (pairs with d2 >= E, the side a 1.0/0.0 mask from one FP32 compare at
+// Ehi = E (1 + eps), applied by multiplication) and counts the pairs between
+// Elo = E (1 - eps) and Ehi, inside the guard band (A.nc).  Without a z cut
+// the w and K sums of all pairs (and, scalar-scalar, the g sums) are the
+// sub-chunk's totals, so they are not accumulated here.
 template <int MODE, bool HAS_M, bool HAS_Z, bool SMALL, bool DUAL, bool TAIL>
-__device__ __forceinline__ void sph_step(const LensS2& L, float lz, const SrcPairS& s, float E, float2 nE, float gE,
-                                         SphAcc& A, bool& near) {
+__device__ __forceinline__ void sph_step(const LensS2& L, float lz, const SrcPairS& s, float Elo, float Ehi,
+                                         SphAcc& A) {
   constexpr bool LI = !HAS_Z;
   float2 d2, th, r, X, Y;
   sph_terms2<MODE, SMALL>(L, s, d2, th, r, X, Y);
@@ -319,8 +321,8 @@ __device__ __forceinline__ void sph_step(const LensS2& L, float lz, const SrcPai
     v0 = lz <= s.zz.x;
     v1 = v1 && lz <= s.zz.y;
   }
+  const float2 vm = make_float2(v0 ? 1.f : 0.f, v1 ? 1.f : 0.f);
   if (HAS_Z || TAIL) {
-    const float2 vm = make_float2(v0 ? 1.f : 0.f, v1 ? 1.f : 0.f);
     r = mul2(r, vm);
     w = mul2(w, vm);
     if (MODE == 0 && HAS_M) K = mul2(K, vm);
@@ -334,18 +336,22 @@ __device__ __forceinline__ void sph_step(const LensS2& L, float lz, const SrcPai
   A.sdw = fma2(th, w, A.sdw);
   if (MODE == 0 && HAS_M && !LI) A.sk = add2(A.sk, K);
   if (DUAL) {
-    const float2 dE = add2(d2, nE);
-    near |= fabsf(dE.x) <= gE;
-    near |= fabsf(dE.y) <= gE;
-    const bool u0 = v0 && d2.x >= E, u1 = v1 && d2.y >= E;
-    const float2 rm = make_float2(u0 ? r.x : 0.f, u1 ? r.y : 0.f);
-    const float2 wm = make_float2(u0 ? w.x : 0.f, u1 ? w.y : 0.f);
+    float2 mh = make_float2(d2.x >= Ehi ? 1.f : 0.f, d2.y >= Ehi ? 1.f : 0.f);
+    const float2 ml = make_float2(d2.x >= Elo ? 1.f : 0.f, d2.y >= Elo ? 1.f : 0.f);
+    if (HAS_Z || TAIL) {
+      A.nc = fma2(add2(ml, make_float2(-mh.x, -mh.y)), vm, A.nc);
+      mh = mul2(mh, vm);
+    } else {
+      A.nc = add2(A.nc, add2(ml, make_float2(-mh.x, -mh.y)));
+    }
+    const float2 rm = mul2(r, mh);  // r, w, K carry the validity mask already
+    const float2 wm = mul2(w, mh);
     A.hgt = fma2(rm, X, A.hgt);
     A.hgx = fma2(rm, Y, A.hgx);
     A.hw = add2(A.hw, wm);
     A.hdw = fma2(th, wm, A.hdw);
-    A.hn += (int)u0 + (int)u1;
-    if (MODE == 0 && HAS_M) A.hk = add2(A.hk, make_float2(u0 ? K.x : 0.f, u1 ? K.y : 0.f));
+    A.hn = add2(A.hn, mh);
+    if (MODE == 0 && HAS_M) A.hk = fma2(K, mh, A.hk);
   }
 }
 
@@ -367,14 +373,11 @@ __device__ __forceinline__ void chunk_single_s(const SrcPairS* __restrict__ S, i
                                                int cls, int blo, float* __restrict__ hcol, const float4 ss) {
   SphAcc A;
   sph_acc_zero(A);
-  bool near = false;
   const int np = cnt >> 1;
 #pragma unroll 2
-  for (int k = 0; k < np; ++k)
-    sph_step<MODE, HAS_M, HAS_Z, SMALL, false, false>(L, lz, S[k], 0.f, dup2(0.f), 0.f, A, near);
+  for (int k = 0; k < np; ++k) sph_step<MODE, HAS_M, HAS_Z, SMALL, false, false>(L, lz, S[k], 0.f, 0.f, A);
   if (cnt & 1)
-    sph_step<MODE, HAS_M, HAS_Z, SMALL, false, true>(L, lz, dup_pair_s(src_of_s(S, cnt - 1)), 0.f, dup2(0.f), 0.f,
-                                                     A, near);
+    sph_step<MODE, HAS_M, HAS_Z, SMALL, false, true>(L, lz, dup_pair_s(src_of_s(S, cnt - 1)), 0.f, 0.f, A);
   if (cls != 1) return;
   float acc[QA];
   sph_totals<MODE, HAS_M, HAS_Z, QA>(A, cnt, ss, acc);
@@ -387,19 +390,19 @@ template <int MODE, bool HAS_M, bool HAS_Z, bool SMALL, int NC, int QA>
 __device__ __forceinline__ void chunk_dual_s(const SrcPairS* __restrict__ S, int cnt, const LensS& Lf,
                                              const LensS2& L, float lz, int cls, int blo, float* __restrict__ hcol,
                                              const BinCtx& C, const float4 ss) {
-  const float E = (cls == 2) ? C.e2f[blo + 1] : 3.0e38f;
-  const float gE = (cls == 2) ? E * C.eps_rel : 0.f;
-  const float2 nE = dup2(-E);
+  // lanes of class 1 (or 0) keep an edge no pair reaches
+  const float E = C.e2f[min(max(blo + 1, 0), C.nb)];
+  const float Elo = (cls == 2) ? E * (1.f - C.eps_rel) : 3.0e38f;
+  const float Ehi = (cls == 2) ? E * (1.f + C.eps_rel) : 3.0e38f;
   SphAcc A;
   sph_acc_zero(A);
-  bool near = false;  // some pair lies within the guard band of E
   const int np = cnt >> 1;
 #pragma unroll 2
-  for (int k = 0; k < np; ++k) sph_step<MODE, HAS_M, HAS_Z, SMALL, true, false>(L, lz, S[k], E, nE, gE, A, near);
+  for (int k = 0; k < np; ++k) sph_step<MODE, HAS_M, HAS_Z, SMALL, true, false>(L, lz, S[k], Elo, Ehi, A);
   if (cnt & 1)
-    sph_step<MODE, HAS_M, HAS_Z, SMALL, true, true>(L, lz, dup_pair_s(src_of_s(S, cnt - 1)), E, nE, gE, A, near);
+    sph_step<MODE, HAS_M, HAS_Z, SMALL, true, true>(L, lz, dup_pair_s(src_of_s(S, cnt - 1)), Elo, Ehi, A);
   if (cls == 0) return;
-  if (near) {  // rare: the sub-chunk is binned pair by pair by the canonical rule
+  if (sum2(A.nc) != 0.f) {  // rare: a pair inside the guard band; the sub-chunk is binned pair by pair
     for (int j = 0; j < cnt; ++j) do_pair_s<MODE, HAS_M, HAS_Z, SMALL, SMALL, NC, QA>(Lf, lz, src_of_s(S, j), hcol, C);
     return;
   }
@@ -409,7 +412,7 @@ __device__ __forceinline__ void chunk_dual_s(const SrcPairS* __restrict__ S, int
   hi[QGX] = sum2(A.hgx);
   hi[QW] = sum2(A.hw);
   hi[QDW] = sum2(A.hdw);
-  hi[QN] = (float)A.hn;
+  hi[QN] = sum2(A.hn);
   if (MODE == 0 && HAS_M) hi[QK] = sum2(A.hk);
   if (cls == 1) {
     hist_add<QA, NC>(hcol, blo, tot);

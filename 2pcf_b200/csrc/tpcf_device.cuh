@@ -208,6 +208,8 @@ __device__ __forceinline__ int classify(float lx, float ly, const float4 box, co
     b1 = edge_index_f32(dmax2 * (1.f + C.eps), C.e2f, C.nb);
   }
   if (b1 < 0 || b0 >= C.nb) return 0;
+  b0 = max(b0, -1);  // every bin below 0 or from nb up is dropped alike
+  b1 = min(b1, C.nb);
   blo = b0;
   if (HAS_Z && !ZREG) return 3;  // z cut: per-pair path unless the register paths apply it
   if (b0 == b1) return 1;

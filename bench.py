@@ -41,7 +41,7 @@ FLOP_PER_PAIR = 26  # shear-scalar, FMA = 2, MUFU = 1 (per binned pair)
 # DRAM bytes read + written by one pair-kernel launch of the default workload,
 # per grid cell side theta_max/D (one-pass ncu captures of
 # dram__bytes_read.sum + dram__bytes_write.sum)
-K_PAIRS_DRAM_BYTES = {24: 68.311e9 + 0.409e9}
+K_PAIRS_DRAM_BYTES = {16: 69.567e9 + 0.403e9, 24: 68.311e9 + 0.409e9, 32: 65.525e9 + 0.403e9}
 SPH_FLOP_PER_PAIR = 52  # spherical shear-scalar: hi/lo unit-vector differences, east/north projection, angle series
 WORKLOAD_DESC = ("tomography: 5 shear bins (0.2,0.5,1.0,1.9,4.0 M) x 5 scalar bins "
                  "(0.1,0.2,0.4,0.7,1.0 M) = 10.0 M objects, 25 cross-pairs in one launch, "
