@@ -31,10 +31,9 @@ __device__ __forceinline__ void flush_hist(float* hist, double* bsum, const doub
       const int qa = (q == QK && QA == 5) ? QW : q;
       for (int b = 0; b < nb; ++b) {
         const float v = hcol[(b * QA + qa) * BT];
-        if (v != 0.f) {  // the column was zeroed before the launch
-          double* p = lens_col + (size_t)(q * nb + b) * lens_stride;
-          *p += (double)v;
-        }
+        // the column was zeroed before the launch; one writer per column, so
+        // the fire-and-forget adds land in program order (deterministic)
+        if (v != 0.f) atomicAdd(lens_col + (size_t)(q * nb + b) * lens_stride, (double)v);
       }
     }
   }

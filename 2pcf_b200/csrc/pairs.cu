@@ -437,9 +437,10 @@ __device__ __forceinline__ TileGeom tile_of(int k, int incl, int ntr, int s0, in
 // Fold this warp's 32 histogram columns into its FP64 sums (times the lens
 // factors val*w or w) and, when lens_col is set, each lane's per-lens FP64
 // column (zeroed before the launch; a lens's pairs between two folds fall in
-// few bins, so only its non-zero cells are added: most of the column's
-// read-modify-writes, and for lanes of one warp mostly the same ones, are
-// skipped); then clear the columns.  Called by all lanes of the warp.
+// few bins, so only its non-zero cells are added, as fire-and-forget FP64
+// reductions: each column has one writer, so the adds land in program order
+// and the result is deterministic, and no load latency is waited for); then
+// clear the columns.  Called by all lanes of the warp.
 template <int QA, int BT>
 __device__ __forceinline__ void warp_fold(const float* hist, float* hcol, double* wsum, const double* fvw,
                                           const double* fw, int nb, double* lens_col, size_t lens_stride, int warp,
@@ -450,10 +451,7 @@ __device__ __forceinline__ void warp_fold(const float* hist, float* hcol, double
       const int qa = (q == QK && QA == 5) ? QW : q;
       for (int b = 0; b < nb; ++b) {
         const float v = hcol[(b * QA + qa) * BT];
-        if (v != 0.f) {
-          double* p = lens_col + (size_t)(q * nb + b) * lens_stride;
-          *p += (double)v;
-        }
+        if (v != 0.f) atomicAdd(lens_col + (size_t)(q * nb + b) * lens_stride, (double)v);
       }
     }
   }
