@@ -68,12 +68,18 @@ __global__ void k_km_assign(const float* __restrict__ x, const float* __restrict
     const float xi = x[i], yi = y[i];
     float best = min_init;
     int bi = -1;
+    // the correctly rounded sqrt (as the reference) only where it can win:
+    // q > best^2 (1 + 1e-5) gives sqrt(q) > best whatever the roundings
+    float tsq = __fmul_rn(min_init, min_init) * 1.00001f;
     for (int j = 0; j < k; ++j) {
       const float dx = __fsub_rn(xi, c[j].x), dy = __fsub_rn(yi, c[j].y);
-      const float d = __fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+      const float q = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+      if (q > tsq) continue;
+      const float d = __fsqrt_rn(q);
       if (d < best) {
         best = d;
         bi = j;
+        tsq = __fmul_rn(best, best) * 1.00001f;
       }
     }
     if (bi != labels[i]) {
@@ -225,12 +231,12 @@ __global__ void __launch_bounds__(1024) k_km_sweep_eq(const float* __restrict__ 
                                                       float min_init, float wmean, float scaling, int sw,
                                                       int penalty, int candidates, int* labels, int* cand,
                                                       float* memb, unsigned long long* n_re) {
-  extern __shared__ unsigned char sm[];
-  float2* c = reinterpret_cast<float2*>(sm);
-  long long* W = reinterpret_cast<long long*>(c + k);
+  extern __shared__ __align__(16) unsigned char sm[];
+  float2* nc = reinterpret_cast<float2*>(sm);  // negated centroids: x - c as x + (-c), the same rounding
+  long long* W = reinterpret_cast<long long*>(nc + k);
   float* f = reinterpret_cast<float*>(W + k);
   for (int j = threadIdx.x; j < k; j += blockDim.x) {
-    c[j] = cen[j];
+    nc[j] = make_float2(-cen[j].x, -cen[j].y);
     W[j] = wfix[j];
   }
   unsigned long long re = 0;
@@ -271,12 +277,12 @@ __global__ void __launch_bounds__(1024) k_km_sweep_eq(const float* __restrict__ 
       // (correctly rounded sqrt, as the reference) is formed only when
       // f^2 (dx^2 + dy^2) <= T^2 (1 + 1e-5): outside that margin d > T for
       // certain, whatever the FP32 roundings, so the labels do not change.
+      // dx^2 + dy^2 is formed for two clusters at once on packed FP32 (each
+      // half rounded as the scalar operations, no contraction); the clusters
+      // are still decided one by one in index order.
       float tsq = __fmul_rn(min_init, min_init) * 1.00001f;
-      for (int j = 0; j < k; ++j) {
-        const float dx = __fsub_rn(xi, c[j].x), dy = __fsub_rn(yi, c[j].y);
-        const float q = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-        const float fj = f[j];
-        if (fj > 0.f && fj * fj * q > tsq) continue;  // (f <= 0 gives d <= 0: always formed)
+      auto visit = [&](int j, float q, float fj) {
+        if (fj > 0.f && fj * fj * q > tsq) return;  // (f <= 0 gives d <= 0: always formed)
         const float d = __fmul_rn(fj, __fsqrt_rn(q));
         if (candidates && d > 0.0f) {
           if (d < best) {
@@ -288,16 +294,31 @@ __global__ void __launch_bounds__(1024) k_km_sweep_eq(const float* __restrict__ 
             cm = __fdiv_rn(d, best);
             ci = j;
           } else {
-            continue;
+            return;
           }
         } else if (d < best) {
           best = d;
           bi = j;
         } else {
-          continue;
+          return;
         }
         const float t = candidates ? fmaxf(best, __fmul_rn(cm, best)) : best;
         tsq = __fmul_rn(t, t) * 1.00001f;
+      };
+      const float2 x2 = make_float2(xi, xi), y2 = make_float2(yi, yi);
+      int j = 0;
+      for (; j + 1 < k; j += 2) {
+        const float4 cc = *reinterpret_cast<const float4*>(nc + j);
+        const float2 ff = *reinterpret_cast<const float2*>(f + j);
+        const float2 dx = __fadd2_rn(x2, make_float2(cc.x, cc.z));
+        const float2 dy = __fadd2_rn(y2, make_float2(cc.y, cc.w));
+        const float2 q = __fadd2_rn(__fmul2_rn(dx, dx), __fmul2_rn(dy, dy));
+        visit(j, q.x, ff.x);
+        visit(j + 1, q.y, ff.y);
+      }
+      if (j < k) {
+        const float dx = __fadd_rn(xi, nc[j].x), dy = __fadd_rn(yi, nc[j].y);
+        visit(j, __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), f[j]);
       }
       if (candidates) {
         cand[i] = ci;
