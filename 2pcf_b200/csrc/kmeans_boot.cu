@@ -215,6 +215,31 @@ tpcf_status fail(tpcf_ctx* c, const Failure& f) {
 }
 
 
+// Packed FP32 add and multiply as single PTX instructions: each half is
+// rounded as the scalar operation, and, written as inline PTX, a product is
+// never fused into a following add (the labels must match the scalar
+// reference bit for bit).
+__device__ __forceinline__ unsigned long long pk2(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ float2 upk2(unsigned long long r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+__device__ __forceinline__ float2 add2_exact(float2 a, float2 b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(r);
+}
+__device__ __forceinline__ float2 mul2_exact(float2 a, float2 b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(r);
+}
+
 // --------------------------------------------------- equal-weight k-means --
 // partition_data with equal_size (src/kmeans.f90:12-262).  From pass 2 on the
 // distance to cluster j is scaled by 1 + (W_j / W_mean - 1) * s (:171-177) and
@@ -278,7 +303,7 @@ __global__ void __launch_bounds__(1024) k_km_sweep_eq(const float* __restrict__ 
       // f^2 (dx^2 + dy^2) <= T^2 (1 + 1e-5): outside that margin d > T for
       // certain, whatever the FP32 roundings, so the labels do not change.
       // dx^2 + dy^2 is formed for two clusters at once on packed FP32 (each
-      // half rounded as the scalar operations, no contraction); the clusters
+      // half rounded as the scalar operations, never fused); the clusters
       // are still decided one by one in index order.
       float tsq = __fmul_rn(min_init, min_init) * 1.00001f;
       auto visit = [&](int j, float q, float fj) {
@@ -310,9 +335,9 @@ __global__ void __launch_bounds__(1024) k_km_sweep_eq(const float* __restrict__ 
       for (; j + 1 < k; j += 2) {
         const float4 cc = *reinterpret_cast<const float4*>(nc + j);
         const float2 ff = *reinterpret_cast<const float2*>(f + j);
-        const float2 dx = __fadd2_rn(x2, make_float2(cc.x, cc.z));
-        const float2 dy = __fadd2_rn(y2, make_float2(cc.y, cc.w));
-        const float2 q = __fadd2_rn(__fmul2_rn(dx, dx), __fmul2_rn(dy, dy));
+        const float2 dx = add2_exact(x2, make_float2(cc.x, cc.z));
+        const float2 dy = add2_exact(y2, make_float2(cc.y, cc.w));
+        const float2 q = add2_exact(mul2_exact(dx, dx), mul2_exact(dy, dy));
         visit(j, q.x, ff.x);
         visit(j + 1, q.y, ff.y);
       }

@@ -167,9 +167,10 @@ __device__ __forceinline__ void do_pair(float lx, float ly, float lz, const floa
 // pairs).  Shear: with P = dx^2 - dy^2, u = 2 dx dy and r = 1/d^2,
 // cos 2phi = P r, sin 2phi = u r (src/tpcf.f90:343-344), so the g_t, g_x
 // terms are r*X and r*Y with X = p P + q u, Y = q P - p u (p = -e1 w,
-// q = -e2 w).  Scalar-scalar: X = kE w, Y = kB w, r = 1.  Each term equals
-// the scalar computation from dx = lx - x, dy = ly - y bit for bit (the
-// packed halves round like the scalar operations; x - lx = -(lx - x)).
+// q = -e2 w).  Scalar-scalar: X = kE w, Y = kB w, r = 1.  Each half of a
+// packed operation rounds like the scalar operation (x - lx = -(lx - x));
+// the compiler may fuse a product into a following add, as it may in scalar
+// code, so a term agrees with a scalar evaluation to within one FMA rounding.
 struct LensP {
   float2 nlx, nly;  // (-lx, -lx), (-ly, -ly)
 };
