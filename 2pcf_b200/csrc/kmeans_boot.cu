@@ -215,31 +215,6 @@ tpcf_status fail(tpcf_ctx* c, const Failure& f) {
 }
 
 
-// Packed FP32 add and multiply as single PTX instructions: each half is
-// rounded as the scalar operation, and, written as inline PTX, a product is
-// never fused into a following add (the labels must match the scalar
-// reference bit for bit).
-__device__ __forceinline__ unsigned long long pk2(float2 a) {
-  unsigned long long r;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
-  return r;
-}
-__device__ __forceinline__ float2 upk2(unsigned long long r) {
-  float2 a;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
-  return a;
-}
-__device__ __forceinline__ float2 add2_exact(float2 a, float2 b) {
-  unsigned long long r;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
-  return upk2(r);
-}
-__device__ __forceinline__ float2 mul2_exact(float2 a, float2 b) {
-  unsigned long long r;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
-  return upk2(r);
-}
-
 // --------------------------------------------------- equal-weight k-means --
 // partition_data with equal_size (src/kmeans.f90:12-262).  From pass 2 on the
 // distance to cluster j is scaled by 1 + (W_j / W_mean - 1) * s (:171-177) and
@@ -256,12 +231,12 @@ __global__ void __launch_bounds__(1024) k_km_sweep_eq(const float* __restrict__ 
                                                       float min_init, float wmean, float scaling, int sw,
                                                       int penalty, int candidates, int* labels, int* cand,
                                                       float* memb, unsigned long long* n_re) {
-  extern __shared__ __align__(16) unsigned char sm[];
-  float2* nc = reinterpret_cast<float2*>(sm);  // negated centroids: x - c as x + (-c), the same rounding
-  long long* W = reinterpret_cast<long long*>(nc + k);
+  extern __shared__ unsigned char sm[];
+  float2* c = reinterpret_cast<float2*>(sm);
+  long long* W = reinterpret_cast<long long*>(c + k);
   float* f = reinterpret_cast<float*>(W + k);
   for (int j = threadIdx.x; j < k; j += blockDim.x) {
-    nc[j] = make_float2(-cen[j].x, -cen[j].y);
+    c[j] = cen[j];
     W[j] = wfix[j];
   }
   unsigned long long re = 0;
@@ -302,12 +277,12 @@ __global__ void __launch_bounds__(1024) k_km_sweep_eq(const float* __restrict__ 
       // (correctly rounded sqrt, as the reference) is formed only when
       // f^2 (dx^2 + dy^2) <= T^2 (1 + 1e-5): outside that margin d > T for
       // certain, whatever the FP32 roundings, so the labels do not change.
-      // dx^2 + dy^2 is formed for two clusters at once on packed FP32 (each
-      // half rounded as the scalar operations, never fused); the clusters
-      // are still decided one by one in index order.
       float tsq = __fmul_rn(min_init, min_init) * 1.00001f;
-      auto visit = [&](int j, float q, float fj) {
-        if (fj > 0.f && fj * fj * q > tsq) return;  // (f <= 0 gives d <= 0: always formed)
+      for (int j = 0; j < k; ++j) {
+        const float dx = __fsub_rn(xi, c[j].x), dy = __fsub_rn(yi, c[j].y);
+        const float q = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+        const float fj = f[j];
+        if (fj > 0.f && fj * fj * q > tsq) continue;  // (f <= 0 gives d <= 0: always formed)
         const float d = __fmul_rn(fj, __fsqrt_rn(q));
         if (candidates && d > 0.0f) {
           if (d < best) {
@@ -319,31 +294,16 @@ __global__ void __launch_bounds__(1024) k_km_sweep_eq(const float* __restrict__ 
             cm = __fdiv_rn(d, best);
             ci = j;
           } else {
-            return;
+            continue;
           }
         } else if (d < best) {
           best = d;
           bi = j;
         } else {
-          return;
+          continue;
         }
         const float t = candidates ? fmaxf(best, __fmul_rn(cm, best)) : best;
         tsq = __fmul_rn(t, t) * 1.00001f;
-      };
-      const float2 x2 = make_float2(xi, xi), y2 = make_float2(yi, yi);
-      int j = 0;
-      for (; j + 1 < k; j += 2) {
-        const float4 cc = *reinterpret_cast<const float4*>(nc + j);
-        const float2 ff = *reinterpret_cast<const float2*>(f + j);
-        const float2 dx = add2_exact(x2, make_float2(cc.x, cc.z));
-        const float2 dy = add2_exact(y2, make_float2(cc.y, cc.w));
-        const float2 q = add2_exact(mul2_exact(dx, dx), mul2_exact(dy, dy));
-        visit(j, q.x, ff.x);
-        visit(j + 1, q.y, ff.y);
-      }
-      if (j < k) {
-        const float dx = __fadd_rn(xi, nc[j].x), dy = __fadd_rn(yi, nc[j].y);
-        visit(j, __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), f[j]);
       }
       if (candidates) {
         cand[i] = ci;
