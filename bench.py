@@ -258,12 +258,14 @@ def marks_timing(tpcf, stream, nb):
     # algorithmic bytes: the marks once (xi_E, xi_B, K [n][n_bin] and the marks
     # weight, FP32) and the maps' val and w [n_map][n] (FP32)
     byt = (3 * 4 * n * nbm + 4 * n) + n_map * 8 * n
-    hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"] \
-        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else 6650.0
+    peaks = load_peaks()
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    hbm_src = "measured (MEASURED_PEAKS.json)" if peaks.get("hbm_gbs") else \
+        "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"
     out["marks_reweight"] = {"maps": n_map, "lenses": n, "n_bin": nbm, "call_ms": ms,
                              "roofline": {"bound": "hbm", "achieved": byt / (ms * 1e-3) / 1e9, "peak": hbm,
                                           "unit": "GB/s", "frac": byt / (ms * 1e-3) / 1e9 / hbm,
-                                          "bytes": byt}}
+                                          "bytes": byt, "peak_source": hbm_src}}
     _, ms = timed(lambda: tpcf.marks_bootstrap([mk], 1000, seed=5, covariance=True, ctx=mctx))
     # each resample re-weights every lens's 3 n_bin + 1 marks: one FP64 FMA
     # each (the multiplicities are drawn on the device), so FP64-bound
