@@ -254,26 +254,35 @@ def marks_timing(tpcf, stream, nb):
     wm = dev(rng.uniform(0.5, 1.5, (n_map, n)).astype(np.float32))
     mctx = tpcf.Context(0)
     mctx.set_stream(stream.cuda_stream)
+    mctx.set_timing(True)  # CUDA events around the partial-sum kernel(s) of each call
     _, ms = timed(lambda: tpcf.calculate_tpcf_from_marks([mk], [val], [wm], ctx=mctx))
+    kms = mctx.stats()["pair_kernel_ms"]
     # algorithmic bytes: the marks once (xi_E, xi_B, K [n][n_bin] and the marks
-    # weight, FP32) and the maps' val and w [n_map][n] (FP32)
+    # weight, FP32) and the maps' val and w [n_map][n] (FP32); 2 FLOP per lens,
+    # marks row and map
     byt = (3 * 4 * n * nbm + 4 * n) + n_map * 8 * n
     peaks = load_peaks()
     hbm = peaks.get("hbm_gbs") or 6650.0
     hbm_src = "measured (MEASURED_PEAKS.json)" if peaks.get("hbm_gbs") else \
         "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"
-    out["marks_reweight"] = {"maps": n_map, "lenses": n, "n_bin": nbm, "call_ms": ms,
-                             "roofline": {"bound": "hbm", "achieved": byt / (ms * 1e-3) / 1e9, "peak": hbm,
-                                          "unit": "GB/s", "frac": byt / (ms * 1e-3) / 1e9 / hbm,
+    p64 = mctx.measure_fp64_peak()
+    out["marks_reweight"] = {"maps": n_map, "lenses": n, "n_bin": nbm, "call_ms": ms, "kernel_ms": kms,
+                             "kernel": "k_marks_dmma (FP64 mma.sync m8n8k4)",
+                             "call_hbm_frac": byt / (ms * 1e-3) / 1e9 / hbm,
+                             "fp64_frac": n * (3 * nbm + 1) * n_map * 2 / (kms * 1e-3) / 1e12 / p64,
+                             "roofline": {"bound": "hbm", "achieved": byt / (kms * 1e-3) / 1e9, "peak": hbm,
+                                          "unit": "GB/s", "frac": byt / (kms * 1e-3) / 1e9 / hbm,
                                           "bytes": byt, "peak_source": hbm_src}}
     _, ms = timed(lambda: tpcf.marks_bootstrap([mk], 1000, seed=5, covariance=True, ctx=mctx))
+    kms = mctx.stats()["pair_kernel_ms"]
     # each resample re-weights every lens's 3 n_bin + 1 marks: one FP64 FMA
-    # each (the multiplicities are drawn on the device), so FP64-bound
+    # each (the multiplicities are drawn on the device), so FP64-bound; the
+    # FP64 tensor instruction and the FP64 FMA pipe have the same peak here
     flop = 1000 * n * (3 * nbm + 1) * 2
-    p64 = mctx.measure_fp64_peak()
-    out["marks_bootstrap"] = {"resamples": 1000, "lenses": n, "call_ms": ms,
-                              "roofline": {"bound": "fp64", "achieved": flop / (ms * 1e-3) / 1e12, "peak": p64,
-                                           "unit": "TFLOP/s", "frac": flop / (ms * 1e-3) / 1e12 / p64,
+    out["marks_bootstrap"] = {"resamples": 1000, "lenses": n, "call_ms": ms, "kernel_ms": kms,
+                              "call_fp64_frac": flop / (ms * 1e-3) / 1e12 / p64,
+                              "roofline": {"bound": "fp64", "achieved": flop / (kms * 1e-3) / 1e12, "peak": p64,
+                                           "unit": "TFLOP/s", "frac": flop / (kms * 1e-3) / 1e12 / p64,
                                            "flop": flop, "peak_source": "FP64 FMA loop measured in this run"}}
     del mk, val, wm
     mctx.close()

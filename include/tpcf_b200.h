@@ -168,7 +168,8 @@ int64_t tpcf_kernel_launches(const tpcf_ctx* ctx);
 
 /* Statistics of the last pair-sum call.  pair_kernel_ms is measured with CUDA
  * events recorded on the context stream around the pair kernel when timing
- * is enabled (tpcf_set_timing), else 0. */
+ * is enabled (tpcf_set_timing), else 0; after tpcf_xi_from_marks and
+ * tpcf_marks_bootstrap it is the summed time of their partial-sum kernels. */
 typedef struct tpcf_stats {
   double pair_kernel_ms;
   double call_ms;

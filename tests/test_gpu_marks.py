@@ -18,12 +18,14 @@ def rand_marks(rng, n, nb):
             "K": rng.uniform(0.5, 1.5, (n, nb)).astype(np.float32)}
 
 
-@pytest.mark.parametrize("nb", [15, 40])
-def test_matches_oracle_for_several_maps(tpcf, oracle, ctx, nb):
+@pytest.mark.parametrize("nb,n_map", [(15, 6), (20, 11), (32, 16), (40, 6)])
+def test_matches_oracle_for_several_maps(tpcf, oracle, ctx, nb, n_map):
+    """n_bin <= 32 sums on the FP64 tensor cores (20, 32: whole 16-byte marks
+    rows; 15: 4-byte copies), wider binnings on the FP64 FMA form; one map
+    tile (6 maps) or two (11, 16)."""
     rng = np.random.default_rng(nb)
     raw = [rand_marks(rng, n, nb) for n in (5000, 0, 12345)]
     marks = [tpcf.MarksField(**m) for m in raw]
-    n_map = 6
     vals = [rng.normal(0, 0.02, (n_map, len(m["x"]))).astype(np.float32) for m in raw]
     ws = [np.where(rng.random((n_map, len(m["x"]))) < 0.05, 0.0,
                    rng.uniform(0.5, 1.5, (n_map, len(m["x"])))).astype(np.float32) for m in raw]
