@@ -188,26 +188,23 @@ struct MultFactors {  // resamples: vw = wm = multiplicity of the lens's unit
 
 // partial[(blk * n_g + g) * R + r], R = 3 n_bin + 1 (E, B, K rows, weight):
 // a split-K product of the marks [lens][R] with the lens factors [lens][n_g]
-// over the block's lenses.
+// over the block's lenses.  This FP64 FMA form serves wide binnings
+// (n_bin > 32, marks read from HBM by the summing loop); narrower ones run on
+// the FP64 tensor cores (k_marks_dmma below).
 //
 // The rows come in quads: four consecutive bins of one quantity (xi_E, xi_B
 // or K; the last quad of a quantity padded with zero bins) and one quad for
 // the marks weight (the weight and three zeros).  A lens group is tg
 // threads, lane 2 quad + half owning rows quad x maps 8 half .. 8 half + 7 as
-// 32 FP64 register sums; per lens it reads its quad (one 16-byte load) and
-// its 8 factors (four 16-byte loads) from shared memory and adds the 32
-// products (FP64 FMA), so the FP64 pipe, not load latency, sets the pace.
+// 32 FP64 register sums; per lens it loads its quad's marks (four values)
+// and its 8 factors (four 16-byte shared-memory loads) and adds the 32
+// products (FP64 FMA).
 // The block takes `chunk` lenses of one field in tiles of kTileL; while it
-// sums one tile the marks and the factors' raw inputs of the next are being
-// copied (cp.async) into the other buffer, and after a barrier the raw
-// inputs become the FP64 factors (zero for lenses left out).  Group k takes
-// the tile's lenses k, k + NG, ...; the groups are summed in fixed order at
-// the end (deterministic, no atomics).
-//
-// Staged marks: quantity k of lens jj at (k (kTileL + 1) + jj) nbp floats
-// (nbp = n_bin rounded up to 4, 16-byte aligned rows; the extra lens slot
-// per quantity puts the three quantities of one lens on consecutive banks),
-// the marks weights as quads at 3 (kTileL + 1) nbp + 4 jj.
+// sums one tile the factors' raw inputs of the next are being copied
+// (cp.async) into shared memory, and after a barrier they become the FP64
+// factors (zero for lenses left out).  Group k takes the tile's lenses k,
+// k + NG, ...; the groups are summed in fixed order at the end
+// (deterministic, no atomics).
 //
 // The factors of one lens are stored as [vw of the 16 maps | 2 pad | wm of
 // the 16 maps | 2 pad] (kLensStride doubles): the four 16-byte loads of a
@@ -225,12 +222,6 @@ constexpr int kMarksThreads = 256;
 constexpr int kMarksBlocks = 2 * 148;
 static_assert(kTileL == 64, "the raw staging areas hold 64 lenses");
 __host__ __device__ inline int marks_quad_bins(int n_bin) { return (n_bin + 3) / 4 * 4; }
-// With STAGE the marks of the next tile are copied into shared memory
-// together with the factors' raw inputs, so the summing loop reads only
-// shared memory; for wide binnings (n_bin > 32) the loop loads the marks
-// from HBM itself.
-int marks_stage_floats(int n_bin) { return 3 * (kTileL + 1) * marks_quad_bins(n_bin) + 4 * kTileL; }
-bool marks_stage(int n_bin) { return n_bin <= 32; }
 // Factors of one tile: raw inputs -> FP64 vw, wm in fac_s, all threads.
 // Consecutive lanes take consecutive maps of one lens, so each warp's stores
 // fill whole 128-byte rows.
@@ -247,7 +238,7 @@ __device__ __forceinline__ void convert_factors(const Fac& fac, const unsigned c
   }
 }
 
-template <class Fac, bool STAGE>
+template <class Fac>
 __global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const MarksField* __restrict__ fields, int n_field,
                                                             const Fac fac, int n_g, int n_bin, int tg,
                                                             long long chunk, double* __restrict__ partial) {
@@ -258,8 +249,6 @@ __global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const Marks
   const int ng = blockDim.x / tg;
   double* fac_s = reinterpret_cast<double*>(sm);  // [kTileL][kLensStride] factors of every row
   unsigned char* raw = sm + TF * sizeof(double);
-  float* mk = reinterpret_cast<float*>(raw + std::max(MapFactors::kRawBytes, MultFactors::kRawBytes));
-  const int MS = 3 * (kTileL + 1) * nbp + 4 * kTileL;  // floats per marks buffer
   const int blk = blockIdx.x;
   int fi = 0;
   while (fi + 1 < n_field && fields[fi + 1].chunk0 <= blk) ++fi;
@@ -272,42 +261,10 @@ __global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const Marks
   const bool live = quad <= 3 * nbq;
   const int k = quad / nbq, c = quad - k * nbq;  // k = 3: the marks weight quad
   const double* fsel = ((k < 2 || Fac::kSame) ? fac_s : fac_s + kWmOffset) + 8 * half;
-  // this lane's quad: staged (lens stride ms) or in HBM (4 c .. of lens j of quantity k)
-  const int moff = k < 3 ? (k * (kTileL + 1)) * nbp + 4 * c : 3 * (kTileL + 1) * nbp;
-  const int ms = k < 3 ? nbp : 4;
+  // this lane's quad in HBM: bins 4 c .. of quantity k of lens j, or the marks weight
   const float* qrow = k == 0 ? F.xiE : k == 1 ? F.xiB : k == 2 ? F.K : F.mw;
 
-  if (STAGE) {  // pad bins and the weight quads' zeros are never copied
-    for (int e = tid; e < 2 * MS; e += nthr) mk[e] = 0.f;
-    __syncthreads();
-  }
-  auto stage_tile = [&](long long t0, int buf) {
-    const int nt = (int)min((long long)kTileL, j1 - t0);
-    fac.stage(F, t0, nt, n_g, raw, tid, nthr);
-    if (STAGE) {
-      float* mb = mk + buf * MS;
-      const size_t o = (size_t)t0 * n_bin;
-      const int nq = nt * n_bin;
-      // whole 16-byte runs when every lens row is (n_bin a multiple of 4)
-      const bool vec = (n_bin & 3) == 0 && al16(F.xiE) && al16(F.xiB) && al16(F.K);
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const float* src = (q == 0 ? F.xiE : q == 1 ? F.xiB : F.K) + o;
-        float* dst = mb + q * (kTileL + 1) * nbp;
-        if (vec) {
-          for (int e = tid; e < nq / 4; e += nthr) cp_async16(dst + 4 * e, src + 4 * e, true);
-        } else {
-          for (int e = tid; e < nq; e += nthr) {
-            const int jj = e / n_bin;
-            cp_async4(dst + jj * nbp + (e - jj * n_bin), src + e, true);
-          }
-        }
-      }
-      const float* mw = F.mw + t0;
-      float* dw = mb + 3 * (kTileL + 1) * nbp;
-      for (int e = tid; e < nt; e += nthr) cp_async4(dw + 4 * e, mw + e, true);
-    }
-  };
+  auto stage_tile = [&](long long t0) { fac.stage(F, t0, (int)min((long long)kTileL, j1 - t0), n_g, raw, tid, nthr); };
   auto convert_tile = [&]() { convert_factors(fac, raw, fac_s, tid, nthr); };
 
   double acc[4][8];
@@ -315,32 +272,25 @@ __global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const Marks
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int g = 0; g < 8; ++g) acc[i][g] = 0.0;
-  if (j0 < j1) stage_tile(j0, 0);
+  if (j0 < j1) stage_tile(j0);
   cp_async_wait_all();
   __syncthreads();
   if (j0 < j1) convert_tile();
   __syncthreads();
-  int buf = 0;
   for (long long t0 = j0; t0 < j1; t0 += kTileL) {
     const int nt = (int)min((long long)kTileL, j1 - t0);
     const bool more = t0 + kTileL < j1;
-    // the raw area was read before the last barrier, the other marks buffer
-    // before the one ahead of it
-    if (more) stage_tile(t0 + kTileL, buf ^ 1);
+    // the raw area was read before the last barrier
+    if (more) stage_tile(t0 + kTileL);
     if (live) {
 #pragma unroll 1
       for (int jj = grp; jj < nt; jj += ng) {
         double m[4];
-        if constexpr (STAGE) {
-          const float4 v = *reinterpret_cast<const float4*>(mk + buf * MS + moff + jj * ms);
-          m[0] = v.x, m[1] = v.y, m[2] = v.z, m[3] = v.w;
-        } else {
-          const long long j = t0 + jj;
+        const long long j = t0 + jj;
 #pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const bool v = k < 3 ? 4 * c + i < n_bin : i == 0;
-            m[i] = v ? (double)__ldg(k < 3 ? qrow + j * n_bin + 4 * c + i : qrow + j) : 0.0;
-          }
+        for (int i = 0; i < 4; ++i) {
+          const bool v = k < 3 ? 4 * c + i < n_bin : i == 0;
+          m[i] = v ? (double)__ldg(k < 3 ? qrow + j * n_bin + 4 * c + i : qrow + j) : 0.0;
         }
         const double2* f2 = reinterpret_cast<const double2*>(fsel + jj * kLensStride);
 #pragma unroll
@@ -355,12 +305,11 @@ __global__ void __launch_bounds__(kMarksThreads, 2) k_marks_partials(const Marks
       }
     }
     cp_async_wait_all();
-    __syncthreads();  // the next tile's copies landed; this tile's factors and marks are no longer read
+    __syncthreads();  // the next tile's copies landed; this tile's factors are no longer read
     if (more) {
       convert_tile();
       __syncthreads();
     }
-    buf ^= 1;
   }
   // groups 1.. add their sums into group 0's, in group order
   double* red = reinterpret_cast<double*>(sm);  // [tg][32]
@@ -605,8 +554,7 @@ int marks_block_threads(int n_bin) {
   return std::max(1, kMarksThreads / tg) * tg;
 }
 size_t marks_smem(int n_bin) {
-  size_t fac = sizeof(double) * kTileL * kLensStride + std::max(MapFactors::kRawBytes, MultFactors::kRawBytes);
-  if (marks_stage(n_bin)) fac += 2 * sizeof(float) * (size_t)marks_stage_floats(n_bin);
+  const size_t fac = sizeof(double) * kTileL * kLensStride + std::max(MapFactors::kRawBytes, MultFactors::kRawBytes);
   const size_t red = sizeof(double) * (size_t)marks_group_threads(n_bin) * 32;
   return std::max(fac, red);
 }
@@ -626,8 +574,8 @@ long long marks_chunk(long long n_lens, int n_bin) {
   const long long per = (n_lens + nbk - 1) / nbk;
   return std::max<long long>(kTileL, (per + kTileL - 1) / kTileL * kTileL);
 }
-// One pass of k_marks_partials over all fields (the staged form when the
-// binning is narrow enough).
+// One pass of the partial sums over all fields: the FP64 tensor-core form for
+// n_bin <= 32, the FP64 FMA form for wider binnings.
 template <class Fac>
 cudaError_t launch_marks_partials(const MarksField* fields, int n_field, int nblk, long long chunk, const Fac& fac,
                                   int n_g, int nb, double* part, unsigned* err, cudaStream_t st) {
@@ -640,17 +588,9 @@ cudaError_t launch_marks_partials(const MarksField* fields, int n_field, int nbl
   }
   const size_t msm = marks_smem(nb);
   const int bt = marks_block_threads(nb), tg = marks_group_threads(nb);
-  if (marks_stage(nb)) {
-    cudaError_t e = cudaFuncSetAttribute(k_marks_partials<Fac, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)msm);
-    if (e != cudaSuccess) return e;
-    k_marks_partials<Fac, true><<<nblk, bt, msm, st>>>(fields, n_field, fac, n_g, nb, tg, chunk, part);
-  } else {
-    cudaError_t e = cudaFuncSetAttribute(k_marks_partials<Fac, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)msm);
-    if (e != cudaSuccess) return e;
-    k_marks_partials<Fac, false><<<nblk, bt, msm, st>>>(fields, n_field, fac, n_g, nb, tg, chunk, part);
-  }
+  cudaError_t e = cudaFuncSetAttribute(k_marks_partials<Fac>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
+  if (e != cudaSuccess) return e;
+  k_marks_partials<Fac><<<nblk, bt, msm, st>>>(fields, n_field, fac, n_g, nb, tg, chunk, part);
   return cudaGetLastError();
 }
 
