@@ -54,6 +54,9 @@ class _Arr:
         if _is_torch(a):
             import torch
             tdt = torch.float32 if dtype == np.float32 else torch.int32
+            if a.is_cuda and a.dtype == tdt and a.is_contiguous():  # used in place
+                self.keep, self.ptr, self.n = a, a.data_ptr(), a.numel()
+                return
             if a.is_cuda:
                 t = a.detach().to(tdt).contiguous()
                 self.keep, self.ptr, self.n = t, t.data_ptr(), t.numel()

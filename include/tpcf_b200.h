@@ -304,8 +304,10 @@ tpcf_status tpcf_marks_load(const char* path, int32_t n_field, const tpcf_marks_
  * the stacked g_t_stacked, g_x_stacked [n_map][n_bin] and weights_stacked
  * [n_map] sum numerators and K over fields.  lens_x, lens_y (nullable) are
  * checked against the marks positions to 1e-5 as the reference does.  FP64
- * accumulation in a fixed order (deterministic).  Inputs may be host or
- * device pointers. */
+ * accumulation in a fixed order (deterministic; n_bin <= 32 on the FP64
+ * tensor instruction).  Inputs may be host or device pointers.  Returns
+ * TPCF_ERR_TIMEOUT when a bounded device wait for a bulk copy ran out (the
+ * outputs are then not written). */
 tpcf_status tpcf_xi_from_marks(tpcf_ctx* ctx, int32_t n_field, const tpcf_marks_field* marks, int32_t n_map,
                                const float* const* val, const float* const* w, const float* const* lens_x,
                                const float* const* lens_y, double* g_t, double* g_x, double* weights,
@@ -323,7 +325,8 @@ tpcf_status tpcf_xi_from_marks(tpcf_ctx* ctx, int32_t n_field, const tpcf_marks_
  * fields (k_guard != 0: 0 where that K <= 0, as the point bootstraps; 0:
  * plain quotients, as the block one), weights [n_boot] = sum_j mult_j w_j,
  * and the [n_bin][n_bin] covariances of g_t and g_x over the resamples.
- * Marks may be host or device pointers. */
+ * Marks may be host or device pointers.  TPCF_ERR_TIMEOUT as for
+ * tpcf_xi_from_marks. */
 tpcf_status tpcf_marks_bootstrap(tpcf_ctx* ctx, int32_t n_field, const tpcf_marks_field* marks,
                                  const int32_t* unit, int64_t n_units, const int32_t* multiplicity,
                                  uint64_t seed, int32_t n_boot, double supersampling, int32_t k_guard,
