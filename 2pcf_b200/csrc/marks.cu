@@ -386,7 +386,8 @@ __device__ __forceinline__ void dmma_884(double& d0, double& d1, double a, doubl
 template <class Fac>
 __global__ void __launch_bounds__(kDmmaMaxThreads, 2) k_marks_dmma(const MarksField* __restrict__ fields, int n_field,
                                                               const Fac fac, int n_g, int n_bin, long long chunk,
-                                                              double* __restrict__ partial, unsigned* __restrict__ err) {
+                                                              double* __restrict__ partial, unsigned* __restrict__ err,
+                                                              int skip_tile, unsigned wait_limit) {
   extern __shared__ __align__(16) unsigned char sm[];
   __shared__ __align__(8) uint64_t full[2];
   constexpr int TF = kTileL * kLensStride;
@@ -438,6 +439,10 @@ __global__ void __launch_bounds__(kDmmaMaxThreads, 2) k_marks_dmma(const MarksFi
   __syncthreads();
   const bool mbulk = (nb & 3) == 0 && al16(F.xiE) && al16(F.xiB) && al16(F.K) && al16(F.mw);
   uint32_t par = 0;  // bit b: parity of buffer b's next mbarrier phase
+  // fault injection for tests (tpcf_debug_inject): the bulk copies of each
+  // block's tile skip_tile are never issued, so the wait on them runs out
+  // after wait_limit polls (both off in every product call)
+  const uint32_t polls = wait_limit ? wait_limit : kWaitPolls;
 
   // starts the copies of tile t0 into buffer b; true when they complete on full[b]
   auto stage_tile = [&](long long t0, int b) -> bool {
@@ -445,7 +450,7 @@ __global__ void __launch_bounds__(kDmmaMaxThreads, 2) k_marks_dmma(const MarksFi
     const bool bm = mbulk && nt == kTileL;
     const bool br = fac.bulk_ok(F, t0, nt);
     float* mb = mk + b * MS;
-    if ((bm || br) && tid == 0) {
+    if ((bm || br) && tid == 0 && (t0 - j0) / kTileL != skip_tile) {
       mbar_arrive_tx(&full[b], (bm ? 4u * (3 * nb + 1) * kTileL : 0u) + (br ? fac.bulk_bytes(n_g) : 0u));
       if (bm) {
         const size_t o = (size_t)t0 * nb;
@@ -485,7 +490,7 @@ __global__ void __launch_bounds__(kDmmaMaxThreads, 2) k_marks_dmma(const MarksFi
     if (!bulk) return true;
     wb = b, wpar = (par >> b) & 1u;
     par ^= 1u << b;
-    return mbar_wait_bounded(&full[b], wpar);
+    return mbar_wait_bounded(&full[b], wpar, polls);
   };
 
   double acc[2][2][2];
@@ -528,7 +533,7 @@ __global__ void __launch_bounds__(kDmmaMaxThreads, 2) k_marks_dmma(const MarksFi
   if (abort) {  // a copy did not land: flag it, give it one more bounded wait, leave
     if (tid == 0) {
       atomicOr(err, kErrTimeout);
-      mbar_wait_bounded(&full[wb], wpar);
+      mbar_wait_bounded(&full[wb], wpar, polls);
     }
     return;
   }
@@ -578,12 +583,14 @@ long long marks_chunk(long long n_lens, int n_bin) {
 // n_bin <= 32, the FP64 FMA form for wider binnings.
 template <class Fac>
 cudaError_t launch_marks_partials(const MarksField* fields, int n_field, int nblk, long long chunk, const Fac& fac,
-                                  int n_g, int nb, double* part, unsigned* err, cudaStream_t st) {
+                                  int n_g, int nb, double* part, unsigned* err, int skip_tile, unsigned wait_limit,
+                                  cudaStream_t st) {
   if (nb <= kDmmaMaxBins) {
     const size_t msm = marks_dmma_smem(nb);
     cudaError_t e = cudaFuncSetAttribute(k_marks_dmma<Fac>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msm);
     if (e != cudaSuccess) return e;
-    k_marks_dmma<Fac><<<nblk, 32 * marks_m_tiles(nb), msm, st>>>(fields, n_field, fac, n_g, nb, chunk, part, err);
+    k_marks_dmma<Fac><<<nblk, 32 * marks_m_tiles(nb), msm, st>>>(fields, n_field, fac, n_g, nb, chunk, part, err,
+                                                                 skip_tile, wait_limit);
     return cudaGetLastError();
   }
   const size_t msm = marks_smem(nb);
@@ -761,7 +768,8 @@ extern "C" tpcf_status tpcf_xi_from_marks(tpcf_ctx* c, int32_t n_field, const tp
       const int g = std::min(MG, n_map - m0);
       if (nblk > 0) {
         timer.mark(st);
-        counted(c, launch_marks_partials(df, n_field, nblk, chunk, MapFactors{m0}, g, nb, part, derr, st),
+        counted(c, launch_marks_partials(df, n_field, nblk, chunk, MapFactors{m0}, g, nb, part, derr, c->skip_tile,
+                                      c->wait_limit, st),
                 "marks partials");
         timer.mark(st);
       }
@@ -893,7 +901,7 @@ extern "C" tpcf_status tpcf_marks_bootstrap(tpcf_ctx* c, int32_t n_field, const 
         timer.mark(st);
         counted(c,
                 launch_marks_partials(df, n_field, nblk, chunk, MultFactors{mult, dunit, n_units}, G, nb, part, derr,
-                                      st),
+                                      c->skip_tile, c->wait_limit, st),
                 "bootstrap partials");
         timer.mark(st);
         const int tot = G * n_field * R;

@@ -196,10 +196,12 @@ tpcf_status tpcf_set_tile_shape(tpcf_ctx* ctx, int32_t group_size, int32_t tile_
  * fail_alloc >= 0: the fail_alloc-th device workspace allocation from now
  * (0 = the next) fails as if cudaMalloc had, and the call returns
  * TPCF_ERR_OOM.  skip_tile >= 0: the planar pair kernel never issues the copy
- * of the source tile with that ring index in each block, so its bounded waits
- * run out after wait_polls polls (0 = the product's 2^22) and the call
- * returns TPCF_ERR_TIMEOUT; every copy that was issued has landed before the
- * kernel exits.  -1 / 0 switch them off.  The context stays usable. */
+ * of the source tile with that ring index in each block (the marks kernel,
+ * n_bin <= 32: the bulk copies of each block's tile with that index), so its
+ * bounded waits run out after wait_polls polls (0 = the product's 2^22) and
+ * the call returns TPCF_ERR_TIMEOUT; every copy that was issued has landed
+ * before the kernel exits.  -1 / 0 switch them off.  The context stays
+ * usable. */
 tpcf_status tpcf_debug_inject(tpcf_ctx* ctx, int64_t fail_alloc, int32_t skip_tile, uint32_t wait_polls);
 
 /* Roofline helper with no counterpart in the reference: measures this GPU's

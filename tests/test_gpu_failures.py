@@ -8,7 +8,9 @@ src/kdtree.f90:119-122, :265-267):
 - a source tile of the pair kernel whose bulk copy is never issued makes the
   bounded mbarrier waits on it run out: the call returns TPCF_ERR_TIMEOUT
   (every copy that was issued has landed before the blocks exit), and the
-  same context then computes the correct result.
+  same context then computes the correct result;
+- the same for the first tile of the marks kernel (xi from marks and the
+  marks bootstrap).
 Invalid arguments and a missing device are covered on the CPU (test_abi)."""
 import ctypes as C
 import time
@@ -67,4 +69,30 @@ def test_bounded_wait_runs_out_then_recovery(tpcf, oracle):
         print(f"tile {tile} never issued, {polls} polls per wait: TIMEOUT after {dt:.3f} s")
     inject(tpcf, ctx)
     check_sums("call after a bounded wait ran out", shear(tpcf, ctx, L, S, bins), can)
+    ctx.close()
+
+
+def test_marks_bounded_wait_runs_out_then_recovery(tpcf, oracle):
+    ctx = tpcf.Context(0)
+    rng = np.random.default_rng(92)
+    n, nb, n_map = 8192, 20, 3
+    raw = {"x": rng.normal(size=n).astype(np.float32), "y": rng.normal(size=n).astype(np.float32),
+           "w": rng.uniform(0.1, 2, n).astype(np.float32),
+           "xi_E": rng.normal(size=(n, nb)).astype(np.float32), "xi_B": rng.normal(size=(n, nb)).astype(np.float32),
+           "K": rng.uniform(0.5, 1.5, (n, nb)).astype(np.float32)}
+    marks = [tpcf.MarksField(**raw)]
+    val = rng.normal(0, 0.02, (n_map, n)).astype(np.float32)
+    w = rng.uniform(0.5, 1.5, (n_map, n)).astype(np.float32)
+    inject(tpcf, ctx, skip_tile=0, wait_polls=1 << 12)
+    for call in (lambda: tpcf.calculate_tpcf_from_marks(marks, [val], [w], ctx=ctx),
+                 lambda: tpcf.marks_bootstrap(marks, 20, seed=3, covariance=False, ctx=ctx)):
+        with pytest.raises(tpcf.TPCFError) as e:
+            call()
+        assert e.value.status == tpcf._lib.TPCF_ERR_TIMEOUT, str(e.value)
+    inject(tpcf, ctx)
+    out = tpcf.calculate_tpcf_from_marks(marks, [val], [w], ctx=ctx)
+    for m in range(n_map):
+        per, _ = oracle.xi_from_marks([raw], [val[m]], [w[m]])
+        np.testing.assert_allclose(out["g_t"][m, 0], per[0]["g_t"], rtol=1e-9)
+        np.testing.assert_allclose(out["weights"][m, 0], per[0]["weights"], rtol=1e-12)
     ctx.close()
