@@ -279,8 +279,13 @@ def marks_timing(tpcf, stream, nb):
     # each (the multiplicities are drawn on the device), so FP64-bound; the
     # FP64 tensor instruction and the FP64 FMA pipe have the same peak here
     flop = 1000 * n * (3 * nbm + 1) * 2
+    # its HBM side: every pass of 16 resamples streams the marks once and the
+    # 16 multiplicity rows (INT32 per lens), ceil(1000 / 16) passes
+    boot_bytes = -(-1000 // 16) * (3 * 4 * n * nbm + 4 * n) + 1000 * 4 * n
     out["marks_bootstrap"] = {"resamples": 1000, "lenses": n, "call_ms": ms, "kernel_ms": kms,
                               "call_fp64_frac": flop / (ms * 1e-3) / 1e12 / p64,
+                              "hbm": {"bytes": boot_bytes, "achieved_gbs": boot_bytes / (kms * 1e-3) / 1e9,
+                                      "frac": boot_bytes / (kms * 1e-3) / 1e9 / hbm, "peak_source": hbm_src},
                               "roofline": {"bound": "fp64", "achieved": flop / (kms * 1e-3) / 1e12, "peak": p64,
                                            "unit": "TFLOP/s", "frac": flop / (kms * 1e-3) / 1e12 / p64,
                                            "flop": flop, "peak_source": "FP64 FMA loop measured in this run"}}
