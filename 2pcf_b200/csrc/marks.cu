@@ -209,7 +209,9 @@ struct MultFactors {  // resamples: vw = wm = multiplicity of the lens's unit
 // The factors of one lens are stored as [vw of the 16 maps | 2 pad | wm of
 // the 16 maps | 2 pad] (kLensStride doubles): the four 16-byte loads of a
 // warp touch at most four distinct chunks (vw or wm, half 0 or 1), on
-// disjoint banks.
+// disjoint banks; in the tensor-core form a B fragment (4 lenses x 8 maps)
+// starts its lens rows 72 words = 8 banks apart, so each half-warp's 16
+// values fall on 32 distinct banks.
 constexpr int kTileL = 64;
 constexpr int kLensStride = 2 * (kMapGroup + 2);
 constexpr int kWmOffset = kMapGroup + 2;
