@@ -623,6 +623,8 @@ def path_stats(tpcf, args):
     import ctypes as C
     import torch
     tpcf._lib.LIB_PATH = os.path.join(ROOT, "2pcf_b200", "libtpcf_b200_stats.so")
+    if not os.path.exists(tpcf._lib.LIB_PATH):
+        raise SystemExit("--path-stats needs the diagnostic build: make -C 2pcf_b200/csrc stats")
     w = workload(args.scale)
     bins = tpcf.create_bins(*w["bins"])
     dev = lambda a: torch.from_numpy(a).cuda()
