@@ -761,7 +761,9 @@ extern "C" tpcf_status tpcf_xi_from_marks(tpcf_ctx* c, int32_t n_field, const tp
     const int R = 3 * nb + 1;
     std::vector<double> sums((size_t)n_map * n_field * R, 0.0);
     double* part = (double*)ws_alloc(c, sizeof(double) * (size_t)std::max(nblk, 1) * kMapGroup * R);
-    double* dout = (double*)ws_alloc(c, sizeof(double) * (size_t)kMapGroup * n_field * R);
+    // the sums of every pass stay on the device until one copy after the
+    // last pass, so the host queues all passes without waiting on any
+    double* dout = (double*)ws_alloc(c, sizeof(double) * sums.size());
     unsigned* derr = (unsigned*)ws_alloc(c, sizeof(unsigned));
     check(cudaMemsetAsync(derr, 0, sizeof(unsigned), st), "memset");
     const int MG = marks_group(nb);
@@ -776,15 +778,15 @@ extern "C" tpcf_status tpcf_xi_from_marks(tpcf_ctx* c, int32_t n_field, const tp
         timer.mark(st);
       }
       const int tot = g * n_field * R;
+      double* dpass = dout + (size_t)m0 * n_field * R;
       if (nblk > 0) {
-        k_marks_reduce<<<(tot + 7) / 8, 256, 0, st>>>(part, df, n_field, nblk, g, R, dout);
+        k_marks_reduce<<<(tot + 7) / 8, 256, 0, st>>>(part, df, n_field, nblk, g, R, dpass);
         counted(c, cudaGetLastError(), "marks reduce");
       } else {
-        check(cudaMemsetAsync(dout, 0, sizeof(double) * tot, st), "memset");
+        check(cudaMemsetAsync(dpass, 0, sizeof(double) * tot, st), "memset");
       }
-      check(cudaMemcpyAsync(sums.data() + (size_t)m0 * n_field * R, dout, sizeof(double) * tot,
-                            cudaMemcpyDeviceToHost, st), "D2H sums");
     }
+    check(cudaMemcpyAsync(sums.data(), dout, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, st), "D2H sums");
     unsigned herr = 0;
     check(cudaMemcpyAsync(&herr, derr, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "D2H err");
     check(cudaStreamSynchronize(st), "sync marks");
@@ -880,8 +882,11 @@ extern "C" tpcf_status tpcf_marks_bootstrap(tpcf_ctx* c, int32_t n_field, const 
     const int R = 3 * nb + 1;
     int* mbuf = multiplicity ? nullptr : (int*)ws_alloc(c, sizeof(int) * (size_t)kMapGroup * n_units);
     double* part = (double*)ws_alloc(c, sizeof(double) * (size_t)std::max(nblk, 1) * kMapGroup * R);
-    double* dout = (double*)ws_alloc(c, sizeof(double) * (size_t)kMapGroup * n_field * R);
     std::vector<double> sums((size_t)n_boot * n_field * R, 0.0);
+    // the sums of every pass stay on the device until one copy after the
+    // last pass, so the host queues all passes without waiting on any
+    double* dout = (double*)ws_alloc(c, sizeof(double) * sums.size());
+    if (nblk == 0) check(cudaMemsetAsync(dout, 0, sizeof(double) * sums.size(), st), "memset");
     unsigned* derr = (unsigned*)ws_alloc(c, sizeof(unsigned));
     check(cudaMemsetAsync(derr, 0, sizeof(unsigned), st), "memset");
     const int MG = marks_group(nb);
@@ -907,12 +912,12 @@ extern "C" tpcf_status tpcf_marks_bootstrap(tpcf_ctx* c, int32_t n_field, const 
                 "bootstrap partials");
         timer.mark(st);
         const int tot = G * n_field * R;
-        k_marks_reduce<<<(tot + 7) / 8, 256, 0, st>>>(part, df, n_field, nblk, G, R, dout);
+        k_marks_reduce<<<(tot + 7) / 8, 256, 0, st>>>(part, df, n_field, nblk, G, R,
+                                                       dout + (size_t)s0 * n_field * R);
         counted(c, cudaGetLastError(), "bootstrap reduce");
-        check(cudaMemcpyAsync(sums.data() + (size_t)s0 * n_field * R, dout, sizeof(double) * tot,
-                              cudaMemcpyDeviceToHost, st), "D2H sums");
       }
     }
+    check(cudaMemcpyAsync(sums.data(), dout, sizeof(double) * sums.size(), cudaMemcpyDeviceToHost, st), "D2H sums");
     unsigned herr = 0;
     check(cudaMemcpyAsync(&herr, derr, sizeof(unsigned), cudaMemcpyDeviceToHost, st), "D2H err");
     check(cudaStreamSynchronize(st), "sync bootstrap");
